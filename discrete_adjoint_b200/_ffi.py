@@ -1,0 +1,195 @@
+"""ctypes view of the C ABI in include/discrete_adjoint.h and include/da_mesh.h.
+
+The shared library is built in-tree (discrete_adjoint_b200/libda_b200.so).  Loading fails
+loudly if it is missing: there is no CPU fallback for the device path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libda_b200.so")
+
+DA_MAX_MATERIALS = 16
+DA_MAX_PILES = 8
+
+DA_OK = 0
+DA_ERR_INVALID = -1
+DA_ERR_CUDA = -2
+DA_ERR_NAN = -3
+DA_ERR_NEG_DEPTH = -4
+DA_ERR_EIGEN = -5
+DA_ERR_TIMEOUT = -6
+DA_ERR_NO_MESH = -7
+DA_ERR_OOM = -8
+DA_ERR_NO_DEVICE = -9
+DA_ERR_UNSUPPORTED = -10
+
+DA_PREC_FP64 = 0
+DA_PREC_FP32_SPLIT = 1
+
+PD = C.POINTER(C.c_double)
+PF = C.POINTER(C.c_float)
+PI32 = C.POINTER(C.c_int32)
+
+
+class da_params(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int32),
+        ("device", C.c_int32),
+        ("epsilon", C.c_double),
+        ("gravity_scale", C.c_double),
+        ("gamma", C.c_double),
+        ("intfrict", C.c_double),
+        ("n_materials", C.c_int32),
+        ("frict_tiny_iters", C.c_int32),
+        ("bedfrict", C.c_double * DA_MAX_MATERIALS),
+        ("frict_tiny_early", C.c_double),
+        ("frict_tiny_late", C.c_double),
+        ("max_time", C.c_double),
+        ("next_output", C.c_double),
+        ("next_save", C.c_double),
+        ("influx_dt", C.c_double),
+    ]
+
+
+class da_mesh_soa(C.Structure):
+    _fields_ = [
+        ("n_cells", C.c_int32),
+        ("nbr", PI32),
+        ("x", PD), ("y", PD),
+        ("dx", PD), ("dy", PD),
+        ("gravity", PD),
+        ("d_gravity", PD),
+        ("curvature", PD),
+        ("material", PI32),
+    ]
+
+
+class da_step_stats(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double),
+        ("time", C.c_double),
+        ("volume", C.c_double),
+        ("hmax", C.c_double),
+        ("iter", C.c_int64),
+    ]
+
+
+class da_dem(C.Structure):
+    _fields_ = [
+        ("nrows", C.c_int32), ("ncols", C.c_int32),
+        ("xmin", C.c_double), ("ymin", C.c_double), ("res", C.c_double),
+        ("elev", PF),
+        ("mat", PI32),
+    ]
+
+
+class da_pile_spec(C.Structure):
+    _fields_ = [
+        ("xc", C.c_double), ("yc", C.c_double),
+        ("height", C.c_double),
+        ("major", C.c_double), ("minor", C.c_double),
+        ("rot_deg", C.c_double),
+        ("vx", C.c_double), ("vy", C.c_double),
+    ]
+
+
+class da_mesh_spec(C.Structure):
+    _fields_ = [
+        ("xmin", C.c_double), ("ymin", C.c_double),
+        ("dx0", C.c_double), ("dy0", C.c_double),
+        ("nx0", C.c_int32), ("ny0", C.c_int32),
+        ("max_level", C.c_int32), ("uniform", C.c_int32),
+        ("refine_margin", C.c_double),
+        ("n_boxes", C.c_int32),
+        ("boxes", PD),
+        ("random_frac", C.c_double),
+        ("seed", C.c_uint64),
+    ]
+
+
+class da_mesh_host(C.Structure):
+    _fields_ = [
+        ("n_cells", C.c_int32), ("max_level", C.c_int32), ("n_piles", C.c_int32),
+        ("level", PI32), ("ix", PI32), ("iy", PI32),
+        ("nbr", PI32),
+        ("x", PD), ("y", PD), ("dx", PD), ("dy", PD),
+        ("elevation", PD),
+        ("zeta", PD),
+        ("curvature", PD),
+        ("gravity", PD),
+        ("d_gravity", PD),
+        ("material", PI32),
+        ("h0", PD), ("hu0", PD), ("hv0", PD),
+        ("dh0_dpile", PD),
+    ]
+
+
+# name -> (restype, argtypes) for every symbol the headers declare
+SIGNATURES = {
+    "da_abi_version": (C.c_int, []),
+    "da_strerror": (C.c_char_p, [C.c_int]),
+    "da_params_default": (None, [C.POINTER(da_params)]),
+    "da_create": (C.c_void_p, [C.POINTER(da_params), C.POINTER(C.c_int)]),
+    "da_destroy": (None, [C.c_void_p]),
+    "da_last_error": (C.c_char_p, [C.c_void_p]),
+    "da_set_params": (C.c_int, [C.c_void_p, C.POINTER(da_params)]),
+    "da_set_time": (C.c_int, [C.c_void_p, C.c_double, C.c_int64]),
+    "da_upload_mesh": (C.c_int, [C.c_void_p, C.POINTER(da_mesh_soa), C.c_int32]),
+    "da_set_state": (C.c_int, [C.c_void_p, PD, PD, PD]),
+    "da_get_state": (C.c_int, [C.c_void_p, PD, PD, PD]),
+    "da_forward_step": (C.c_int, [C.c_void_p, C.POINTER(da_step_stats)]),
+    "da_forward_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_step_stats)]),
+    "da_forward_run_timed": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_step_stats), PD]),
+    "da_forward_profile": (C.c_int, [C.c_void_p, C.c_int32, PD]),
+    "da_forward_kernel_name": (C.c_char_p, [C.c_int32]),
+    "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,
+                                C.c_double, C.c_double, C.POINTER(C.POINTER(da_mesh_host))]),
+    "da_mesh_free": (None, [C.POINTER(da_mesh_host)]),
+    "da_mesh_view": (C.c_int, [C.POINTER(da_mesh_host), C.POINTER(da_mesh_soa)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libda_b200.so and binds every declared symbol (raises if any is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m discrete_adjoint_b200._build` "
+            "(there is no CPU fallback for the device path)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class DAError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(PD)
+
+
+def fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(PF)
+
+
+def iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(PI32)

@@ -1,0 +1,474 @@
+// C ABI entry points: context lifecycle, mesh/state transfer and forward stepping.
+// Declared in include/discrete_adjoint.h; each replaces a reference call site named there.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "da_internal.h"
+
+namespace da {
+
+int set_error(da_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_check(da_ctx *ctx, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return DA_OK;
+    const int code = (e == cudaErrorMemoryAllocation) ? DA_ERR_OOM : DA_ERR_CUDA;
+    return set_error(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// gmfggetcoef (src/geoflow/getcoef.f:19-66) depends on the state only through sgn(vel)
+// and two guards; the three signed values are formed here once per material.
+static double coef_signed(double bedfrict, double intfrict, double s) {
+    const double cosphi = std::cos(intfrict);
+    const double tandel = std::tan(bedfrict);
+    const double ab = 1.0 - (1.0 + tandel * tandel) * (cosphi * cosphi);
+    return (2.0 / (cosphi * cosphi)) * (1.0 - s * std::sqrt(ab < 0. ? -ab : ab)) - 1.0;
+}
+
+void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc) {
+    std::memset(mc, 0, sizeof(*mc));
+    for (int m = 0; m < p.n_materials; ++m) {
+        for (int s = -1; s <= 1; ++s) {
+            double k = coef_signed(p.bedfrict[m], p.intfrict, double(s));
+            if (k < 0.0) k = 0.0;
+            mc->kact_sgn[m][s + 1] = k * p.epsilon;
+        }
+        mc->tan_bed[m] = std::tan(p.bedfrict[m]);
+    }
+    mc->kact_rest = 1.0 * p.epsilon;
+    mc->epsilon = p.epsilon;
+    mc->sin_int = std::sin(p.intfrict);
+    mc->gamma = p.gamma;
+    mc->n_materials = p.n_materials;
+    tc->next_output = p.next_output;
+    tc->next_save = p.next_save;
+    tc->max_time = p.max_time;
+    tc->influx_dt = p.influx_dt;
+    tc->gravity_scale = p.gravity_scale;
+    tc->epsilon = p.epsilon;
+    tc->frict_tiny_early = p.frict_tiny_early;
+    tc->frict_tiny_late = p.frict_tiny_late;
+    tc->frict_tiny_iters = p.frict_tiny_iters;
+}
+
+static bool params_ok(const da_params *p) {
+    if (!p) return false;
+    if (p->precision != DA_PREC_FP64 && p->precision != DA_PREC_FP32_SPLIT) return false;
+    if (p->n_materials < 1 || p->n_materials > DA_MAX_MATERIALS) return false;
+    if (!(p->epsilon > 0) || !(p->gravity_scale > 0) || !(p->gamma > 0)) return false;
+    return true;
+}
+
+template <class T>
+static void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+static void free_mesh(da_ctx *ctx) {
+    DevMesh &d = ctx->mesh;
+    dfree(d.nbr); dfree(d.mat); dfree(d.bflag);
+    dfree(d.x); dfree(d.y); dfree(d.dx); dfree(d.dy);
+    dfree(d.g); dfree(d.dg); dfree(d.curv);
+    dfree(d.fdx); dfree(d.fdy); dfree(d.fg); dfree(d.fdg); dfree(d.fcurv);
+    d.n = 0;
+    d.epoch = -1;
+}
+
+static void free_state(da_ctx *ctx) {
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
+    dfree(ctx->kact);
+    dfree(ctx->slopes);
+    dfree(ctx->vol_part);
+    ctx->have_state = false;
+}
+
+static void drop_graphs(da_ctx *ctx) {
+    for (int b = 0; b < 2; ++b) {
+        if (ctx->step_graph[b]) cudaGraphExecDestroy(ctx->step_graph[b]);
+        ctx->step_graph[b] = nullptr;
+    }
+}
+
+template <class T>
+static int upload(da_ctx *ctx, T **dst, const T *src, size_t count) {
+    int st = cuda_check(ctx, cudaMalloc((void **)dst, sizeof(T) * (count ? count : 1)), "cudaMalloc(mesh)");
+    if (st) return st;
+    return cuda_check(ctx, cudaMemcpyAsync(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream),
+                      "copy mesh");
+}
+
+static int sync_scalars(da_ctx *ctx) {
+    int st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
+                        "read scalars");
+    if (st) return st;
+    st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+    if (st) return st;
+    if (ctx->hsc->err) {
+        const int code = ctx->hsc->err;
+        return set_error(ctx, code, code == DA_ERR_EIGEN ? "wave speed above 1e9 (get_coef_and_eigen)"
+                                                         : "non-finite state after update (update_states)");
+    }
+    return DA_OK;
+}
+
+static void fill_stats(const da_ctx *ctx, da_step_stats *out) {
+    if (!out) return;
+    out->dt = ctx->hsc->dt;
+    out->time = ctx->hsc->time;
+    out->volume = ctx->hsc->volume;
+    out->hmax = ctx->hsc->hmax;
+    out->iter = ctx->hsc->iter;
+}
+
+}  // namespace da
+
+using namespace da;
+
+extern "C" {
+
+int da_abi_version(void) { return DA_ABI_VERSION; }
+
+const char *da_strerror(int code) {
+    switch (code) {
+        case DA_OK: return "ok";
+        case DA_ERR_INVALID: return "invalid argument or call order";
+        case DA_ERR_CUDA: return "CUDA runtime error";
+        case DA_ERR_NAN: return "non-finite state";
+        case DA_ERR_NEG_DEPTH: return "negative depth";
+        case DA_ERR_EIGEN: return "wave speed above 1e9";
+        case DA_ERR_TIMEOUT: return "device wait timed out";
+        case DA_ERR_NO_MESH: return "no mesh uploaded";
+        case DA_ERR_OOM: return "device out of memory";
+        case DA_ERR_NO_DEVICE: return "no CUDA device";
+        case DA_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown error";
+    }
+}
+
+void da_params_default(da_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->precision = DA_PREC_FP64;
+    p->device = 0;
+    p->epsilon = 1.0;
+    p->gravity_scale = 1.0;
+    p->gamma = 1.0;
+    p->intfrict = 30.0 * 3.1415926 / 180.0;  // constant.h:37 PI, datread.C:379-400 deg->rad
+    p->n_materials = 1;
+    p->bedfrict[0] = 20.0 * 3.1415926 / 180.0;
+    p->frict_tiny_iters = 50;
+    p->frict_tiny_early = 0.1;
+    p->frict_tiny_late = 0.000000001;
+    p->max_time = HUGE_VAL;
+    p->next_output = HUGE_VAL;
+    p->next_save = HUGE_VAL;
+    p->influx_dt = HUGE_VAL;
+}
+
+da_ctx *da_create(const da_params *p, int *err) {
+    int dummy;
+    if (!err) err = &dummy;
+    if (!params_ok(p)) {
+        *err = DA_ERR_INVALID;
+        return nullptr;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        *err = DA_ERR_NO_DEVICE;
+        return nullptr;
+    }
+    if (p->device < 0 || p->device >= ndev) {
+        *err = DA_ERR_INVALID;
+        return nullptr;
+    }
+    da_ctx *ctx = new (std::nothrow) da_ctx();
+    if (!ctx) {
+        *err = DA_ERR_OOM;
+        return nullptr;
+    }
+    ctx->p = *p;
+    ctx->device = p->device;
+    fill_consts(ctx->p, &ctx->mc, &ctx->tc);
+    int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->dsc, sizeof(DevScalars)), "cudaMalloc(scalars)");
+    if (!st) st = cuda_check(ctx, cudaMallocHost((void **)&ctx->hsc, sizeof(DevScalars)), "cudaMallocHost");
+    if (st) {
+        *err = st;
+        da_destroy(ctx);
+        return nullptr;
+    }
+    std::memset(ctx->hsc, 0, sizeof(DevScalars));
+    {
+        const double init = 10000000.0;  // min_dx_dy_evalue start value, get_coef_and_eigen.C:36
+        std::memcpy(&ctx->hsc->acc_min_dxe, &init, sizeof(init));
+    }
+    st = cuda_check(ctx, cudaMemcpy(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice), "init scalars");
+    if (st) {
+        *err = st;
+        da_destroy(ctx);
+        return nullptr;
+    }
+    *err = DA_OK;
+    return ctx;
+}
+
+void da_destroy(da_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graphs(ctx);
+    free_mesh(ctx);
+    free_state(ctx);
+    if (ctx->dsc) cudaFree(ctx->dsc);
+    if (ctx->hsc) cudaFreeHost(ctx->hsc);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *da_last_error(const da_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int da_set_params(da_ctx *ctx, const da_params *p) {
+    if (!ctx) return DA_ERR_INVALID;
+    if (!params_ok(p) || p->precision != ctx->p.precision || p->device != ctx->p.device)
+        return set_error(ctx, DA_ERR_INVALID, "da_set_params: invalid parameters or precision/device change");
+    ctx->p = *p;
+    fill_consts(ctx->p, &ctx->mc, &ctx->tc);
+    drop_graphs(ctx);
+    return DA_OK;
+}
+
+int da_set_time(da_ctx *ctx, double time, int64_t iter) {
+    if (!ctx) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (st) return st;
+    st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "read scalars");
+    if (st) return st;
+    ctx->hsc->time = time;
+    ctx->hsc->iter = iter;
+    ctx->hsc->err = 0;
+    return cuda_check(ctx, cudaMemcpy(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice), "write scalars");
+}
+
+int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
+    if (!ctx) return DA_ERR_INVALID;
+    if (!m || m->n_cells <= 0 || !m->nbr || !m->x || !m->y || !m->dx || !m->dy || !m->gravity || !m->d_gravity ||
+        !m->curvature || !m->material)
+        return set_error(ctx, DA_ERR_INVALID, "da_upload_mesh: missing array");
+    const int n = m->n_cells;
+    // host-side validation: neighbour indices in range, materials in range
+    std::vector<uint8_t> bflag(n), mat(n);
+    for (int i = 0; i < n; ++i) {
+        uint8_t b = 0;
+        for (int s = 0; s < 4; ++s) {
+            const int a = m->nbr[(size_t)s * n + i], c = m->nbr[(size_t)(s + 4) * n + i];
+            if (a < -1 || a >= n || c < -1 || c >= n || ((a < 0) != (c < 0)))
+                return set_error(ctx, DA_ERR_INVALID, "da_upload_mesh: neighbour index out of range");
+            if (a < 0) b |= uint8_t(1u << s);
+            else if (c != a) b |= uint8_t(0x10u << s);
+        }
+        bflag[i] = b;
+        if (m->material[i] < 0 || m->material[i] >= ctx->p.n_materials)
+            return set_error(ctx, DA_ERR_INVALID, "da_upload_mesh: material index out of range");
+        mat[i] = uint8_t(m->material[i]);
+        if (!(m->dx[i] > 0) || !(m->dy[i] > 0))
+            return set_error(ctx, DA_ERR_INVALID, "da_upload_mesh: non-positive cell size");
+    }
+    cudaSetDevice(ctx->device);
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (st) return st;
+    drop_graphs(ctx);
+    free_mesh(ctx);
+    free_state(ctx);
+    DevMesh &d = ctx->mesh;
+    d.n = n;
+    d.epoch = epoch;
+    const bool fp64 = ctx->p.precision == DA_PREC_FP64;
+    if (!st) st = upload(ctx, &d.nbr, m->nbr, (size_t)8 * n);
+    if (!st) st = upload(ctx, &d.bflag, bflag.data(), (size_t)n);
+    if (!st) st = upload(ctx, &d.mat, mat.data(), (size_t)n);
+    if (fp64) {
+        if (!st) st = upload(ctx, &d.x, m->x, (size_t)n);
+        if (!st) st = upload(ctx, &d.y, m->y, (size_t)n);
+        if (!st) st = upload(ctx, &d.dx, m->dx, (size_t)n);
+        if (!st) st = upload(ctx, &d.dy, m->dy, (size_t)n);
+        if (!st) st = upload(ctx, &d.g, m->gravity, (size_t)3 * n);
+        if (!st) st = upload(ctx, &d.dg, m->d_gravity, (size_t)2 * n);
+        if (!st) st = upload(ctx, &d.curv, m->curvature, (size_t)2 * n);
+    } else {
+        std::vector<float> tmp((size_t)3 * n);
+        auto conv = [&](const double *src, size_t cnt, float **dst) {
+            for (size_t k = 0; k < cnt; ++k) tmp[k] = float(src[k]);
+            return upload(ctx, dst, tmp.data(), cnt);
+        };
+        if (!st) st = conv(m->dx, n, &d.fdx);
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        if (!st) st = conv(m->dy, n, &d.fdy);
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        if (!st) st = conv(m->gravity, (size_t)3 * n, &d.fg);
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        if (!st) st = conv(m->d_gravity, (size_t)2 * n, &d.fdg);
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        if (!st) st = conv(m->curvature, (size_t)2 * n, &d.fcurv);
+    }
+    if (!st) st = forward_alloc(ctx);
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (st) {
+        free_mesh(ctx);
+        free_state(ctx);
+    }
+    return st;
+}
+
+int da_set_state(da_ctx *ctx, const double *h, const double *hu, const double *hv) {
+    if (!ctx || !h || !hu || !hv) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_set_state: no mesh");
+    cudaSetDevice(ctx->device);
+    const int n = ctx->mesh.n;
+    const double *src[3] = {h, hu, hv};
+    int st = DA_OK;
+    if (ctx->p.precision == DA_PREC_FP64) {
+        for (int v = 0; v < 3 && !st; ++v)
+            st = cuda_check(ctx, cudaMemcpyAsync(ctx->U[ctx->cur][v], src[v], sizeof(double) * n,
+                                                 cudaMemcpyHostToDevice, ctx->stream), "copy state");
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    } else {
+        std::vector<float> tmp(n);
+        for (int v = 0; v < 3 && !st; ++v) {
+            for (int i = 0; i < n; ++i) tmp[i] = float(src[v][i]);
+            st = cuda_check(ctx, cudaMemcpy(ctx->U[ctx->cur][v], tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice),
+                            "copy state");
+        }
+    }
+    if (!st) ctx->have_state = true;
+    return st;
+}
+
+int da_get_state(da_ctx *ctx, double *h, double *hu, double *hv) {
+    if (!ctx || !h || !hu || !hv) return DA_ERR_INVALID;
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_get_state: no state");
+    cudaSetDevice(ctx->device);
+    const int n = ctx->mesh.n;
+    double *dst[3] = {h, hu, hv};
+    int st = DA_OK;
+    if (ctx->p.precision == DA_PREC_FP64) {
+        for (int v = 0; v < 3 && !st; ++v)
+            st = cuda_check(ctx, cudaMemcpyAsync(dst[v], ctx->U[ctx->cur][v], sizeof(double) * n,
+                                                 cudaMemcpyDeviceToHost, ctx->stream), "copy state");
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    } else {
+        std::vector<float> tmp(n);
+        for (int v = 0; v < 3 && !st; ++v) {
+            st = cuda_check(ctx, cudaMemcpyAsync(tmp.data(), ctx->U[ctx->cur][v], sizeof(float) * n,
+                                                 cudaMemcpyDeviceToHost, ctx->stream), "copy state");
+            if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+            for (int i = 0; i < n && !st; ++i) dst[v][i] = double(tmp[i]);
+        }
+    }
+    return st;
+}
+
+int da_forward_step(da_ctx *ctx, da_step_stats *out) {
+    if (!ctx) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_step: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_step: no state");
+    cudaSetDevice(ctx->device);
+    int st = launch_forward_step(ctx);
+    if (!st) st = sync_scalars(ctx);
+    fill_stats(ctx, out);
+    return st;
+}
+
+int da_forward_run(da_ctx *ctx, int32_t nsteps, da_step_stats *last) {
+    return da_forward_run_timed(ctx, nsteps, last, nullptr);
+}
+
+int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, double *device_ms) {
+    if (!ctx || nsteps < 0) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_run: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_run: no state");
+    cudaSetDevice(ctx->device);
+    int st = DA_OK;
+    // Two steps (one ping-pong cycle) per graph launch; one graph per starting buffer.
+    const int cur0 = ctx->cur;
+    if (nsteps >= 2 && !ctx->step_graph[cur0]) {
+        cudaGraph_t g;
+        st = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        if (st) return st;
+        int s1 = launch_forward_step(ctx);
+        int s2 = s1 ? s1 : launch_forward_step(ctx);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        ctx->cur = cur0;  // capture advanced the ping-pong index without running anything
+        if (s2) return s2;
+        st = cuda_check(ctx, e, "end capture");
+        if (st) return st;
+        st = cuda_check(ctx, cudaGraphInstantiate(&ctx->step_graph[cur0], g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        if (st) return st;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (device_ms) {
+        st = cuda_check(ctx, cudaEventCreate(&e0), "event");
+        if (!st) st = cuda_check(ctx, cudaEventCreate(&e1), "event");
+        if (!st) st = cuda_check(ctx, cudaEventRecord(e0, ctx->stream), "event record");
+    }
+    int k = 0;
+    for (; k + 1 < nsteps && !st; k += 2)
+        st = cuda_check(ctx, cudaGraphLaunch(ctx->step_graph[cur0], ctx->stream), "graph launch");
+    if (!st && k < nsteps) st = launch_forward_step(ctx);
+    if (device_ms && !st) {
+        st = cuda_check(ctx, cudaEventRecord(e1, ctx->stream), "event record");
+        if (!st) st = cuda_check(ctx, cudaEventSynchronize(e1), "event sync");
+        float ms = 0.f;
+        if (!st) st = cuda_check(ctx, cudaEventElapsedTime(&ms, e0, e1), "event time");
+        *device_ms = ms;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (!st) st = sync_scalars(ctx);
+    fill_stats(ctx, last);
+    return st;
+}
+
+const char *da_forward_kernel_name(int32_t k) {
+    static const char *names[DA_FWD_KERNELS] = {"k_coef", "k_dt", "k_update", "k_volume"};
+    return (k >= 0 && k < DA_FWD_KERNELS) ? names[k] : "";
+}
+
+int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
+    if (!ctx || nsteps <= 0 || !kernel_ms) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_profile: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_profile: no state");
+    cudaSetDevice(ctx->device);
+    cudaEvent_t ev[DA_FWD_KERNELS + 1];
+    int st = DA_OK;
+    int made = 0;
+    for (; made < DA_FWD_KERNELS + 1 && !st; ++made) st = cuda_check(ctx, cudaEventCreate(&ev[made]), "event");
+    double acc[DA_FWD_KERNELS] = {0, 0, 0, 0};
+    for (int s = 0; s < nsteps && !st; ++s) {
+        st = launch_forward_step(ctx, ev);
+        if (!st) st = cuda_check(ctx, cudaEventSynchronize(ev[DA_FWD_KERNELS]), "event sync");
+        for (int k = 0; k < DA_FWD_KERNELS && !st; ++k) {
+            float ms = 0.f;
+            st = cuda_check(ctx, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "event time");
+            acc[k] += ms;
+        }
+    }
+    for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+    if (!st) st = sync_scalars(ctx);
+    for (int k = 0; k < DA_FWD_KERNELS; ++k) kernel_ms[k] = acc[k] / nsteps;
+    return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+// Internal declarations shared by the CUDA translation units of libda_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "discrete_adjoint.h"
+
+#define DA_TINY 1.e-4  // GEOFLOW_TINY, src/header/constant.h:68
+
+namespace da {
+
+// Per-material constants formed on the host once per parameter change (host libm, so the
+// device never evaluates a transcendental and the FP64 path matches the CPU bit for bit).
+//   kact_sgn[m][s+1]: gmfggetcoef's K_act/pass for sgn(vel) = s, clamped at 0, times epsilon
+//   tan_bed[m]     : tan(bedfrict[m])             (residual.C:231)
+struct MatConsts {
+    double kact_sgn[DA_MAX_MATERIALS][3];
+    double tan_bed[DA_MAX_MATERIALS];
+    double kact_rest;     // 1 * epsilon: no yield or dry cell (getcoef.f:129-142)
+    double epsilon;
+    double sin_int;       // sin(intfrict)               (residual.C:227)
+    double gamma;
+    int32_t n_materials;
+};
+
+// Scalars that live on the device so that whole step loops run without host round trips.
+struct DevScalars {
+    double time;          // TimeProps::time
+    double dt;            // last dt
+    double hmax;          // max h over wet cells (last coef pass)
+    double min_dxe;       // min over wet cells of min(dx,dy)/evalue (last coef pass)
+    double volume;        // sum dx*dy*h after the last update
+    double frict_tiny;    // MatProps::frict_tiny of the current step (hpfem.C:232-235)
+    long long iter;       // TimeProps::iter
+    unsigned long long acc_min_dxe;  // running min, bit pattern of a positive double
+    unsigned long long acc_hmax;     // running max, bit pattern of a non-negative double
+    int err;              // sticky DA_ERR_* raised on the device
+    int pad;
+};
+
+// Time-clipping targets (TimeProps::ndnextoutput / ndnextsave / ndmaxtime) and the
+// frict_tiny schedule (hpfem.C:232-235), passed by value to the dt kernel.
+struct TimeConsts {
+    double next_output, next_save, max_time, influx_dt;
+    double gravity_scale, epsilon;
+    double frict_tiny_early, frict_tiny_late;
+    long long frict_tiny_iters;
+};
+
+// Device copy of the flattened mesh.  FP64 path reads the double arrays; the FP32-split
+// path reads the float copies.
+struct DevMesh {
+    int32_t n = 0;
+    int32_t epoch = -1;
+    int32_t *nbr = nullptr;         // [8][n]
+    uint8_t *mat = nullptr;         // [n]
+    uint8_t *bflag = nullptr;       // [n] bit s: side s is a domain boundary; bit 4+s: side s has 2 neighbours
+    double *x = nullptr, *y = nullptr, *dx = nullptr, *dy = nullptr;
+    double *g = nullptr;            // [3][n]
+    double *dg = nullptr;           // [2][n]
+    double *curv = nullptr;         // [2][n]
+    float *fdx = nullptr, *fdy = nullptr;
+    float *fg = nullptr, *fdg = nullptr, *fcurv = nullptr;
+};
+
+}  // namespace da
+
+struct da_ctx {
+    da_params p{};
+    da::MatConsts mc{};
+    da::TimeConsts tc{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    da::DevMesh mesh;
+    // state, ping-pong; FP64 or FP32 per precision
+    void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int cur = 0;
+    void *kact = nullptr;            // [n] Real
+    void *slopes = nullptr;          // [6][n] Real
+    double *vol_part = nullptr;      // [nblocks] per-block volume partials
+    int nblocks = 0;
+    da::DevScalars *dsc = nullptr;   // device scalars
+    da::DevScalars *hsc = nullptr;   // pinned host mirror
+    // graphs of two forward steps, one per starting ping-pong buffer (captured lazily,
+    // dropped on mesh or parameter change)
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+    std::string err;
+    bool have_state = false;
+};
+
+namespace da {
+
+int set_error(da_ctx *ctx, int code, const std::string &msg);
+int cuda_check(da_ctx *ctx, cudaError_t e, const char *what);
+void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
+
+// forward_fp64.cu / forward_fp32.cu
+// ev (optional): DA_FWD_KERNELS + 1 events recorded around the launches
+int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev = nullptr);
+int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev);
+int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev);
+int forward_alloc(da_ctx *ctx);
+void forward_free(da_ctx *ctx);
+
+}  // namespace da

@@ -1,0 +1,9 @@
+// FP32-split path of the forward step: state, fluxes and sources in FP32 (FMA allowed);
+// the dt min-reduction, dt arithmetic and the volume sum stay in FP64.
+#include "forward_impl.cuh"
+
+namespace da {
+
+int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev) { return fwd::launch_step_t<float>(ctx, ev); }
+
+}  // namespace da

@@ -1,0 +1,170 @@
+"""Python mirror of the reference's hot-path call sites over the C ABI.
+
+The reference drives one explicit step per call of
+    step(El_Table, NodeTable, myid, nump, matprops, timeprops, pileprops, fluxprops,
+         statprops, &order_flag, outline, discharge, adaptflag)      src/geoflow/step.C:29-32
+with material data in MatProps (src/header/properties.h:527-640) and time data in
+TimeProps (properties.h:321-520).  Here the mesh tables are a flattened Mesh held on the
+device by a GeoflowContext; MatProps/TimeProps keep the reference's field names.
+Errors that the reference handles with printf+exit raise DAError instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _ffi
+from .mesh import Mesh
+
+PI_REF = 3.1415926  # src/header/constant.h:37, used for degree -> radian in datread.C:379-400
+
+
+@dataclass
+class MatProps:
+    """The fields of MatProps that the step reads.  Angles in degrees as in frict.data."""
+    intfrict_deg: float = 30.0
+    bedfrict_deg: list = field(default_factory=lambda: [20.0])
+    epsilon: float = 1.0
+    gravity_scale: float = 1.0
+    gamma: float = 1.0
+    frict_tiny_iters: int = 50
+    frict_tiny_early: float = 0.1
+    frict_tiny_late: float = 0.000000001
+
+    @staticmethod
+    def rad(deg: float) -> float:
+        return deg * PI_REF / 180.0
+
+
+@dataclass
+class TimeProps:
+    """TimeProps fields that clip dt (incrtime, properties.h:397-410); nondimensional."""
+    maxtime: float = math.inf
+    nextoutput: float = math.inf
+    nextsave: float = math.inf
+    time: float = 0.0
+    iter: int = 0
+
+
+def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
+                influx_dt: float = math.inf) -> _ffi.da_params:
+    p = _ffi.da_params()
+    _ffi.load().da_params_default(C.byref(p))
+    p.precision = precision
+    p.device = device
+    p.epsilon = mat.epsilon
+    p.gravity_scale = mat.gravity_scale
+    p.gamma = mat.gamma
+    p.intfrict = MatProps.rad(mat.intfrict_deg)
+    p.n_materials = len(mat.bedfrict_deg)
+    for k, b in enumerate(mat.bedfrict_deg):
+        p.bedfrict[k] = MatProps.rad(b)
+    p.frict_tiny_iters = mat.frict_tiny_iters
+    p.frict_tiny_early = mat.frict_tiny_early
+    p.frict_tiny_late = mat.frict_tiny_late
+    p.max_time = tp.maxtime
+    p.next_output = tp.nextoutput
+    p.next_save = tp.nextsave
+    p.influx_dt = influx_dt
+    return p
+
+
+@dataclass
+class StepStats:
+    dt: float
+    time: float
+    volume: float
+    hmax: float
+    iter: int
+
+
+class GeoflowContext:
+    """One device context: flattened mesh + state resident in HBM."""
+
+    def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
+                 device: int = 0, influx_dt: float = math.inf):
+        self.lib = _ffi.load()
+        self.mat = mat
+        self.tp = tp or TimeProps()
+        self.precision = precision
+        self.params = make_params(mat, self.tp, precision, device, influx_dt)
+        err = C.c_int(0)
+        self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
+        if not self.ctx:
+            raise _ffi.DAError(err.value, "da_create failed: " + self.lib.da_strerror(err.value).decode())
+        self.mesh: Mesh | None = None
+        if self.tp.time or self.tp.iter:
+            self.set_time(self.tp.time, self.tp.iter)
+
+    def _check(self, st: int, what: str):
+        if st != 0:
+            msg = self.lib.da_last_error(self.ctx).decode() if self.ctx else ""
+            raise _ffi.DAError(st, f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.da_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- mesh / state
+    def upload_mesh(self, mesh: Mesh, epoch: int = 0):
+        self.mesh = mesh
+        self._check(self.lib.da_upload_mesh(self.ctx, C.byref(mesh.soa()), epoch), "da_upload_mesh")
+
+    def set_state(self, h, hu, hv):
+        h, hu, hv = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, hu, hv))
+        self._check(self.lib.da_set_state(self.ctx, _ffi.dptr(h), _ffi.dptr(hu), _ffi.dptr(hv)), "da_set_state")
+
+    def get_state(self):
+        n = self.mesh.n
+        h, hu, hv = np.empty(n), np.empty(n), np.empty(n)
+        self._check(self.lib.da_get_state(self.ctx, _ffi.dptr(h), _ffi.dptr(hu), _ffi.dptr(hv)), "da_get_state")
+        return h, hu, hv
+
+    def set_time(self, time: float, iteration: int):
+        self._check(self.lib.da_set_time(self.ctx, time, iteration), "da_set_time")
+
+    # ---- stepping
+    def step(self) -> StepStats:
+        """One step() (order_flag = 1)."""
+        s = _ffi.da_step_stats()
+        self._check(self.lib.da_forward_step(self.ctx, C.byref(s)), "da_forward_step")
+        return StepStats(s.dt, s.time, s.volume, s.hmax, s.iter)
+
+    def run(self, nsteps: int) -> StepStats:
+        s = _ffi.da_step_stats()
+        self._check(self.lib.da_forward_run(self.ctx, nsteps, C.byref(s)), "da_forward_run")
+        return StepStats(s.dt, s.time, s.volume, s.hmax, s.iter)
+
+    def run_timed(self, nsteps: int):
+        """(stats, device ms between events on the context stream around the nsteps steps)."""
+        s = _ffi.da_step_stats()
+        ms = C.c_double(0.0)
+        self._check(self.lib.da_forward_run_timed(self.ctx, nsteps, C.byref(s), C.byref(ms)), "da_forward_run_timed")
+        return StepStats(s.dt, s.time, s.volume, s.hmax, s.iter), ms.value
+
+    def profile(self, nsteps: int) -> dict:
+        """Mean device ms per forward kernel over nsteps (events around every launch)."""
+        out = np.zeros(4)
+        self._check(self.lib.da_forward_profile(self.ctx, nsteps, _ffi.dptr(out)), "da_forward_profile")
+        return {self.lib.da_forward_kernel_name(k).decode(): float(out[k]) for k in range(4)}
+
+
+def step(ctx: GeoflowContext) -> StepStats:
+    """step() of src/geoflow/step.C:29 on a device-resident context."""
+    return ctx.step()

@@ -1,0 +1,88 @@
+/*
+ * da_mesh.h -- host-side mesh and input preparation (C ABI).
+ *
+ * The reference builds its mesh with the preprocessor (src/preproc) and adapts it
+ * with src/adapt; both stay on the host and out of the GPU path.  This module gives
+ * a host-only stand-in that produces the same kind of flattened mesh the hot path
+ * consumes: a 2:1-balanced quadtree over a rectangular domain, cells in Morton
+ * (space-filling-curve) order, neighbour and hanging-neighbour tables, and the
+ * static per-cell fields that the reference computes once per adapt:
+ *   gravity vector     Element::calc_gravity_vector  src/datstr/element2.C:3545-3564
+ *   d gravity          Element::calc_d_gravity       src/datstr/element2.C:3574-3653
+ *   slope, curvature   Get_slope / Get_curvature     src/gisapi/GisApi.C:705-838
+ *   initial pile       elliptical_pile_height        src/main/init_piles.C:167-277
+ * Nothing here touches a GPU.
+ */
+#ifndef DA_MESH_H
+#define DA_MESH_H
+
+#include <stdint.h>
+#include "discrete_adjoint.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Elevation raster, GRASS layout (row 0 is the northern edge, src/gisapi/GisApi.C:153-193). */
+typedef struct da_dem {
+    int32_t nrows, ncols;
+    double xmin, ymin;         /* south-west corner */
+    double res;                /* post spacing */
+    const float *elev;         /* [nrows*ncols] */
+    const int32_t *mat;        /* optional [nrows*ncols] 0-based material ids, or NULL */
+} da_dem;
+
+/* One pile (PileProps, src/header/properties.h:199-270); paraboloid shape. */
+typedef struct da_pile_spec {
+    double xc, yc;             /* centre */
+    double height;             /* PileProps::pileheight */
+    double major, minor;       /* radii */
+    double rot_deg;            /* orientation of the major axis */
+    double vx, vy;             /* initial velocity */
+} da_pile_spec;
+
+typedef struct da_mesh_spec {
+    double xmin, ymin;         /* domain south-west corner */
+    double dx0, dy0;           /* base (level 0) cell size */
+    int32_t nx0, ny0;          /* base grid */
+    int32_t max_level;         /* finest level (<= 20) */
+    int32_t uniform;           /* 1: every cell at max_level */
+    double refine_margin;      /* pile ellipses are grown by this distance before refining */
+    int32_t n_boxes;           /* extra axis-aligned refinement boxes */
+    const double *boxes;       /* [4*n_boxes] xmin,xmax,ymin,ymax */
+    double random_frac;        /* fraction of cells refined at random (tests: hanging nodes everywhere) */
+    uint64_t seed;
+} da_mesh_spec;
+
+/* Host-owned mesh.  All arrays have n_cells entries per component. */
+typedef struct da_mesh_host {
+    int32_t n_cells;
+    int32_t max_level;
+    int32_t n_piles;
+    int32_t *level;            /* [n] */
+    int32_t *ix, *iy;          /* [n] integer cell coordinates at their level */
+    int32_t *nbr;              /* [8][n] */
+    double *x, *y, *dx, *dy;   /* [n] */
+    double *elevation;         /* [n] */
+    double *zeta;              /* [2][n] terrain slope dz/dx, dz/dy */
+    double *curvature;         /* [2][n] */
+    double *gravity;           /* [3][n] */
+    double *d_gravity;         /* [2][n] */
+    int32_t *material;         /* [n] */
+    double *h0, *hu0, *hv0;    /* [n] initial state */
+    double *dh0_dpile;         /* [n_piles][n] d h0 / d pile height */
+} da_mesh_host;
+
+/* Builds the mesh.  gravity_scale and length_scale follow MatProps (1 for SI runs). */
+int da_mesh_build(const da_mesh_spec *spec, const da_dem *dem, const da_pile_spec *piles,
+                  int32_t n_piles, double length_scale, double gravity_scale,
+                  da_mesh_host **out);
+void da_mesh_free(da_mesh_host *m);
+/* Fills a da_mesh_soa view whose pointers alias the host mesh. */
+int da_mesh_view(const da_mesh_host *m, da_mesh_soa *view);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DA_MESH_H */

@@ -1,0 +1,151 @@
+/*
+ * discrete_adjoint.h -- C ABI of the B200 finite-volume step and its discrete adjoint.
+ *
+ * This is the drop-in boundary that replaces the per-timestep hot path of the
+ * TITAN2D-derived solver (haghakhani/discrete_adjoint).  The reference has no
+ * plugin or FFI layer; its boundary is a set of C++ call sites, and each entry
+ * point below names the call site it replaces:
+ *
+ *   step()                 src/geoflow/step.C:29-275         (called at src/main/hpfem.C:271)
+ *     slopes()             src/geoflow/slopes.C:25-83
+ *     get_coef_and_eigen() src/geoflow/get_coef_and_eigen.C:29-180
+ *     TimeProps::incrtime  src/header/properties.h:397-410
+ *     calc_edge_states<>() src/geoflow/edge_states.C:37-77
+ *     correct()            src/geoflow/corrector.C:36-193 -> update_states() src/adjoint/residual.C:162-275
+ *   dual_solver()          src/adjoint/dual_solver.C:80-273  (called at src/main/hpfem.C:406)
+ *     calc_jacobian()      src/adjoint/calc_jacobain.C:40-153
+ *     calc_adjoint()       src/adjoint/calc_adjoint.C:35-167
+ *     error_compute()      src/adjoint/error_compute.C:24-119
+ *
+ * Conventions (the reference's own are printf+exit; here nothing exits):
+ *   - every function returns DA_OK (0) or a negative DA_ERR_* code;
+ *     da_last_error() gives a one-line message for the last failure on a context;
+ *   - host buffers are owned by the caller, device buffers by the context;
+ *   - one context per host thread; calls are stream-ordered and not re-entrant.
+ *
+ * Mesh layout ("flattened quadtree"): cells are in space-filling-curve order.
+ * Sides are numbered relative to the cell's positive-x side, as the reference
+ * does with Element::positive_x_side (src/datstr/element2.C:694-716):
+ *   side 0 = +x (xp), 1 = +y (yp), 2 = -x (xm), 3 = -y (ym).
+ * nbr[s*n + i] (s = 0..3) is the first neighbour across side s (Element::neighbor[s]),
+ * nbr[(s+4)*n + i] the second one (Element::neighbor[s+4]); the two differ only where
+ * the side carries two finer neighbours (edge-midpoint node S_C_CON, constant.h:42);
+ * -1 marks the domain boundary (neigh_proc == INIT, constant.h:48).
+ */
+#ifndef DISCRETE_ADJOINT_H
+#define DISCRETE_ADJOINT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DA_ABI_VERSION 1
+
+#define DA_MAX_MATERIALS 16
+#define DA_MAX_PILES 8
+
+/* return codes */
+#define DA_OK 0
+#define DA_ERR_INVALID (-1)     /* bad argument, size or call order */
+#define DA_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define DA_ERR_NAN (-3)         /* NaN/Inf in the state (residual.C:137-147, :272-273) */
+#define DA_ERR_NEG_DEPTH (-4)   /* reserved: negative depth that the clamp could not absorb */
+#define DA_ERR_EIGEN (-5)       /* wave speed above 1e9 (get_coef_and_eigen.C:144-156) */
+#define DA_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */
+#define DA_ERR_NO_MESH (-7)     /* no mesh uploaded yet */
+#define DA_ERR_OOM (-8)         /* device allocation failed */
+#define DA_ERR_NO_DEVICE (-9)   /* no CUDA device visible */
+#define DA_ERR_UNSUPPORTED (-10)
+
+/* precision modes */
+#define DA_PREC_FP64 0          /* plain: every operation in FP64, no contraction, reference order */
+#define DA_PREC_FP32_SPLIT 1    /* FP32 state/flux/source; FP64 dt, volume and functional sums */
+
+/* Material and time-stepping properties used on the hot path.
+ * Mirrors the fields of MatProps (src/header/properties.h:527-640) and
+ * TimeProps (properties.h:321-520) that step() reads.  Angles in radians. */
+typedef struct da_params {
+    int32_t precision;           /* DA_PREC_* */
+    int32_t device;              /* CUDA device ordinal */
+    double epsilon;              /* MatProps::epsilon = HEIGHT_SCALE/LENGTH_SCALE */
+    double gravity_scale;        /* MatProps::GRAVITY_SCALE */
+    double gamma;                /* MatProps::gamma, limiter factor (1 in hpfem.C:82) */
+    double intfrict;             /* MatProps::intfrict */
+    int32_t n_materials;         /* 1..DA_MAX_MATERIALS */
+    int32_t frict_tiny_iters;    /* hpfem.C:232-235: frict_tiny = early while iter < this */
+    double bedfrict[DA_MAX_MATERIALS]; /* MatProps::bedfrict, 0-based material index */
+    double frict_tiny_early;     /* 0.1 */
+    double frict_tiny_late;      /* 1e-9 */
+    double max_time;             /* TimeProps::ndmaxtime */
+    double next_output;          /* TimeProps::ndnextoutput (clips dt) */
+    double next_save;            /* TimeProps::ndnextsave (clips dt) */
+    double influx_dt;            /* dt[2] of get_coef_and_eigen.C:49-77; HUGE_VAL when no source is active */
+} da_params;
+
+/* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
+typedef struct da_mesh_soa {
+    int32_t n_cells;
+    const int32_t *nbr;        /* [8][n] neighbour table, -1 = domain boundary */
+    const double *x, *y;       /* [n] cell centres (Element::coord) */
+    const double *dx, *dy;     /* [n] cell sizes (Element::dx) */
+    const double *gravity;     /* [3][n] Element::gravity */
+    const double *d_gravity;   /* [2][n] Element::d_gravity (d gz/dx, d gz/dy) */
+    const double *curvature;   /* [2][n] Element::curvature */
+    const int32_t *material;   /* [n] 0-based material index */
+} da_mesh_soa;
+
+/* Per-step scalars (the hot-path parts of get_coef_and_eigen / step / calc_stats). */
+typedef struct da_step_stats {
+    double dt;                 /* time step taken (after incrtime clipping) */
+    double time;               /* TimeProps::time after the step */
+    double volume;             /* realvolume of step.C:205, sum dx*dy*h after the update (FP64) */
+    double hmax;               /* max h over wet cells before the update */
+    int64_t iter;              /* TimeProps::iter after the step */
+} da_step_stats;
+
+typedef struct da_ctx da_ctx;
+
+/* ---- context lifecycle ------------------------------------------------------------- */
+void da_params_default(da_params *p);
+/* Creates a context on p->device.  *err receives the status (may be NULL). */
+da_ctx *da_create(const da_params *p, int *err);
+void da_destroy(da_ctx *ctx);
+const char *da_last_error(const da_ctx *ctx);
+const char *da_strerror(int code);
+int da_abi_version(void);
+/* Replaces the material/time parameters of a live context (MatProps/TimeProps edits between steps). */
+int da_set_params(da_ctx *ctx, const da_params *p);
+/* TimeProps::time and ::iter (restart, or the adjoint's rewind). */
+int da_set_time(da_ctx *ctx, double time, int64_t iter);
+
+/* ---- mesh and state transfer ------------------------------------------------------- */
+/* Once per adapt (hpfem.C:243-267): copies the flattened mesh to the device. */
+int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *mesh, int32_t epoch);
+int da_set_state(da_ctx *ctx, const double *h, const double *hu, const double *hv);
+int da_get_state(da_ctx *ctx, double *h, double *hu, double *hv);
+
+/* ---- forward stepping -------------------------------------------------------------- */
+/* One step() (order_flag = 1). */
+int da_forward_step(da_ctx *ctx, da_step_stats *out);
+/* nsteps step() calls back to back, device-resident, captured in a CUDA graph. */
+int da_forward_run(da_ctx *ctx, int32_t nsteps, da_step_stats *last);
+/* As da_forward_run; *device_ms receives the time between CUDA events recorded on the
+ * context's stream before the first and after the last launch. */
+int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, double *device_ms);
+
+/* ---- tracing (the reference's Timer class, properties.h:43-71, moved onto the device) --- */
+#define DA_FWD_KERNELS 4  /* coef, dt, update, volume */
+/* Runs nsteps forward steps with CUDA events around every launch on the context's stream and
+ * returns the mean device time of each forward kernel in ms (kernel_ms[DA_FWD_KERNELS]) and
+ * the names in kernel order through da_forward_kernel_name().  The state advances. */
+int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms);
+const char *da_forward_kernel_name(int32_t k);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DISCRETE_ADJOINT_H */

@@ -1,0 +1,110 @@
+"""Device forward step against the oracle (restated reference), through the C ABI."""
+import numpy as np
+import pytest
+
+import oracle
+from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, inputs, make_params
+from discrete_adjoint_b200.mesh import Mesh, MeshSpec
+
+pytestmark = pytest.mark.gpu
+
+# FP32-split tolerance against the FP64 oracle (relative L2 over the mesh)
+FP32_REL_L2_H = 1e-4
+FP32_REL_L2_MOM = 1e-3
+
+
+def oracle_run(w, nsteps, tp=None):
+    m = w.mesh
+    o = oracle.Oracle(make_params(w.mat, tp or TimeProps()), m)
+    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+    rc, dts, st = o.run(h, hu, hv, nsteps)
+    assert rc == 0
+    return h, hu, hv, dts, st
+
+
+def gpu_ctx(w, precision=_ffi.DA_PREC_FP64, tp=None):
+    ctx = GeoflowContext(w.mat, tp or TimeProps(), precision=precision)
+    ctx.upload_mesh(w.mesh)
+    ctx.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
+    return ctx
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3, 7])
+def test_fp64_bit_exact_vs_oracle_100_steps(seed):
+    w = inputs.test_case(seed=seed)
+    h, hu, hv, dts, st = oracle_run(w, 100)
+    with gpu_ctx(w) as ctx:
+        gdts = [ctx.step().dt for _ in range(100)]
+        gh, ghu, ghv = ctx.get_state()
+    assert np.array_equal(np.array(gdts), dts)
+    assert np.array_equal(gh, h) and np.array_equal(ghu, hu) and np.array_equal(ghv, hv)
+
+
+def test_fp64_graph_run_equals_single_steps():
+    w = inputs.test_case(seed=4)
+    h, hu, hv, dts, st = oracle_run(w, 101)
+    with gpu_ctx(w) as ctx:
+        s = ctx.run(101)
+        gh, ghu, ghv = ctx.get_state()
+    assert s.iter == 101 and s.time == st.time and s.dt == dts[-1]
+    assert np.array_equal(gh, h) and np.array_equal(ghu, hu) and np.array_equal(ghv, hv)
+    assert abs(s.volume - st.volume) <= 1e-12 * st.volume
+
+
+def test_fp64_workload1_bit_exact_200_steps():
+    w = inputs.workload1()
+    h, hu, hv, dts, st = oracle_run(w, 200)
+    with gpu_ctx(w) as ctx:
+        s = ctx.run(200)
+        gh, ghu, ghv = ctx.get_state()
+    assert s.time == st.time
+    assert np.array_equal(gh, h) and np.array_equal(ghu, hu) and np.array_equal(ghv, hv)
+
+
+def test_fp64_time_clipping_and_schedule():
+    w = inputs.test_case(seed=2)
+    tp = TimeProps(maxtime=2.5, nextoutput=1.0)
+    h, hu, hv, dts, st = oracle_run(w, 60, tp=tp)
+    with gpu_ctx(w, tp=tp) as ctx:
+        s = ctx.run(60)
+        gh, _, _ = ctx.get_state()
+    assert s.time == st.time
+    assert np.array_equal(gh, h)
+
+
+@pytest.mark.parametrize("seed", [1, 3])
+def test_fp32_split_close_to_fp64_oracle(seed):
+    w = inputs.test_case(seed=seed)
+    h, hu, hv, dts, st = oracle_run(w, 100)
+    with gpu_ctx(w, precision=_ffi.DA_PREC_FP32_SPLIT) as ctx:
+        s = ctx.run(100)
+        gh, ghu, ghv = ctx.get_state()
+    eh, eu, ev = rel_l2(gh, h), rel_l2(ghu, hu), rel_l2(ghv, hv)
+    print(f"fp32-split rel L2 after 100 steps: h {eh:.3e} hu {eu:.3e} hv {ev:.3e}; time {s.time} vs {st.time}")
+    assert eh < FP32_REL_L2_H
+    assert eu < FP32_REL_L2_MOM and ev < FP32_REL_L2_MOM
+
+
+def test_errors_are_codes_not_exits():
+    w = inputs.test_case(seed=1)
+    ctx = GeoflowContext(w.mat, TimeProps())
+    with pytest.raises(_ffi.DAError) as e:
+        ctx.step()
+    assert e.value.code == _ffi.DA_ERR_NO_MESH
+    bad = Mesh(**w.mesh.arrays())
+    bad.nbr[0, 5] = w.mesh.n + 3
+    with pytest.raises(_ffi.DAError) as e:
+        ctx.upload_mesh(bad)
+    assert e.value.code == _ffi.DA_ERR_INVALID
+    ctx.upload_mesh(w.mesh)
+    h = w.mesh.h0.copy()
+    h[np.argmax(h)] = np.nan
+    ctx.set_state(h, w.mesh.hu0, w.mesh.hv0)
+    with pytest.raises(_ffi.DAError) as e:
+        ctx.run(3)
+    assert e.value.code in (_ffi.DA_ERR_NAN,)
+    ctx.close()
