@@ -87,3 +87,67 @@ class Oracle:
         self.lib.orc_edge_fluxes(C.byref(self.params), C.byref(self.soa), _ffi.dptr(h), _ffi.dptr(hu),
                                  _ffi.dptr(hv), _ffi.dptr(kact), _ffi.dptr(F))
         return F
+
+
+# ---------------------------------------------------------------- reference harness
+REF_EXE = os.path.join(HERE, "_ref", "ref_harness")
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_EXE)
+
+
+def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf"), ref_static: bool = False,
+                  workdir: str | None = None) -> dict:
+    """Runs the reference's own compiled step() (oracle/_ref/ref_harness) nsteps times.
+
+    mat: MatProps (degrees, as in frict.data).  Returns dt history, time, final state, and the
+    per-cell slopes, k act/pass and edge-node fluxes of the last step, plus the gravity and
+    d_gravity fields the reference used.
+    """
+    import struct
+    import subprocess
+    import tempfile
+
+    from discrete_adjoint_b200.solver import MatProps
+    n = mesh.n
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<6i", 0x31484144, n, mesh.max_level, len(mat.bedfrict_deg), nsteps,
+                                int(ref_static)))
+            f.write(np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma,
+                              maxtime], dtype="<f8").tobytes())
+            f.write(bed.astype("<f8").tobytes())
+            for a in (mesh.nbr, mesh.level, mesh.ix, mesh.iy, mesh.material):
+                f.write(np.ascontiguousarray(a, dtype="<i4").tobytes())
+            for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature,
+                      h, hu, hv):
+                f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+        r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    magic, n2, ns = struct.unpack_from("<3i", raw, 0)
+    assert magic == 0x314F4144 and n2 == n and ns == nsteps
+    off = 12
+    arr = np.frombuffer(raw, dtype="<f8", offset=off)
+    k = 0
+
+    def take(cnt):
+        nonlocal k
+        v = arr[k:k + cnt].copy()
+        k += cnt
+        return v
+
+    out = {"dt": take(nsteps), "time": float(take(1)[0])}
+    out["h"], out["hu"], out["hv"] = take(n), take(n), take(n)
+    out["slopes"] = take(6 * n).reshape(6, n)
+    out["kact"] = take(n)
+    out["flux"] = take(12 * n).reshape(4, 3, n)
+    out["gravity"] = take(3 * n).reshape(3, n)
+    out["d_gravity"] = take(2 * n).reshape(2, n)
+    return out

@@ -1,0 +1,52 @@
+"""Generates the golden fixtures in this directory from the reference's own compiled step().
+
+Run in a container that has the reference sources (it builds oracle/_ref/ref_harness with
+oracle/ref_build.py, then runs it):   python tests/golden/make_golden.py
+Each fixture holds a small flattened mesh (seeded, hanging nodes on many sides, two
+materials), the initial state, and what the reference's step() produced from it:
+dt history, final state, and the slopes, k act/pass and edge-node fluxes of the last step.
+Fixture "static_*" also holds gravity and d_gravity from Element::calc_gravity_vector and
+Element::calc_d_gravity.
+"""
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+import oracle  # noqa: E402
+from oracle import ref_build  # noqa: E402
+from discrete_adjoint_b200 import inputs  # noqa: E402
+
+CASES = [
+    # name, seed, nx0, ny0, max_level, random_frac, nsteps
+    ("fwd_s11_60", 11, 12, 8, 2, 0.4, 60),
+    ("fwd_s12_120", 12, 12, 8, 2, 0.3, 120),
+    ("fwd_s13_uniform_30", 13, 10, 6, 1, 0.0, 30),
+]
+
+
+def main():
+    ref_build.build()
+    for name, seed, nx0, ny0, L, frac, nsteps in CASES:
+        w = inputs.test_case(seed=seed, nx0=nx0, ny0=ny0, max_level=L, random_frac=frac)
+        m = w.mesh
+        r = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, nsteps)
+        st = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, 1, ref_static=True)
+        arrs = {("mesh_" + k): v for k, v in m.arrays().items()}
+        arrs.update({("ref_" + k): v for k, v in r.items()})
+        arrs["ref_static_gravity"] = st["gravity"]
+        arrs["ref_static_d_gravity"] = st["d_gravity"]
+        arrs["nsteps"] = np.int64(nsteps)
+        arrs["intfrict_deg"] = np.float64(w.mat.intfrict_deg)
+        arrs["bedfrict_deg"] = np.array(w.mat.bedfrict_deg, dtype=np.float64)
+        p = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(p, **arrs)
+        print(p, m.n, "cells", os.path.getsize(p) // 1024, "KiB")
+
+
+if __name__ == "__main__":
+    main()
