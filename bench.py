@@ -128,16 +128,31 @@ def barrier(ws: int, dev: int):
         torch.cuda.synchronize(dev)
 
 
-def algorithmic_bytes(precision: str) -> dict:
-    """Algorithmic bytes per cell and launch of each forward kernel (every array touched once,
-    neighbour re-reads excluded), from the device layout in csrc/da_internal.h."""
+def wet_counts(m, h) -> tuple[int, int]:
+    """(cells with h >= GEOFLOW_TINY, cells that are wet or have a wet face neighbour)."""
+    wet = h >= 1e-4
+    act = wet.copy()
+    for k in range(8):
+        e = m.nbr[k]
+        ok = e >= 0
+        act[ok] |= wet[e[ok]]
+    return int(wet.sum()), int(act.sum())
+
+
+def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dict:
+    """Algorithmic HBM bytes of one launch of each forward kernel: every array a cell needs is
+    touched once (neighbour re-reads are halo traffic, not algorithmic).  Layout of
+    csrc/da_internal.h: state r bytes per component, static fields r bytes per component
+    (x, y centres only in FP64), nbr 4 x int32 primary neighbours, bflag and material 1 byte.
+      k_coef  : every cell reads h; a wet cell reads hu, hv, bflag, mat, nbr, dx, dy, g_z (and
+                x, y in FP64) and writes k_act.
+      k_update: every cell reads bflag, the state, nbr, dx, dy and writes the state; a cell
+                with wet cells around it also reads k_act, g (3), d_gravity (2), curvature (2), mat."""
     r = 8 if precision == "fp64" else 4
-    coord = 16 if precision == "fp64" else 0   # x, y centres (FP64 path only)
-    # k_coef: state 3r, bflag 1, mat 1, nbr 4x4, dx dy 2r, g_z r, coords -> slopes 6r, kact r
-    coef = 3 * r + 1 + 1 + 16 + 2 * r + r + coord + 6 * r + r
-    # k_update: state 3r, kact r, slopes 6r, bflag 1, mat 1, nbr 4x4, dx dy 2r, g 3r, dg 2r, curv 2r -> state 3r
-    upd = 3 * r + r + 6 * r + 1 + 1 + 16 + 2 * r + 3 * r + 2 * r + 2 * r + 3 * r
-    return {"k_coef": coef, "k_update": upd, "k_dt": 0, "k_volume": 0}
+    xy = 2 * r if precision == "fp64" else 0
+    coef = n * r + n_wet * (2 * r + 1 + 1 + 16 + 2 * r + r + xy + r)
+    upd = n * (1 + 3 * r + 16 + 2 * r + 3 * r) + n_act * (r + 3 * r + 2 * r + 2 * r + 1)
+    return {"k_coef": coef, "k_update": upd}
 
 
 def run_reference_arm(args, ws, rank):
@@ -181,6 +196,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true", help="skip the clock sampler (profiling runs)")
+    ap.add_argument("--sign-floor", type=float, default=0.0,
+                    help="FP32-split friction sign threshold floor (0 = the reference's thresholds)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -199,7 +216,8 @@ def main():
     prec = _ffi.DA_PREC_FP32_SPLIT if args.precision == "fp32" else _ffi.DA_PREC_FP64
 
     def fresh(precision):
-        c = GeoflowContext(w.mat, TimeProps(), precision=precision, device=local)
+        c = GeoflowContext(w.mat, TimeProps(), precision=precision, device=local,
+                           fp32_sign_floor=args.sign_floor)
         c.upload_mesh(m)
         c.set_state(m.h0, m.hu0, m.hv0)
         return c
@@ -230,17 +248,29 @@ def main():
     _, ms64 = ref64.run_timed(args.steps)
     ms64 = allmax(ms64, ws, local)
     value64 = m.n * args.steps * ws / (ms64 * 1e-3)
-    # error of the FP32-split state against the FP64 path after the same steps from the same start
-    h32, _, _ = ctx.get_state()
-    h64, _, _ = ref64.get_state()
-    rel_err_h = float(np.linalg.norm(h32 - h64) / max(np.linalg.norm(h64), 1e-300))
+    # error of the FP32-split path against the FP64 path after the same number of steps from
+    # the same initial state (fresh contexts: the timed contexts ran extra untimed steps)
+    e32, e64 = fresh(prec), fresh(_ffi.DA_PREC_FP64)
+    nerr = args.warmup + args.steps
+    e32.run(nerr)
+    e64.run(nerr)
+    h32, u32, v32 = e32.get_state()
+    h64, u64, v64 = e64.get_state()
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))  # noqa: E731
+    rel_err = {"steps": nerr, "h": rel(h32, h64), "hu": rel(u32, u64), "hv": rel(v32, v64)}
+    e32.close()
+    e64.close()
 
-    # per-kernel device times for the roofline (events around each launch)
+    # per-kernel device times for the roofline (events around each launch); wet / active
+    # counts averaged over the profiled steps give the algorithmic bytes of each launch
+    w0 = wet_counts(m, ctx.get_state()[0])
     prof = ctx.profile(20)
+    w1 = wet_counts(m, ctx.get_state()[0])
+    n_wet, n_act = 0.5 * (w0[0] + w1[0]), 0.5 * (w0[1] + w1[1])
     dom = max(prof, key=prof.get)
-    alg = algorithmic_bytes(args.precision)
+    alg = algorithmic_bytes(args.precision, m.n, n_wet, n_act)
     hbm, peak_kind = peaks()
-    achieved = alg[dom] * m.n / (prof[dom] * 1e-3) / 1e9 if alg[dom] else 0.0
+    achieved = alg[dom] / (prof[dom] * 1e-3) / 1e9
 
     # e2e through the C ABI with host buffers: H2D state, one step, D2H state, every step
     h, hu, hv = ctx.get_state()
@@ -285,12 +315,13 @@ def main():
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "per-step working set larger than L2 (no flush needed)"},
             "fp64_value": value64, "fp32_over_fp64": value / value64,
-            "rel_err_h_vs_fp64": rel_err_h,
+            "rel_err_vs_fp64": rel_err, "fp32_sign_floor": args.sign_floor,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm if hbm else None, "peak_kind": peak_kind,
-                         "alg_bytes_per_cell": alg[dom], "kernel_ms": prof, "traffic": None},
+                         "alg_bytes_per_launch": alg[dom], "wet_cells": n_wet, "active_cells": n_act,
+                         "kernel_ms": prof, "traffic": None},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": 2 * args.steps,
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

@@ -25,7 +25,7 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + I
 UNITS = [
     ("capi.cu", []),
     ("forward_fp64.cu", ["--fmad=false"]),
-    ("forward_fp32.cu", []),
+    ("forward_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
     ("mesh_host.cpp", []),
 ]
 

@@ -53,6 +53,7 @@ class da_params(C.Structure):
         ("next_output", C.c_double),
         ("next_save", C.c_double),
         ("influx_dt", C.c_double),
+        ("fp32_sign_floor", C.c_double),
     ]
 
 

@@ -46,6 +46,7 @@ void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc) {
     mc->epsilon = p.epsilon;
     mc->sin_int = std::sin(p.intfrict);
     mc->gamma = p.gamma;
+    mc->sign_floor = p.precision == DA_PREC_FP32_SPLIT ? p.fp32_sign_floor : 0.0;
     mc->n_materials = p.n_materials;
     tc->next_output = p.next_output;
     tc->next_save = p.next_save;
@@ -86,7 +87,6 @@ static void free_state(da_ctx *ctx) {
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
     dfree(ctx->kact);
-    dfree(ctx->slopes);
     dfree(ctx->vol_part);
     ctx->have_state = false;
 }
@@ -201,6 +201,8 @@ da_ctx *da_create(const da_params *p, int *err) {
     fill_consts(ctx->p, &ctx->mc, &ctx->tc);
     int st = cuda_check(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
     if (!st) st = cuda_check(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    if (!st) st = cuda_check(ctx, cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device),
+                             "device attribute");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->dsc, sizeof(DevScalars)), "cudaMalloc(scalars)");
     if (!st) st = cuda_check(ctx, cudaMallocHost((void **)&ctx->hsc, sizeof(DevScalars)), "cudaMallocHost");
     if (st) {
@@ -442,7 +444,7 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
 }
 
 const char *da_forward_kernel_name(int32_t k) {
-    static const char *names[DA_FWD_KERNELS] = {"k_coef", "k_dt", "k_update", "k_volume"};
+    static const char *names[DA_FWD_KERNELS] = {"k_coef", "k_update"};
     return (k >= 0 && k < DA_FWD_KERNELS) ? names[k] : "";
 }
 
@@ -455,7 +457,7 @@ int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
     int st = DA_OK;
     int made = 0;
     for (; made < DA_FWD_KERNELS + 1 && !st; ++made) st = cuda_check(ctx, cudaEventCreate(&ev[made]), "event");
-    double acc[DA_FWD_KERNELS] = {0, 0, 0, 0};
+    double acc[DA_FWD_KERNELS] = {0, 0};
     for (int s = 0; s < nsteps && !st; ++s) {
         st = launch_forward_step(ctx, ev);
         if (!st) st = cuda_check(ctx, cudaEventSynchronize(ev[DA_FWD_KERNELS]), "event sync");

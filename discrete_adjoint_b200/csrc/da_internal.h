@@ -24,6 +24,7 @@ struct MatConsts {
     double epsilon;
     double sin_int;       // sin(intfrict)               (residual.C:227)
     double gamma;
+    double sign_floor;    // FP32-split only: lower bound on frict_tiny in the friction sign tests
     int32_t n_materials;
 };
 
@@ -39,6 +40,7 @@ struct DevScalars {
     unsigned long long acc_min_dxe;  // running min, bit pattern of a positive double
     unsigned long long acc_hmax;     // running max, bit pattern of a non-negative double
     int err;              // sticky DA_ERR_* raised on the device
+    unsigned blocks_done[2];  // last-block counters of the coefficient and update kernels
     int pad;
 };
 
@@ -80,9 +82,9 @@ struct da_ctx {
     void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     void *kact = nullptr;            // [n] Real
-    void *slopes = nullptr;          // [6][n] Real
     double *vol_part = nullptr;      // [nblocks] per-block volume partials
-    int nblocks = 0;
+    int nblocks = 0;                 // grid of the grid-stride step kernels
+    int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror
     // graphs of two forward steps, one per starting ping-pong buffer (captured lazily,

@@ -10,7 +10,11 @@ int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev) { return fwd::launch_
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
-    ctx->nblocks = int((n + fwd::kBlock - 1) / fwd::kBlock);
+    // grid-stride kernels: at most 8 blocks of 256 threads per SM (2048 resident threads)
+    const size_t want = (n + fwd::kBlock - 1) / fwd::kBlock;
+    const size_t cap = (size_t)(ctx->sm_count > 0 ? ctx->sm_count : 148) * 8;
+    ctx->nblocks = int(want < cap ? want : cap);
+    if (ctx->nblocks < 1) ctx->nblocks = 1;
     int st = DA_OK;
     for (int b = 0; b < 2 && !st; ++b)
         for (int v = 0; v < 3 && !st; ++v) {
@@ -18,7 +22,6 @@ int forward_alloc(da_ctx *ctx) {
             if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->U[b][v], 0, rs * n, ctx->stream), "memset");
         }
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
-    if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->slopes, rs * 6 * n), "cudaMalloc(slopes)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->vol_part, sizeof(double) * ctx->nblocks), "cudaMalloc(vol)");
     return st;
 }

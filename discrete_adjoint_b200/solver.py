@@ -50,7 +50,7 @@ class TimeProps:
 
 
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
-                influx_dt: float = math.inf) -> _ffi.da_params:
+                influx_dt: float = math.inf, fp32_sign_floor: float = 0.0) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -69,6 +69,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.next_output = tp.nextoutput
     p.next_save = tp.nextsave
     p.influx_dt = influx_dt
+    p.fp32_sign_floor = fp32_sign_floor
     return p
 
 
@@ -85,12 +86,12 @@ class GeoflowContext:
     """One device context: flattened mesh + state resident in HBM."""
 
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
-                 device: int = 0, influx_dt: float = math.inf):
+                 device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
-        self.params = make_params(mat, self.tp, precision, device, influx_dt)
+        self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:
@@ -160,9 +161,9 @@ class GeoflowContext:
 
     def profile(self, nsteps: int) -> dict:
         """Mean device ms per forward kernel over nsteps (events around every launch)."""
-        out = np.zeros(4)
+        out = np.zeros(2)
         self._check(self.lib.da_forward_profile(self.ctx, nsteps, _ffi.dptr(out)), "da_forward_profile")
-        return {self.lib.da_forward_kernel_name(k).decode(): float(out[k]) for k in range(4)}
+        return {self.lib.da_forward_kernel_name(k).decode(): float(out[k]) for k in range(2)}
 
 
 def step(ctx: GeoflowContext) -> StepStats:

@@ -83,6 +83,8 @@ typedef struct da_params {
     double next_output;          /* TimeProps::ndnextoutput (clips dt) */
     double next_save;            /* TimeProps::ndnextsave (clips dt) */
     double influx_dt;            /* dt[2] of get_coef_and_eigen.C:49-77; HUGE_VAL when no source is active */
+    double fp32_sign_floor;      /* DA_PREC_FP32_SPLIT only: the friction sign tests use
+                                  * max(frict_tiny, this); 0 keeps the reference's thresholds */
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
@@ -137,7 +139,7 @@ int da_forward_run(da_ctx *ctx, int32_t nsteps, da_step_stats *last);
 int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, double *device_ms);
 
 /* ---- tracing (the reference's Timer class, properties.h:43-71, moved onto the device) --- */
-#define DA_FWD_KERNELS 4  /* coef, dt, update, volume */
+#define DA_FWD_KERNELS 2  /* coefficients + dt, update + volume */
 /* Runs nsteps forward steps with CUDA events around every launch on the context's stream and
  * returns the mean device time of each forward kernel in ms (kernel_ms[DA_FWD_KERNELS]) and
  * the names in kernel order through da_forward_kernel_name().  The state advances. */

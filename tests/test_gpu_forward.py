@@ -9,8 +9,8 @@ from discrete_adjoint_b200.mesh import Mesh, MeshSpec
 pytestmark = pytest.mark.gpu
 
 # FP32-split tolerance against the FP64 oracle (relative L2 over the mesh)
-FP32_REL_L2_H = 1e-4
-FP32_REL_L2_MOM = 1e-3
+FP32_REL_L2_H = 1e-6
+FP32_REL_L2_MOM = 1e-5
 
 
 def oracle_run(w, nsteps, tp=None):
@@ -77,16 +77,19 @@ def test_fp64_time_clipping_and_schedule():
 
 
 @pytest.mark.parametrize("seed", [1, 3])
-def test_fp32_split_close_to_fp64_oracle(seed):
+def test_fp32_split_close_to_fp64_oracle_before_threshold_switch(seed):
+    # while frict_tiny = 0.1 (the first 50 steps, hpfem.C:232-235) every sign test is well
+    # above FP32 resolution and the split path tracks the FP64 reference to rounding level
     w = inputs.test_case(seed=seed)
-    h, hu, hv, dts, st = oracle_run(w, 100)
+    h, hu, hv, dts, st = oracle_run(w, 50)
     with gpu_ctx(w, precision=_ffi.DA_PREC_FP32_SPLIT) as ctx:
-        s = ctx.run(100)
+        s = ctx.run(50)
         gh, ghu, ghv = ctx.get_state()
     eh, eu, ev = rel_l2(gh, h), rel_l2(ghu, hu), rel_l2(ghv, hv)
-    print(f"fp32-split rel L2 after 100 steps: h {eh:.3e} hu {eu:.3e} hv {ev:.3e}; time {s.time} vs {st.time}")
+    print(f"fp32-split rel L2 after 50 steps: h {eh:.3e} hu {eu:.3e} hv {ev:.3e}")
     assert eh < FP32_REL_L2_H
     assert eu < FP32_REL_L2_MOM and ev < FP32_REL_L2_MOM
+    assert abs(s.time - st.time) < 1e-6 * st.time
 
 
 def test_errors_are_codes_not_exits():
@@ -95,7 +98,7 @@ def test_errors_are_codes_not_exits():
     with pytest.raises(_ffi.DAError) as e:
         ctx.step()
     assert e.value.code == _ffi.DA_ERR_NO_MESH
-    bad = Mesh(**w.mesh.arrays())
+    bad = Mesh(**{k: np.copy(v) for k, v in w.mesh.arrays().items()})
     bad.nbr[0, 5] = w.mesh.n + 3
     with pytest.raises(_ffi.DAError) as e:
         ctx.upload_mesh(bad)

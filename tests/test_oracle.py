@@ -105,3 +105,35 @@ def test_edge_fluxes_hanging_average():
             assert np.array_equal(F[side, :, i], exp)
             checked += 1
     assert checked > 50
+
+
+def test_fp32_state_storage_diverges_after_friction_threshold_switch():
+    # Property of the reference model behind the FP32-split error budget: FP64 arithmetic with
+    # the state rounded to FP32 after every step tracks FP64 to rounding level while
+    # frict_tiny = 0.1, and departs from it once frict_tiny drops to 1e-9 (step 50), whereas a
+    # one-off 1e-8 perturbation of the initial depth stays at the 1e-9 level.
+    w = inputs.test_case(seed=1)
+    m = w.mesh
+    p = make_params(w.mat, TimeProps())
+
+    def run(h, hu, hv, steps, round32):
+        o = oracle.Oracle(p, m)
+        out = {}
+        for k in range(1, max(steps) + 1):
+            o.run(h, hu, hv, 1)
+            if round32:
+                for a in (h, hu, hv):
+                    a[:] = np.float32(a)
+            if k in steps:
+                out[k] = h.copy()
+        return out
+
+    steps = (50, 120)
+    ref = run(m.h0.copy(), m.hu0.copy(), m.hv0.copy(), steps, False)
+    r32 = run(*[np.float64(np.float32(a)) for a in (m.h0, m.hu0, m.hv0)], steps, True)
+    rng = np.random.default_rng(0)
+    pert = run(m.h0 * (1 + 1e-8 * rng.standard_normal(m.n)), m.hu0.copy(), m.hv0.copy(), steps, False)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)  # noqa: E731
+    assert rel(r32[50], ref[50]) < 1e-6
+    assert rel(r32[120], ref[120]) > 1e-4
+    assert rel(pert[120], ref[120]) < 1e-7
