@@ -54,6 +54,8 @@ class da_params(C.Structure):
         ("next_save", C.c_double),
         ("influx_dt", C.c_double),
         ("fp32_sign_floor", C.c_double),
+        ("tile_culling", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
 

@@ -88,6 +88,10 @@ static void free_state(da_ctx *ctx) {
         for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
     dfree(ctx->kact);
     dfree(ctx->vol_part);
+    dfree(ctx->tile_vol);
+    dfree(ctx->active);
+    dfree(ctx->clean);
+    dfree(ctx->tile_wet);
     ctx->have_state = false;
 }
 
@@ -172,6 +176,8 @@ void da_params_default(da_params *p) {
     p->next_output = HUGE_VAL;
     p->next_save = HUGE_VAL;
     p->influx_dt = HUGE_VAL;
+    p->fp32_sign_floor = 0.0;
+    p->tile_culling = 1;
 }
 
 da_ctx *da_create(const da_params *p, int *err) {
@@ -242,7 +248,8 @@ const char *da_last_error(const da_ctx *ctx) { return ctx ? ctx->err.c_str() : "
 
 int da_set_params(da_ctx *ctx, const da_params *p) {
     if (!ctx) return DA_ERR_INVALID;
-    if (!params_ok(p) || p->precision != ctx->p.precision || p->device != ctx->p.device)
+    if (!params_ok(p) || p->precision != ctx->p.precision || p->device != ctx->p.device ||
+        (ctx->mesh.n > 0 && p->tile_culling != ctx->p.tile_culling))
         return set_error(ctx, DA_ERR_INVALID, "da_set_params: invalid parameters or precision/device change");
     ctx->p = *p;
     fill_consts(ctx->p, &ctx->mc, &ctx->tc);
@@ -353,6 +360,8 @@ int da_set_state(da_ctx *ctx, const double *h, const double *hu, const double *h
                             "copy state");
         }
     }
+    if (!st) st = forward_state_changed(ctx);
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (!st) ctx->have_state = true;
     return st;
 }

@@ -82,8 +82,13 @@ struct da_ctx {
     void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     void *kact = nullptr;            // [n] Real
-    double *vol_part = nullptr;      // [nblocks] per-block volume partials
-    int nblocks = 0;                 // grid of the grid-stride step kernels
+    double *vol_part = nullptr;      // [ntiles] per-tile volume partials of the last update
+    double *tile_vol = nullptr;      // [ntiles] cached volume partial of each tile
+    unsigned *active = nullptr;      // [ceil(n/32)] bit per cell: wet or next to a wet cell
+    uint8_t *clean = nullptr;        // [ntiles] 1 when both state buffers hold the same tile
+    uint8_t *tile_wet = nullptr;     // [ntiles] 1 when the tile held a wet cell after the last update
+    int ntiles = 0;                  // tiles of 256 consecutive cells
+    int nblocks = 0;                 // grid of the persistent step kernels
     int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror
@@ -106,6 +111,7 @@ int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev = nullptr);
 int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev);
 int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev);
 int forward_alloc(da_ctx *ctx);
+int forward_state_changed(da_ctx *ctx);
 void forward_free(da_ctx *ctx);
 
 }  // namespace da

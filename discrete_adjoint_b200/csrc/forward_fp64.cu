@@ -10,11 +10,11 @@ int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev) { return fwd::launch_
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
-    // grid-stride kernels: at most 8 blocks of 256 threads per SM (2048 resident threads)
-    const size_t want = (n + fwd::kBlock - 1) / fwd::kBlock;
-    const size_t cap = (size_t)(ctx->sm_count > 0 ? ctx->sm_count : 148) * 8;
-    ctx->nblocks = int(want < cap ? want : cap);
-    if (ctx->nblocks < 1) ctx->nblocks = 1;
+    ctx->ntiles = int((n + fwd::kBlock - 1) / fwd::kBlock);
+    // persistent kernels: 4 blocks of 256 threads per SM, never more blocks than tiles
+    const int cap = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
+    ctx->nblocks = ctx->ntiles < cap ? ctx->ntiles : cap;
+    const size_t words = (n + 31) / 32;
     int st = DA_OK;
     for (int b = 0; b < 2 && !st; ++b)
         for (int v = 0; v < 3 && !st; ++v) {
@@ -23,6 +23,22 @@ int forward_alloc(da_ctx *ctx) {
         }
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->vol_part, sizeof(double) * ctx->nblocks), "cudaMalloc(vol)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_wet, ctx->ntiles), "cudaMalloc(tile_wet)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_vol, sizeof(double) * ctx->ntiles), "cudaMalloc(vol)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->active, sizeof(unsigned) * words), "cudaMalloc(active)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * words, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->clean, ctx->ntiles), "cudaMalloc(clean)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->clean, 0, ctx->ntiles, ctx->stream), "memset");
+    return st;
+}
+
+int forward_state_changed(da_ctx *ctx) {
+    // the buffers no longer hold the same tiles, any tile may be wet, no cell is marked active
+    int st = cuda_check(ctx, cudaMemsetAsync(ctx->clean, 0, ctx->ntiles, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_wet, 1, ctx->ntiles, ctx->stream), "memset");
+    if (!st)
+        st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * ((ctx->mesh.n + 31) / 32), ctx->stream),
+                        "memset");
     return st;
 }
 

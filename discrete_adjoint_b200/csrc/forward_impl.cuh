@@ -68,39 +68,61 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 }
 
 // ----------------------------------------------------------------------------- k_coef
+// Persistent grid-stride loop over tiles of kBlock cells, one thread per cell.  With tile
+// culling, a tile that held no wet cell after the last update is skipped (its depths cannot have
+// changed since).  Wet cells (h >= GEOFLOW_TINY) mark themselves and their face neighbours in
+// the active bitmask that k_update reads: a cell outside that set has zero fluxes and no
+// sources this step.
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact, MatConsts mc,
-                                                 TimeConsts tc, DevScalars *sc) {
+__global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
+                                                 unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
+                                                 int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc) {
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
-        const R h = U.h[i];
-        if (!(h >= R(DA_TINY))) {
-            // dry (or NaN, caught by k_update): k act/pass is never read for h < GEOFLOW_TINY
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (cull && !tile_wet[t]) continue;
+        const int i = t * kBlock + threadIdx.x;
+        bool wet = false;
+        if (i < m.n) {
+            const R h = U.h[i];
             if (!(h == h)) raise_err(sc, DA_ERR_NAN);
-            continue;
+            wet = h >= R(DA_TINY);
+            if (wet) {
+                const uint8_t bf = m.bflag[i];
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    if (bf & (1 << s)) continue;
+                    const int e = m.nbr[(size_t)s * m.n + i];
+                    atomicOr(&active[e >> 5], 1u << (e & 31));
+                    if (bf & (0x10 << s)) {
+                        const int e2 = m.nbr[(size_t)(s + 4) * m.n + i];
+                        atomicOr(&active[e2 >> 5], 1u << (e2 & 31));
+                    }
+                }
+                if (!(h > R(DA_TINY))) {  // h == GEOFLOW_TINY: dry for get_coef_and_eigen, wet for the fluxes
+                    kact[i] = R(mc.kact_rest);
+                } else {
+                    const R ui[3] = {h, U.hu[i], U.hv[i]};
+                    R s[6];
+                    cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
+                    const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s);
+                    kact[i] = k;
+                    const R gz = grav<R>(m, 2, i);
+                    const R vx = ui[1] / h, vy = ui[2] / h;
+                    const R c = sqrt(k * gz * h);
+                    const R evx = dabs(vx) + c, evy = dabs(vy) + c;
+                    const R ev = evx > evy ? evx : evy;
+                    if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
+                    const R dxm = cell_dx<R>(m, i), dym = cell_dy<R>(m, i);
+                    const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
+                    const unsigned long long hb = __double_as_longlong(double(h));
+                    my_min = rb < my_min ? rb : my_min;
+                    my_max = hb > my_max ? hb : my_max;
+                }
+            }
         }
-        if (!(h > R(DA_TINY))) {  // h == GEOFLOW_TINY: dry for get_coef_and_eigen, wet for the fluxes
-            kact[i] = R(mc.kact_rest);
-            continue;
-        }
-        const uint8_t bf = m.bflag[i];
-        const R ui[3] = {h, U.hu[i], U.hv[i]};
-        R s[6];
-        cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
-        const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s);
-        kact[i] = k;
-        const R gz = grav<R>(m, 2, i);
-        const R vx = ui[1] / h, vy = ui[2] / h;
-        const R c = sqrt(k * gz * h);
-        const R evx = dabs(vx) + c, evy = dabs(vy) + c;
-        const R ev = evx > evy ? evx : evy;
-        if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
-        const R dxm = cell_dx<R>(m, i), dym = cell_dy<R>(m, i);
-        const double ratio = double((dxm > dym ? dym : dxm) / ev);
-        const unsigned long long rb = __double_as_longlong(ratio), hb = __double_as_longlong(double(h));
-        my_min = rb < my_min ? rb : my_min;
-        my_max = hb > my_max ? hb : my_max;
+        const unsigned self = __ballot_sync(0xffffffffu, wet);
+        if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
     }
     my_min = warp_min_u64(my_min);
     my_max = warp_max_u64(my_max);
@@ -116,126 +138,143 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
     }
 }
 
-// ---------------------------------------------------------------------------- k_update
+// Full corrector update of one active cell (fluxes + sources), reference order.
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
-                                                   const R *__restrict__ kact, MatConsts mc, DevScalars *sc,
-                                                   double *__restrict__ vol_part) {
-    __shared__ double red[kBlock / 32];
-    double vol = 0.0;
-    const R dt = R(sc->dt);
-    const R ft0 = R(sc->frict_tiny);
-    const R ft = ft0 > R(mc.sign_floor) ? ft0 : R(mc.sign_floor);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
-        const uint8_t bf = m.bflag[i];
-        const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
-        bool wet = prev[0] >= R(DA_TINY);
-        if (!wet) {
+__device__ __forceinline__ void update_cell(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact,
+                                            const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
+                                            R st[3]) {
+    const uint8_t bf = m.bflag[i];
+    const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
+    const R gz = grav<R>(m, 2, i);
+    R div[2][3];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                if (bf & (1 << s)) continue;
-                if (U.h[m.nbr[(size_t)s * m.n + i]] >= R(DA_TINY)) wet = true;
-                if ((bf & (0x10 << s)) && U.h[m.nbr[(size_t)(s + 4) * m.n + i]] >= R(DA_TINY)) wet = true;
-            }
-        }
-        const R dxc = cell_dx<R>(m, i), dyc = cell_dy<R>(m, i);
-        if (!wet) {
-            // every flux of this cell is zero and it has no sources: the update returns prev
-            O.h[i] = prev[0];
-            O.hu[i] = prev[1];
-            O.hv[i] = prev[2];
-            if (!(prev[0] == prev[0] && prev[1] == prev[1] && prev[2] == prev[2])) raise_err(sc, DA_ERR_NAN);
-            vol += double(dxc) * double(dyc) * double(prev[0]);
+    for (int d = 0; d < 2; ++d) {
+        if (bf & ((1 << d) | (1 << (d + 2)))) {
+            // an outflow side copies the opposite side's flux: the difference is exactly 0
+            div[d][0] = div[d][1] = div[d][2] = R(0);
             continue;
         }
-        const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
-        const R gz = grav<R>(m, 2, i);
-        R div[2][3];
+        Hfv<R> self;
+        dirflux<R>(d, prev[0], prev[1], prev[2], ki, gz, self);
+        R Fm[3], Fp[3];
+        side_flux<R>(m, U, kact, i, bf, d + 2, self, Fm);
+        side_flux<R>(m, U, kact, i, bf, d, self, Fp);
 #pragma unroll
-        for (int d = 0; d < 2; ++d) {
-            if (bf & ((1 << d) | (1 << (d + 2)))) {
-                // an outflow side copies the opposite side's flux: the difference is exactly 0
-                div[d][0] = div[d][1] = div[d][2] = R(0);
-                continue;
-            }
-            Hfv<R> self;
-            dirflux<R>(d, prev[0], prev[1], prev[2], ki, gz, self);
-            R Fm[3], Fp[3];
-            side_flux<R>(m, U, kact, i, bf, d + 2, self, Fm);
-            side_flux<R>(m, U, kact, i, bf, d, self, Fp);
-#pragma unroll
-            for (int v = 0; v < 3; ++v) div[d][v] = Fp[v] - Fm[v];
-        }
-        R dtdx, dtdy;
-        if constexpr (sizeof(R) == 8) {
-            dtdx = dt / dxc;
-            dtdy = dt / dyc;
-        } else {
-            dtdx = dt * (1.0f / dxc);
-            dtdy = dt * (1.0f / dyc);
-        }
-        R st[3];
-#pragma unroll
-        for (int v = 0; v < 3; ++v) st[v] = prev[v] - dtdx * div[0][v] - dtdy * div[1][v];
-        if (st[0] < R(0)) st[0] = R(0);
-        if (prev[0] > R(DA_TINY)) {
-            R s[6];
-            cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
-            R vel0, vel1, h_inv;
-            if constexpr (sizeof(R) == 8) {
-                vel0 = prev[1] / prev[0];
-                vel1 = prev[2] / prev[0];
-                h_inv = 1. / prev[0];
-            } else {
-                h_inv = 1.0f / prev[0];
-                vel0 = prev[1] * h_inv;
-                vel1 = prev[2] * h_inv;
-            }
-            R tmp = h_inv * (s[4] - vel0 * s[3]);
-            const R sg0 = tiny_sgn(tmp, ft);
-            const R sg2 = tiny_sgn(vel0, ft);
-            tmp = h_inv * (s[2] - vel1 * s[0]);
-            const R sg1 = tiny_sgn(tmp, ft);
-            const R sg3 = tiny_sgn(vel1, ft);
-            const R sin_int = R(mc.sin_int);
-            const R tan_bed = R(mc.tan_bed[m.mat[i]]);
-            R s1 = grav<R>(m, 0, i) * prev[0];
-            R s2 = sg0 * prev[0] * ki * (gz * s[3] + dgrav<R>(m, 1, i) * prev[0]) * sin_int;
-            R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * curvat<R>(m, 0, i), R(0.0)) * tan_bed;
-            st[1] += dt * (s1 - s2 - s3);
-            s1 = grav<R>(m, 1, i) * prev[0];
-            s2 = sg1 * prev[0] * ki * (gz * s[0] + dgrav<R>(m, 0, i) * prev[0]) * sin_int;
-            s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, i), R(0.0)) * tan_bed;
-            st[2] += dt * (s1 - s2 - s3);
-        }
-        if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
-        O.h[i] = st[0];
-        O.hu[i] = st[1];
-        O.hv[i] = st[2];
-        vol += double(dxc) * double(dyc) * double(st[0]);
+        for (int v = 0; v < 3; ++v) div[d][v] = Fp[v] - Fm[v];
     }
-    // fixed-order reduction of the volume: warp shuffle, block, then the last block over blocks
-    vol = warp_sum(vol);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vol;
+    R dtdx, dtdy;
+    if constexpr (sizeof(R) == 8) {
+        dtdx = dt / dxc;
+        dtdy = dt / dyc;
+    } else {
+        dtdx = dt * (1.0f / dxc);
+        dtdy = dt * (1.0f / dyc);
+    }
+#pragma unroll
+    for (int v = 0; v < 3; ++v) st[v] = prev[v] - dtdx * div[0][v] - dtdy * div[1][v];
+    if (st[0] < R(0)) st[0] = R(0);
+    if (prev[0] > R(DA_TINY)) {
+        R s[6];
+        cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
+        R vel0, vel1, h_inv;
+        if constexpr (sizeof(R) == 8) {
+            vel0 = prev[1] / prev[0];
+            vel1 = prev[2] / prev[0];
+            h_inv = 1. / prev[0];
+        } else {
+            h_inv = 1.0f / prev[0];
+            vel0 = prev[1] * h_inv;
+            vel1 = prev[2] * h_inv;
+        }
+        R tmp = h_inv * (s[4] - vel0 * s[3]);
+        const R sg0 = tiny_sgn(tmp, ft);
+        const R sg2 = tiny_sgn(vel0, ft);
+        tmp = h_inv * (s[2] - vel1 * s[0]);
+        const R sg1 = tiny_sgn(tmp, ft);
+        const R sg3 = tiny_sgn(vel1, ft);
+        const R sin_int = R(mc.sin_int);
+        const R tan_bed = R(mc.tan_bed[m.mat[i]]);
+        R s1 = grav<R>(m, 0, i) * prev[0];
+        R s2 = sg0 * prev[0] * ki * (gz * s[3] + dgrav<R>(m, 1, i) * prev[0]) * sin_int;
+        R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * curvat<R>(m, 0, i), R(0.0)) * tan_bed;
+        st[1] += dt * (s1 - s2 - s3);
+        s1 = grav<R>(m, 1, i) * prev[0];
+        s2 = sg1 * prev[0] * ki * (gz * s[0] + dgrav<R>(m, 0, i) * prev[0]) * sin_int;
+        s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, i), R(0.0)) * tan_bed;
+        st[2] += dt * (s1 - s2 - s3);
+    }
+}
+
+// Sum of a block's values in a fixed order (warp shuffle, then warps in order); thread 0 holds it.
+__device__ __forceinline__ double block_sum(double v, double *red) {
+    v = warp_sum(v);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
 #pragma unroll
         for (int w = 0; w < kBlock / 32; ++w) t += red[w];
-        vol_part[blockIdx.x] = t;
+    return t;
+}
+
+// ---------------------------------------------------------------------------- k_update
+// Persistent grid-stride loop over tiles of kBlock consecutive cells.  A tile with no active
+// cell is copied; when both ping-pong buffers already hold it (clean) it is not touched at all
+// and its cached volume partial is reused (tile culling; off when cull == 0).  In an active tile,
+// inactive cells are copied and active ones get the full update.  The active words are cleared
+// here, and each processed tile records whether it holds a wet cell for the next k_coef.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
+                                                   const R *__restrict__ kact, unsigned *__restrict__ active,
+                                                   uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
+                                                   double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
+                                                   DevScalars *sc, double *__restrict__ vol_part) {
+    __shared__ double red[kBlock / 32];
+    const int lane = threadIdx.x & 31;
+    const R dt = R(sc->dt);
+    const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
+    double vol_acc = 0.0;  // thread 0: this block's tiles, in tile order
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int i = t * kBlock + threadIdx.x;
+        const unsigned word = (i < m.n) ? active[i >> 5] : 0u;
+        const bool tile_active = __syncthreads_or(word != 0u);
+        if (!tile_active && cull && clean[t]) {
+            if (threadIdx.x == 0) vol_acc += tile_vol[t];
+            continue;
+        }
+        double vol = 0.0;
+        bool wet_after = false;
+        if (i < m.n) {
+            const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
+            const R dxc = cell_dx<R>(m, i), dyc = cell_dy<R>(m, i);
+            R st[3] = {prev[0], prev[1], prev[2]};
+            if (word & (1u << lane)) update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
+            if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
+            O.h[i] = st[0];
+            O.hu[i] = st[1];
+            O.hv[i] = st[2];
+            vol = double(dxc) * double(dyc) * double(st[0]);
+            wet_after = st[0] >= R(DA_TINY);
+        }
+        __syncwarp();
+        if (lane == 0 && word) active[i >> 5] = 0u;
+        const bool any_wet = __syncthreads_or(wet_after);
+        const double tv = block_sum(vol, red);
+        if (threadIdx.x == 0) {
+            tile_vol[t] = tv;
+            vol_acc += tv;
+            clean[t] = tile_active ? 0 : 1;
+            tile_wet[t] = any_wet ? 1 : 0;
+        }
     }
+    if (threadIdx.x == 0) vol_part[blockIdx.x] = vol_acc;
     if (last_block(&sc->blocks_done[1])) {
         double t = 0.0;
         for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += ((volatile double *)vol_part)[b];
-        t = warp_sum(t);
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-        __syncthreads();
+        t = block_sum(t, red);
         if (threadIdx.x == 0) {
-            double u = 0.0;
-#pragma unroll
-            for (int w = 0; w < kBlock / 32; ++w) u += red[w];
-            sc->volume = u;
+            sc->volume = t;
             sc->blocks_done[1] = 0;
         }
     }
@@ -248,10 +287,13 @@ int launch_step_t(da_ctx *ctx, cudaEvent_t *ev = nullptr) {
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> O{(R *)ctx->U[o][0], (R *)ctx->U[o][1], (R *)ctx->U[o][2]};
     R *kact = (R *)ctx->kact;
+    const int tiles = ctx->ntiles, grid = ctx->nblocks, cull = ctx->p.tile_culling;
     if (ev) cudaEventRecord(ev[0], ctx->stream);
-    k_coef<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->mc, ctx->tc, ctx->dsc);
+    k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull, ctx->mc, ctx->tc,
+                                                ctx->dsc);
     if (ev) cudaEventRecord(ev[1], ctx->stream);
-    k_update<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->mc, ctx->dsc, ctx->vol_part);
+    k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
+                                                  ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part);
     if (ev) cudaEventRecord(ev[2], ctx->stream);
     ctx->cur = o;
     return cuda_check(ctx, cudaGetLastError(), "forward step launch");

@@ -50,7 +50,8 @@ class TimeProps:
 
 
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
-                influx_dt: float = math.inf, fp32_sign_floor: float = 0.0) -> _ffi.da_params:
+                influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
+                tile_culling: bool = True) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -70,6 +71,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.next_save = tp.nextsave
     p.influx_dt = influx_dt
     p.fp32_sign_floor = fp32_sign_floor
+    p.tile_culling = int(tile_culling)
     return p
 
 
@@ -86,12 +88,13 @@ class GeoflowContext:
     """One device context: flattened mesh + state resident in HBM."""
 
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
-                 device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0):
+                 device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
+                 tile_culling: bool = True):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
-        self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor)
+        self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:

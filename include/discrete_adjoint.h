@@ -85,6 +85,10 @@ typedef struct da_params {
     double influx_dt;            /* dt[2] of get_coef_and_eigen.C:49-77; HUGE_VAL when no source is active */
     double fp32_sign_floor;      /* DA_PREC_FP32_SPLIT only: the friction sign tests use
                                   * max(frict_tiny, this); 0 keeps the reference's thresholds */
+    int32_t tile_culling;        /* 1: tiles of 256 cells with no wet cell in or next to them are
+                                  * not rewritten when both state buffers already hold them
+                                  * (results are bit-identical); 0: every cell is rewritten */
+    int32_t reserved0;
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */

@@ -22,8 +22,8 @@ def oracle_run(w, nsteps, tp=None):
     return h, hu, hv, dts, st
 
 
-def gpu_ctx(w, precision=_ffi.DA_PREC_FP64, tp=None):
-    ctx = GeoflowContext(w.mat, tp or TimeProps(), precision=precision)
+def gpu_ctx(w, precision=_ffi.DA_PREC_FP64, tp=None, tile_culling=True):
+    ctx = GeoflowContext(w.mat, tp or TimeProps(), precision=precision, tile_culling=tile_culling)
     ctx.upload_mesh(w.mesh)
     ctx.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
     return ctx
@@ -90,6 +90,33 @@ def test_fp32_split_close_to_fp64_oracle_before_threshold_switch(seed):
     assert eh < FP32_REL_L2_H
     assert eu < FP32_REL_L2_MOM and ev < FP32_REL_L2_MOM
     assert abs(s.time - st.time) < 1e-6 * st.time
+
+
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+def test_tile_culling_is_bit_identical(precision):
+    # a large mostly-dry mesh so that many tiles are culled, long enough for the flow to spread
+    w = inputs.workload1()
+    out = []
+    for cull in (False, True):
+        with gpu_ctx(w, precision=precision, tile_culling=cull) as ctx:
+            s = ctx.run(150)
+            out.append((ctx.get_state(), s))
+    (a, sa), (b, sb) = out
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    assert sa.time == sb.time and sa.volume == sb.volume
+
+
+def test_set_state_resets_culling():
+    w = inputs.test_case(seed=2)
+    h, hu, hv, dts, st = oracle_run(w, 30)
+    with gpu_ctx(w) as ctx:
+        ctx.run(7)
+        ctx.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
+        ctx.set_time(0.0, 0)
+        ctx.run(30)
+        gh, ghu, ghv = ctx.get_state()
+    assert np.array_equal(gh, h) and np.array_equal(ghu, hu) and np.array_equal(ghv, hv)
 
 
 def test_errors_are_codes_not_exits():
