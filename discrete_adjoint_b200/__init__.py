@@ -6,7 +6,8 @@ it raises (there is no CPU fallback).
 """
 from . import _ffi
 from .mesh import DEM, Mesh, MeshSpec, Pile
-from .solver import GeoflowContext, MatProps, StepStats, TimeProps, make_params, step
+from .solver import (GeoflowContext, Gradient, MatProps, StepStats, TimeProps, adjoint_run, adjoint_step,
+                     make_params, set_dt_replay, step)
 
-__all__ = ["_ffi", "DEM", "Mesh", "MeshSpec", "Pile", "GeoflowContext", "MatProps", "StepStats", "TimeProps",
-           "make_params", "step"]
+__all__ = ["_ffi", "DEM", "Mesh", "MeshSpec", "Pile", "GeoflowContext", "Gradient", "MatProps", "StepStats",
+           "TimeProps", "adjoint_run", "adjoint_step", "make_params", "set_dt_replay", "step"]

@@ -26,6 +26,9 @@ UNITS = [
     ("capi.cu", []),
     ("forward_fp64.cu", ["--fmad=false"]),
     ("forward_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
+    ("adjoint_fp64.cu", []),
+    ("adjoint_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
+    ("adjoint_host.cu", []),
     ("mesh_host.cpp", []),
 ]
 

@@ -132,6 +132,24 @@ class da_mesh_host(C.Structure):
     ]
 
 
+class da_functional(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("pad", C.c_int32), ("box", C.c_double * 4)]
+
+
+class da_gradient(C.Structure):
+    _fields_ = [
+        ("J", C.c_double),
+        ("dJ_dbedfrict", C.c_double * DA_MAX_MATERIALS),
+        ("dJ_dintfrict", C.c_double),
+        ("dJ_dpile", C.c_double * DA_MAX_PILES),
+        ("forward_steps", C.c_int64),
+        ("snapshots", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
+DA_FUNC_H2_BOX = 1
+
 # name -> (restype, argtypes) for every symbol the headers declare
 SIGNATURES = {
     "da_abi_version": (C.c_int, []),
@@ -148,6 +166,10 @@ SIGNATURES = {
     "da_forward_step": (C.c_int, [C.c_void_p, C.POINTER(da_step_stats)]),
     "da_forward_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_step_stats)]),
     "da_forward_run_timed": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_step_stats), PD]),
+    "da_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(da_functional), C.c_int32, C.c_int32, PD, C.c_int32,
+                                 C.POINTER(da_gradient), PD]),
+    "da_adjoint_step": (C.c_int, [C.c_void_p, PD, PD, C.POINTER(da_gradient)]),
+    "da_set_dt_replay": (C.c_int, [C.c_void_p, PD, C.c_int32, C.c_int64]),
     "da_forward_profile": (C.c_int, [C.c_void_p, C.c_int32, PD]),
     "da_forward_kernel_name": (C.c_char_p, [C.c_int32]),
     "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,

@@ -1,0 +1,395 @@
+// Host side of the adjoint: workspace, the k act/pass parameter-derivative tables, the optimal
+// binomial checkpoint schedule, and the C ABI entry points da_adjoint_run / da_adjoint_step /
+// da_set_dt_replay.
+//
+// The reference's dual_solver (src/adjoint/dual_solver.C:80-273) walks the recorded steps
+// backward from gz files written every 50 steps (SolRec, src/datstr/dualmesh.C:82-147).  Here
+// the forward states live in HBM only at checkpoints; the reverse sweep recomputes the steps in
+// between.  The placement minimises recomputation for the given number of slots: T(l, c), the
+// forward steps needed to reverse l steps with c free slots, obeys
+//     T(1, c) = 0,  T(l, 0) = l(l-1)/2,  T(l, c) = min_m [ m + T(l-m, c-1) + T(m, c) ],
+// the recursion of binomial checkpointing (Griewank's revolve), solved by dynamic programming.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "da_internal.h"
+
+namespace da {
+
+int launch_adjoint_step_fp64(da_ctx *, int, int, const double *, double);
+int launch_adjoint_step_fp32(da_ctx *, int, int, const double *, double);
+int launch_adjoint_seed_fp64(da_ctx *, int, const double *);
+int launch_adjoint_seed_fp32(da_ctx *, int, const double *);
+int launch_adjoint_reduce_fp64(da_ctx *, int, int);
+int launch_adjoint_reduce_fp32(da_ctx *, int, int);
+int forward_state_changed(da_ctx *ctx);
+
+int launch_adjoint_step(da_ctx *ctx, int a, int b, const double *sec2, double c) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_step_fp64(ctx, a, b, sec2, c)
+                                            : launch_adjoint_step_fp32(ctx, a, b, sec2, c);
+}
+int launch_adjoint_seed(da_ctx *ctx, int b, const double box[4]) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_seed_fp64(ctx, b, box) : launch_adjoint_seed_fp32(ctx, b, box);
+}
+int launch_adjoint_reduce(da_ctx *ctx, int a, int np) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_reduce_fp64(ctx, a, np)
+                                            : launch_adjoint_reduce_fp32(ctx, a, np);
+}
+
+namespace {
+
+size_t rsize(const da_ctx *ctx) { return ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+// d kact / d phi_bed and d phi_int of gmfggetcoef's three signed branches (getcoef.f:19-66):
+// k = (2/c^2)(1 - s sqrt|1 - (1 + t^2) c^2|) - 1 with c = cos phi_int, t = tan phi_bed, times
+// epsilon; a branch clamped at zero has zero derivative.
+void kact_derivatives(const da_params &p, double *dkb, double *dki) {
+    for (int m = 0; m < DA_MAX_MATERIALS; ++m)
+        for (int k = 0; k < 3; ++k) dkb[m * 3 + k] = dki[m * 3 + k] = 0.0;
+    const double c = std::cos(p.intfrict), sn = std::sin(p.intfrict);
+    for (int m = 0; m < p.n_materials; ++m) {
+        const double t = std::tan(p.bedfrict[m]);
+        const double A = 1.0 - (1.0 + t * t) * (c * c);
+        const double Q = std::sqrt(std::fabs(A));
+        const double sA = A > 0 ? 1.0 : (A < 0 ? -1.0 : 0.0);
+        const double dA_db = -(c * c) * 2.0 * t * (1.0 + t * t);
+        const double dA_di = 2.0 * (1.0 + t * t) * c * sn;
+        const double dQ_db = Q > 0 ? sA * dA_db / (2.0 * Q) : 0.0;
+        const double dQ_di = Q > 0 ? sA * dA_di / (2.0 * Q) : 0.0;
+        for (int s = -1; s <= 1; ++s) {
+            const double k0 = (2.0 / (c * c)) * (1.0 - s * Q) - 1.0;
+            if (k0 < 0.0) continue;
+            dkb[m * 3 + s + 1] = p.epsilon * (2.0 / (c * c)) * (-s) * dQ_db;
+            dki[m * 3 + s + 1] = p.epsilon * ((4.0 * sn / (c * c * c)) * (1.0 - s * Q) + (2.0 / (c * c)) * (-s) * dQ_di);
+        }
+    }
+}
+
+int adj_alloc(da_ctx *ctx, int nsnap) {
+    const size_t n = (size_t)ctx->mesh.n;
+    const size_t rs = rsize(ctx);
+    int st = DA_OK;
+    if (ctx->adj_n != (int)n) {
+        auto fr = [](void *p) { if (p) cudaFree(p); };
+        fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
+        fr(ctx->red_out); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter);
+        for (int b = 0; b < 2; ++b)
+            for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
+        for (void *s : ctx->snaps) fr(s);
+        ctx->snaps.clear();
+        ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
+        ctx->red_out = ctx->seed_part = ctx->seed_J = nullptr; ctx->seed_counter = nullptr;
+        st = cuda_check(ctx, cudaMalloc((void **)&ctx->mask, n), "cudaMalloc(mask)");
+        for (int b = 0; b < 2 && !st; ++b)
+            for (int v = 0; v < 3 && !st; ++v) st = cuda_check(ctx, cudaMalloc(&ctx->lam[b][v], rs * n), "cudaMalloc(lam)");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->adjA, sizeof(double) * 3 * n), "cudaMalloc(A)");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->adjB, sizeof(double) * 4 * n), "cudaMalloc(B)");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->gbed, sizeof(double) * n), "cudaMalloc(gbed)");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->gint, sizeof(double) * n), "cudaMalloc(gint)");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->dk_tab, sizeof(double) * 2 * DA_MAX_MATERIALS * 3), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_out, sizeof(double) * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_part, sizeof(double) * ctx->nblocks), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_J, sizeof(double)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_counter, sizeof(unsigned)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seed_counter, 0, sizeof(unsigned), ctx->stream), "memset");
+        if (st) return st;
+        ctx->adj_n = (int)n;
+    }
+    while ((int)ctx->snaps.size() < nsnap && !st) {
+        void *p = nullptr;
+        st = cuda_check(ctx, cudaMalloc(&p, rs * 3 * n + sizeof(DevScalars)), "cudaMalloc(snapshot)");
+        if (!st) ctx->snaps.push_back(p);
+    }
+    return st;
+}
+
+// snapshot layout: [3][n] state of R, then a DevScalars (time, iter, ...)
+int store(da_ctx *ctx, int slot) {
+    const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
+    char *base = (char *)ctx->snaps[slot];
+    int st = DA_OK;
+    for (int v = 0; v < 3 && !st; ++v)
+        st = cuda_check(ctx, cudaMemcpyAsync(base + v * rs * n, ctx->U[ctx->cur][v], rs * n, cudaMemcpyDeviceToDevice,
+                                             ctx->stream), "snapshot store");
+    if (!st)
+        st = cuda_check(ctx, cudaMemcpyAsync(base + 3 * rs * n, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
+                                             ctx->stream), "snapshot store");
+    return st;
+}
+
+int restore(da_ctx *ctx, int slot) {
+    const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
+    char *base = (char *)ctx->snaps[slot];
+    int st = DA_OK;
+    for (int v = 0; v < 3 && !st; ++v)
+        st = cuda_check(ctx, cudaMemcpyAsync(ctx->U[ctx->cur][v], base + v * rs * n, rs * n, cudaMemcpyDeviceToDevice,
+                                             ctx->stream), "snapshot restore");
+    if (!st)
+        st = cuda_check(ctx, cudaMemcpyAsync(ctx->dsc, base + 3 * rs * n, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
+                                             ctx->stream), "snapshot restore");
+    if (!st) st = forward_state_changed(ctx);
+    return st;
+}
+
+struct Schedule {
+    int N = 0, C = 0;
+    std::vector<long long> cost;  // [(N+1) x (C+1)]
+    std::vector<int> split;
+    long long &T(int l, int c) { return cost[(size_t)l * (C + 1) + c]; }
+    int &S(int l, int c) { return split[(size_t)l * (C + 1) + c]; }
+    void build(int n, int c) {
+        N = n;
+        C = c;
+        cost.assign((size_t)(N + 1) * (C + 1), 0);
+        split.assign((size_t)(N + 1) * (C + 1), 0);
+        for (int l = 1; l <= N; ++l) {
+            T(l, 0) = (long long)l * (l - 1) / 2;
+            for (int cc = 1; cc <= C; ++cc) {
+                if (l == 1) {
+                    T(l, cc) = 0;
+                    continue;
+                }
+                long long best = -1;
+                int arg = 1;
+                for (int m = 1; m < l; ++m) {
+                    const long long v = m + T(l - m, cc - 1) + T(m, cc);
+                    if (best < 0 || v < best) {
+                        best = v;
+                        arg = m;
+                    }
+                }
+                T(l, cc) = best;
+                S(l, cc) = arg;
+            }
+        }
+    }
+};
+
+struct Runner {
+    da_ctx *ctx;
+    Schedule sch;
+    std::vector<int> free_slots;
+    int lam_cur = 0;  // buffer holding lambda^{n+1}
+    bool seeded = false;
+    double box[4];
+    double sec2[DA_MAX_MATERIALS];
+    double cos_int;
+    long long fsteps = 0;
+
+    int advance(int k) {
+        int st = DA_OK;
+        for (int s = 0; s < k && !st; ++s) st = launch_forward_step(ctx);
+        fsteps += k;
+        return st;
+    }
+    int youturn() {
+        int st = launch_forward_step(ctx, nullptr, ctx->mask);  // replay step n with its branch codes
+        ++fsteps;
+        if (!st && !seeded) {
+            st = launch_adjoint_seed(ctx, lam_cur, box);  // U^N is the state just produced
+            seeded = true;
+        }
+        if (!st) st = launch_adjoint_step(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
+        lam_cur = 1 - lam_cur;
+        return st;
+    }
+    int reverse(int a, int b, int slot_a) {
+        int st = DA_OK;
+        const int l = b - a;
+        if (l == 1) {
+            st = restore(ctx, slot_a);
+            if (!st) st = youturn();
+            return st;
+        }
+        const int c = (int)free_slots.size() < sch.C ? (int)free_slots.size() : sch.C;
+        if (c == 0) {
+            for (int k = b - 1; k >= a && !st; --k) {
+                st = restore(ctx, slot_a);
+                if (!st) st = advance(k - a);
+                if (!st) st = youturn();
+            }
+            return st;
+        }
+        const int m = a + sch.S(l, c);
+        st = restore(ctx, slot_a);
+        if (!st) st = advance(m - a);
+        const int slot_m = free_slots.back();
+        free_slots.pop_back();
+        if (!st) st = store(ctx, slot_m);
+        if (!st) st = reverse(m, b, slot_m);
+        free_slots.push_back(slot_m);
+        if (!st) st = reverse(a, m, slot_a);
+        return st;
+    }
+};
+
+int sync_check(da_ctx *ctx) {
+    int st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
+                        "read scalars");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "device error during the adjoint sweep");
+    return st;
+}
+
+int upload_tables(da_ctx *ctx, double *sec2, double *cos_int) {
+    std::vector<double> tab(2 * DA_MAX_MATERIALS * 3);
+    kact_derivatives(ctx->p, tab.data(), tab.data() + DA_MAX_MATERIALS * 3);
+    for (int m = 0; m < DA_MAX_MATERIALS; ++m) {
+        const double t = m < ctx->p.n_materials ? std::tan(ctx->p.bedfrict[m]) : 0.0;
+        sec2[m] = 1.0 + t * t;
+    }
+    *cos_int = std::cos(ctx->p.intfrict);
+    int st = cuda_check(ctx, cudaMemcpy(ctx->dk_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice),
+                        "upload tables");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->gbed, 0, sizeof(double) * ctx->mesh.n, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->gint, 0, sizeof(double) * ctx->mesh.n, ctx->stream), "memset");
+    return st;
+}
+
+int copy_lambda_out(da_ctx *ctx, int buf, double *host) {
+    const size_t n = (size_t)ctx->mesh.n;
+    int st = DA_OK;
+    if (ctx->p.precision == DA_PREC_FP64) {
+        for (int v = 0; v < 3 && !st; ++v)
+            st = cuda_check(ctx, cudaMemcpyAsync(host + v * n, ctx->lam[buf][v], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                                 ctx->stream), "copy lambda");
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    } else {
+        std::vector<float> tmp(n);
+        for (int v = 0; v < 3 && !st; ++v) {
+            st = cuda_check(ctx, cudaMemcpy(tmp.data(), ctx->lam[buf][v], sizeof(float) * n, cudaMemcpyDeviceToHost),
+                            "copy lambda");
+            for (size_t i = 0; i < n && !st; ++i) host[v * n + i] = tmp[i];
+        }
+    }
+    return st;
+}
+
+int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out) {
+    int st = launch_adjoint_reduce(ctx, lam0, n_piles);
+    std::vector<double> red(DA_MAX_MATERIALS + 1 + DA_MAX_PILES, 0.0);
+    const int nout = ctx->p.n_materials + 1 + n_piles;
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(red.data(), ctx->red_out, sizeof(double) * nout, cudaMemcpyDeviceToHost,
+                                                  ctx->stream), "read gradient");
+    double J = 0.0;
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(&J, ctx->seed_J, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+                             "read J");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (st || !out) return st;
+    std::memset(out, 0, sizeof(*out));
+    out->J = J;
+    for (int m = 0; m < ctx->p.n_materials; ++m) out->dJ_dbedfrict[m] = red[m];
+    out->dJ_dintfrict = red[ctx->p.n_materials];
+    for (int q = 0; q < n_piles; ++q) out->dJ_dpile[q] = red[ctx->p.n_materials + 1 + q];
+    return st;
+}
+
+}  // namespace
+}  // namespace da
+
+using namespace da;
+
+extern "C" {
+
+int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0) {
+    if (!ctx || (dts && n <= 0)) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (ctx->dt_replay) cudaFree(ctx->dt_replay);
+    ctx->dt_replay = nullptr;
+    ctx->tc.dt_replay = nullptr;
+    ctx->tc.n_replay = 0;
+    if (!dts || st) return st;
+    st = cuda_check(ctx, cudaMalloc((void **)&ctx->dt_replay, sizeof(double) * n), "cudaMalloc(dt replay)");
+    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->dt_replay, dts, sizeof(double) * n, cudaMemcpyHostToDevice), "copy dts");
+    if (st) return st;
+    ctx->tc.dt_replay = ctx->dt_replay;
+    ctx->tc.iter0 = iter0;
+    ctx->tc.n_replay = n;
+    for (int b = 0; b < 2; ++b) {
+        if (ctx->step_graph[b]) cudaGraphExecDestroy(ctx->step_graph[b]);
+        ctx->step_graph[b] = nullptr;
+    }
+    return DA_OK;
+}
+
+int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, da_gradient *partial) {
+    if (!ctx || !lambda_next || !lambda_out) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_adjoint_step: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_step: no state");
+    cudaSetDevice(ctx->device);
+    int st = adj_alloc(ctx, 1);
+    double sec2[DA_MAX_MATERIALS], cos_int;
+    if (!st) st = upload_tables(ctx, sec2, &cos_int);
+    const size_t n = (size_t)ctx->mesh.n;
+    // lambda_next into buffer 0
+    if (!st) {
+        if (ctx->p.precision == DA_PREC_FP64) {
+            for (int v = 0; v < 3 && !st; ++v)
+                st = cuda_check(ctx, cudaMemcpy(ctx->lam[0][v], lambda_next + v * n, sizeof(double) * n,
+                                                cudaMemcpyHostToDevice), "copy lambda");
+        } else {
+            std::vector<float> tmp(n);
+            for (int v = 0; v < 3 && !st; ++v) {
+                for (size_t i = 0; i < n; ++i) tmp[i] = float(lambda_next[v * n + i]);
+                st = cuda_check(ctx, cudaMemcpy(ctx->lam[0][v], tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice),
+                                "copy lambda");
+            }
+        }
+    }
+    if (!st) st = store(ctx, 0);
+    if (!st) st = launch_forward_step(ctx, nullptr, ctx->mask);
+    if (!st) st = launch_adjoint_step(ctx, 0, 1, sec2, cos_int);
+    if (!st) st = restore(ctx, 0);
+    if (!st) st = sync_check(ctx);
+    if (!st) st = copy_lambda_out(ctx, 1, lambda_out);
+    if (!st && partial) {
+        // parameter parts only (the pile term needs lambda^0 of a whole run)
+        st = fill_gradient(ctx, 1, 0, partial);
+        if (!st) partial->J = 0.0;
+    }
+    return st;
+}
+
+int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
+                   int32_t n_piles, da_gradient *out, double *lambda0) {
+    if (!ctx || !f || nsteps <= 0 || nsnapshots < 0 || n_piles < 0 || n_piles > DA_MAX_PILES ||
+        (n_piles > 0 && !dh0_dpile) || f->kind != DA_FUNC_H2_BOX)
+        return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_adjoint_run: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_run: no state");
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->mesh.n;
+    int st = adj_alloc(ctx, nsnapshots + 1);
+    Runner r;
+    r.ctx = ctx;
+    for (int q = 0; q < 4; ++q) r.box[q] = f->box[q];
+    if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
+    if (!st && n_piles > 0) {
+        if (ctx->dh0) cudaFree(ctx->dh0);
+        ctx->dh0 = nullptr;
+        st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * n * n_piles), "cudaMalloc(dh0)");
+        if (!st)
+            st = cuda_check(ctx, cudaMemcpy(ctx->dh0, dh0_dpile, sizeof(double) * n * n_piles, cudaMemcpyHostToDevice),
+                            "copy dh0");
+    }
+    if (st) return st;
+    r.sch.build(nsteps, nsnapshots);
+    for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
+    st = store(ctx, 0);
+    if (!st) st = r.reverse(0, nsteps, 0);
+    if (!st) st = restore(ctx, 0);
+    if (!st) st = sync_check(ctx);
+    if (!st && lambda0) st = copy_lambda_out(ctx, r.lam_cur, lambda0);
+    if (!st) st = fill_gradient(ctx, r.lam_cur, n_piles, out);
+    if (!st && out) {
+        out->forward_steps = r.fsteps;
+        out->snapshots = nsnapshots;
+    }
+    return st;
+}
+
+}  // extern "C"

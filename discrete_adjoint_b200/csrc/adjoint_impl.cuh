@@ -1,0 +1,488 @@
+// Discrete adjoint of one forward step (order_flag = 1), matrix free, for sm_100a.
+//
+// The reference assembles 9 blocks of 3x3 d R^n / d U^{n-1} per element (calc_jacobian,
+// src/adjoint/calc_jacobain.C:40-153; calc_jacobian_elem, compute_jacobian_elem.C:15-121; flux
+// Jacobians dual_riemannflux, src/datstr/dualmesh.C:1628-1843) and multiplies their transposes
+// into the adjoint (calc_adjoint_elem, src/adjoint/calc_adjoint.C:74-167).  Here the transpose
+// of the step is applied without forming blocks:
+//   k_adj_src    (one pass over cells i): with lambda_eff_i = lambda^{n+1}_i (depth row dropped
+//                where the forward step clamped h at zero), the source terms of update_states
+//                (residual.C:162-275) give d(lambda_eff_i . dt S_i)/dU_i (A_i) and the
+//                coefficients B_i that the limited depth slopes of cell i pass to its neighbours
+//                (the limiter branch is replayed from U^n, as DualElem::get_slopes_prev +
+//                hslope_sens do, dualmesh.C:1393-1626);
+//   k_adj_gather (one pass over cells j): lambda^n_j = lambda_eff_j + A_j + sum over the
+//                Riemann fluxes on j's sides of (dF/dU_j)^T mu, with mu the flux weight of the
+//                edge in both cells that use it (hanging sides weigh 1/2, outflow directions 0),
+//                plus the slope coefficients B of the neighbours for j.
+// k act/pass and the depth clamp come from the branch codes recorded while the forward step was
+// replayed; the time step is the forward's (frozen).  Parameter sensitivities (basal friction per
+// material, internal friction, through tan/sin in the sources and through k act/pass in fluxes
+// and sources) are accumulated per cell in FP64 and reduced at the end.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fv_device.cuh"
+
+namespace da {
+namespace adj {
+namespace {
+
+using namespace fv;
+
+constexpr int kBlock = 256;
+
+// k act/pass of a recorded code (0 rest, 1..3 sgn(vel) = -1, 0, +1)
+template <class R>
+__device__ __forceinline__ R kact_of(const MatConsts &mc, int mat, uint8_t code) {
+    return code == 0 ? R(mc.kact_rest) : R(mc.kact_sgn[mat][code - 1]);
+}
+
+template <class R>
+__device__ __forceinline__ void lam_eff(const StateRef<R> &L, const uint8_t *__restrict__ mask, int i, R out[3]) {
+    out[0] = (mask[i] & 4) ? R(0) : L.h[i];
+    out[1] = L.hu[i];
+    out[2] = L.hv[i];
+}
+
+// Derivative data of the limited depth slope in one direction (Element::get_slopes for j = 0):
+// slope = fac * min(gamma|dp|, gamma|dm|, |dc|); g_dp, g_dm = d slope / d dp, d dm.
+template <class R>
+struct SlopeD {
+    R g_dp, g_dm, dxp, dxm;
+};
+
+template <class R>
+__device__ __forceinline__ void h_slope_deriv(const MeshArgs &m, const R *__restrict__ H, int i, uint8_t bf, R gamma,
+                                              R hi, SlopeD<R> out[2]) {
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+        const int ep = m.nbr[(size_t)dir * m.n + i];
+        const int em = m.nbr[(size_t)(dir + 2) * m.n + i];
+        const bool two_p = bf & (0x10 << dir), two_m = bf & (0x10 << (dir + 2));
+        R dxp, dxm, dp, dm;
+        if constexpr (sizeof(R) == 8) {
+            const double *co = dir == 0 ? m.x : m.y;
+            dxp = co[ep] - co[i];
+            dxm = co[i] - co[em];
+            dp = (H[ep] - hi) / dxp;
+            if (two_p) dp = .5 * (dp + (H[m.nbr[(size_t)(dir + 4) * m.n + i]] - hi) / dxp);
+            dm = (hi - H[em]) / dxm;
+            if (two_m) dm = .5 * (dm + (hi - H[m.nbr[(size_t)(dir + 6) * m.n + i]]) / dxm);
+        } else {
+            const float *sz = dir == 0 ? m.fdx : m.fdy;
+            const float si = sz[i];
+            dxp = 0.5f * (sz[ep] + si);
+            dxm = 0.5f * (sz[em] + si);
+            const float ip = 1.0f / dxp, im = 1.0f / dxm;
+            dp = (H[ep] - hi) * ip;
+            if (two_p) dp = 0.5f * (dp + (H[m.nbr[(size_t)(dir + 4) * m.n + i]] - hi) * ip);
+            dm = (hi - H[em]) * im;
+            if (two_m) dm = 0.5f * (dm + (hi - H[m.nbr[(size_t)(dir + 6) * m.n + i]]) * im);
+        }
+        const R dc = (dp * dxm + dm * dxp) / (dxm + dxp);
+        const R fac = R(.5) * (c_sgn(dp) + c_sgn(dm));
+        const R a = gamma * dabs(dp), b = gamma * dabs(dm), c = dabs(dc);
+        // selection order of c_dmin1(a, b, c) (geoflow.h:112-120)
+        int sel = 0;
+        R mn = a;
+        if (mn > b) { mn = b; sel = 1; }
+        if (mn > c) { mn = c; sel = 2; }
+        const auto sgnf = [](R v) { return v > R(0) ? R(1) : (v < R(0) ? R(-1) : R(0)); };
+        R gdp = 0, gdm = 0;
+        if (sel == 0) gdp = fac * gamma * sgnf(dp);
+        else if (sel == 1) gdm = fac * gamma * sgnf(dm);
+        else {
+            const R gc = fac * sgnf(dc) / (dxm + dxp);
+            gdp = gc * dxm;
+            gdm = gc * dxp;
+        }
+        out[dir] = SlopeD<R>{gdp, gdm, dxp, dxm};
+    }
+}
+
+// Forward pieces of one side's Riemann flux with what the reverse sweep needs.
+template <class R>
+struct Side {
+    R h, hu, hv, k, gz;
+    Hfv<R> f;
+    R vel, a;
+};
+
+template <class R>
+__device__ __forceinline__ void make_side(int dir, R h, R hu, R hv, R k, R gz, Side<R> &s) {
+    s.h = h; s.hu = hu; s.hv = hv; s.k = k; s.gz = gz;
+    dirflux<R>(dir, h, hu, hv, k, gz, s.f);
+    if (h < R(DA_TINY)) {
+        s.vel = s.a = R(0);
+    } else {
+        s.a = sqrt(k * h * gz);
+        s.vel = (dir == 0 ? hu : hv) / h;
+    }
+}
+
+// Reverse of dirflux for a wet side: adjoints of (u, f, s) -> adjoints of (h, hu, hv, k).
+template <class R>
+__device__ __forceinline__ void dirflux_adj(int dir, const Side<R> &s, const R au[3], const R af[3], const R as[3],
+                                            R g[3], R &gk) {
+    if (s.h < R(DA_TINY)) {
+        g[0] = g[1] = g[2] = R(0);
+        gk = R(0);
+        return;
+    }
+    const R vel = s.vel, a = s.a, h = s.h;
+    const R da_dh = a > R(0) ? R(0.5) * a / h : R(0);
+    const R da_dk = (a > R(0) && s.k > R(0)) ? R(0.5) * a / s.k : R(0);
+    const R avel_s = as[0] + as[1] + as[2];
+    const R aa = -as[0] + as[2];
+    if (dir == 0) {
+        const R avel = af[1] * s.hu + af[2] * s.hv + avel_s;
+        const R aaa = aa + af[1] * a * h;
+        g[0] = au[0] + af[1] * R(0.5) * a * a - avel * vel / h + aaa * da_dh;
+        g[1] = au[1] + af[0] + af[1] * vel + avel / h;
+        g[2] = au[2] + af[2] * vel;
+        gk = aaa * da_dk;
+    } else {
+        const R avel = af[1] * s.hu + af[2] * s.hv + avel_s;
+        const R aaa = aa + af[2] * a * h;
+        g[0] = au[0] + af[2] * R(0.5) * a * a - avel * vel / h + aaa * da_dh;
+        g[1] = au[1] + af[1] * vel;
+        g[2] = au[2] + af[0] + af[2] * vel + avel / h;
+        gk = aaa * da_dk;
+    }
+}
+
+// mu^T dF/d(left, right) for F = riemannflux(left, right) (element2.C:2228-2264), with the
+// branch decisions of the forward evaluation.
+template <class R>
+__device__ __forceinline__ void riemann_adj(int dir, const Side<R> &L, const Side<R> &Rt, const R mu[3], R gL[3],
+                                            R gR[3], R &gkL, R &gkR) {
+    gL[0] = gL[1] = gL[2] = gR[0] = gR[1] = gR[2] = R(0);
+    gkL = gkR = R(0);
+    const Hfv<R> &l = L.f, &r = Rt.f;
+    if (l.u[0] == R(0) && r.u[0] == R(0)) return;
+    R sl, sr;
+    // speed sources: 0 = the zero bound, 1 = wet-wet pick, 2 = dry-side formula
+    int which_l = 0, which_r = 0;
+    bool l_from_left = false, r_from_left = false;
+    if (l.u[0] == R(0)) {
+        const R cl = R(2.0) * r.s[0] - r.s[1], cr = R(2.0) * r.s[2] - r.s[1];
+        sl = rmin(R(0), cl);
+        sr = rmax(R(0), cr);
+        which_l = (R(0) > cl) ? 2 : 0;
+        which_r = (R(0) > cr) ? 0 : 2;
+        l_from_left = r_from_left = false;
+    } else if (r.u[0] == R(0)) {
+        const R cl = R(2.0) * l.s[0] - l.s[1], cr = R(2.0) * l.s[2] - l.s[1];
+        sl = rmin(R(0), cl);
+        sr = rmax(R(0), cr);
+        which_l = (R(0) > cl) ? 2 : 0;
+        which_r = (R(0) > cr) ? 0 : 2;
+        l_from_left = r_from_left = true;
+    } else {
+        const R ml = rmin(l.s[0], r.s[0]);
+        l_from_left = !(l.s[0] > r.s[0]);
+        const R mr = rmax(l.s[2], r.s[2]);
+        r_from_left = l.s[2] > r.s[2];
+        sl = rmin(R(0), ml);
+        sr = rmax(R(0), mr);
+        which_l = (R(0) > ml) ? 1 : 0;
+        which_r = (R(0) > mr) ? 0 : 1;
+    }
+    R afl[3] = {0, 0, 0}, afr[3] = {0, 0, 0}, aul[3] = {0, 0, 0}, aur[3] = {0, 0, 0};
+    R asl[3] = {0, 0, 0}, asr[3] = {0, 0, 0};
+    if (sl >= R(0)) {
+        afl[0] = mu[0]; afl[1] = mu[1]; afl[2] = mu[2];
+    } else if (sr <= R(0)) {
+        afr[0] = mu[0]; afr[1] = mu[1]; afr[2] = mu[2];
+    } else {
+        const R D = sr - sl;
+        R a_sr = 0, a_sl = 0;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const R du = r.u[v] - l.u[v];
+            const R F = (sr * l.f[v] - sl * r.f[v] + sl * sr * du) / D;
+            afl[v] = mu[v] * sr / D;
+            afr[v] = -mu[v] * sl / D;
+            aur[v] = mu[v] * sl * sr / D;
+            aul[v] = -aur[v];
+            a_sr += mu[v] * (l.f[v] + sl * du - F) / D;
+            a_sl += mu[v] * (-r.f[v] + sr * du + F) / D;
+        }
+        // route d/dsl, d/dsr to the Davis speeds they were taken from
+        if (which_l == 1) {
+            if (l_from_left) asl[0] += a_sl; else asr[0] += a_sl;
+        } else if (which_l == 2) {
+            if (l_from_left) { asl[0] += R(2) * a_sl; asl[1] -= a_sl; } else { asr[0] += R(2) * a_sl; asr[1] -= a_sl; }
+        }
+        if (which_r == 1) {
+            if (r_from_left) asl[2] += a_sr; else asr[2] += a_sr;
+        } else if (which_r == 2) {
+            if (r_from_left) { asl[2] += R(2) * a_sr; asl[1] -= a_sr; } else { asr[2] += R(2) * a_sr; asr[1] -= a_sr; }
+        }
+    }
+    // asl/asr above hold the speed adjoints of the left / right side respectively
+    dirflux_adj<R>(dir, L, aul, afl, asl, gL, gkL);
+    dirflux_adj<R>(dir, Rt, aur, afr, asr, gR, gkR);
+}
+
+struct AdjArgs {
+    const uint8_t *__restrict__ mask;   // branch codes of the replayed forward step
+    double *__restrict__ A;             // [3][n] source adjoint of each cell (FP64)
+    double *__restrict__ B;             // [4][n] slope coefficients per side
+    double *__restrict__ gbed;          // [n] running d J / d phi_bed of each cell (its material)
+    double *__restrict__ gint;          // [n] running d J / d phi_int of each cell
+    const double *__restrict__ dk_dbed; // [DA_MAX_MATERIALS][3] d kact / d phi_bed per sgn branch
+    const double *__restrict__ dk_dint; // [DA_MAX_MATERIALS][3]
+    double sec2_bed[DA_MAX_MATERIALS];  // 1 + tan^2(phi_bed)
+    double cos_int;
+};
+
+__device__ __forceinline__ double dk_of(const double *tab, int mat, uint8_t code) {
+    return code == 0 ? 0.0 : tab[mat * 3 + (code - 1)];
+}
+
+// ------------------------------------------------------------------------- k_adj_src
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, MatConsts mc,
+                                                    AdjArgs aa, const DevScalars *__restrict__ sc, R sign_floor) {
+    const R dt = R(sc->dt);
+    const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+        double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
+        const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
+        if (prev[0] > R(DA_TINY)) {
+            R le[3];
+            lam_eff<R>(Lnext, aa.mask, i, le);
+            const R nu_u = dt * le[1], nu_v = dt * le[2];
+            if (nu_u != R(0) || nu_v != R(0)) {
+                const uint8_t bf = m.bflag[i];
+                const int mat = m.mat[i];
+                const uint8_t code = aa.mask[i] & 3;
+                const R k = kact_of<R>(mc, mat, code);
+                R s[6];
+                cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
+                R vel0, vel1, h_inv;
+                if constexpr (sizeof(R) == 8) {
+                    vel0 = prev[1] / prev[0];
+                    vel1 = prev[2] / prev[0];
+                    h_inv = 1. / prev[0];
+                } else {
+                    h_inv = 1.0f / prev[0];
+                    vel0 = prev[1] * h_inv;
+                    vel1 = prev[2] * h_inv;
+                }
+                const R sg0 = tiny_sgn(h_inv * (s[4] - vel0 * s[3]), ft);
+                const R sg2 = tiny_sgn(vel0, ft);
+                const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
+                const R sg3 = tiny_sgn(vel1, ft);
+                const R h = prev[0];
+                const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i), gz = grav<R>(m, 2, i);
+                const R dgx = dgrav<R>(m, 0, i), dgy = dgrav<R>(m, 1, i);
+                const R kx = curvat<R>(m, 0, i), ky = curvat<R>(m, 1, i);
+                const R sin_int = R(mc.sin_int), tan_bed = R(mc.tan_bed[mat]);
+                const R Px = gz * h + vel0 * prev[1] * kx, Py = gz * h + vel1 * prev[2] * ky;
+                const R px = Px > R(0) ? R(1) : R(0), py = Py > R(0) ? R(1) : R(0);
+                const R wx = gz * s[3] + dgy * h, wy = gz * s[0] + dgx * h;
+                A[0] = double(nu_u * (gx - sg0 * k * sin_int * (wx + dgy * h) - sg2 * tan_bed * px * (gz - vel0 * vel0 * kx)) +
+                              nu_v * (gy - sg1 * k * sin_int * (wy + dgx * h) - sg3 * tan_bed * py * (gz - vel1 * vel1 * ky)));
+                A[1] = double(nu_u * (-sg2 * tan_bed * px * R(2) * vel0 * kx));
+                A[2] = double(nu_v * (-sg3 * tan_bed * py * R(2) * vel1 * ky));
+                // the limited depth slopes of this cell (zero on boundary cells)
+                if (!(bf & 0x0F)) {
+                    SlopeD<R> sd[2];
+                    h_slope_deriv<R>(m, U.h, i, bf, R(mc.gamma), h, sd);
+                    const R cx = -nu_v * sg1 * h * k * gz * sin_int;  // on d h / dx
+                    const R cy = -nu_u * sg0 * h * k * gz * sin_int;  // on d h / dy
+                    A[0] += double(cx * (-sd[0].g_dp / sd[0].dxp + sd[0].g_dm / sd[0].dxm) +
+                                   cy * (-sd[1].g_dp / sd[1].dxp + sd[1].g_dm / sd[1].dxm));
+                    B[0] = double(cx * sd[0].g_dp / sd[0].dxp);
+                    B[2] = double(-cx * sd[0].g_dm / sd[0].dxm);
+                    B[1] = double(cy * sd[1].g_dp / sd[1].dxp);
+                    B[3] = double(-cy * sd[1].g_dm / sd[1].dxm);
+                }
+                // parameter sensitivities of the sources
+                const double dJ_dk = double(-nu_u * sg0 * h * wx * sin_int - nu_v * sg1 * h * wy * sin_int);
+                const double dJ_dsin = double(-nu_u * sg0 * h * k * wx - nu_v * sg1 * h * k * wy);
+                const double dJ_dtan = double(-nu_u * sg2 * (Px > R(0) ? Px : R(0)) - nu_v * sg3 * (Py > R(0) ? Py : R(0)));
+                const double gb = dJ_dtan * aa.sec2_bed[mat] + dJ_dk * dk_of(aa.dk_dbed, mat, code);
+                const double gi = dJ_dsin * aa.cos_int + dJ_dk * dk_of(aa.dk_dint, mat, code);
+                if (gb != 0.0) aa.gbed[i] += gb;
+                if (gi != 0.0) aa.gint[i] += gi;
+            }
+        }
+        aa.A[i] = A[0];
+        aa.A[(size_t)m.n + i] = A[1];
+        aa.A[(size_t)2 * m.n + i] = A[2];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) aa.B[(size_t)s * m.n + i] = B[s];
+    }
+}
+
+// Flux weight of cell c for its side s: -dt/dx on a plus side, +dt/dx on a minus side, halved
+// when the side carries two finer neighbours, zero when c's direction has an outflow side.
+template <class R>
+__device__ __forceinline__ R side_weight(const MeshArgs &m, int c, uint8_t bf, int s, R dt) {
+    const int d = s & 1;
+    if (bf & ((1 << d) | (1 << (d + 2)))) return R(0);
+    const R dxc = d == 0 ? cell_dx<R>(m, c) : cell_dy<R>(m, c);
+    R w = (s < 2 ? -dt : dt) / dxc;
+    if (bf & (0x10 << s)) w = R(0.5) * w;
+    return w;
+}
+
+template <class R>
+__device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &U, const MatConsts &mc,
+                                          const uint8_t *__restrict__ mask, int c, int dir, Side<R> &s) {
+    const R h = U.h[c];
+    const R k = h >= R(DA_TINY) ? kact_of<R>(mc, m.mat[c], mask[c] & 3) : R(0);
+    make_side<R>(dir, h, U.hu[c], U.hv[c], k, grav<R>(m, 2, c), s);
+}
+
+// ---------------------------------------------------------------------- k_adj_gather
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, StateOut<R> Lout,
+                                                       MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
+    const R dt = R(sc->dt);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m.n; j += gridDim.x * blockDim.x) {
+        R lj[3];
+        lam_eff<R>(Lnext, aa.mask, j, lj);
+        double out[3] = {double(lj[0]) + aa.A[j], double(lj[1]) + aa.A[(size_t)m.n + j],
+                         double(lj[2]) + aa.A[(size_t)2 * m.n + j]};
+        const uint8_t bf = m.bflag[j];
+        double dJ_dkj = 0.0;
+        // only cells with a wet cell among themselves and their neighbours see fluxes
+        bool any_wet = U.h[j] >= R(DA_TINY);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (bf & (1 << s)) continue;
+            const int d = s & 1;
+            const bool plus = s < 2;
+            const int ne = (bf & (0x10 << s)) ? 2 : 1;
+            for (int q = 0; q < ne; ++q) {
+                const int k = m.nbr[(size_t)(s + 4 * q) * m.n + j];
+                const uint8_t bk = m.bflag[k];
+                // slope coefficient of neighbour k for j (k's side s^2 faces j)
+                double bk_s = aa.B[(size_t)(s ^ 2) * m.n + k];
+                if (bk & (0x10 << (s ^ 2))) bk_s *= 0.5;
+                out[0] += bk_s;
+                const bool wet_k = U.h[k] >= R(DA_TINY);
+                if (!(wet_k || U.h[j] >= R(DA_TINY))) continue;
+                any_wet = true;
+                const R wj = side_weight<R>(m, j, bf, s, dt);
+                const R wk = side_weight<R>(m, k, bk, s ^ 2, dt);
+                if (wj == R(0) && wk == R(0)) continue;
+                R lk[3];
+                lam_eff<R>(Lnext, aa.mask, k, lk);
+                const R mu[3] = {wj * lj[0] + wk * lk[0], wj * lj[1] + wk * lk[1], wj * lj[2] + wk * lk[2]};
+                if (mu[0] == R(0) && mu[1] == R(0) && mu[2] == R(0)) continue;
+                Side<R> sj, sk;
+                load_side<R>(m, U, mc, aa.mask, j, d, sj);
+                load_side<R>(m, U, mc, aa.mask, k, d, sk);
+                R gL[3], gR[3], gkL, gkR;
+                if (plus) {
+                    riemann_adj<R>(d, sj, sk, mu, gL, gR, gkL, gkR);
+                    out[0] += double(gL[0]); out[1] += double(gL[1]); out[2] += double(gL[2]);
+                    dJ_dkj += double(gkL);
+                } else {
+                    riemann_adj<R>(d, sk, sj, mu, gL, gR, gkL, gkR);
+                    out[0] += double(gR[0]); out[1] += double(gR[1]); out[2] += double(gR[2]);
+                    dJ_dkj += double(gkR);
+                }
+            }
+        }
+        (void)any_wet;
+        Lout.h[j] = R(out[0]);
+        Lout.hu[j] = R(out[1]);
+        Lout.hv[j] = R(out[2]);
+        if (dJ_dkj != 0.0) {
+            const uint8_t code = aa.mask[j] & 3;
+            const int mat = m.mat[j];
+            aa.gbed[j] += dJ_dkj * dk_of(aa.dk_dbed, mat, code);
+            aa.gint[j] += dJ_dkj * dk_of(aa.dk_dint, mat, code);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------ k_adj_seed
+// J = sum over cells with centre in the box of h^2 dx dy; lambda^N = dJ/dU^N.  FP64 partials per
+// block, summed in block order by the last block.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_seed(MeshArgs m, StateRef<R> U, StateOut<R> L, double x0, double x1,
+                                                     double y0, double y1, double *__restrict__ part,
+                                                     double *__restrict__ J, unsigned *__restrict__ counter) {
+    __shared__ double red[kBlock / 32];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+        double xc, yc;
+        if constexpr (sizeof(R) == 8) {
+            xc = m.x[i];
+            yc = m.y[i];
+        } else {
+            xc = m.x ? m.x[i] : 0.0;
+            yc = m.y ? m.y[i] : 0.0;
+        }
+        const bool in = xc >= x0 && xc <= x1 && yc >= y0 && yc <= y1;
+        const double h = double(U.h[i]);
+        const double area = double(cell_dx<R>(m, i)) * double(cell_dy<R>(m, i));
+        L.h[i] = in ? R(2.0 * h * area) : R(0);
+        L.hu[i] = R(0);
+        L.hv[i] = R(0);
+        if (in) acc += h * h * area;
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double t = 0.0;
+        for (int b = 0; b < gridDim.x; ++b) t += ((volatile double *)part)[b];
+        *J = t;
+        *counter = 0;
+    }
+}
+
+// Per-material sums of the running per-cell parameter sensitivities, plus the pile-height
+// products sum_i lambda_h,i dh0_i/dP_p.  One block per output, fixed order.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_reduce(MeshArgs m, StateRef<R> L0, const double *__restrict__ gbed,
+                                                       const double *__restrict__ gint,
+                                                       const double *__restrict__ dh0, int n_mat, int n_piles,
+                                                       double *__restrict__ out) {
+    __shared__ double red[kBlock / 32];
+    const int o = blockIdx.x;  // 0..n_mat-1 bed per material, n_mat internal, then piles
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < m.n; i += blockDim.x) {
+        if (o < n_mat) {
+            if (m.mat[i] == o) acc += gbed[i];
+        } else if (o == n_mat) {
+            acc += gint[i];
+        } else {
+            acc += double(L0.h[i]) * dh0[(size_t)(o - n_mat - 1) * m.n + i];
+        }
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) t += red[w];
+        out[o] = t;
+    }
+}
+
+}  // namespace
+}  // namespace adj
+}  // namespace da

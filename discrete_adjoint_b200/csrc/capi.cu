@@ -95,6 +95,19 @@ static void free_state(da_ctx *ctx) {
     ctx->have_state = false;
 }
 
+static void free_adjoint(da_ctx *ctx) {
+    auto fr = [](void *p) { if (p) cudaFree(p); };
+    fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
+    fr(ctx->red_out); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter); fr(ctx->dh0);
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
+    for (void *s : ctx->snaps) fr(s);
+    ctx->snaps.clear();
+    ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
+    ctx->red_out = ctx->seed_part = ctx->seed_J = ctx->dh0 = nullptr; ctx->seed_counter = nullptr;
+    ctx->adj_n = 0;
+}
+
 static void drop_graphs(da_ctx *ctx) {
     for (int b = 0; b < 2; ++b) {
         if (ctx->step_graph[b]) cudaGraphExecDestroy(ctx->step_graph[b]);
@@ -238,6 +251,8 @@ void da_destroy(da_ctx *ctx) {
     drop_graphs(ctx);
     free_mesh(ctx);
     free_state(ctx);
+    free_adjoint(ctx);
+    if (ctx->dt_replay) cudaFree(ctx->dt_replay);
     if (ctx->dsc) cudaFree(ctx->dsc);
     if (ctx->hsc) cudaFreeHost(ctx->hsc);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -300,6 +315,7 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     drop_graphs(ctx);
     free_mesh(ctx);
     free_state(ctx);
+    free_adjoint(ctx);
     DevMesh &d = ctx->mesh;
     d.n = n;
     d.epoch = epoch;
@@ -307,9 +323,10 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     if (!st) st = upload(ctx, &d.nbr, m->nbr, (size_t)8 * n);
     if (!st) st = upload(ctx, &d.bflag, bflag.data(), (size_t)n);
     if (!st) st = upload(ctx, &d.mat, mat.data(), (size_t)n);
+    // centres: the FP64 step uses them; both precisions test functional boxes with them
+    if (!st) st = upload(ctx, &d.x, m->x, (size_t)n);
+    if (!st) st = upload(ctx, &d.y, m->y, (size_t)n);
     if (fp64) {
-        if (!st) st = upload(ctx, &d.x, m->x, (size_t)n);
-        if (!st) st = upload(ctx, &d.y, m->y, (size_t)n);
         if (!st) st = upload(ctx, &d.dx, m->dx, (size_t)n);
         if (!st) st = upload(ctx, &d.dy, m->dy, (size_t)n);
         if (!st) st = upload(ctx, &d.g, m->gravity, (size_t)3 * n);

@@ -51,6 +51,9 @@ struct TimeConsts {
     double gravity_scale, epsilon;
     double frict_tiny_early, frict_tiny_late;
     long long frict_tiny_iters;
+    const double *dt_replay;  // when set, step k takes dt_replay[k - iter0] instead of the CFL dt
+    long long iter0;
+    long long n_replay;
 };
 
 // Device copy of the flattened mesh.  FP64 path reads the double arrays; the FP32-split
@@ -97,6 +100,21 @@ struct da_ctx {
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
     std::string err;
     bool have_state = false;
+    // adjoint workspace (allocated on first use)
+    uint8_t *mask = nullptr;         // [n] branch codes of the replayed forward step
+    void *lam[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    double *adjA = nullptr;          // [3][n]
+    double *adjB = nullptr;          // [4][n]
+    double *gbed = nullptr, *gint = nullptr;  // [n] running parameter sensitivities
+    double *dk_tab = nullptr;        // [2][DA_MAX_MATERIALS][3] d kact / d phi_bed, d phi_int
+    double *red_out = nullptr;       // [DA_MAX_MATERIALS + 1 + DA_MAX_PILES]
+    double *seed_part = nullptr;     // [nblocks]
+    double *seed_J = nullptr;
+    unsigned *seed_counter = nullptr;
+    double *dh0 = nullptr;           // [n_piles][n]
+    std::vector<void *> snaps;       // checkpoint slots, 3 state arrays each
+    double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
+    int adj_n = 0;
 };
 
 namespace da {
@@ -107,10 +125,15 @@ void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
 
 // forward_fp64.cu / forward_fp32.cu
 // ev (optional): DA_FWD_KERNELS + 1 events recorded around the launches
-int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev = nullptr);
-int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev);
-int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev);
+// record_mask (optional): branch codes of the step for the adjoint (full sweep)
+int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev = nullptr, uint8_t *record_mask = nullptr);
+int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask);
+int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask);
 int forward_alloc(da_ctx *ctx);
+// adjoint_fp64.cu / adjoint_fp32.cu
+int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
+int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
+int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
 int forward_state_changed(da_ctx *ctx);
 void forward_free(da_ctx *ctx);
 

@@ -5,7 +5,9 @@
 
 namespace da {
 
-int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev) { return fwd::launch_step_t<double>(ctx, ev); }
+int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask) {
+    return fwd::launch_step_t<double>(ctx, ev, record_mask);
+}
 
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
@@ -42,9 +44,9 @@ int forward_state_changed(da_ctx *ctx) {
     return st;
 }
 
-int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev) {
-    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, ev);
-    return launch_forward_step_fp32(ctx, ev);
+int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask) {
+    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, ev, record_mask);
+    return launch_forward_step_fp32(ctx, ev, record_mask);
 }
 
 }  // namespace da

@@ -43,6 +43,11 @@ __device__ void finalize_dt(DevScalars *sc, const TimeConsts &tc) {
     if (time + dt > tc.next_output) dt = tc.next_output - time;
     if (time + dt > tc.next_save) dt = tc.next_save - time;
     if (time + dt > tc.max_time) dt = tc.max_time - time;
+    if (tc.dt_replay) {
+        // frozen time-step sequence (tangent/finite-difference checks of the adjoint)
+        const long long k = sc->iter - tc.iter0;
+        dt = (k >= 0 && k < tc.n_replay) ? tc.dt_replay[k] : 0.0;
+    }
     sc->frict_tiny = sc->iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
     sc->dt = dt;
     sc->time = time + dt;
@@ -73,10 +78,13 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // changed since).  Wet cells (h >= GEOFLOW_TINY) mark themselves and their face neighbours in
 // the active bitmask that k_update reads: a cell outside that set has zero fluxes and no
 // sources this step.
-template <class R>
+// RECORD: also writes the branch code of every cell into mask (0 dry / at rest, 1..3 for
+// sgn(vel) = -1, 0, +1 of gmfggetcoef) for the adjoint's replay; tile culling must be off.
+template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
                                                  unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
-                                                 int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc) {
+                                                 int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
+                                                 uint8_t *__restrict__ mask = nullptr) {
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -87,6 +95,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
             const R h = U.h[i];
             if (!(h == h)) raise_err(sc, DA_ERR_NAN);
             wet = h >= R(DA_TINY);
+            uint8_t code = 0;
             if (wet) {
                 const uint8_t bf = m.bflag[i];
 #pragma unroll
@@ -105,7 +114,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
                     const R ui[3] = {h, U.hu[i], U.hv[i]};
                     R s[6];
                     cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
-                    const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s);
+                    const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
                     kact[i] = k;
                     const R gz = grav<R>(m, 2, i);
                     const R vx = ui[1] / h, vy = ui[2] / h;
@@ -120,6 +129,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
                     my_max = hb > my_max ? hb : my_max;
                 }
             }
+            if (RECORD) mask[i] = code;
         }
         const unsigned self = __ballot_sync(0xffffffffu, wet);
         if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
@@ -140,7 +150,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
 
 // Full corrector update of one active cell (fluxes + sources), reference order.
 template <class R>
-__device__ __forceinline__ void update_cell(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact,
+__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact,
                                             const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
                                             R st[3]) {
     const uint8_t bf = m.bflag[i];
@@ -172,7 +182,8 @@ __device__ __forceinline__ void update_cell(const MeshArgs &m, const StateRef<R>
     }
 #pragma unroll
     for (int v = 0; v < 3; ++v) st[v] = prev[v] - dtdx * div[0][v] - dtdy * div[1][v];
-    if (st[0] < R(0)) st[0] = R(0);
+    const bool clamped = st[0] < R(0);
+    if (clamped) st[0] = R(0);
     if (prev[0] > R(DA_TINY)) {
         R s[6];
         cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
@@ -203,6 +214,7 @@ __device__ __forceinline__ void update_cell(const MeshArgs &m, const StateRef<R>
         s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, i), R(0.0)) * tan_bed;
         st[2] += dt * (s1 - s2 - s3);
     }
+    return clamped;
 }
 
 // Sum of a block's values in a fixed order (warp shuffle, then warps in order); thread 0 holds it.
@@ -224,12 +236,14 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 // and its cached volume partial is reused (tile culling; off when cull == 0).  In an active tile,
 // inactive cells are copied and active ones get the full update.  The active words are cleared
 // here, and each processed tile records whether it holds a wet cell for the next k_coef.
-template <class R>
+// RECORD: sets bit 2 of mask for cells whose depth was clamped at zero.
+template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
                                                    const R *__restrict__ kact, unsigned *__restrict__ active,
                                                    uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
                                                    double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
-                                                   DevScalars *sc, double *__restrict__ vol_part) {
+                                                   DevScalars *sc, double *__restrict__ vol_part,
+                                                   uint8_t *__restrict__ mask = nullptr) {
     __shared__ double red[kBlock / 32];
     const int lane = threadIdx.x & 31;
     const R dt = R(sc->dt);
@@ -249,7 +263,10 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
             const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
             const R dxc = cell_dx<R>(m, i), dyc = cell_dy<R>(m, i);
             R st[3] = {prev[0], prev[1], prev[2]};
-            if (word & (1u << lane)) update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
+            if (word & (1u << lane)) {
+                const bool clamped = update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
+                if (RECORD && clamped) mask[i] |= uint8_t(4);
+            }
             if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
             O.h[i] = st[0];
             O.hu[i] = st[1];
@@ -281,13 +298,23 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
 }
 
 template <class R>
-int launch_step_t(da_ctx *ctx, cudaEvent_t *ev = nullptr) {
+int launch_step_t(da_ctx *ctx, cudaEvent_t *ev = nullptr, uint8_t *record_mask = nullptr) {
     const MeshArgs m = mesh_args(ctx);
     const int c = ctx->cur, o = 1 - c;
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> O{(R *)ctx->U[o][0], (R *)ctx->U[o][1], (R *)ctx->U[o][2]};
     R *kact = (R *)ctx->kact;
     const int tiles = ctx->ntiles, grid = ctx->nblocks, cull = ctx->p.tile_culling;
+    if (record_mask) {
+        // branch recording for the adjoint: full sweep, codes for every cell
+        k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, 0, ctx->mc,
+                                                          ctx->tc, ctx->dsc, record_mask);
+        k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
+                                                            ctx->tile_vol, tiles, 0, ctx->mc, ctx->dsc, ctx->vol_part,
+                                                            record_mask);
+        ctx->cur = o;
+        return cuda_check(ctx, cudaGetLastError(), "forward step launch");
+    }
     if (ev) cudaEventRecord(ev[0], ctx->stream);
     k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull, ctx->mc, ctx->tc,
                                                 ctx->dsc);

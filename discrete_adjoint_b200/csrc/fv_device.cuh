@@ -174,8 +174,10 @@ __device__ __forceinline__ void cell_slopes(const MeshArgs &m, const StateRef<R>
 
 // k act/pass of a wet cell (h > GEOFLOW_TINY), gmfggetcoef (getcoef.f:19-66), from the table
 // of the three sgn(vel) values per material.
+// code (optional): 0 for the rest value, 1 + (sgn(vel) + 1) otherwise.
 template <class R>
-__device__ __forceinline__ R cell_kact(const MatConsts &mc, int mat, R h, R hu, R hv, const R s[6]) {
+__device__ __forceinline__ R cell_kact(const MatConsts &mc, int mat, R h, R hu, R hv, const R s[6],
+                                       uint8_t *code = nullptr) {
     R vel;
     if constexpr (sizeof(R) == 8) {
         vel = s[1] / h - hu * s[0] / (h * h) + s[5] / h - hv * s[3] / (h * h);
@@ -185,7 +187,12 @@ __device__ __forceinline__ R cell_kact(const MatConsts &mc, int mat, R h, R hu, 
     }
     const int sg = fsgn(vel, R(DA_TINY));
     R k = R(mc.kact_sgn[mat][sg + 1]);
-    if (dabs(hu / h) < R(DA_TINY) && dabs(hv / h) < R(DA_TINY)) k = R(mc.kact_rest);
+    uint8_t c = uint8_t(sg + 2);
+    if (dabs(hu / h) < R(DA_TINY) && dabs(hv / h) < R(DA_TINY)) {
+        k = R(mc.kact_rest);
+        c = 0;
+    }
+    if (code) *code = c;
     return k;
 }
 

@@ -169,6 +169,61 @@ class GeoflowContext:
         return {self.lib.da_forward_kernel_name(k).decode(): float(out[k]) for k in range(2)}
 
 
+@dataclass
+class Gradient:
+    """dJ/d(parameters) of one adjoint run (angles in radians)."""
+    J: float
+    dJ_dbedfrict: list
+    dJ_dintfrict: float
+    dJ_dpile: list
+    forward_steps: int
+    snapshots: int
+    lambda0: np.ndarray | None = None
+
+
+def _grad(g: _ffi.da_gradient, n_mat: int, n_piles: int, lam0=None) -> Gradient:
+    return Gradient(g.J, list(g.dJ_dbedfrict[:n_mat]), g.dJ_dintfrict, list(g.dJ_dpile[:n_piles]),
+                    int(g.forward_steps), int(g.snapshots), lam0)
+
+
+def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpile=None,
+                want_lambda0: bool = False) -> Gradient:
+    """dual_solver() of src/adjoint/dual_solver.C:80 over nsteps steps from the current state, for
+    J = sum of h^2 dx dy over the cells whose centre lies in box = (xmin, xmax, ymin, ymax)."""
+    f = _ffi.da_functional(_ffi.DA_FUNC_H2_BOX, 0, (C.c_double * 4)(*box))
+    n = ctx.mesh.n
+    dh = None
+    n_piles = 0
+    if dh0_dpile is not None and len(dh0_dpile):
+        dh = np.ascontiguousarray(dh0_dpile, dtype=np.float64).reshape(-1, n)
+        n_piles = dh.shape[0]
+    lam0 = np.zeros(3 * n) if want_lambda0 else None
+    g = _ffi.da_gradient()
+    ctx._check(ctx.lib.da_adjoint_run(ctx.ctx, C.byref(f), nsteps, nsnapshots,
+                                      _ffi.dptr(dh) if dh is not None else None, n_piles, C.byref(g),
+                                      _ffi.dptr(lam0) if lam0 is not None else None), "da_adjoint_run")
+    return _grad(g, len(ctx.mat.bedfrict_deg), n_piles, None if lam0 is None else lam0.reshape(3, n))
+
+
+def adjoint_step(ctx: GeoflowContext, lam_next) -> tuple:
+    """(lambda^n, parameter parts) for one reverse step at the context's current state."""
+    n = ctx.mesh.n
+    ln = np.ascontiguousarray(lam_next, dtype=np.float64).reshape(3 * n)
+    out = np.zeros(3 * n)
+    g = _ffi.da_gradient()
+    ctx._check(ctx.lib.da_adjoint_step(ctx.ctx, _ffi.dptr(ln), _ffi.dptr(out), C.byref(g)), "da_adjoint_step")
+    return out.reshape(3, n), _grad(g, len(ctx.mat.bedfrict_deg), 0)
+
+
+def set_dt_replay(ctx: GeoflowContext, dts, iter0: int = 0):
+    """Freezes the time-step sequence (None clears it)."""
+    if dts is None:
+        ctx._check(ctx.lib.da_set_dt_replay(ctx.ctx, None, 0, 0), "da_set_dt_replay")
+        return
+    d = np.ascontiguousarray(dts, dtype=np.float64)
+    ctx._check(ctx.lib.da_set_dt_replay(ctx.ctx, _ffi.dptr(d), len(d), iter0), "da_set_dt_replay")
+
+
 def step(ctx: GeoflowContext) -> StepStats:
     """step() of src/geoflow/step.C:29 on a device-resident context."""
     return ctx.step()

@@ -142,6 +142,46 @@ int da_forward_run(da_ctx *ctx, int32_t nsteps, da_step_stats *last);
  * context's stream before the first and after the last launch. */
 int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, double *device_ms);
 
+/* ---- adjoint ------------------------------------------------------------------------------
+ * Replaces dual_solver() (src/adjoint/dual_solver.C:80-273) with calc_jacobian()/calc_adjoint()
+ * (calc_jacobain.C:40-153, calc_adjoint.C:35-167) taken over every step, backward in time.
+ * The adjoint is the exact transpose of the forward step as it is computed here (k act/pass and
+ * all thresholds replayed from recorded branch codes, the time-step sequence frozen), so it is
+ * checked against central finite differences of the same forward step.  Forward states are kept
+ * in HBM at nsnapshots checkpoints placed by an optimal binomial schedule and recomputed between
+ * them (the reference stores every step to gz files instead, dualmesh.C:82-147). */
+#define DA_FUNC_H2_BOX 1          /* J = sum over cells with centre in box of h^2 dx dy, final step */
+
+typedef struct da_functional {
+    int32_t kind;                 /* DA_FUNC_H2_BOX */
+    int32_t pad;
+    double box[4];                /* xmin, xmax, ymin, ymax */
+} da_functional;
+
+typedef struct da_gradient {
+    double J;                             /* functional value at the final step */
+    double dJ_dbedfrict[DA_MAX_MATERIALS];/* per material, radians */
+    double dJ_dintfrict;                  /* radians */
+    double dJ_dpile[DA_MAX_PILES];        /* per pile height (needs dh0_dpile) */
+    int64_t forward_steps;                /* forward steps executed, recomputation included */
+    int32_t snapshots;                    /* checkpoints held */
+    int32_t pad;
+} da_gradient;
+
+/* Runs nsteps forward steps from the context's current state and time, then the adjoint back to
+ * the start.  dh0_dpile: [n_piles][n] derivative of the initial depth with respect to each pile
+ * height (may be NULL when n_piles == 0).  lambda0 (optional, host [3][n]): dJ/dU at the start.
+ * The context's state and time are restored to the start on return. */
+int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots,
+                   const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0);
+/* One reverse step at the current state U^n: lambda_out = (dU^{n+1}/dU^n)^T lambda_next (host
+ * arrays [3][n]).  Replays the forward step to record its branches and time step, then restores
+ * the state and time.  The parameter parts of this step are returned in partial (may be NULL). */
+int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, da_gradient *partial);
+/* Freezes the time-step sequence: step iter0 + k takes dts[k] (k < n) instead of the CFL dt;
+ * dts == NULL clears it.  Used for finite-difference checks of the adjoint. */
+int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0);
+
 /* ---- tracing (the reference's Timer class, properties.h:43-71, moved onto the device) --- */
 #define DA_FWD_KERNELS 2  /* coefficients + dt, update + volume */
 /* Runs nsteps forward steps with CUDA events around every launch on the context's stream and
