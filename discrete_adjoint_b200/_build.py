@@ -29,6 +29,7 @@ UNITS = [
     ("adjoint_fp64.cu", []),
     ("adjoint_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
     ("adjoint_host.cu", []),
+    ("noalloc.cu", ["--fmad=false"]),
     ("mesh_host.cpp", []),
 ]
 

@@ -170,6 +170,8 @@ SIGNATURES = {
                                  C.POINTER(da_gradient), PD]),
     "da_adjoint_step": (C.c_int, [C.c_void_p, PD, PD, C.POINTER(da_gradient)]),
     "da_set_dt_replay": (C.c_int, [C.c_void_p, PD, C.c_int32, C.c_int64]),
+    "da_forward_step_noalloc": (C.c_int, [C.POINTER(da_params), C.POINTER(da_mesh_soa), PD, PD, PD, PD, PD, PD,
+                                          C.c_double, C.c_int64, C.c_void_p, C.POINTER(da_step_stats)]),
     "da_forward_profile": (C.c_int, [C.c_void_p, C.c_int32, PD]),
     "da_forward_kernel_name": (C.c_char_p, [C.c_int32]),
     "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,

@@ -190,6 +190,28 @@ int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0);
 int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms);
 const char *da_forward_kernel_name(int32_t k);
 
+/* ---- one step without any device allocation ------------------------------------------------
+ * No counterpart in the reference: an addition for callers that may not allocate device memory
+ * themselves or through this library, such as a plugin whose host application owns all of the
+ * GPU's memory, or a real-time loop in which allocating is forbidden.  The caller passes device
+ * pointers for the flattened mesh (same layout as da_upload_mesh's, FP64), for the state in and
+ * for the state out (in and out must not overlap); the step's temporaries live in one fixed
+ * array of about 10.7 MB that every GPU loading this library holds until the process exits.
+ * Meshes with more than DA_NOALLOC_MAX_CELLS cells are rejected with DA_ERR_UNSUPPORTED, as is
+ * any precision but DA_PREC_FP64; a neighbour or material index out of range gives
+ * DA_ERR_INVALID before the step runs.  time/iter are TimeProps::time and ::iter before the
+ * step; out receives the step's scalars.  stream is a cudaStream_t (NULL: the default stream);
+ * the call returns after the step has finished on it.
+ * The first call on a device resolves the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All calls share the one
+ * array, which keeps the last call's contents: calls that overlap on a GPU (other streams, other
+ * host threads) race with each other and must be serialised by the caller.  The result is
+ * bit-identical to da_forward_step on a context with the same parameters. */
+#define DA_NOALLOC_MAX_CELLS (1 << 20)
+int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *dev_mesh, const double *h, const double *hu,
+                            const double *hv, double *h_out, double *hu_out, double *hv_out, double time,
+                            int64_t iter, void *stream, da_step_stats *out);
+
 #ifdef __cplusplus
 }
 #endif
