@@ -1,24 +1,30 @@
-"""Benchmark: cell-updates/s of the finite-volume step on the B200 (see the workload below).
+"""Benchmark of the B200 finite-volume step and its discrete adjoint.
 
-python bench.py --gpus N --steps K --warmup W [--impl ours|reference] [--precision fp32|fp64]
+    python bench.py --gpus N --steps K --warmup W [--impl ours|reference]
 
-A "step" is one explicit time step (step(), src/geoflow/step.C:29-275) over the whole mesh of
-the workload: hill + noise terrain 20 km x 20 km, three piles, four materials, adaptive mesh
-refined to 5 m (~3.7M active cells).  value = cells x steps / device seconds (max over ranks);
-e2e = the same through the C ABI with host buffers, H2D of the state before and D2H after
-every step inside the timed region.
+Headline (the metric named for this path): forward + adjoint cell-updates/s, FP32-split against
+plain FP64, on the 1M-cell workload: 5 km x 5 km plane-and-runout terrain at 4.9 m (1024^2
+cells), one 30 m x 100 m pile, 512 time steps, J = sum of h^2 dx dy over a 500 m x 500 m box at
+the final step, gradients with respect to pile height, basal and internal friction, 32 HBM
+checkpoints (binomial schedule).  One benchmark "step" is one whole forward + adjoint run over the
+512-step horizon; value = cells x 512 x K / device seconds (max over ranks).  A cell-update is one
+cell advanced one forward step and taken back through its adjoint step, recomputation included.
+
+Also reported: the same run in FP64, the FP32-split errors against it (J, gradients, lambda^0),
+the forward step alone on the 3.75M-cell adaptive workload (hill + noise, 3 piles, 4 materials),
+per-kernel device times (tracing), the roofline of the dominant kernel, e2e through the C ABI
+with host buffers, clocks, and a CPU baseline.
 
 Multi-GPU: the workload is one instance, so N > 1 runs N independent replicas (one per rank,
-"weak" scaling, no data-path collective); the barrier and the max over ranks stay.
+"weak" scaling, no data-path collective); barrier and max over ranks stay.
 
---impl reference: the reference's CPU algorithm (oracle/_ref when the reference compiled here,
-else the oracle restatement) timed on this host's cores, rank 0 only.
+--impl reference: the reference's own step() compiled from its sources (oracle/_ref/ref_harness,
+when built) timed on this host, else the oracle restatement; rank 0 only.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -32,6 +38,8 @@ if ROOT not in sys.path:
 import numpy as np  # noqa: E402
 
 METRIC = "cell-updates/s fwd+adjoint, FP32-split & batched vs plain FP64 GPU at ≤1e-5 rel err"
+HORIZON = 512
+SNAPSHOTS = 32
 
 
 def peaks():
@@ -105,8 +113,7 @@ def dist_init():
         import datetime
 
         import torch.distributed as dist
-        backend = "nccl"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
 
@@ -140,64 +147,174 @@ def wet_counts(m, h) -> tuple[int, int]:
 
 
 def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dict:
-    """Algorithmic HBM bytes of one launch of each forward kernel: every array a cell needs is
-    touched once (neighbour re-reads are halo traffic, not algorithmic).  Layout of
-    csrc/da_internal.h: state r bytes per component, static fields r bytes per component
-    (x, y centres only in FP64), nbr 4 x int32 primary neighbours, bflag and material 1 byte.
-      k_coef  : every cell reads h; a wet cell reads hu, hv, bflag, mat, nbr, dx, dy, g_z (and
-                x, y in FP64) and writes k_act.
-      k_update: every cell reads bflag, the state, nbr, dx, dy and writes the state; a cell
-                with wet cells around it also reads k_act, g (3), d_gravity (2), curvature (2), mat."""
+    """Algorithmic HBM bytes of one launch of each kernel over the whole mesh: every array a cell
+    needs is touched once; neighbour re-reads are halo traffic, not algorithmic.  Layout of
+    csrc/da_internal.h, r = bytes per real (8 FP64, 4 FP32):
+      k_coef        every cell reads h; a wet cell reads hu, hv, bflag, mat, nbr (4 x int32), dx,
+                    dy, g_z (+ x, y in FP64) and writes k_act
+      k_update      every cell reads bflag, the state, dx, dy and writes the state; an active cell
+                    also reads nbr, k_act, g (3), d_gravity (2), curvature (2), mat
+      k_*_record    as above plus one mask byte written per cell
+      k_adj_src     every cell reads h; a wet cell reads hu, hv, lambda (hu, hv), mask, bflag, mat,
+                    nbr, statics (dx, dy, g, dg, curv [+ x, y]) and writes A (3 x 8) and B (4 x 8)
+                    and updates two FP64 sensitivities
+      k_adj_gather  every cell reads its mask byte and lambda and writes lambda; an active cell also
+                    reads h, bflag, nbr, A (3 x 8) and updates two FP64 sensitivities"""
     r = 8 if precision == "fp64" else 4
     xy = 2 * r if precision == "fp64" else 0
     coef = n * r + n_wet * (2 * r + 1 + 1 + 16 + 2 * r + r + xy + r)
-    upd = n * (1 + 3 * r + 16 + 2 * r + 3 * r) + n_act * (r + 3 * r + 2 * r + 2 * r + 1)
-    return {"k_coef": coef, "k_update": upd}
+    upd = n * (1 + 3 * r + 2 * r + 3 * r) + n_act * (16 + r + 3 * r + 2 * r + 2 * r + 1)
+    src = n * r + n_wet * (2 * r + 2 * r + 1 + 1 + 1 + 16 + 2 * r + 7 * r + xy + 24 + 32 + 32)
+    gat = n * (1 + 3 * r + 3 * r) + n_act * (r + 1 + 16 + 24 + 32)
+    return {"k_coef": coef, "k_update": upd, "k_coef_record": coef + n, "k_update_record": upd + n,
+            "k_adj_src": src, "k_adj_gather": gat}
+
+
+def reference_forward_rate(w, max_seconds: float = 20.0):
+    """cell-updates/s of the reference's own step() (oracle/_ref/ref_harness) on this host, or of the
+    oracle restatement when the harness is not built; (rate, kind, sample)."""
+    import oracle
+    from discrete_adjoint_b200 import TimeProps, make_params
+    m = w.mesh
+    if oracle.reference_available():
+        r1 = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, 2)
+        per = max(r1["step_seconds"] / 2, 1e-6)
+        steps = int(max(2, min(200, max_seconds / per)))
+        r = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, steps)
+        return (m.n * steps / r["step_seconds"], "reference",
+                f"{steps} steps of the {m.n}-cell workload through the reference's own step() "
+                "(compiled from its sources by oracle/ref_build.py), 1 thread, wall time of the step loop")
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+    t0 = time.perf_counter()
+    o.run(h, hu, hv, 1)
+    per = time.perf_counter() - t0
+    steps = int(max(1, min(200, max_seconds / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    o.run(h, hu, hv, steps)
+    dt = time.perf_counter() - t0
+    return (m.n * steps / dt, "port",
+            f"{steps} steps of the {m.n}-cell workload through the oracle restatement, 1 thread")
 
 
 def run_reference_arm(args, ws, rank):
     if rank != 0:
         return
-    from discrete_adjoint_b200 import TimeProps, inputs, make_params
-    import oracle
-    w = inputs.workload2()
-    m = w.mesh
-    p = make_params(w.mat, TimeProps())
-    o = oracle.Oracle(p, m)
-    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
-    o.run(h, hu, hv, 1)  # warm caches and page in
-    t0 = time.perf_counter()
-    rc, _, _ = o.run(h, hu, hv, 1)
-    one = time.perf_counter() - t0
-    per_step = max(1, int(20.0 / max(one, 1e-3)))
-    steps = max(1, min(per_step, args.steps))
-    t0 = time.perf_counter()
-    rc, _, _ = o.run(h, hu, hv, steps)
-    dt = time.perf_counter() - t0
-    v = m.n * steps / dt
+    from discrete_adjoint_b200 import inputs
+    w = inputs.workload3()
+    v, kind, sample = reference_forward_rate(w)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "cells": m.n, "precision": "fp64"},
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-                             "sample": f"{steps} steps of the {m.n}-cell workload, 1 thread (oracle restatement; "
-                                       "the reference itself needs MPI/HDF5/Fortran and is not built here)"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w.mesh.n * HORIZON / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "cells": w.mesh.n, "horizon": HORIZON,
+                       "note": "forward steps only: the reference's adjoint driver takes a single backward step "
+                               "(dual_solver.C:183-207), so its forward rate bounds a CPU fwd+adjoint rate from above"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def fwdadj(args, ws, local):
+    from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, adjoint_run, inputs
+    w = inputs.workload3()
+    m = w.mesh
+    box = inputs.WORKLOAD3_BOX
+    out = {}
+
+    def fresh(prec):
+        c = GeoflowContext(w.mat, TimeProps(), precision=prec, device=local)
+        c.upload_mesh(m)
+        c.set_state(m.h0, m.hu0, m.hv0)
+        return c
+
+    sampler = ClockSampler(local)
+    for name, prec in (("fp32", _ffi.DA_PREC_FP32_SPLIT), ("fp64", _ffi.DA_PREC_FP64)):
+        c = fresh(prec)
+        for _ in range(args.warmup):
+            adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
+        if name == "fp32" and not args.no_clocks:
+            sampler.start()
+            time.sleep(0.3)
+        barrier(ws, local)
+        ms = 0.0
+        g = None
+        for _ in range(args.steps):
+            g = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
+            ms += g.device_ms
+        barrier(ws, local)
+        if name == "fp32" and not args.no_clocks:
+            t_end = time.time() + 1.0
+            while time.time() < t_end:
+                adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
+        ms = allmax(ms, ws, local)
+        gl = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, want_lambda0=True)
+        out[name] = {"ms": ms, "value": m.n * HORIZON * args.steps * ws / (ms * 1e-3), "grad": gl,
+                     "forward_steps": g.forward_steps}
+        if name == "fp32":
+            out["clocks"] = sampler.stop() if not args.no_clocks else {"sm_mhz": None, "sm_max_mhz": None,
+                                                                         "reasons": ["not sampled"]}
+            # per-kernel device times of one traced run
+            c.set_tracing(True)
+            adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
+            out["trace"] = c.trace()
+            c.set_tracing(False)
+            # e2e through the C ABI with host buffers: H2D of the initial state, the run, D2H of
+            # the gradients and lambda^0
+            h0, hu0, hv0 = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+            barrier(ws, local)
+            t0 = time.perf_counter()
+            for _ in range(args.e2e_steps):
+                c.set_state(h0, hu0, hv0)
+                c.set_time(0.0, 0)
+                ge = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, want_lambda0=True)
+            e2e_s = allmax(time.perf_counter() - t0, ws, local)
+            out["e2e"] = {"value": m.n * HORIZON * args.e2e_steps * ws / e2e_s, "unit": "cell-updates/s",
+                          "h2d_bytes_per_step": 3 * 8 * m.n, "d2h_bytes_per_step": 3 * 8 * m.n + 8 * 32}
+            out["e2e_J_matches"] = bool(ge.J == gl.J)
+        c.close()
+    # wet / active counts over the horizon (forward states sampled every 64 steps)
+    c = fresh(_ffi.DA_PREC_FP64)
+    wv_, av_ = [], []
+    for k in range(0, HORIZON + 1, 64):
+        if k:
+            c.run(64)
+        wv, av = wet_counts(m, c.get_state()[0])
+        wv_.append(wv)
+        av_.append(av)
+    c.close()
+    out["n_wet"], out["n_act"] = float(np.mean(wv_)), float(np.mean(av_))
+    return w, out
+
+
+def forward_config2(args, ws, local):
+    from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, inputs
+    w = inputs.workload2()
+    m = w.mesh
+    res = {}
+    for name, prec, cull in (("fp32", _ffi.DA_PREC_FP32_SPLIT, True),
+                             ("fp32_full_sweep", _ffi.DA_PREC_FP32_SPLIT, False),
+                             ("fp64", _ffi.DA_PREC_FP64, True)):
+        c = GeoflowContext(w.mat, TimeProps(), precision=prec, device=local, tile_culling=cull)
+        c.upload_mesh(m)
+        c.set_state(m.h0, m.hu0, m.hv0)
+        c.run(5)
+        _, ms = c.run_timed(300)
+        ms = allmax(ms, ws, local)
+        res[name] = {"value": m.n * 300 * ws / (ms * 1e-3), "ms_per_step": ms / 300, "kernel_ms": c.profile(20)}
+        c.close()
+    return w, res
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3, help="timed forward+adjoint runs (512 time steps each)")
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-clocks", action="store_true", help="skip the clock sampler (profiling runs)")
-    ap.add_argument("--sign-floor", type=float, default=0.0,
-                    help="FP32-split friction sign threshold floor (0 = the reference's thresholds)")
+    ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-forward", action="store_true", help="skip the forward-only section")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -209,138 +326,61 @@ def main():
             dist.destroy_process_group()
         return
 
-    from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, inputs
-
-    w = inputs.workload2()
+    from discrete_adjoint_b200 import inputs
+    w, r = fwdadj(args, ws, local)
     m = w.mesh
-    prec = _ffi.DA_PREC_FP32_SPLIT if args.precision == "fp32" else _ffi.DA_PREC_FP64
+    a, b = r["fp64"]["grad"], r["fp32"]["grad"]
+    rel = lambda x, y: abs(x - y) / max(abs(y), 1e-300)  # noqa: E731
+    errs = {"J": rel(b.J, a.J), "dJ_dpile": rel(b.dJ_dpile[0], a.dJ_dpile[0]),
+            "dJ_dbedfrict": rel(b.dJ_dbedfrict[0], a.dJ_dbedfrict[0]),
+            "dJ_dintfrict": rel(b.dJ_dintfrict, a.dJ_dintfrict),
+            "lambda0_rel_l2": float(np.linalg.norm(b.lambda0 - a.lambda0) / max(np.linalg.norm(a.lambda0), 1e-300))}
 
-    def fresh(precision, cull=True):
-        c = GeoflowContext(w.mat, TimeProps(), precision=precision, device=local,
-                           fp32_sign_floor=args.sign_floor, tile_culling=cull)
-        c.upload_mesh(m)
-        c.set_state(m.h0, m.hu0, m.hv0)
-        return c
-
-    ctx = fresh(prec)
-    ctx.run(args.warmup)
-    sampler = ClockSampler(local)
-    if not args.no_clocks:
-        sampler.start()
-        time.sleep(0.4)
-    barrier(ws, local)
-    stats, ms = ctx.run_timed(args.steps)
-    barrier(ws, local)
-    if not args.no_clocks:
-        # keep the GPU loaded until the sampler has seen a few samples (untimed)
-        t_end = time.time() + 1.2
-        while time.time() < t_end:
-            ctx.run(50)
-        clocks = sampler.stop()
-    else:
-        clocks = {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["not sampled (--no-clocks)"]}
-    ms_max = allmax(ms, ws, local)
-    value = m.n * args.steps * ws / (ms_max * 1e-3)
-
-    # the same step without tile culling: every cell rewritten every step
-    full = fresh(prec, cull=False)
-    full.run(args.warmup)
-    _, msf = full.run_timed(args.steps)
-    msf = allmax(msf, ws, local)
-    value_full = m.n * args.steps * ws / (msf * 1e-3)
-    w0 = wet_counts(m, full.get_state()[0])
-    prof_full = full.profile(20)
-    w1 = wet_counts(m, full.get_state()[0])
-    n_wet, n_act = 0.5 * (w0[0] + w1[0]), 0.5 * (w0[1] + w1[1])
-    full.close()
-
-    # plain FP64 path on the same workload, same step count (the metric's comparison)
-    ref64 = fresh(_ffi.DA_PREC_FP64)
-    ref64.run(args.warmup)
-    _, ms64 = ref64.run_timed(args.steps)
-    ms64 = allmax(ms64, ws, local)
-    value64 = m.n * args.steps * ws / (ms64 * 1e-3)
-    # error of the FP32-split path against the FP64 path after the same number of steps from
-    # the same initial state (fresh contexts: the timed contexts ran extra untimed steps)
-    e32, e64 = fresh(prec), fresh(_ffi.DA_PREC_FP64)
-    nerr = args.warmup + args.steps
-    e32.run(nerr)
-    e64.run(nerr)
-    h32, u32, v32 = e32.get_state()
-    h64, u64, v64 = e64.get_state()
-    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))  # noqa: E731
-    rel_err = {"steps": nerr, "h": rel(h32, h64), "hu": rel(u32, u64), "hv": rel(v32, v64)}
-    e32.close()
-    e64.close()
-
-    # per-kernel device times for the roofline (events around each launch); wet / active
-    # counts averaged over the profiled steps give the algorithmic bytes of each launch
-    # The roofline is taken on the full sweep (tile culling off: every cell read and written),
-    # whose algorithmic bytes are defined per cell; the culled step is reported beside it.
-    prof = ctx.profile(20)
-    dom = max(prof_full, key=prof_full.get)
-    alg = algorithmic_bytes(args.precision, m.n, n_wet, n_act)
+    # roofline of the dominant kernel of the traced FP32-split run
+    tr = r["trace"]
+    dom = max(tr, key=lambda k: tr[k][0])
+    alg = algorithmic_bytes("fp32", m.n, r["n_wet"], r["n_act"])
     hbm, peak_kind = peaks()
-    achieved = alg[dom] / (prof_full[dom] * 1e-3) / 1e9
+    avg_ms = tr[dom][0] / tr[dom][1]
+    achieved = alg.get(dom, 0.0) / (avg_ms * 1e-3) / 1e9
 
-    # e2e through the C ABI with host buffers: H2D state, one step, D2H state, every step
-    h, hu, hv = ctx.get_state()
-    h, hu, hv = np.ascontiguousarray(h), np.ascontiguousarray(hu), np.ascontiguousarray(hv)
-    barrier(ws, local)
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
-        ctx.set_state(h, hu, hv)
-        ctx.run(1)
-        h, hu, hv = ctx.get_state()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = allmax(e2e_s, ws, local)
-    e2e_value = m.n * args.e2e_steps * ws / e2e_s
-    elt = 8 if args.precision == "fp64" else 4
-    h2d = 3 * elt * m.n
-    d2h = 3 * elt * m.n
+    fwd = None
+    if not args.no_forward:
+        w2, f2 = forward_config2(args, ws, local)
+        fwd = {"workload": w2.name, "cells": w2.mesh.n, "steps": 300,
+               "value_fp32_split": f2["fp32"]["value"], "value_fp32_full_sweep": f2["fp32_full_sweep"]["value"],
+               "value_fp64": f2["fp64"]["value"], "kernel_ms": {k: v["kernel_ms"] for k, v in f2.items()}}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        import oracle
-        from discrete_adjoint_b200 import make_params
-        o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
-        ch, chu, chv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
-        t0 = time.perf_counter()
-        o.run(ch, chu, chv, 1)
-        one = time.perf_counter() - t0
-        ns = max(1, min(10, int(15.0 / max(one, 1e-3))))
-        t0 = time.perf_counter()
-        o.run(ch, chu, chv, ns)
-        cs = time.perf_counter() - t0
-        cpu = {"value": m.n * ns / cs, "unit": "cell-updates/s", "cores": 1, "kind": "port",
-               "sample": f"{ns} forward steps of the same {m.n}-cell workload, FP64 oracle restatement, 1 thread"}
+        v, kind, sample = reference_forward_rate(w, 15.0)
+        cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+               "sample": sample + "; forward steps only (no CPU fwd+adjoint sweep exists)"}
 
     if rank == 0:
+        launches_per_run = sum(n for _, n in tr.values())
         line = {
-            "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-            "config": {"workload": w.name + " -- forward step only (adjoint not yet in the timed step)",
-                       "cells": m.n, "precision": "fp32-split" if args.precision == "fp32" else "fp64",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "per-step working set larger than L2 (no flush needed)"},
-            "fp64_value": value64, "fp32_over_fp64": value / value64,
-            "full_sweep_value": value_full, "full_sweep_kernel_ms": prof_full,
-            "rel_err_vs_fp64": rel_err, "fp32_sign_floor": args.sign_floor,
-            "roofline": {"bound": "hbm", "kernel": dom + " (full sweep)", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s",
-                         "frac": achieved / hbm if hbm else None, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": alg[dom], "wet_cells": n_wet, "active_cells": n_act,
-                         "kernel_ms_full_sweep": prof_full, "kernel_ms_culled": prof, "traffic": None},
-            "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 2 * args.steps,
-            "clocks": clocks,
+            "metric": METRIC, "value": r["fp32"]["value"], "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["fp32"]["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "cells": m.n, "horizon": HORIZON, "snapshots": SNAPSHOTS,
+                       "functional": "sum h^2 dx dy over box " + str(inputs.WORKLOAD3_BOX),
+                       "precision": "fp32-split", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "per-run working set larger than L2 (no flush needed)",
+                       "forward_steps_per_run": r["fp32"]["forward_steps"]},
+            "fp64_value": r["fp64"]["value"], "fp32_over_fp64": r["fp32"]["value"] / r["fp64"]["value"],
+            "rel_err_fp32_vs_fp64": errs,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind, "alg_bytes_per_launch": alg.get(dom),
+                         "avg_launch_ms": avg_ms, "wet_cells_avg": r["n_wet"], "active_cells_avg": r["n_act"],
+                         "trace_ms_launches": {k: [round(v[0], 4), v[1]] for k, v in tr.items()}, "traffic": None},
+            "e2e": r["e2e"],
+            "gpu_launches": int(launches_per_run * args.steps),
+            "clocks": r["clocks"],
             "cpu_baseline": cpu,
+            "forward_only": fwd,
         }
         print(json.dumps(line))
-    ctx.close()
-    ref64.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -145,6 +145,7 @@ class da_gradient(C.Structure):
         ("forward_steps", C.c_int64),
         ("snapshots", C.c_int32),
         ("pad", C.c_int32),
+        ("device_ms", C.c_double),
     ]
 
 
@@ -174,6 +175,9 @@ SIGNATURES = {
                                           C.c_double, C.c_int64, C.c_void_p, C.POINTER(da_step_stats)]),
     "da_forward_profile": (C.c_int, [C.c_void_p, C.c_int32, PD]),
     "da_forward_kernel_name": (C.c_char_p, [C.c_int32]),
+    "da_set_tracing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "da_trace_read": (C.c_int, [C.c_void_p, C.c_int32, PD, C.POINTER(C.c_int64)]),
+    "da_trace_name": (C.c_char_p, [C.c_int32]),
     "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,
                                 C.c_double, C.c_double, C.POINTER(C.POINTER(da_mesh_host))]),
     "da_mesh_free": (None, [C.POINTER(da_mesh_host)]),

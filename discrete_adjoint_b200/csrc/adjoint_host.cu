@@ -111,12 +111,14 @@ int store(da_ctx *ctx, int slot) {
     const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
     char *base = (char *)ctx->snaps[slot];
     int st = DA_OK;
+    trace_begin(ctx, TR_SNAPSHOT);
     for (int v = 0; v < 3 && !st; ++v)
         st = cuda_check(ctx, cudaMemcpyAsync(base + v * rs * n, ctx->U[ctx->cur][v], rs * n, cudaMemcpyDeviceToDevice,
                                              ctx->stream), "snapshot store");
     if (!st)
         st = cuda_check(ctx, cudaMemcpyAsync(base + 3 * rs * n, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
                                              ctx->stream), "snapshot store");
+    trace_end(ctx);
     return st;
 }
 
@@ -124,12 +126,14 @@ int restore(da_ctx *ctx, int slot) {
     const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
     char *base = (char *)ctx->snaps[slot];
     int st = DA_OK;
+    trace_begin(ctx, TR_SNAPSHOT);
     for (int v = 0; v < 3 && !st; ++v)
         st = cuda_check(ctx, cudaMemcpyAsync(ctx->U[ctx->cur][v], base + v * rs * n, rs * n, cudaMemcpyDeviceToDevice,
                                              ctx->stream), "snapshot restore");
     if (!st)
         st = cuda_check(ctx, cudaMemcpyAsync(ctx->dsc, base + 3 * rs * n, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
                                              ctx->stream), "snapshot restore");
+    trace_end(ctx);
     if (!st) st = forward_state_changed(ctx);
     return st;
 }
@@ -186,7 +190,7 @@ struct Runner {
         return st;
     }
     int youturn() {
-        int st = launch_forward_step(ctx, nullptr, ctx->mask);  // replay step n with its branch codes
+        int st = launch_forward_step(ctx, ctx->mask);  // replay step n with its branch codes
         ++fsteps;
         if (!st && !seeded) {
             st = launch_adjoint_seed(ctx, lam_cur, box);  // U^N is the state just produced
@@ -341,7 +345,7 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
         }
     }
     if (!st) st = store(ctx, 0);
-    if (!st) st = launch_forward_step(ctx, nullptr, ctx->mask);
+    if (!st) st = launch_forward_step(ctx, ctx->mask);
     if (!st) st = launch_adjoint_step(ctx, 0, 1, sec2, cos_int);
     if (!st) st = restore(ctx, 0);
     if (!st) st = sync_check(ctx);
@@ -379,15 +383,26 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
     if (st) return st;
     r.sch.build(nsteps, nsnapshots);
     for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
     st = store(ctx, 0);
     if (!st) st = r.reverse(0, nsteps, 0);
     if (!st) st = restore(ctx, 0);
+    cudaEventRecord(e1, ctx->stream);
     if (!st) st = sync_check(ctx);
+    float dev_ms = 0.f;
+    if (!st) cudaEventElapsedTime(&dev_ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!st) st = trace_flush(ctx);
     if (!st && lambda0) st = copy_lambda_out(ctx, r.lam_cur, lambda0);
     if (!st) st = fill_gradient(ctx, r.lam_cur, n_piles, out);
     if (!st && out) {
         out->forward_steps = r.fsteps;
         out->snapshots = nsnapshots;
+        out->device_ms = dev_ms;
     }
     return st;
 }

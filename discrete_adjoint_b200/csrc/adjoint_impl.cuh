@@ -250,8 +250,11 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
     const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
         double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
-        const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
-        if (prev[0] > R(DA_TINY)) {
+        const R h_i = U.h[i];
+        // A and B exist for wet cells only; k_adj_gather reads them only there
+        if (!(h_i > R(DA_TINY))) continue;
+        const R prev[3] = {h_i, U.hu[i], U.hv[i]};
+        {
             R le[3];
             lam_eff<R>(Lnext, aa.mask, i, le);
             const R nu_u = dt * le[1], nu_v = dt * le[2];
@@ -345,14 +348,25 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
                                                        MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
     const R dt = R(sc->dt);
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m.n; j += gridDim.x * blockDim.x) {
+        const uint8_t mj = aa.mask[j];
+        if (!(mj & 8)) {
+            // not active in the forward step: its update was the identity, and no neighbour is wet
+            Lout.h[j] = Lnext.h[j];
+            Lout.hu[j] = Lnext.hu[j];
+            Lout.hv[j] = Lnext.hv[j];
+            continue;
+        }
         R lj[3];
         lam_eff<R>(Lnext, aa.mask, j, lj);
-        double out[3] = {double(lj[0]) + aa.A[j], double(lj[1]) + aa.A[(size_t)m.n + j],
-                         double(lj[2]) + aa.A[(size_t)2 * m.n + j]};
+        double out[3] = {double(lj[0]), double(lj[1]), double(lj[2])};
+        const R h_j = U.h[j];
+        if (h_j > R(DA_TINY)) {
+            out[0] += aa.A[j];
+            out[1] += aa.A[(size_t)m.n + j];
+            out[2] += aa.A[(size_t)2 * m.n + j];
+        }
         const uint8_t bf = m.bflag[j];
         double dJ_dkj = 0.0;
-        // only cells with a wet cell among themselves and their neighbours see fluxes
-        bool any_wet = U.h[j] >= R(DA_TINY);
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             if (bf & (1 << s)) continue;
@@ -362,13 +376,14 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
             for (int q = 0; q < ne; ++q) {
                 const int k = m.nbr[(size_t)(s + 4 * q) * m.n + j];
                 const uint8_t bk = m.bflag[k];
-                // slope coefficient of neighbour k for j (k's side s^2 faces j)
-                double bk_s = aa.B[(size_t)(s ^ 2) * m.n + k];
-                if (bk & (0x10 << (s ^ 2))) bk_s *= 0.5;
-                out[0] += bk_s;
-                const bool wet_k = U.h[k] >= R(DA_TINY);
-                if (!(wet_k || U.h[j] >= R(DA_TINY))) continue;
-                any_wet = true;
+                const R h_k = U.h[k];
+                if (h_k > R(DA_TINY)) {
+                    // slope coefficient of neighbour k for j (k's side s^2 faces j)
+                    double bk_s = aa.B[(size_t)(s ^ 2) * m.n + k];
+                    if (bk & (0x10 << (s ^ 2))) bk_s *= 0.5;
+                    out[0] += bk_s;
+                }
+                if (!(h_k >= R(DA_TINY) || h_j >= R(DA_TINY))) continue;
                 const R wj = side_weight<R>(m, j, bf, s, dt);
                 const R wk = side_weight<R>(m, k, bk, s ^ 2, dt);
                 if (wj == R(0) && wk == R(0)) continue;
@@ -391,7 +406,6 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
                 }
             }
         }
-        (void)any_wet;
         Lout.h[j] = R(out[0]);
         Lout.hu[j] = R(out[1]);
         Lout.hv[j] = R(out[2]);

@@ -32,8 +32,12 @@ int step_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_
     const AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
     const int grid = ctx->nblocks;
     const R floor = R(ctx->mc.sign_floor);
+    trace_begin(ctx, TR_ADJ_SRC);
     k_adj_src<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, Ln, ctx->mc, aa, ctx->dsc, floor);
+    trace_end(ctx);
+    trace_begin(ctx, TR_ADJ_GATHER);
     k_adj_gather<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, Ln, Lo, ctx->mc, aa, ctx->dsc);
+    trace_end(ctx);
     return cuda_check(ctx, cudaGetLastError(), "adjoint step launch");
 }
 
@@ -43,8 +47,10 @@ int seed_t(da_ctx *ctx, int lam_out, const double box[4]) {
     const int c = ctx->cur;
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
+    trace_begin(ctx, TR_ADJ_SEED);
     k_adj_seed<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, Lo, box[0], box[1], box[2], box[3], ctx->seed_part,
                                                              ctx->seed_J, ctx->seed_counter);
+    trace_end(ctx);
     return cuda_check(ctx, cudaGetLastError(), "adjoint seed launch");
 }
 
@@ -53,8 +59,10 @@ int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
     const MeshArgs m = mesh_args(ctx);
     StateRef<R> L{(const R *)ctx->lam[lam0][0], (const R *)ctx->lam[lam0][1], (const R *)ctx->lam[lam0][2]};
     const int nout = ctx->p.n_materials + 1 + n_piles;
+    trace_begin(ctx, TR_ADJ_REDUCE);
     k_adj_reduce<R><<<nout, kBlock, 0, ctx->stream>>>(m, L, ctx->gbed, ctx->gint, ctx->dh0, ctx->p.n_materials, n_piles,
                                                        ctx->red_out);
+    trace_end(ctx);
     return cuda_check(ctx, cudaGetLastError(), "adjoint reduce launch");
 }
 

@@ -17,6 +17,45 @@ int set_error(da_ctx *ctx, int code, const std::string &msg) {
     return code;
 }
 
+void trace_begin(da_ctx *ctx, int kind) {
+    TraceState &t = ctx->trace;
+    if (!t.on) return;
+    TraceState::Pending p{kind, nullptr, nullptr};
+    for (cudaEvent_t *e : {&p.a, &p.b}) {
+        if (!t.pool.empty()) {
+            *e = t.pool.back();
+            t.pool.pop_back();
+        } else if (cudaEventCreate(e) != cudaSuccess) {
+            *e = nullptr;
+        }
+    }
+    if (p.a) cudaEventRecord(p.a, ctx->stream);
+    t.pending.push_back(p);
+}
+
+void trace_end(da_ctx *ctx) {
+    TraceState &t = ctx->trace;
+    if (!t.on || t.pending.empty()) return;
+    if (t.pending.back().b) cudaEventRecord(t.pending.back().b, ctx->stream);
+}
+
+int trace_flush(da_ctx *ctx) {
+    TraceState &t = ctx->trace;
+    if (t.pending.empty()) return DA_OK;
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "trace sync");
+    for (auto &p : t.pending) {
+        float ms = 0.f;
+        if (!st && p.a && p.b && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+            t.total_ms[p.kind] += ms;
+            t.launches[p.kind] += 1;
+        }
+        if (p.a) t.pool.push_back(p.a);
+        if (p.b) t.pool.push_back(p.b);
+    }
+    t.pending.clear();
+    return st;
+}
+
 int cuda_check(da_ctx *ctx, cudaError_t e, const char *what) {
     if (e == cudaSuccess) return DA_OK;
     const int code = (e == cudaErrorMemoryAllocation) ? DA_ERR_OOM : DA_ERR_CUDA;
@@ -252,6 +291,8 @@ void da_destroy(da_ctx *ctx) {
     free_mesh(ctx);
     free_state(ctx);
     free_adjoint(ctx);
+    trace_flush(ctx);
+    for (cudaEvent_t e : ctx->trace.pool) cudaEventDestroy(e);
     if (ctx->dt_replay) cudaFree(ctx->dt_replay);
     if (ctx->dsc) cudaFree(ctx->dsc);
     if (ctx->hsc) cudaFreeHost(ctx->hsc);
@@ -430,7 +471,8 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
     int st = DA_OK;
     // Two steps (one ping-pong cycle) per graph launch; one graph per starting buffer.
     const int cur0 = ctx->cur;
-    if (nsteps >= 2 && !ctx->step_graph[cur0]) {
+    const bool use_graph = !ctx->trace.on;
+    if (use_graph && nsteps >= 2 && !ctx->step_graph[cur0]) {
         cudaGraph_t g;
         st = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (st) return st;
@@ -452,9 +494,10 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
         if (!st) st = cuda_check(ctx, cudaEventRecord(e0, ctx->stream), "event record");
     }
     int k = 0;
-    for (; k + 1 < nsteps && !st; k += 2)
-        st = cuda_check(ctx, cudaGraphLaunch(ctx->step_graph[cur0], ctx->stream), "graph launch");
-    if (!st && k < nsteps) st = launch_forward_step(ctx);
+    if (use_graph)
+        for (; k + 1 < nsteps && !st; k += 2)
+            st = cuda_check(ctx, cudaGraphLaunch(ctx->step_graph[cur0], ctx->stream), "graph launch");
+    for (; k < nsteps && !st; ++k) st = launch_forward_step(ctx);
     if (device_ms && !st) {
         st = cuda_check(ctx, cudaEventRecord(e1, ctx->stream), "event record");
         if (!st) st = cuda_check(ctx, cudaEventSynchronize(e1), "event sync");
@@ -479,23 +522,48 @@ int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_profile: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_profile: no state");
     cudaSetDevice(ctx->device);
-    cudaEvent_t ev[DA_FWD_KERNELS + 1];
-    int st = DA_OK;
-    int made = 0;
-    for (; made < DA_FWD_KERNELS + 1 && !st; ++made) st = cuda_check(ctx, cudaEventCreate(&ev[made]), "event");
-    double acc[DA_FWD_KERNELS] = {0, 0};
-    for (int s = 0; s < nsteps && !st; ++s) {
-        st = launch_forward_step(ctx, ev);
-        if (!st) st = cuda_check(ctx, cudaEventSynchronize(ev[DA_FWD_KERNELS]), "event sync");
-        for (int k = 0; k < DA_FWD_KERNELS && !st; ++k) {
-            float ms = 0.f;
-            st = cuda_check(ctx, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]), "event time");
-            acc[k] += ms;
-        }
-    }
-    for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+    TraceState &t = ctx->trace;
+    const bool was_on = t.on;
+    int st = trace_flush(ctx);
+    double tot0[2] = {t.total_ms[TR_COEF], t.total_ms[TR_UPDATE]};
+    long long n0[2] = {t.launches[TR_COEF], t.launches[TR_UPDATE]};
+    t.on = true;
+    for (int s = 0; s < nsteps && !st; ++s) st = launch_forward_step(ctx);
+    if (!st) st = trace_flush(ctx);
+    t.on = was_on;
     if (!st) st = sync_scalars(ctx);
-    for (int k = 0; k < DA_FWD_KERNELS; ++k) kernel_ms[k] = acc[k] / nsteps;
+    const int kinds[2] = {TR_COEF, TR_UPDATE};
+    for (int k = 0; k < DA_FWD_KERNELS; ++k) {
+        const long long c = t.launches[kinds[k]] - n0[k];
+        kernel_ms[k] = c > 0 ? (t.total_ms[kinds[k]] - tot0[k]) / c : 0.0;
+    }
+    return st;
+}
+
+static const char *kTraceNames[TR_COUNT] = {"k_coef",       "k_update",     "k_coef_record", "k_update_record",
+                                            "k_adj_src",    "k_adj_gather", "k_adj_seed",    "k_adj_reduce",
+                                            "snapshot_copy"};
+
+const char *da_trace_name(int32_t k) { return (k >= 0 && k < TR_COUNT) ? kTraceNames[k] : ""; }
+
+int da_set_tracing(da_ctx *ctx, int32_t on) {
+    if (!ctx) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = trace_flush(ctx);
+    for (int k = 0; k < TR_COUNT; ++k) {
+        ctx->trace.total_ms[k] = 0.0;
+        ctx->trace.launches[k] = 0;
+    }
+    ctx->trace.on = on != 0;
+    return st;
+}
+
+int da_trace_read(da_ctx *ctx, int32_t k, double *total_ms, int64_t *launches) {
+    if (!ctx || k < 0 || k >= TR_COUNT || !total_ms || !launches) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = trace_flush(ctx);
+    *total_ms = ctx->trace.total_ms[k];
+    *launches = ctx->trace.launches[k];
     return st;
 }
 

@@ -72,6 +72,25 @@ struct DevMesh {
     float *fg = nullptr, *fdg = nullptr, *fcurv = nullptr;
 };
 
+// Tracing: CUDA events around every launch of the step and the adjoint, summed per kernel
+// (the reference's Timer class, src/header/properties.h:43-71, moved onto the device).
+enum TraceKind {
+    TR_COEF, TR_UPDATE, TR_COEF_REC, TR_UPDATE_REC, TR_ADJ_SRC, TR_ADJ_GATHER, TR_ADJ_SEED, TR_ADJ_REDUCE,
+    TR_SNAPSHOT, TR_COUNT
+};
+
+struct TraceState {
+    struct Pending {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    std::vector<Pending> pending;
+    double total_ms[TR_COUNT] = {};
+    long long launches[TR_COUNT] = {};
+};
+
 }  // namespace da
 
 struct da_ctx {
@@ -115,20 +134,24 @@ struct da_ctx {
     std::vector<void *> snaps;       // checkpoint slots, 3 state arrays each
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
     int adj_n = 0;
+    da::TraceState trace;
 };
 
 namespace da {
 
 int set_error(da_ctx *ctx, int code, const std::string &msg);
+void trace_begin(da_ctx *ctx, int kind);
+void trace_end(da_ctx *ctx);
+int trace_flush(da_ctx *ctx);
 int cuda_check(da_ctx *ctx, cudaError_t e, const char *what);
 void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
 
 // forward_fp64.cu / forward_fp32.cu
 // ev (optional): DA_FWD_KERNELS + 1 events recorded around the launches
 // record_mask (optional): branch codes of the step for the adjoint (full sweep)
-int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev = nullptr, uint8_t *record_mask = nullptr);
-int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask);
-int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask);
+int launch_forward_step(da_ctx *ctx, uint8_t *record_mask = nullptr);
+int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask);
+int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask);
 int forward_alloc(da_ctx *ctx);
 // adjoint_fp64.cu / adjoint_fp32.cu
 int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);

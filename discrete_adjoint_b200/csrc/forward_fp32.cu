@@ -4,8 +4,8 @@
 
 namespace da {
 
-int launch_forward_step_fp32(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask) {
-    return fwd::launch_step_t<float>(ctx, ev, record_mask);
+int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask) {
+    return fwd::launch_step_t<float>(ctx, record_mask);
 }
 
 }  // namespace da

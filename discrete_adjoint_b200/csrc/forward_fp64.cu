@@ -5,8 +5,8 @@
 
 namespace da {
 
-int launch_forward_step_fp64(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask) {
-    return fwd::launch_step_t<double>(ctx, ev, record_mask);
+int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
+    return fwd::launch_step_t<double>(ctx, record_mask);
 }
 
 int forward_alloc(da_ctx *ctx) {
@@ -44,9 +44,9 @@ int forward_state_changed(da_ctx *ctx) {
     return st;
 }
 
-int launch_forward_step(da_ctx *ctx, cudaEvent_t *ev, uint8_t *record_mask) {
-    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, ev, record_mask);
-    return launch_forward_step_fp32(ctx, ev, record_mask);
+int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {
+    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, record_mask);
+    return launch_forward_step_fp32(ctx, record_mask);
 }
 
 }  // namespace da

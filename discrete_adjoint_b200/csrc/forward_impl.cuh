@@ -236,7 +236,7 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 // and its cached volume partial is reused (tile culling; off when cull == 0).  In an active tile,
 // inactive cells are copied and active ones get the full update.  The active words are cleared
 // here, and each processed tile records whether it holds a wet cell for the next k_coef.
-// RECORD: sets bit 2 of mask for cells whose depth was clamped at zero.
+// RECORD: sets bit 3 of mask for the active cells and bit 2 for those whose depth was clamped.
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
                                                    const R *__restrict__ kact, unsigned *__restrict__ active,
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
             R st[3] = {prev[0], prev[1], prev[2]};
             if (word & (1u << lane)) {
                 const bool clamped = update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
-                if (RECORD && clamped) mask[i] |= uint8_t(4);
+                if (RECORD) mask[i] |= uint8_t(clamped ? 4 + 8 : 8);  // bit 3: active this step
             }
             if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
             O.h[i] = st[0];
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
 }
 
 template <class R>
-int launch_step_t(da_ctx *ctx, cudaEvent_t *ev = nullptr, uint8_t *record_mask = nullptr) {
+int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
     const MeshArgs m = mesh_args(ctx);
     const int c = ctx->cur, o = 1 - c;
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
@@ -307,21 +307,25 @@ int launch_step_t(da_ctx *ctx, cudaEvent_t *ev = nullptr, uint8_t *record_mask =
     const int tiles = ctx->ntiles, grid = ctx->nblocks, cull = ctx->p.tile_culling;
     if (record_mask) {
         // branch recording for the adjoint: full sweep, codes for every cell
+        trace_begin(ctx, TR_COEF_REC);
         k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, 0, ctx->mc,
                                                           ctx->tc, ctx->dsc, record_mask);
+        trace_end(ctx);
+        trace_begin(ctx, TR_UPDATE_REC);
         k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
                                                             ctx->tile_vol, tiles, 0, ctx->mc, ctx->dsc, ctx->vol_part,
                                                             record_mask);
-        ctx->cur = o;
-        return cuda_check(ctx, cudaGetLastError(), "forward step launch");
+        trace_end(ctx);
+    } else {
+        trace_begin(ctx, TR_COEF);
+        k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull, ctx->mc,
+                                                    ctx->tc, ctx->dsc);
+        trace_end(ctx);
+        trace_begin(ctx, TR_UPDATE);
+        k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
+                                                      ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part);
+        trace_end(ctx);
     }
-    if (ev) cudaEventRecord(ev[0], ctx->stream);
-    k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull, ctx->mc, ctx->tc,
-                                                ctx->dsc);
-    if (ev) cudaEventRecord(ev[1], ctx->stream);
-    k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                  ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part);
-    if (ev) cudaEventRecord(ev[2], ctx->stream);
     ctx->cur = o;
     return cuda_check(ctx, cudaGetLastError(), "forward step launch");
 }

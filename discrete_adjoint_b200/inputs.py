@@ -96,15 +96,20 @@ def workload1(seed: int = 0) -> Workload:
 
 
 def workload3(cells_per_side: int = 1024, seed: int = 0) -> Workload:
-    """The plane-and-runout terrain on 5 km x 5 km at uniform resolution (~1M cells)."""
+    """The plane-and-runout terrain (30 deg plane meeting a flat runout) on 5 km x 5 km at uniform
+    resolution (1024^2 ~ 1M cells, 4.9 m), the 30 m x 100 m paraboloid pile 300 m downslope of the
+    top, phi_bed 20, phi_int 30; 512 steps; J = sum of h^2 dx dy over a 500 m x 500 m box."""
     L = 5000.0
     dem = inclined_plane(L, L, 5.0, 30.0, 3000.0)
-    piles = [Pile(750.0, 2500.0, 30.0, 250.0, 250.0)]
+    piles = [Pile(300.0, 2500.0, 30.0, 100.0, 100.0)]
     base = cells_per_side // 16
     spec = MeshSpec(xmin=0.0, ymin=0.0, dx0=L / base, dy0=L / base, nx0=base, ny0=base, max_level=4, uniform=True)
     mesh = Mesh.build(spec, dem, piles)
-    return Workload(f"inclined-plane 5km x 5km uniform {cells_per_side}^2", mesh,
+    return Workload(f"inclined-plane 5km x 5km uniform {cells_per_side}^2, 1 pile", mesh,
                     MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 512)
+
+
+WORKLOAD3_BOX = (350.0, 850.0, 2250.0, 2750.0)
 
 
 def test_case(seed: int = 1, nx0: int = 24, ny0: int = 16, max_level: int = 2, random_frac: float = 0.35,

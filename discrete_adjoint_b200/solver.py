@@ -162,6 +162,19 @@ class GeoflowContext:
         self._check(self.lib.da_forward_run_timed(self.ctx, nsteps, C.byref(s), C.byref(ms)), "da_forward_run_timed")
         return StepStats(s.dt, s.time, s.volume, s.hmax, s.iter), ms.value
 
+    def set_tracing(self, on: bool):
+        self._check(self.lib.da_set_tracing(self.ctx, int(on)), "da_set_tracing")
+
+    def trace(self) -> dict:
+        """{kernel: (total device ms, launches)} since tracing was switched on."""
+        out = {}
+        for k in range(9):
+            ms, n = C.c_double(), C.c_int64()
+            self._check(self.lib.da_trace_read(self.ctx, k, C.byref(ms), C.byref(n)), "da_trace_read")
+            if n.value:
+                out[self.lib.da_trace_name(k).decode()] = (ms.value, n.value)
+        return out
+
     def profile(self, nsteps: int) -> dict:
         """Mean device ms per forward kernel over nsteps (events around every launch)."""
         out = np.zeros(2)
@@ -178,12 +191,13 @@ class Gradient:
     dJ_dpile: list
     forward_steps: int
     snapshots: int
+    device_ms: float = 0.0
     lambda0: np.ndarray | None = None
 
 
 def _grad(g: _ffi.da_gradient, n_mat: int, n_piles: int, lam0=None) -> Gradient:
     return Gradient(g.J, list(g.dJ_dbedfrict[:n_mat]), g.dJ_dintfrict, list(g.dJ_dpile[:n_piles]),
-                    int(g.forward_steps), int(g.snapshots), lam0)
+                    int(g.forward_steps), int(g.snapshots), float(g.device_ms), lam0)
 
 
 def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpile=None,

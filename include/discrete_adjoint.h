@@ -166,6 +166,7 @@ typedef struct da_gradient {
     int64_t forward_steps;                /* forward steps executed, recomputation included */
     int32_t snapshots;                    /* checkpoints held */
     int32_t pad;
+    double device_ms;                     /* device time of the run (CUDA events on its stream) */
 } da_gradient;
 
 /* Runs nsteps forward steps from the context's current state and time, then the adjoint back to
@@ -189,6 +190,14 @@ int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0);
  * the names in kernel order through da_forward_kernel_name().  The state advances. */
 int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms);
 const char *da_forward_kernel_name(int32_t k);
+/* Tracing of every launch of the step and the adjoint (forward runs then skip CUDA graphs):
+ * on != 0 starts it with cleared sums, 0 stops it.  da_trace_read returns, for kernel kind k in
+ * [0, DA_TRACE_KINDS), the summed device time in ms and the number of launches; da_trace_name
+ * names the kind. */
+#define DA_TRACE_KINDS 9
+int da_set_tracing(da_ctx *ctx, int32_t on);
+int da_trace_read(da_ctx *ctx, int32_t k, double *total_ms, int64_t *launches);
+const char *da_trace_name(int32_t k);
 
 /* ---- one step without any device allocation ------------------------------------------------
  * No counterpart in the reference: an addition for callers that may not allocate device memory

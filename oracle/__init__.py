@@ -131,6 +131,10 @@ def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf
         if r.returncode != 0:
             raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
         raw = open(fout, "rb").read()
+        step_seconds = float("nan")
+        for line in r.stderr.splitlines():
+            if line.startswith("ref_harness_step_seconds="):
+                step_seconds = float(line.split("=", 1)[1])
     magic, n2, ns = struct.unpack_from("<3i", raw, 0)
     assert magic == 0x314F4144 and n2 == n and ns == nsteps
     off = 12
@@ -143,7 +147,7 @@ def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf
         k += cnt
         return v
 
-    out = {"dt": take(nsteps), "time": float(take(1)[0])}
+    out = {"dt": take(nsteps), "time": float(take(1)[0]), "step_seconds": step_seconds}
     out["h"], out["hu"], out["hv"] = take(n), take(n), take(n)
     out["slopes"] = take(6 * n).reshape(6, n)
     out["kact"] = take(n)

@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cassert>
 #include <cmath>
 #include <cstdint>
@@ -258,6 +259,7 @@ int main(int argc, char **argv) {
     // ---- time loop of the driver (hpfem.C:222-357) with adaptation off
     std::vector<double> dts(nsteps);
     int order_flag = 1;
+    const auto t_start = std::chrono::steady_clock::now();
     for (int it = 0; it < nsteps; ++it) {
         if (timeprops.iter < 50)
             matprops.frict_tiny = 0.1;
@@ -267,6 +269,9 @@ int main(int argc, char **argv) {
              &outline, &discharge, 0);
         dts[it] = timeprops.dtime;
     }
+    const double step_seconds =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    std::fprintf(stderr, "ref_harness_step_seconds=%.9f\n", step_seconds);
 
     // ---- output in the flattened cell order
     FILE *o = std::fopen(argv[2], "wb");
