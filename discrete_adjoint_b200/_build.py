@@ -30,6 +30,7 @@ UNITS = [
     ("adjoint_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
     ("adjoint_host.cu", []),
     ("noalloc.cu", ["--fmad=false"]),
+    ("snapshot.cu", []),
     ("mesh_host.cpp", []),
 ]
 

@@ -100,43 +100,16 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
     }
     while ((int)ctx->snaps.size() < nsnap && !st) {
         void *p = nullptr;
-        st = cuda_check(ctx, cudaMalloc(&p, rs * 3 * n + sizeof(DevScalars)), "cudaMalloc(snapshot)");
+        st = cuda_check(ctx, cudaMalloc(&p, snapshot_bytes(ctx)), "cudaMalloc(snapshot)");
         if (!st) ctx->snaps.push_back(p);
     }
     return st;
 }
 
-// snapshot layout: [3][n] state of R, then a DevScalars (time, iter, ...)
-int store(da_ctx *ctx, int slot) {
-    const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
-    char *base = (char *)ctx->snaps[slot];
-    int st = DA_OK;
-    trace_begin(ctx, TR_SNAPSHOT);
-    for (int v = 0; v < 3 && !st; ++v)
-        st = cuda_check(ctx, cudaMemcpyAsync(base + v * rs * n, ctx->U[ctx->cur][v], rs * n, cudaMemcpyDeviceToDevice,
-                                             ctx->stream), "snapshot store");
-    if (!st)
-        st = cuda_check(ctx, cudaMemcpyAsync(base + 3 * rs * n, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
-                                             ctx->stream), "snapshot store");
-    trace_end(ctx);
-    return st;
-}
-
-int restore(da_ctx *ctx, int slot) {
-    const size_t n = (size_t)ctx->mesh.n, rs = rsize(ctx);
-    char *base = (char *)ctx->snaps[slot];
-    int st = DA_OK;
-    trace_begin(ctx, TR_SNAPSHOT);
-    for (int v = 0; v < 3 && !st; ++v)
-        st = cuda_check(ctx, cudaMemcpyAsync(ctx->U[ctx->cur][v], base + v * rs * n, rs * n, cudaMemcpyDeviceToDevice,
-                                             ctx->stream), "snapshot restore");
-    if (!st)
-        st = cuda_check(ctx, cudaMemcpyAsync(ctx->dsc, base + 3 * rs * n, sizeof(DevScalars), cudaMemcpyDeviceToDevice,
-                                             ctx->stream), "snapshot restore");
-    trace_end(ctx);
-    if (!st) st = forward_state_changed(ctx);
-    return st;
-}
+// One launch each (csrc/snapshot.cu): the state, the tile wet flags and the step scalars; a
+// restore fills both state buffers so that tile culling stays valid.
+int store(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], true); }
+int restore(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], false); }
 
 struct Schedule {
     int N = 0, C = 0;
@@ -344,6 +317,8 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
             }
         }
     }
+    // the caller's lambda differs from buffer 1 everywhere
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream), "memset");
     if (!st) st = store(ctx, 0);
     if (!st) st = launch_forward_step(ctx, ctx->mask);
     if (!st) st = launch_adjoint_step(ctx, 0, 1, sec2, cos_int);

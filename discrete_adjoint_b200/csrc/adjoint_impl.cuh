@@ -30,7 +30,7 @@ namespace {
 
 using namespace fv;
 
-constexpr int kBlock = 256;
+constexpr int kBlock = kTileCells;  // one thread per cell of a tile
 
 // k act/pass of a recorded code (0 rest, 1..3 sgn(vel) = -1, 0, +1)
 template <class R>
@@ -38,12 +38,19 @@ __device__ __forceinline__ R kact_of(const MatConsts &mc, int mat, uint8_t code)
     return code == 0 ? R(mc.kact_rest) : R(mc.kact_sgn[mat][code - 1]);
 }
 
+// Mask byte of cell i in the current recording step: tiles the step did not list count as zero.
+__device__ __forceinline__ uint8_t mask_of(const uint8_t *__restrict__ mask, const int *__restrict__ epoch, int rec_id,
+                                           int i) {
+    return epoch[i >> 8] == rec_id ? mask[i] : uint8_t(0);
+}
+
 template <class R>
-__device__ __forceinline__ void lam_eff(const StateRef<R> &L, const uint8_t *__restrict__ mask, int i, R out[3]) {
-    out[0] = (mask[i] & 4) ? R(0) : L.h[i];
+__device__ __forceinline__ void lam_eff(const StateRef<R> &L, uint8_t mk, int i, R out[3]) {
+    out[0] = (mk & 4) ? R(0) : L.h[i];
     out[1] = L.hu[i];
     out[2] = L.hv[i];
 }
+
 
 // Derivative data of the limited depth slope in one direction (Element::get_slopes for j = 0):
 // slope = fac * min(gamma|dp|, gamma|dm|, |dc|); g_dp, g_dm = d slope / d dp, d dm.
@@ -228,6 +235,11 @@ __device__ __forceinline__ void riemann_adj(int dir, const Side<R> &L, const Sid
 
 struct AdjArgs {
     const uint8_t *__restrict__ mask;   // branch codes of the replayed forward step
+    const int *__restrict__ tile_epoch; // recording step that last listed each tile
+    const uint8_t *__restrict__ tile_act;
+    uint8_t *__restrict__ lam_clean;    // both adjoint buffers hold the same tile
+    int rec_id;
+    int ntiles;
     double *__restrict__ A;             // [3][n] source adjoint of each cell (FP64)
     double *__restrict__ B;             // [4][n] slope coefficients per side
     double *__restrict__ gbed;          // [n] running d J / d phi_bed of each cell (its material)
@@ -246,9 +258,17 @@ __device__ __forceinline__ double dk_of(const double *tab, int mat, uint8_t code
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, MatConsts mc,
                                                     AdjArgs aa, const DevScalars *__restrict__ sc, R sign_floor) {
+    __shared__ int list[kBlock];
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+    for (int round = 0; sched_more(round, aa.ntiles); ++round) {
+      const int tq = sched_tile(round);
+      // a wet cell is active, so its tile was listed by the recording step and had an active cell
+      const bool need = tq < aa.ntiles && aa.tile_epoch[tq] == aa.rec_id && aa.tile_act[tq];
+      const int cnt = compact_tiles(need, tq, list);
+      for (int q = 0; q < cnt; ++q) {
+        const int i = list[q] * kBlock + threadIdx.x;
+        if (i >= m.n) continue;
         double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
         const R h_i = U.h[i];
         // A and B exist for wet cells only; k_adj_gather reads them only there
@@ -256,12 +276,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
         const R prev[3] = {h_i, U.hu[i], U.hv[i]};
         {
             R le[3];
-            lam_eff<R>(Lnext, aa.mask, i, le);
+            const uint8_t mi = aa.mask[i];
+            lam_eff<R>(Lnext, mi, i, le);
             const R nu_u = dt * le[1], nu_v = dt * le[2];
             if (nu_u != R(0) || nu_v != R(0)) {
                 const uint8_t bf = m.bflag[i];
                 const int mat = m.mat[i];
-                const uint8_t code = aa.mask[i] & 3;
+                const uint8_t code = mi & 3;
                 const R k = kact_of<R>(mc, mat, code);
                 R s[6];
                 cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
@@ -319,6 +340,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
         aa.A[(size_t)2 * m.n + i] = A[2];
 #pragma unroll
         for (int s = 0; s < 4; ++s) aa.B[(size_t)s * m.n + i] = B[s];
+      }
     }
 }
 
@@ -335,10 +357,10 @@ __device__ __forceinline__ R side_weight(const MeshArgs &m, int c, uint8_t bf, i
 }
 
 template <class R>
-__device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &U, const MatConsts &mc,
-                                          const uint8_t *__restrict__ mask, int c, int dir, Side<R> &s) {
+__device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &U, const MatConsts &mc, uint8_t mk,
+                                          int c, int dir, Side<R> &s) {
     const R h = U.h[c];
-    const R k = h >= R(DA_TINY) ? kact_of<R>(mc, m.mat[c], mask[c] & 3) : R(0);
+    const R k = h >= R(DA_TINY) ? kact_of<R>(mc, m.mat[c], mk & 3) : R(0);
     make_side<R>(dir, h, U.hu[c], U.hv[c], k, grav<R>(m, 2, c), s);
 }
 
@@ -346,9 +368,20 @@ __device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, StateOut<R> Lout,
                                                        MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
+    __shared__ int list[kBlock];
     const R dt = R(sc->dt);
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m.n; j += gridDim.x * blockDim.x) {
-        const uint8_t mj = aa.mask[j];
+    for (int round = 0; sched_more(round, aa.ntiles); ++round) {
+      const int tq = sched_tile(round);
+      bool need = false;
+      if (tq < aa.ntiles) need = (aa.tile_epoch[tq] == aa.rec_id && aa.tile_act[tq]) || !aa.lam_clean[tq];
+      const int cnt = compact_tiles(need, tq, list);
+      for (int q = 0; q < cnt; ++q) {
+        const int t = list[q];
+        const bool tile_active = aa.tile_epoch[t] == aa.rec_id && aa.tile_act[t];
+        if (threadIdx.x == 0) aa.lam_clean[t] = tile_active ? 0 : 1;
+        const int j = t * kBlock + threadIdx.x;
+        if (j >= m.n) continue;
+        const uint8_t mj = tile_active ? aa.mask[j] : uint8_t(0);
         if (!(mj & 8)) {
             // not active in the forward step: its update was the identity, and no neighbour is wet
             Lout.h[j] = Lnext.h[j];
@@ -357,7 +390,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
             continue;
         }
         R lj[3];
-        lam_eff<R>(Lnext, aa.mask, j, lj);
+        lam_eff<R>(Lnext, mj, j, lj);
         double out[3] = {double(lj[0]), double(lj[1]), double(lj[2])};
         const R h_j = U.h[j];
         if (h_j > R(DA_TINY)) {
@@ -373,8 +406,8 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
             const int d = s & 1;
             const bool plus = s < 2;
             const int ne = (bf & (0x10 << s)) ? 2 : 1;
-            for (int q = 0; q < ne; ++q) {
-                const int k = m.nbr[(size_t)(s + 4 * q) * m.n + j];
+            for (int qq = 0; qq < ne; ++qq) {
+                const int k = m.nbr[(size_t)(s + 4 * qq) * m.n + j];
                 const uint8_t bk = m.bflag[k];
                 const R h_k = U.h[k];
                 if (h_k > R(DA_TINY)) {
@@ -387,13 +420,14 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
                 const R wj = side_weight<R>(m, j, bf, s, dt);
                 const R wk = side_weight<R>(m, k, bk, s ^ 2, dt);
                 if (wj == R(0) && wk == R(0)) continue;
+                const uint8_t mk = mask_of(aa.mask, aa.tile_epoch, aa.rec_id, k);
                 R lk[3];
-                lam_eff<R>(Lnext, aa.mask, k, lk);
+                lam_eff<R>(Lnext, mk, k, lk);
                 const R mu[3] = {wj * lj[0] + wk * lk[0], wj * lj[1] + wk * lk[1], wj * lj[2] + wk * lk[2]};
                 if (mu[0] == R(0) && mu[1] == R(0) && mu[2] == R(0)) continue;
                 Side<R> sj, sk;
-                load_side<R>(m, U, mc, aa.mask, j, d, sj);
-                load_side<R>(m, U, mc, aa.mask, k, d, sk);
+                load_side<R>(m, U, mc, mj, j, d, sj);
+                load_side<R>(m, U, mc, mk, k, d, sk);
                 R gL[3], gR[3], gkL, gkR;
                 if (plus) {
                     riemann_adj<R>(d, sj, sk, mu, gL, gR, gkL, gkR);
@@ -410,11 +444,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
         Lout.hu[j] = R(out[1]);
         Lout.hv[j] = R(out[2]);
         if (dJ_dkj != 0.0) {
-            const uint8_t code = aa.mask[j] & 3;
+            const uint8_t code = mj & 3;
             const int mat = m.mat[j];
             aa.gbed[j] += dJ_dkj * dk_of(aa.dk_dbed, mat, code);
             aa.gint[j] += dJ_dkj * dk_of(aa.dk_dint, mat, code);
         }
+      }
     }
 }
 

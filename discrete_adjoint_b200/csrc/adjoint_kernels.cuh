@@ -10,6 +10,11 @@ template <class R>
 AdjArgs adj_args(da_ctx *ctx, const double *sec2, double cos_int) {
     AdjArgs a;
     a.mask = ctx->mask;
+    a.tile_epoch = ctx->tile_epoch;
+    a.tile_act = ctx->tile_act;
+    a.lam_clean = ctx->lam_clean;
+    a.rec_id = ctx->rec_id;
+    a.ntiles = ctx->ntiles;
     a.A = ctx->adjA;
     a.B = ctx->adjB;
     a.gbed = ctx->gbed;
@@ -47,6 +52,8 @@ int seed_t(da_ctx *ctx, int lam_out, const double box[4]) {
     const int c = ctx->cur;
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
+    // lambda^N is written everywhere: the two adjoint buffers differ on every tile
+    cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream);
     trace_begin(ctx, TR_ADJ_SEED);
     k_adj_seed<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, Lo, box[0], box[1], box[2], box[3], ctx->seed_part,
                                                              ctx->seed_J, ctx->seed_counter);

@@ -131,6 +131,9 @@ static void free_state(da_ctx *ctx) {
     dfree(ctx->active);
     dfree(ctx->clean);
     dfree(ctx->tile_wet);
+    dfree(ctx->tile_epoch);
+    dfree(ctx->tile_act);
+    dfree(ctx->lam_clean);
     ctx->have_state = false;
 }
 

@@ -109,6 +109,10 @@ struct da_ctx {
     unsigned *active = nullptr;      // [ceil(n/32)] bit per cell: wet or next to a wet cell
     uint8_t *clean = nullptr;        // [ntiles] 1 when both state buffers hold the same tile
     uint8_t *tile_wet = nullptr;     // [ntiles] 1 when the tile held a wet cell after the last update
+    int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
+    uint8_t *tile_act = nullptr;     // [ntiles] the tile had an active cell in that step
+    uint8_t *lam_clean = nullptr;    // [ntiles] both adjoint buffers hold the same tile
+    int rec_id = 0;                  // id of the current recording step
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the persistent step kernels
     int sm_count = 0;
@@ -158,6 +162,9 @@ int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2
 int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
 int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
 int forward_state_changed(da_ctx *ctx);
+// snapshot.cu
+size_t snapshot_bytes(const da_ctx *ctx);
+int launch_snapshot(da_ctx *ctx, void *slot, bool store);
 void forward_free(da_ctx *ctx);
 
 }  // namespace da

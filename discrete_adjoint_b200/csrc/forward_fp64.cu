@@ -26,6 +26,11 @@ int forward_alloc(da_ctx *ctx) {
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->vol_part, sizeof(double) * ctx->nblocks), "cudaMalloc(vol)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_wet, ctx->ntiles), "cudaMalloc(tile_wet)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_epoch, sizeof(int) * ctx->ntiles), "cudaMalloc(epoch)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_epoch, 0xff, sizeof(int) * ctx->ntiles, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_act, ctx->ntiles), "cudaMalloc(tile_act)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->lam_clean, ctx->ntiles), "cudaMalloc(lam_clean)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream), "memset");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_vol, sizeof(double) * ctx->ntiles), "cudaMalloc(vol)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->active, sizeof(unsigned) * words), "cudaMalloc(active)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * words, ctx->stream), "memset");

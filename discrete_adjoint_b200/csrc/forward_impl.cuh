@@ -27,7 +27,7 @@ namespace {  // internal linkage: each precision TU keeps its own copy
 
 using namespace fv;
 
-constexpr int kBlock = 256;
+constexpr int kBlock = kTileCells;  // one thread per cell of a tile
 
 // dt from the reduced CFL bound and hmax (get_coef_and_eigen.C:168-179 with the single-rank
 // MPI_Allreduce(MIN)), then TimeProps::incrtime.  frict_tiny follows hpfem.C:232-235 with the
@@ -72,67 +72,72 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
     return last;
 }
 
+
 // ----------------------------------------------------------------------------- k_coef
-// Persistent grid-stride loop over tiles of kBlock cells, one thread per cell.  With tile
-// culling, a tile that held no wet cell after the last update is skipped (its depths cannot have
-// changed since).  Wet cells (h >= GEOFLOW_TINY) mark themselves and their face neighbours in
-// the active bitmask that k_update reads: a cell outside that set has zero fluxes and no
-// sources this step.
-// RECORD: also writes the branch code of every cell into mask (0 dry / at rest, 1..3 for
-// sgn(vel) = -1, 0, +1 of gmfggetcoef) for the adjoint's replay; tile culling must be off.
+// One thread per cell of each listed tile.  With tile culling, a tile that held no wet cell
+// after the last update is not listed (its depths cannot have changed since).  Wet cells
+// (h >= GEOFLOW_TINY) also mark themselves and their face neighbours in the active bitmask that
+// k_update reads: a cell outside that set has zero fluxes and no sources this step.
+// RECORD: also writes the branch code of every cell of a listed tile into mask (0 dry / at rest,
+// 1..3 for sgn(vel) = -1, 0, +1 of gmfggetcoef) for the adjoint's replay.
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
                                                  unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
                                                  int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
                                                  uint8_t *__restrict__ mask = nullptr) {
+    __shared__ int list[kBlock];
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (cull && !tile_wet[t]) continue;
-        const int i = t * kBlock + threadIdx.x;
-        bool wet = false;
-        if (i < m.n) {
-            const R h = U.h[i];
-            if (!(h == h)) raise_err(sc, DA_ERR_NAN);
-            wet = h >= R(DA_TINY);
-            uint8_t code = 0;
-            if (wet) {
-                const uint8_t bf = m.bflag[i];
+    for (int round = 0; sched_more(round, ntiles); ++round) {
+        const int tq = sched_tile(round);
+        const bool need = tq < ntiles && (!cull || tile_wet[tq]);
+        const int cnt = compact_tiles(need, tq, list);
+        for (int q = 0; q < cnt; ++q) {
+            const int i = list[q] * kBlock + threadIdx.x;
+            bool wet = false;
+            if (i < m.n) {
+                const R h = U.h[i];
+                if (!(h == h)) raise_err(sc, DA_ERR_NAN);
+                wet = h >= R(DA_TINY);
+                uint8_t code = 0;
+                if (wet) {
+                    const uint8_t bf = m.bflag[i];
 #pragma unroll
-                for (int s = 0; s < 4; ++s) {
-                    if (bf & (1 << s)) continue;
-                    const int e = m.nbr[(size_t)s * m.n + i];
-                    atomicOr(&active[e >> 5], 1u << (e & 31));
-                    if (bf & (0x10 << s)) {
-                        const int e2 = m.nbr[(size_t)(s + 4) * m.n + i];
-                        atomicOr(&active[e2 >> 5], 1u << (e2 & 31));
+                    for (int s = 0; s < 4; ++s) {
+                        if (bf & (1 << s)) continue;
+                        const int e = m.nbr[(size_t)s * m.n + i];
+                        atomicOr(&active[e >> 5], 1u << (e & 31));
+                        if (bf & (0x10 << s)) {
+                            const int e2 = m.nbr[(size_t)(s + 4) * m.n + i];
+                            atomicOr(&active[e2 >> 5], 1u << (e2 & 31));
+                        }
+                    }
+                    if (!(h > R(DA_TINY))) {  // h == GEOFLOW_TINY: dry for get_coef_and_eigen, wet for the fluxes
+                        kact[i] = R(mc.kact_rest);
+                    } else {
+                        const R ui[3] = {h, U.hu[i], U.hv[i]};
+                        R s[6];
+                        cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
+                        const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
+                        kact[i] = k;
+                        const R gz = grav<R>(m, 2, i);
+                        const R vx = ui[1] / h, vy = ui[2] / h;
+                        const R c = sqrt(k * gz * h);
+                        const R evx = dabs(vx) + c, evy = dabs(vy) + c;
+                        const R ev = evx > evy ? evx : evy;
+                        if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
+                        const R dxm = cell_dx<R>(m, i), dym = cell_dy<R>(m, i);
+                        const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
+                        const unsigned long long hb = __double_as_longlong(double(h));
+                        my_min = rb < my_min ? rb : my_min;
+                        my_max = hb > my_max ? hb : my_max;
                     }
                 }
-                if (!(h > R(DA_TINY))) {  // h == GEOFLOW_TINY: dry for get_coef_and_eigen, wet for the fluxes
-                    kact[i] = R(mc.kact_rest);
-                } else {
-                    const R ui[3] = {h, U.hu[i], U.hv[i]};
-                    R s[6];
-                    cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
-                    const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
-                    kact[i] = k;
-                    const R gz = grav<R>(m, 2, i);
-                    const R vx = ui[1] / h, vy = ui[2] / h;
-                    const R c = sqrt(k * gz * h);
-                    const R evx = dabs(vx) + c, evy = dabs(vy) + c;
-                    const R ev = evx > evy ? evx : evy;
-                    if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
-                    const R dxm = cell_dx<R>(m, i), dym = cell_dy<R>(m, i);
-                    const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
-                    const unsigned long long hb = __double_as_longlong(double(h));
-                    my_min = rb < my_min ? rb : my_min;
-                    my_max = hb > my_max ? hb : my_max;
-                }
+                if (RECORD) mask[i] = code;
             }
-            if (RECORD) mask[i] = code;
+            const unsigned self = __ballot_sync(0xffffffffu, wet);
+            if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
         }
-        const unsigned self = __ballot_sync(0xffffffffu, wet);
-        if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
     }
     my_min = warp_min_u64(my_min);
     my_max = warp_max_u64(my_max);
@@ -231,64 +236,83 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // ---------------------------------------------------------------------------- k_update
-// Persistent grid-stride loop over tiles of kBlock consecutive cells.  A tile with no active
-// cell is copied; when both ping-pong buffers already hold it (clean) it is not touched at all
-// and its cached volume partial is reused (tile culling; off when cull == 0).  In an active tile,
-// inactive cells are copied and active ones get the full update.  The active words are cleared
-// here, and each processed tile records whether it holds a wet cell for the next k_coef.
-// RECORD: sets bit 3 of mask for the active cells and bit 2 for those whose depth was clamped.
+// Tiles of kBlock consecutive cells through the strided tile list.  A tile is listed when it has
+// an active cell, or when its two ping-pong buffers differ (not clean), or when culling is off.
+// In a listed tile, active cells get the full update and the others are copied (their update is
+// the identity).  A tile that is not listed is already identical in both buffers.  Each listed
+// tile stores its volume partial, its clean flag and whether it now holds a wet cell; the last
+// block sums every tile's partial in tile order, so the volume does not depend on culling.
+// RECORD: every cell of a listed tile gets its full mask byte (the k_coef code of a wet cell,
+// bit 3 active, bit 2 depth clamped) and the tile records the step id (tile_epoch) and whether
+// it had an active cell (tile_act); masks of tiles with another epoch count as zero.
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
                                                    const R *__restrict__ kact, unsigned *__restrict__ active,
                                                    uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
                                                    double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
                                                    DevScalars *sc, double *__restrict__ vol_part,
-                                                   uint8_t *__restrict__ mask = nullptr) {
+                                                   uint8_t *__restrict__ mask = nullptr, int *__restrict__ tile_epoch = nullptr,
+                                                   uint8_t *__restrict__ tile_act = nullptr, int rec_id = 0) {
     __shared__ double red[kBlock / 32];
+    __shared__ int list[kBlock];
     const int lane = threadIdx.x & 31;
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
-    double vol_acc = 0.0;  // thread 0: this block's tiles, in tile order
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int i = t * kBlock + threadIdx.x;
-        const unsigned word = (i < m.n) ? active[i >> 5] : 0u;
-        const bool tile_active = __syncthreads_or(word != 0u);
-        if (!tile_active && cull && clean[t]) {
-            if (threadIdx.x == 0) vol_acc += tile_vol[t];
-            continue;
-        }
-        double vol = 0.0;
-        bool wet_after = false;
-        if (i < m.n) {
-            const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
-            const R dxc = cell_dx<R>(m, i), dyc = cell_dy<R>(m, i);
-            R st[3] = {prev[0], prev[1], prev[2]};
-            if (word & (1u << lane)) {
-                const bool clamped = update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
-                if (RECORD) mask[i] |= uint8_t(clamped ? 4 + 8 : 8);  // bit 3: active this step
+    for (int round = 0; sched_more(round, ntiles); ++round) {
+        const int tq = sched_tile(round);
+        bool need = false;
+        if (tq < ntiles) {
+            need = !cull || !clean[tq];
+            if (!need) {
+                const int w0 = tq * (kBlock / 32);
+                const int nw = (m.n + 31) / 32;
+                for (int w = 0; w < kBlock / 32 && !need; ++w)
+                    if (w0 + w < nw && active[w0 + w]) need = true;
             }
-            if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
-            O.h[i] = st[0];
-            O.hu[i] = st[1];
-            O.hv[i] = st[2];
-            vol = double(dxc) * double(dyc) * double(st[0]);
-            wet_after = st[0] >= R(DA_TINY);
         }
-        __syncwarp();
-        if (lane == 0 && word) active[i >> 5] = 0u;
-        const bool any_wet = __syncthreads_or(wet_after);
-        const double tv = block_sum(vol, red);
-        if (threadIdx.x == 0) {
-            tile_vol[t] = tv;
-            vol_acc += tv;
-            clean[t] = tile_active ? 0 : 1;
-            tile_wet[t] = any_wet ? 1 : 0;
+        const int cnt = compact_tiles(need, tq, list);
+        for (int q = 0; q < cnt; ++q) {
+            const int t = list[q];
+            const int i = t * kBlock + threadIdx.x;
+            const unsigned word = (i < m.n) ? active[i >> 5] : 0u;
+            const bool tile_active = __syncthreads_or(word != 0u);
+            double vol = 0.0;
+            bool wet_after = false;
+            if (i < m.n) {
+                const R prev[3] = {U.h[i], U.hu[i], U.hv[i]};
+                const R dxc = cell_dx<R>(m, i), dyc = cell_dy<R>(m, i);
+                R st[3] = {prev[0], prev[1], prev[2]};
+                const bool act = word & (1u << lane);
+                bool clamped = false;
+                if (act) clamped = update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
+                if (RECORD)
+                    mask[i] = uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0));
+                if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
+                O.h[i] = st[0];
+                O.hu[i] = st[1];
+                O.hv[i] = st[2];
+                vol = double(dxc) * double(dyc) * double(st[0]);
+                wet_after = st[0] >= R(DA_TINY);
+            }
+            __syncwarp();
+            if (lane == 0 && word) active[i >> 5] = 0u;
+            const bool any_wet = __syncthreads_or(wet_after);
+            const double tv = block_sum(vol, red);
+            if (threadIdx.x == 0) {
+                tile_vol[t] = tv;
+                clean[t] = tile_active ? 0 : 1;
+                tile_wet[t] = any_wet ? 1 : 0;
+                if (RECORD) {
+                    tile_epoch[t] = rec_id;
+                    tile_act[t] = tile_active ? 1 : 0;
+                }
+            }
         }
     }
-    if (threadIdx.x == 0) vol_part[blockIdx.x] = vol_acc;
+    (void)vol_part;
     if (last_block(&sc->blocks_done[1])) {
         double t = 0.0;
-        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x) t += ((volatile double *)vol_part)[b];
+        for (int b = threadIdx.x; b < ntiles; b += blockDim.x) t += ((volatile double *)tile_vol)[b];
         t = block_sum(t, red);
         if (threadIdx.x == 0) {
             sc->volume = t;
@@ -306,15 +330,16 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
     R *kact = (R *)ctx->kact;
     const int tiles = ctx->ntiles, grid = ctx->nblocks, cull = ctx->p.tile_culling;
     if (record_mask) {
-        // branch recording for the adjoint: full sweep, codes for every cell
+        // branch recording for the adjoint: codes and flags for every cell of the listed tiles
+        ++ctx->rec_id;
         trace_begin(ctx, TR_COEF_REC);
-        k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, 0, ctx->mc,
-                                                          ctx->tc, ctx->dsc, record_mask);
+        k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull,
+                                                          ctx->mc, ctx->tc, ctx->dsc, record_mask);
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE_REC);
         k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                            ctx->tile_vol, tiles, 0, ctx->mc, ctx->dsc, ctx->vol_part,
-                                                            record_mask);
+                                                            ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part,
+                                                            record_mask, ctx->tile_epoch, ctx->tile_act, ctx->rec_id);
         trace_end(ctx);
     } else {
         trace_begin(ctx, TR_COEF);

@@ -318,5 +318,44 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 __device__ __forceinline__ void raise_err(DevScalars *sc, int code) { atomicCAS(&sc->err, 0, code); }
 
+// ------------------------------------------------------------------ tile scheduling
+// Cells are grouped in tiles of kTileCells consecutive (Morton-ordered) cells, one thread per
+// cell.  Round r of block b tests tiles (r * kTileCells + q) * gridDim.x + b, q = thread index:
+// consecutive tiles go to consecutive blocks, so the few wet tiles of a compact flow spread over
+// the grid instead of queueing in one block.  The tiles that need work are compacted into
+// shared memory (increasing order) and processed one after another by the whole block.
+constexpr int kTileCells = 256;
+
+__device__ __forceinline__ int sched_tile(int round) {
+    return (round * kTileCells + (int)threadIdx.x) * (int)gridDim.x + (int)blockIdx.x;
+}
+
+__device__ __forceinline__ bool sched_more(int round, int ntiles) {
+    return (long long)round * kTileCells * gridDim.x < ntiles;
+}
+
+// Needs blockDim.x == kTileCells; returns the number of tiles listed.
+__device__ __forceinline__ int compact_tiles(bool need, int tile, int *list) {
+    __shared__ int warp_count[kTileCells / 32];
+    __shared__ int total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned b = __ballot_sync(0xffffffffu, need);
+    if (lane == 0) warp_count[warp] = __popc(b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < kTileCells / 32; ++w) {
+            const int c = warp_count[w];
+            warp_count[w] = acc;
+            acc += c;
+        }
+        total = acc;
+    }
+    __syncthreads();
+    if (need) list[warp_count[warp] + __popc(b & ((1u << lane) - 1u))] = tile;
+    __syncthreads();
+    return total;
+}
+
 }  // namespace fv
 }  // namespace da
