@@ -26,7 +26,7 @@ UNITS = [
     ("capi.cu", []),
     ("forward_fp64.cu", ["--fmad=false"]),
     ("forward_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
-    ("adjoint_fp64.cu", []),
+    ("adjoint_fp64.cu", ["--fmad=false"]),
     ("adjoint_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
     ("adjoint_host.cu", []),
     ("noalloc.cu", ["--fmad=false"]),

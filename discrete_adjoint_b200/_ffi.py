@@ -55,7 +55,7 @@ class da_params(C.Structure):
         ("influx_dt", C.c_double),
         ("fp32_sign_floor", C.c_double),
         ("tile_culling", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("grid_blocks", C.c_int32),
     ]
 
 
@@ -70,6 +70,15 @@ class da_mesh_soa(C.Structure):
         ("curvature", PD),
         ("material", PI32),
     ]
+
+
+DA_TUNE_MAX = 8
+DA_TRACE_KINDS = 11
+
+
+class da_tune_result(C.Structure):
+    _fields_ = [("n", C.c_int32), ("best", C.c_int32), ("grid", C.c_int32 * DA_TUNE_MAX),
+                ("ms_per_step", C.c_double * DA_TUNE_MAX)]
 
 
 class da_step_stats(C.Structure):
@@ -178,6 +187,8 @@ SIGNATURES = {
     "da_set_tracing": (C.c_int, [C.c_void_p, C.c_int32]),
     "da_trace_read": (C.c_int, [C.c_void_p, C.c_int32, PD, C.POINTER(C.c_int64)]),
     "da_trace_name": (C.c_char_p, [C.c_int32]),
+    "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
+    "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
     "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,
                                 C.c_double, C.c_double, C.POINTER(C.POINTER(da_mesh_host))]),
     "da_mesh_free": (None, [C.POINTER(da_mesh_host)]),

@@ -27,6 +27,12 @@ int launch_adjoint_reduce_fp64(da_ctx *, int, int);
 int launch_adjoint_reduce_fp32(da_ctx *, int, int);
 int forward_state_changed(da_ctx *ctx);
 
+int launch_youturn_fp64(da_ctx *, int, int, const double *, double);
+int launch_youturn_fp32(da_ctx *, int, int, const double *, double);
+int launch_youturn(da_ctx *ctx, int a, int b, const double *sec2, double c) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_youturn_fp64(ctx, a, b, sec2, c)
+                                            : launch_youturn_fp32(ctx, a, b, sec2, c);
+}
 int launch_adjoint_step(da_ctx *ctx, int a, int b, const double *sec2, double c) {
     return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_step_fp64(ctx, a, b, sec2, c)
                                             : launch_adjoint_step_fp32(ctx, a, b, sec2, c);
@@ -75,13 +81,13 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
     if (ctx->adj_n != (int)n) {
         auto fr = [](void *p) { if (p) cudaFree(p); };
         fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
-        fr(ctx->red_out); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter);
+        fr(ctx->red_out); fr(ctx->red_part); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter);
         for (int b = 0; b < 2; ++b)
             for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
         for (void *s : ctx->snaps) fr(s);
         ctx->snaps.clear();
         ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
-        ctx->red_out = ctx->seed_part = ctx->seed_J = nullptr; ctx->seed_counter = nullptr;
+        ctx->red_out = ctx->red_part = ctx->seed_part = ctx->seed_J = nullptr; ctx->seed_counter = nullptr;
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->mask, n), "cudaMalloc(mask)");
         for (int b = 0; b < 2 && !st; ++b)
             for (int v = 0; v < 3 && !st; ++v) st = cuda_check(ctx, cudaMalloc(&ctx->lam[b][v], rs * n), "cudaMalloc(lam)");
@@ -91,6 +97,7 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->gint, sizeof(double) * n), "cudaMalloc(gint)");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->dk_tab, sizeof(double) * 2 * DA_MAX_MATERIALS * 3), "cudaMalloc");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_out, sizeof(double) * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_part, sizeof(double) * kAdjReduceParts * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES)), "cudaMalloc");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_part, sizeof(double) * ctx->nblocks), "cudaMalloc");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_J, sizeof(double)), "cudaMalloc");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_counter, sizeof(unsigned)), "cudaMalloc");
@@ -155,21 +162,33 @@ struct Runner {
     double sec2[DA_MAX_MATERIALS];
     double cos_int;
     long long fsteps = 0;
+    int pos = -1;  // step index of the live forward state; -1 = not a checkpointed state
 
+    // the live state is already the checkpoint right after a store: no copy back
+    int restore_at(int slot, int step) {
+        if (pos == step) return DA_OK;
+        pos = step;
+        return restore(ctx, slot);
+    }
     int advance(int k) {
-        int st = DA_OK;
-        for (int s = 0; s < k && !st; ++s) st = launch_forward_step(ctx);
+        const int st = launch_forward_steps(ctx, k);
         fsteps += k;
+        pos += k;
         return st;
     }
     int youturn() {
-        int st = launch_forward_step(ctx, ctx->mask);  // replay step n with its branch codes
+        int st = DA_OK;
         ++fsteps;
-        if (!st && !seeded) {
-            st = launch_adjoint_seed(ctx, lam_cur, box);  // U^N is the state just produced
+        pos = -1;  // past the step that is being taken back
+        if (!seeded) {
+            // the last step: replay, seed lambda^N from U^N (the state just produced), reverse
+            st = launch_forward_step(ctx, ctx->mask);
+            if (!st) st = launch_adjoint_seed(ctx, lam_cur, box);
             seeded = true;
+            if (!st) st = launch_adjoint_step(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
+        } else {
+            st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
         }
-        if (!st) st = launch_adjoint_step(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
         lam_cur = 1 - lam_cur;
         return st;
     }
@@ -177,21 +196,21 @@ struct Runner {
         int st = DA_OK;
         const int l = b - a;
         if (l == 1) {
-            st = restore(ctx, slot_a);
+            st = restore_at(slot_a, a);
             if (!st) st = youturn();
             return st;
         }
         const int c = (int)free_slots.size() < sch.C ? (int)free_slots.size() : sch.C;
         if (c == 0) {
             for (int k = b - 1; k >= a && !st; --k) {
-                st = restore(ctx, slot_a);
+                st = restore_at(slot_a, a);
                 if (!st) st = advance(k - a);
                 if (!st) st = youturn();
             }
             return st;
         }
         const int m = a + sch.S(l, c);
-        st = restore(ctx, slot_a);
+        st = restore_at(slot_a, a);
         if (!st) st = advance(m - a);
         const int slot_m = free_slots.back();
         free_slots.pop_back();
@@ -245,8 +264,8 @@ int copy_lambda_out(da_ctx *ctx, int buf, double *host) {
     return st;
 }
 
-int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out) {
-    int st = launch_adjoint_reduce(ctx, lam0, n_piles);
+int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool reduced = false) {
+    int st = reduced ? DA_OK : launch_adjoint_reduce(ctx, lam0, n_piles);
     std::vector<double> red(DA_MAX_MATERIALS + 1 + DA_MAX_PILES, 0.0);
     const int nout = ctx->p.n_materials + 1 + n_piles;
     if (!st) st = cuda_check(ctx, cudaMemcpyAsync(red.data(), ctx->red_out, sizeof(double) * nout, cudaMemcpyDeviceToHost,
@@ -363,8 +382,10 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
     cudaEventCreate(&e1);
     cudaEventRecord(e0, ctx->stream);
     st = store(ctx, 0);
+    r.pos = 0;
     if (!st) st = r.reverse(0, nsteps, 0);
     if (!st) st = restore(ctx, 0);
+    if (!st) st = launch_adjoint_reduce(ctx, r.lam_cur, n_piles);  // the gradient sums are in the timed region
     cudaEventRecord(e1, ctx->stream);
     if (!st) st = sync_check(ctx);
     float dev_ms = 0.f;
@@ -373,7 +394,7 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
     cudaEventDestroy(e1);
     if (!st) st = trace_flush(ctx);
     if (!st && lambda0) st = copy_lambda_out(ctx, r.lam_cur, lambda0);
-    if (!st) st = fill_gradient(ctx, r.lam_cur, n_piles, out);
+    if (!st) st = fill_gradient(ctx, r.lam_cur, n_piles, out, /*reduced=*/true);
     if (!st && out) {
         out->forward_steps = r.fsteps;
         out->snapshots = nsnapshots;

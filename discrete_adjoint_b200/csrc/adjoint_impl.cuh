@@ -233,17 +233,19 @@ __device__ __forceinline__ void riemann_adj(int dir, const Side<R> &L, const Sid
     dirflux_adj<R>(dir, Rt, aur, afr, asr, gR, gkR);
 }
 
+// Arrays written and read within one launch of the fused step kernel carry no __restrict__
+// (coherent loads, no read-only cache).
 struct AdjArgs {
-    const uint8_t *__restrict__ mask;   // branch codes of the replayed forward step
-    const int *__restrict__ tile_epoch; // recording step that last listed each tile
-    const uint8_t *__restrict__ tile_act;
-    uint8_t *__restrict__ lam_clean;    // both adjoint buffers hold the same tile
+    const uint8_t *mask;                // branch codes of the replayed forward step
+    const int *tile_epoch;              // recording step that last listed each tile
+    const uint8_t *tile_act;
+    uint8_t *lam_clean;                 // both adjoint buffers hold the same tile
     int rec_id;
     int ntiles;
-    double *__restrict__ A;             // [3][n] source adjoint of each cell (FP64)
-    double *__restrict__ B;             // [4][n] slope coefficients per side
-    double *__restrict__ gbed;          // [n] running d J / d phi_bed of each cell (its material)
-    double *__restrict__ gint;          // [n] running d J / d phi_int of each cell
+    double *A;                          // [3][n] source adjoint of each cell (FP64)
+    double *B;                          // [4][n] slope coefficients per side
+    double *gbed;                       // [n] running d J / d phi_bed of each cell (its material)
+    double *gint;                       // [n] running d J / d phi_int of each cell
     const double *__restrict__ dk_dbed; // [DA_MAX_MATERIALS][3] d kact / d phi_bed per sgn branch
     const double *__restrict__ dk_dint; // [DA_MAX_MATERIALS][3]
     double sec2_bed[DA_MAX_MATERIALS];  // 1 + tan^2(phi_bed)
@@ -256,11 +258,8 @@ __device__ __forceinline__ double dk_of(const double *tab, int mat, uint8_t code
 
 // ------------------------------------------------------------------------- k_adj_src
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, MatConsts mc,
-                                                    AdjArgs aa, const DevScalars *__restrict__ sc, R sign_floor) {
-    __shared__ int list[kBlock];
-    const R dt = R(sc->dt);
-    const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
+__device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
+                                              const MatConsts &mc, const AdjArgs &aa, R dt, R ft, int *list) {
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       // a wet cell is active, so its tile was listed by the recording step and had an active cell
@@ -344,6 +343,15 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
     }
 }
 
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, MatConsts mc,
+                                                    AdjArgs aa, const DevScalars *__restrict__ sc, R sign_floor) {
+    __shared__ int list[kBlock];
+    const R dt = R(sc->dt);
+    const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
+    adj_src_phase<R>(m, U, Lnext, mc, aa, dt, ft, list);
+}
+
 // Flux weight of cell c for its side s: -dt/dx on a plus side, +dt/dx on a minus side, halved
 // when the side carries two finer neighbours, zero when c's direction has an outflow side.
 template <class R>
@@ -366,10 +374,9 @@ __device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &
 
 // ---------------------------------------------------------------------- k_adj_gather
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, StateOut<R> Lout,
-                                                       MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
-    __shared__ int list[kBlock];
-    const R dt = R(sc->dt);
+__device__ __forceinline__ void adj_gather_phase(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
+                                                 const StateOut<R> &Lout, const MatConsts &mc, const AdjArgs &aa, R dt,
+                                                 int *list) {
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       bool need = false;
@@ -453,6 +460,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U
     }
 }
 
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, StateOut<R> Lout,
+                                                       MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
+    __shared__ int list[kBlock];
+    adj_gather_phase<R>(m, U, Lnext, Lout, mc, aa, R(sc->dt), list);
+}
+
 // ------------------------------------------------------------------------ k_adj_seed
 // J = sum over cells with centre in the box of h^2 dx dy; lambda^N = dJ/dU^N.  FP64 partials per
 // block, summed in block order by the last block.
@@ -504,16 +518,22 @@ __global__ void __launch_bounds__(kBlock) k_adj_seed(MeshArgs m, StateRef<R> U, 
 }
 
 // Per-material sums of the running per-cell parameter sensitivities, plus the pile-height
-// products sum_i lambda_h,i dh0_i/dP_p.  One block per output, fixed order.
+// products sum_i lambda_h,i dh0_i/dP_p.  Two launches with a fixed order: block (b, o) sums
+// output o over the b-th of kReduceParts contiguous cell ranges, then one block per output adds
+// the parts in order.
+constexpr int kReduceParts = kAdjReduceParts;
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_adj_reduce(MeshArgs m, StateRef<R> L0, const double *__restrict__ gbed,
                                                        const double *__restrict__ gint,
                                                        const double *__restrict__ dh0, int n_mat, int n_piles,
-                                                       double *__restrict__ out) {
+                                                       double *__restrict__ part) {
     __shared__ double red[kBlock / 32];
-    const int o = blockIdx.x;  // 0..n_mat-1 bed per material, n_mat internal, then piles
+    const int o = blockIdx.y;  // 0..n_mat-1 bed per material, n_mat internal, then piles
+    const int per = (m.n + kReduceParts - 1) / kReduceParts;
+    const int i0 = blockIdx.x * per, i1 = min(m.n, i0 + per);
     double acc = 0.0;
-    for (int i = threadIdx.x; i < m.n; i += blockDim.x) {
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         if (o < n_mat) {
             if (m.mat[i] == o) acc += gbed[i];
         } else if (o == n_mat) {
@@ -528,7 +548,20 @@ __global__ void __launch_bounds__(kBlock) k_adj_reduce(MeshArgs m, StateRef<R> L
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < kBlock / 32; ++w) t += red[w];
-        out[o] = t;
+        part[(size_t)o * kReduceParts + blockIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kReduceParts) k_adj_reduce_final(const double *__restrict__ part,
+                                                                   double *__restrict__ out) {
+    __shared__ double red[kReduceParts / 32];
+    double v = warp_sum(part[(size_t)blockIdx.x * kReduceParts + threadIdx.x]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kReduceParts / 32; ++w) t += red[w];
+        out[blockIdx.x] = t;
     }
 }
 

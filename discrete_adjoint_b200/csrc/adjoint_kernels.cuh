@@ -1,6 +1,7 @@
 // Launchers of the adjoint kernels for one precision (included by adjoint_fp64.cu / _fp32.cu).
 #pragma once
 #include "adjoint_impl.cuh"
+#include "forward_impl.cuh"
 
 namespace da {
 namespace adj {
@@ -35,7 +36,7 @@ int step_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_
     StateRef<R> Ln{(const R *)ctx->lam[lam_in][0], (const R *)ctx->lam[lam_in][1], (const R *)ctx->lam[lam_in][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
     const AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
-    const int grid = ctx->nblocks;
+    const int grid = ctx->grid;
     const R floor = R(ctx->mc.sign_floor);
     trace_begin(ctx, TR_ADJ_SRC);
     k_adj_src<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, Ln, ctx->mc, aa, ctx->dsc, floor);
@@ -67,10 +68,105 @@ int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
     StateRef<R> L{(const R *)ctx->lam[lam0][0], (const R *)ctx->lam[lam0][1], (const R *)ctx->lam[lam0][2]};
     const int nout = ctx->p.n_materials + 1 + n_piles;
     trace_begin(ctx, TR_ADJ_REDUCE);
-    k_adj_reduce<R><<<nout, kBlock, 0, ctx->stream>>>(m, L, ctx->gbed, ctx->gint, ctx->dh0, ctx->p.n_materials, n_piles,
-                                                       ctx->red_out);
+    k_adj_reduce<R><<<dim3(kReduceParts, nout), kBlock, 0, ctx->stream>>>(m, L, ctx->gbed, ctx->gint, ctx->dh0,
+                                                                           ctx->p.n_materials, n_piles, ctx->red_part);
+    k_adj_reduce_final<<<nout, kReduceParts, 0, ctx->stream>>>(ctx->red_part, ctx->red_out);
     trace_end(ctx);
     return cuda_check(ctx, cudaGetLastError(), "adjoint reduce launch");
+}
+
+// ------------------------------------------------------------------------ k_youturn
+// One whole reverse step in one cooperative launch: the forward step of U^n replayed with its
+// branch codes recorded (coefficient phase, barrier, dt, update phase), a barrier, the source
+// adjoint, a barrier and the gather, i.e. the four launches of the separate path with grid
+// barriers instead of kernel boundaries.  U^n stays in buffer cur; U^{n+1} goes to cur ^ 1.
+// Block 0 writes the step's scalars and the volume at the end, as the separate kernels do.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
+                                                    uint8_t *clean, uint8_t *tile_wet, double *tile_vol, int ntiles,
+                                                    int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
+                                                    uint8_t *mask, int *tile_epoch, uint8_t *tile_act, int rec_id,
+                                                    StateRef<R> Ln, StateOut<R> Lo, AdjArgs aa) {
+    __shared__ double red[kBlock / 32];
+    __shared__ int list[kBlock];
+    const double time = sc->time;
+    const long long iter = sc->iter;
+    const StateRef<R> U{S.h[cur], S.hu[cur], S.hv[cur]};
+    const StateOut<R> O{S.h[cur ^ 1], S.hu[cur ^ 1], S.hv[cur ^ 1]};
+    unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
+    fwd::coef_phase<R, true>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
+    fwd::push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
+    if (!fwd::grid_sync(sc)) return;
+    const double min_dxe = __longlong_as_double(__ldcg(&sc->acc_min_dxe));
+    const double hmax = __longlong_as_double(__ldcg(&sc->acc_hmax));
+    double dt, ft;
+    fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+    const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
+    fwd::update_phase<R, true>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, R(dt), ftr, mask,
+                               tile_epoch, tile_act, rec_id, list, red);
+    if (!fwd::grid_sync(sc)) return;
+    adj_src_phase<R>(m, U, Ln, mc, aa, R(dt), ftr, list);
+    if (!fwd::grid_sync(sc)) return;
+    adj_gather_phase<R>(m, U, Ln, Lo, mc, aa, R(dt), list);
+    if (blockIdx.x == 0) {
+        const double v = fwd::volume_sum(tile_vol, ntiles, red);
+        if (threadIdx.x == 0) {
+            sc->volume = v;
+            sc->time = time + dt;
+            sc->iter = iter + 1;
+            sc->dt = dt;
+            sc->frict_tiny = ft;
+            sc->min_dxe = min_dxe;
+            sc->hmax = hmax;
+            sc->acc_min_dxe = fwd::kMinDxeStart;
+            sc->acc_hmax = 0ull;
+        }
+    }
+}
+
+// The live state is U^n in buffer cur; afterwards U^{n+1} is (cur flips) and lambda^n is in
+// lam_out.
+template <class R>
+int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int) {
+    const int pi = sizeof(R) == 8;
+    if (ctx->coop_cap_yt[pi] <= 0) {
+        int per_sm = 0;
+        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_youturn<R>, kBlock, 0),
+                            "occupancy");
+        if (st) return st;
+        ctx->coop_cap_yt[pi] = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
+    }
+    const int cap = ctx->coop_cap_yt[pi];
+    if (cap <= 0) return set_error(ctx, DA_ERR_UNSUPPORTED, "reverse-step kernel cannot be resident");
+    const int grid = ctx->grid < cap ? ctx->grid : cap;
+    ++ctx->rec_id;
+    MeshArgs m = mesh_args(ctx);
+    fwd::StatePair<R> S;
+    for (int b = 0; b < 2; ++b) {
+        S.h[b] = (R *)ctx->U[b][0];
+        S.hu[b] = (R *)ctx->U[b][1];
+        S.hv[b] = (R *)ctx->U[b][2];
+    }
+    int cur = ctx->cur, ntiles = ctx->ntiles, cull = ctx->p.tile_culling, rec_id = ctx->rec_id;
+    R *kact = (R *)ctx->kact;
+    unsigned *active = ctx->active;
+    uint8_t *clean = ctx->clean, *tile_wet = ctx->tile_wet, *mask = ctx->mask, *tile_act = ctx->tile_act;
+    int *tile_epoch = ctx->tile_epoch;
+    double *tile_vol = ctx->tile_vol;
+    MatConsts mc = ctx->mc;
+    TimeConsts tc = ctx->tc;
+    DevScalars *sc = ctx->dsc;
+    StateRef<R> Ln{(const R *)ctx->lam[lam_in][0], (const R *)ctx->lam[lam_in][1], (const R *)ctx->lam[lam_in][2]};
+    StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
+    AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
+    void *args[] = {&m,  &S,     &cur,   &kact,       &active,  &clean,  &tile_wet, &tile_vol, &ntiles, &cull,
+                    &mc, &tc,    &sc,    &mask,       &tile_epoch, &tile_act, &rec_id, &Ln, &Lo, &aa};
+    trace_begin(ctx, TR_YOUTURN);
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_youturn<R>, grid, kBlock, args, 0, ctx->stream);
+    trace_end(ctx);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "reverse-step launch");
+    ctx->cur = cur ^ 1;
+    return DA_OK;
 }
 
 }  // namespace

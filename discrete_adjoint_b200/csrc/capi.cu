@@ -20,7 +20,7 @@ int set_error(da_ctx *ctx, int code, const std::string &msg) {
 void trace_begin(da_ctx *ctx, int kind) {
     TraceState &t = ctx->trace;
     if (!t.on) return;
-    TraceState::Pending p{kind, nullptr, nullptr};
+    TraceState::Pending p{kind, 1, nullptr, nullptr};
     for (cudaEvent_t *e : {&p.a, &p.b}) {
         if (!t.pool.empty()) {
             *e = t.pool.back();
@@ -33,9 +33,10 @@ void trace_begin(da_ctx *ctx, int kind) {
     t.pending.push_back(p);
 }
 
-void trace_end(da_ctx *ctx) {
+void trace_end(da_ctx *ctx, int steps) {
     TraceState &t = ctx->trace;
     if (!t.on || t.pending.empty()) return;
+    t.pending.back().steps = steps;
     if (t.pending.back().b) cudaEventRecord(t.pending.back().b, ctx->stream);
 }
 
@@ -48,6 +49,7 @@ int trace_flush(da_ctx *ctx) {
         if (!st && p.a && p.b && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
             t.total_ms[p.kind] += ms;
             t.launches[p.kind] += 1;
+            t.steps[p.kind] += p.steps;
         }
         if (p.a) t.pool.push_back(p.a);
         if (p.b) t.pool.push_back(p.b);
@@ -103,6 +105,7 @@ static bool params_ok(const da_params *p) {
     if (p->precision != DA_PREC_FP64 && p->precision != DA_PREC_FP32_SPLIT) return false;
     if (p->n_materials < 1 || p->n_materials > DA_MAX_MATERIALS) return false;
     if (!(p->epsilon > 0) || !(p->gravity_scale > 0) || !(p->gamma > 0)) return false;
+    if (p->grid_blocks < 0 || p->grid_blocks > (1 << 20)) return false;
     return true;
 }
 
@@ -126,7 +129,6 @@ static void free_state(da_ctx *ctx) {
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
     dfree(ctx->kact);
-    dfree(ctx->vol_part);
     dfree(ctx->tile_vol);
     dfree(ctx->active);
     dfree(ctx->clean);
@@ -140,13 +142,13 @@ static void free_state(da_ctx *ctx) {
 static void free_adjoint(da_ctx *ctx) {
     auto fr = [](void *p) { if (p) cudaFree(p); };
     fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
-    fr(ctx->red_out); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter); fr(ctx->dh0);
+    fr(ctx->red_out); fr(ctx->red_part); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter); fr(ctx->dh0);
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
     for (void *s : ctx->snaps) fr(s);
     ctx->snaps.clear();
     ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
-    ctx->red_out = ctx->seed_part = ctx->seed_J = ctx->dh0 = nullptr; ctx->seed_counter = nullptr;
+    ctx->red_out = ctx->red_part = ctx->seed_part = ctx->seed_J = ctx->dh0 = nullptr; ctx->seed_counter = nullptr;
     ctx->adj_n = 0;
 }
 
@@ -171,12 +173,24 @@ static int sync_scalars(da_ctx *ctx) {
     if (st) return st;
     st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
     if (st) return st;
+    if (ctx->hsc->err == DA_ERR_TIMEOUT) {
+        // a multi-step launch gave up at a grid barrier: restart its arrival count
+        cudaMemsetAsync(&ctx->dsc->bar_count, 0, sizeof(unsigned), ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
     if (ctx->hsc->err) {
         const int code = ctx->hsc->err;
         return set_error(ctx, code, code == DA_ERR_EIGEN ? "wave speed above 1e9 (get_coef_and_eigen)"
                                                          : "non-finite state after update (update_states)");
     }
     return DA_OK;
+}
+
+void update_grid(da_ctx *ctx) {
+    const int per_sm4 = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
+    int g = ctx->p.grid_blocks > 0 ? ctx->p.grid_blocks : per_sm4;
+    if (ctx->ntiles > 0 && g > ctx->ntiles) g = ctx->ntiles;
+    ctx->grid = g > 0 ? g : 1;
 }
 
 static void fill_stats(const da_ctx *ctx, da_step_stats *out) {
@@ -233,6 +247,7 @@ void da_params_default(da_params *p) {
     p->influx_dt = HUGE_VAL;
     p->fp32_sign_floor = 0.0;
     p->tile_culling = 1;
+    p->grid_blocks = 0;
 }
 
 da_ctx *da_create(const da_params *p, int *err) {
@@ -275,6 +290,7 @@ da_ctx *da_create(const da_params *p, int *err) {
     {
         const double init = 10000000.0;  // min_dx_dy_evalue start value, get_coef_and_eigen.C:36
         std::memcpy(&ctx->hsc->acc_min_dxe, &init, sizeof(init));
+        std::memcpy(&ctx->hsc->acc_alt_min_dxe, &init, sizeof(init));
     }
     st = cuda_check(ctx, cudaMemcpy(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice), "init scalars");
     if (st) {
@@ -312,6 +328,7 @@ int da_set_params(da_ctx *ctx, const da_params *p) {
         return set_error(ctx, DA_ERR_INVALID, "da_set_params: invalid parameters or precision/device change");
     ctx->p = *p;
     fill_consts(ctx->p, &ctx->mc, &ctx->tc);
+    update_grid(ctx);
     drop_graphs(ctx);
     return DA_OK;
 }
@@ -472,35 +489,14 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_run: no state");
     cudaSetDevice(ctx->device);
     int st = DA_OK;
-    // Two steps (one ping-pong cycle) per graph launch; one graph per starting buffer.
-    const int cur0 = ctx->cur;
-    const bool use_graph = !ctx->trace.on;
-    if (use_graph && nsteps >= 2 && !ctx->step_graph[cur0]) {
-        cudaGraph_t g;
-        st = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        if (st) return st;
-        int s1 = launch_forward_step(ctx);
-        int s2 = s1 ? s1 : launch_forward_step(ctx);
-        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
-        ctx->cur = cur0;  // capture advanced the ping-pong index without running anything
-        if (s2) return s2;
-        st = cuda_check(ctx, e, "end capture");
-        if (st) return st;
-        st = cuda_check(ctx, cudaGraphInstantiate(&ctx->step_graph[cur0], g, 0), "graph instantiate");
-        cudaGraphDestroy(g);
-        if (st) return st;
-    }
+    // the whole run is one cooperative launch of the multi-step kernel
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (device_ms) {
         st = cuda_check(ctx, cudaEventCreate(&e0), "event");
         if (!st) st = cuda_check(ctx, cudaEventCreate(&e1), "event");
         if (!st) st = cuda_check(ctx, cudaEventRecord(e0, ctx->stream), "event record");
     }
-    int k = 0;
-    if (use_graph)
-        for (; k + 1 < nsteps && !st; k += 2)
-            st = cuda_check(ctx, cudaGraphLaunch(ctx->step_graph[cur0], ctx->stream), "graph launch");
-    for (; k < nsteps && !st; ++k) st = launch_forward_step(ctx);
+    if (!st) st = launch_forward_steps(ctx, nsteps);
     if (device_ms && !st) {
         st = cuda_check(ctx, cudaEventRecord(e1, ctx->stream), "event record");
         if (!st) st = cuda_check(ctx, cudaEventSynchronize(e1), "event sync");
@@ -545,7 +541,7 @@ int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
 
 static const char *kTraceNames[TR_COUNT] = {"k_coef",       "k_update",     "k_coef_record", "k_update_record",
                                             "k_adj_src",    "k_adj_gather", "k_adj_seed",    "k_adj_reduce",
-                                            "snapshot_copy"};
+                                            "snapshot_copy", "k_steps", "k_youturn"};
 
 const char *da_trace_name(int32_t k) { return (k >= 0 && k < TR_COUNT) ? kTraceNames[k] : ""; }
 
@@ -556,6 +552,7 @@ int da_set_tracing(da_ctx *ctx, int32_t on) {
     for (int k = 0; k < TR_COUNT; ++k) {
         ctx->trace.total_ms[k] = 0.0;
         ctx->trace.launches[k] = 0;
+        ctx->trace.steps[k] = 0;
     }
     ctx->trace.on = on != 0;
     return st;
@@ -570,4 +567,92 @@ int da_trace_read(da_ctx *ctx, int32_t k, double *total_ms, int64_t *launches) {
     return st;
 }
 
+int da_trace_steps(da_ctx *ctx, int32_t k, int64_t *steps) {
+    if (!ctx || k < 0 || k >= TR_COUNT || !steps) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = trace_flush(ctx);
+    *steps = ctx->trace.steps[k];
+    return st;
+}
+
 }  // extern "C"
+
+// ---------------------------------------------------------------------------- autotuner
+// Times nsteps forward steps from the current state for each candidate grid (1, 2, 3, 4, 6 and
+// 8 blocks per SM, capped at the tile count) and keeps the fastest.  The state, time and
+// iteration are put back after every trial, so the tuning leaves the run where it was.
+int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
+    using namespace da;
+    if (!ctx || nsteps < 1) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_autotune: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_autotune: no state");
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->mesh.n;
+    const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
+    int st = sync_scalars(ctx);
+    if (st) return st;
+    const DevScalars saved_sc = *ctx->hsc;
+    const int cur0 = ctx->cur;
+    void *saved[3] = {nullptr, nullptr, nullptr};
+    for (int v = 0; v < 3 && !st; ++v) {
+        st = cuda_check(ctx, cudaMalloc(&saved[v], rs * n), "cudaMalloc(autotune)");
+        if (!st)
+            st = cuda_check(ctx, cudaMemcpyAsync(saved[v], ctx->U[cur0][v], rs * n, cudaMemcpyDeviceToDevice, ctx->stream),
+                            "save state");
+    }
+    auto put_back = [&]() -> int {
+        ctx->cur = cur0;
+        int s = DA_OK;
+        for (int v = 0; v < 3 && !s; ++v)
+            s = cuda_check(ctx, cudaMemcpyAsync(ctx->U[cur0][v], saved[v], rs * n, cudaMemcpyDeviceToDevice, ctx->stream),
+                           "restore state");
+        *ctx->hsc = saved_sc;
+        if (!s) s = cuda_check(ctx, cudaMemcpyAsync(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice,
+                                                    ctx->stream), "restore scalars");
+        if (!s) s = forward_state_changed(ctx);
+        if (!s) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        return s;
+    };
+    const int sm = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    const int mult[6] = {1, 2, 3, 4, 6, 8};
+    int cand[DA_TUNE_MAX], nc = 0;
+    for (int k = 0; k < 6; ++k) {
+        int g = mult[k] * sm;
+        if (g > ctx->ntiles) g = ctx->ntiles;
+        bool dup = false;
+        for (int j = 0; j < nc; ++j) dup |= cand[j] == g;
+        if (!dup && nc < DA_TUNE_MAX) cand[nc++] = g;
+    }
+    const int32_t grid0 = ctx->p.grid_blocks;
+    double best_ms = HUGE_VAL;
+    int best = 0;
+    da_tune_result r;
+    std::memset(&r, 0, sizeof(r));
+    for (int k = 0; k < nc && !st; ++k) {
+        ctx->p.grid_blocks = cand[k];
+        update_grid(ctx);
+        drop_graphs(ctx);
+        st = put_back();
+        if (!st) st = launch_forward_step(ctx);  // the first step after a state change sweeps every tile
+        double ms = 0.0;
+        if (!st) st = da_forward_run_timed(ctx, nsteps, nullptr, &ms);
+        r.grid[k] = cand[k];
+        r.ms_per_step[k] = ms / nsteps;
+        if (!st && ms < best_ms) {
+            best_ms = ms;
+            best = k;
+        }
+    }
+    r.n = nc;
+    r.best = best;
+    ctx->p.grid_blocks = st ? grid0 : cand[best];
+    update_grid(ctx);
+    drop_graphs(ctx);
+    const int st2 = put_back();
+    for (int v = 0; v < 3; ++v)
+        if (saved[v]) cudaFree(saved[v]);
+    if (!st) st = st2;
+    if (!st && out) *out = r;
+    return st;
+}
+

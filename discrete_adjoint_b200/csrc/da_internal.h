@@ -29,6 +29,8 @@ struct MatConsts {
 };
 
 // Scalars that live on the device so that whole step loops run without host round trips.
+constexpr int kAdjReduceParts = 128;  // cell ranges of the gradient reduction
+
 struct DevScalars {
     double time;          // TimeProps::time
     double dt;            // last dt
@@ -42,6 +44,10 @@ struct DevScalars {
     int err;              // sticky DA_ERR_* raised on the device
     unsigned blocks_done[2];  // last-block counters of the coefficient and update kernels
     int pad;
+    unsigned long long acc_alt_min_dxe;  // the multi-step kernel's second accumulator pair
+    unsigned long long acc_alt_hmax;     // (odd steps of a launch), same start values
+    unsigned bar_count;   // grid barrier of the multi-step kernel: blocks arrived
+    unsigned bar_gen;     // and barrier generation
 };
 
 // Time-clipping targets (TimeProps::ndnextoutput / ndnextsave / ndmaxtime) and the
@@ -76,12 +82,13 @@ struct DevMesh {
 // (the reference's Timer class, src/header/properties.h:43-71, moved onto the device).
 enum TraceKind {
     TR_COEF, TR_UPDATE, TR_COEF_REC, TR_UPDATE_REC, TR_ADJ_SRC, TR_ADJ_GATHER, TR_ADJ_SEED, TR_ADJ_REDUCE,
-    TR_SNAPSHOT, TR_COUNT
+    TR_SNAPSHOT, TR_STEPS, TR_YOUTURN, TR_COUNT
 };
 
 struct TraceState {
     struct Pending {
         int kind;
+        int steps;  // time steps the launch covers
         cudaEvent_t a, b;
     };
     bool on = false;
@@ -89,6 +96,7 @@ struct TraceState {
     std::vector<Pending> pending;
     double total_ms[TR_COUNT] = {};
     long long launches[TR_COUNT] = {};
+    long long steps[TR_COUNT] = {};
 };
 
 }  // namespace da
@@ -104,7 +112,6 @@ struct da_ctx {
     void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     void *kact = nullptr;            // [n] Real
-    double *vol_part = nullptr;      // [ntiles] per-tile volume partials of the last update
     double *tile_vol = nullptr;      // [ntiles] cached volume partial of each tile
     unsigned *active = nullptr;      // [ceil(n/32)] bit per cell: wet or next to a wet cell
     uint8_t *clean = nullptr;        // [ntiles] 1 when both state buffers hold the same tile
@@ -114,7 +121,10 @@ struct da_ctx {
     uint8_t *lam_clean = nullptr;    // [ntiles] both adjoint buffers hold the same tile
     int rec_id = 0;                  // id of the current recording step
     int ntiles = 0;                  // tiles of 256 consecutive cells
-    int nblocks = 0;                 // grid of the persistent step kernels
+    int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
+    int grid = 0;                    // grid of the tiled step kernels (da_params.grid_blocks)
+    int coop_cap[2] = {0, 0};        // resident blocks of k_steps (FP32, FP64), 0 = not queried
+    int coop_cap_yt[2] = {0, 0};     // resident blocks of k_youturn
     int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror
@@ -131,6 +141,7 @@ struct da_ctx {
     double *gbed = nullptr, *gint = nullptr;  // [n] running parameter sensitivities
     double *dk_tab = nullptr;        // [2][DA_MAX_MATERIALS][3] d kact / d phi_bed, d phi_int
     double *red_out = nullptr;       // [DA_MAX_MATERIALS + 1 + DA_MAX_PILES]
+    double *red_part = nullptr;      // [same x kAdjReduceParts] partial sums of the gradient reduction
     double *seed_part = nullptr;     // [nblocks]
     double *seed_J = nullptr;
     unsigned *seed_counter = nullptr;
@@ -145,20 +156,27 @@ namespace da {
 
 int set_error(da_ctx *ctx, int code, const std::string &msg);
 void trace_begin(da_ctx *ctx, int kind);
-void trace_end(da_ctx *ctx);
+void trace_end(da_ctx *ctx, int steps = 1);
 int trace_flush(da_ctx *ctx);
 int cuda_check(da_ctx *ctx, cudaError_t e, const char *what);
 void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
 
 // forward_fp64.cu / forward_fp32.cu
-// ev (optional): DA_FWD_KERNELS + 1 events recorded around the launches
-// record_mask (optional): branch codes of the step for the adjoint (full sweep)
+// record_mask (optional): branch codes of the step for the adjoint (listed tiles; tile_epoch)
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask = nullptr);
 int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask);
 int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask);
+// nsteps whole steps in one cooperative launch (k_steps); same results as nsteps single steps
+int launch_forward_steps(da_ctx *ctx, int nsteps);
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps);
+int launch_forward_steps_fp32(da_ctx *ctx, int nsteps);
 int forward_alloc(da_ctx *ctx);
+// capi.cu: grid of the tiled kernels from da_params.grid_blocks, the SM count and the tile count
+void update_grid(da_ctx *ctx);
 // adjoint_fp64.cu / adjoint_fp32.cu
 int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
+// replayed forward step + adjoint step in one cooperative launch (k_youturn)
+int launch_youturn(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
 int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
 int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
 int forward_state_changed(da_ctx *ctx);

@@ -7,5 +7,6 @@ namespace da {
 int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<float>(ctx, record_mask);
 }
+int launch_forward_steps_fp32(da_ctx *ctx, int nsteps) { return fwd::launch_steps_t<float>(ctx, nsteps); }
 
 }  // namespace da

@@ -8,6 +8,7 @@ namespace da {
 int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<double>(ctx, record_mask);
 }
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps) { return fwd::launch_steps_t<double>(ctx, nsteps); }
 
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
@@ -16,7 +17,9 @@ int forward_alloc(da_ctx *ctx) {
     // persistent kernels: 4 blocks of 256 threads per SM, never more blocks than tiles
     const int cap = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
     ctx->nblocks = ctx->ntiles < cap ? ctx->ntiles : cap;
-    const size_t words = (n + 31) / 32;
+    update_grid(ctx);
+    // the active bitmask is padded to whole tiles (8 words each) for the 16-byte tile tests
+    const size_t words = (size_t)ctx->ntiles * (fwd::kBlock / 32);
     int st = DA_OK;
     for (int b = 0; b < 2 && !st; ++b)
         for (int v = 0; v < 3 && !st; ++v) {
@@ -24,7 +27,6 @@ int forward_alloc(da_ctx *ctx) {
             if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->U[b][v], 0, rs * n, ctx->stream), "memset");
         }
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->vol_part, sizeof(double) * ctx->nblocks), "cudaMalloc(vol)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_wet, ctx->ntiles), "cudaMalloc(tile_wet)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_epoch, sizeof(int) * ctx->ntiles), "cudaMalloc(epoch)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_epoch, 0xff, sizeof(int) * ctx->ntiles, ctx->stream), "memset");
@@ -47,6 +49,11 @@ int forward_state_changed(da_ctx *ctx) {
         st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * ((ctx->mesh.n + 31) / 32), ctx->stream),
                         "memset");
     return st;
+}
+
+int launch_forward_steps(da_ctx *ctx, int nsteps) {
+    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps);
+    return launch_forward_steps_fp32(ctx, nsteps);
 }
 
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {

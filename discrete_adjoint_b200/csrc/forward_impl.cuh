@@ -32,29 +32,39 @@ constexpr int kBlock = kTileCells;  // one thread per cell of a tile
 // dt from the reduced CFL bound and hmax (get_coef_and_eigen.C:168-179 with the single-rank
 // MPI_Allreduce(MIN)), then TimeProps::incrtime.  frict_tiny follows hpfem.C:232-235 with the
 // iteration count before the increment.
-__device__ void finalize_dt(DevScalars *sc, const TimeConsts &tc) {
-    const double min_dxe = __longlong_as_double(*(volatile unsigned long long *)&sc->acc_min_dxe);
-    const double hmax = __longlong_as_double(*(volatile unsigned long long *)&sc->acc_hmax);
+__device__ __forceinline__ void step_dt(double min_dxe, double hmax, double time, long long iter,
+                                        const TimeConsts &tc, double &dt_out, double &ft_out) {
     const double g0 = 0.5 * min_dxe;
     const double g1 = -0.9 * sqrt(hmax * (tc.epsilon) * (tc.gravity_scale) / 9.8);
     double dt = 0.5 * (g0 > -g1 ? -g1 : g0);
     if (dt == 0.0) dt = 0.5 * tc.influx_dt;
-    const double time = sc->time;
     if (time + dt > tc.next_output) dt = tc.next_output - time;
     if (time + dt > tc.next_save) dt = tc.next_save - time;
     if (time + dt > tc.max_time) dt = tc.max_time - time;
     if (tc.dt_replay) {
         // frozen time-step sequence (tangent/finite-difference checks of the adjoint)
-        const long long k = sc->iter - tc.iter0;
+        const long long k = iter - tc.iter0;
         dt = (k >= 0 && k < tc.n_replay) ? tc.dt_replay[k] : 0.0;
     }
-    sc->frict_tiny = sc->iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
+    dt_out = dt;
+    ft_out = iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
+}
+
+constexpr unsigned long long kMinDxeStart = 0x416312D000000000ull;  // bits of 1e7, get_coef_and_eigen.C:36
+
+__device__ void finalize_dt(DevScalars *sc, const TimeConsts &tc) {
+    const double min_dxe = __longlong_as_double(*(volatile unsigned long long *)&sc->acc_min_dxe);
+    const double hmax = __longlong_as_double(*(volatile unsigned long long *)&sc->acc_hmax);
+    const double time = sc->time;
+    double dt, ft;
+    step_dt(min_dxe, hmax, time, sc->iter, tc, dt, ft);
+    sc->frict_tiny = ft;
     sc->dt = dt;
     sc->time = time + dt;
     sc->min_dxe = min_dxe;
     sc->hmax = hmax;
     sc->iter += 1;
-    sc->acc_min_dxe = __double_as_longlong(10000000.0);  // get_coef_and_eigen.C:36
+    sc->acc_min_dxe = kMinDxeStart;
     sc->acc_hmax = 0ull;
 }
 
@@ -80,14 +90,12 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // k_update reads: a cell outside that set has zero fluxes and no sources this step.
 // RECORD: also writes the branch code of every cell of a listed tile into mask (0 dry / at rest,
 // 1..3 for sgn(vel) = -1, 0, +1 of gmfggetcoef) for the adjoint's replay.
-template <class R, bool RECORD = false>
-__global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
-                                                 unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
-                                                 int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
-                                                 uint8_t *__restrict__ mask = nullptr) {
-    __shared__ int list[kBlock];
-    unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
-    unsigned long long my_max = 0ull;
+// The thread's CFL min and hmax (bit patterns of positive doubles) accumulate in my_min / my_max.
+template <class R, bool RECORD>
+__device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> &U, R *kact, unsigned *active,
+                                           const uint8_t *tile_wet, int ntiles, int cull, const MatConsts &mc,
+                                           DevScalars *sc, uint8_t *mask, int *list, unsigned long long &my_min,
+                                           unsigned long long &my_max) {
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
         const bool need = tq < ntiles && (!cull || tile_wet[tq]);
@@ -139,12 +147,29 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
             if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
         }
     }
+}
+
+// Warp-reduced CFL min / hmax into one accumulator pair.
+__device__ __forceinline__ void push_minmax(unsigned long long my_min, unsigned long long my_max,
+                                            unsigned long long *acc_min, unsigned long long *acc_max) {
     my_min = warp_min_u64(my_min);
     my_max = warp_max_u64(my_max);
     if ((threadIdx.x & 31) == 0) {
-        if (my_min != 0x7FF0000000000000ull) atomicMin(&sc->acc_min_dxe, my_min);
-        if (my_max) atomicMax(&sc->acc_hmax, my_max);
+        if (my_min != 0x7FF0000000000000ull) atomicMin(acc_min, my_min);
+        if (my_max) atomicMax(acc_max, my_max);
     }
+}
+
+template <class R, bool RECORD = false>
+__global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
+                                                 unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
+                                                 int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
+                                                 uint8_t *__restrict__ mask = nullptr) {
+    __shared__ int list[kBlock];
+    unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
+    unsigned long long my_max = 0ull;
+    coef_phase<R, RECORD>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
+    push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (last_block(&sc->blocks_done[0])) {
         if (threadIdx.x == 0) {
             finalize_dt(sc, tc);
@@ -155,7 +180,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
 
 // Full corrector update of one active cell (fluxes + sources), reference order.
 template <class R>
-__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact,
+__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *kact,
                                             const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
                                             R st[3]) {
     const uint8_t bf = m.bflag[i];
@@ -240,34 +265,30 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 // an active cell, or when its two ping-pong buffers differ (not clean), or when culling is off.
 // In a listed tile, active cells get the full update and the others are copied (their update is
 // the identity).  A tile that is not listed is already identical in both buffers.  Each listed
-// tile stores its volume partial, its clean flag and whether it now holds a wet cell; the last
-// block sums every tile's partial in tile order, so the volume does not depend on culling.
+// tile stores its volume partial, its clean flag and whether it now holds a wet cell; the volume
+// is the sum of every tile's partial in a fixed order, so it depends neither on culling nor on
+// the grid.
 // RECORD: every cell of a listed tile gets its full mask byte (the k_coef code of a wet cell,
 // bit 3 active, bit 2 depth clamped) and the tile records the step id (tile_epoch) and whether
 // it had an active cell (tile_act); masks of tiles with another epoch count as zero.
-template <class R, bool RECORD = false>
-__global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
-                                                   const R *__restrict__ kact, unsigned *__restrict__ active,
-                                                   uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
-                                                   double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
-                                                   DevScalars *sc, double *__restrict__ vol_part,
-                                                   uint8_t *__restrict__ mask = nullptr, int *__restrict__ tile_epoch = nullptr,
-                                                   uint8_t *__restrict__ tile_act = nullptr, int rec_id = 0) {
-    __shared__ double red[kBlock / 32];
-    __shared__ int list[kBlock];
+template <class R, bool RECORD>
+__device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R> &U, const StateOut<R> &O,
+                                             const R *kact, unsigned *active, uint8_t *clean, uint8_t *tile_wet,
+                                             double *tile_vol, int ntiles, int cull, const MatConsts &mc,
+                                             DevScalars *sc, R dt, R ft, uint8_t *mask, int *tile_epoch,
+                                             uint8_t *tile_act, int rec_id, int *list, double *red) {
     const int lane = threadIdx.x & 31;
-    const R dt = R(sc->dt);
-    const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
         bool need = false;
         if (tq < ntiles) {
             need = !cull || !clean[tq];
             if (!need) {
-                const int w0 = tq * (kBlock / 32);
-                const int nw = (m.n + 31) / 32;
-                for (int w = 0; w < kBlock / 32 && !need; ++w)
-                    if (w0 + w < nw && active[w0 + w]) need = true;
+                // the tile's 8 bitmask words in two 16-byte loads (the bitmask is padded to
+                // whole tiles)
+                const uint4 *w4 = reinterpret_cast<const uint4 *>(active + (size_t)tq * (kBlock / 32));
+                const uint4 a = w4[0], b = w4[1];
+                need = (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
             }
         }
         const int cnt = compact_tiles(need, tq, list);
@@ -309,14 +330,149 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
             }
         }
     }
-    (void)vol_part;
+}
+
+// Sum of the tiles' volume partials in a fixed order (thread q takes tiles q, q + 256, ... in
+// four interleaved running sums; then the block sum); every thread of the calling block must
+// enter.  Loads go through L2 (the partials were written by other blocks).
+__device__ __forceinline__ double volume_sum(const double *tile_vol, int ntiles, double *red) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int b = threadIdx.x;
+    for (; b + 3 * kBlock < ntiles; b += 4 * kBlock) {
+        a0 += __ldcg(tile_vol + b);
+        a1 += __ldcg(tile_vol + b + kBlock);
+        a2 += __ldcg(tile_vol + b + 2 * kBlock);
+        a3 += __ldcg(tile_vol + b + 3 * kBlock);
+    }
+    for (; b < ntiles; b += kBlock) a0 += __ldcg(tile_vol + b);
+    return block_sum((a0 + a1) + (a2 + a3), red);
+}
+
+template <class R, bool RECORD = false>
+__global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
+                                                   const R *__restrict__ kact, unsigned *__restrict__ active,
+                                                   uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
+                                                   double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
+                                                   DevScalars *sc, uint8_t *__restrict__ mask = nullptr,
+                                                   int *__restrict__ tile_epoch = nullptr,
+                                                   uint8_t *__restrict__ tile_act = nullptr, int rec_id = 0) {
+    __shared__ double red[kBlock / 32];
+    __shared__ int list[kBlock];
+    const R dt = R(sc->dt);
+    const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
+    update_phase<R, RECORD>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, dt, ft, mask,
+                            tile_epoch, tile_act, rec_id, list, red);
     if (last_block(&sc->blocks_done[1])) {
-        double t = 0.0;
-        for (int b = threadIdx.x; b < ntiles; b += blockDim.x) t += ((volatile double *)tile_vol)[b];
-        t = block_sum(t, red);
+        const double t = volume_sum(tile_vol, ntiles, red);
         if (threadIdx.x == 0) {
             sc->volume = t;
             sc->blocks_done[1] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- k_steps
+// nsteps whole steps in one cooperative launch (all blocks resident): per step the coefficient
+// phase, a grid barrier, dt (every block forms the same dt from the same reduced values), the
+// update phase and a second barrier.  Odd and even steps accumulate the CFL min / hmax in two
+// pairs, so block 0 can restart one pair while the other is read.  time and iteration advance
+// in registers; block 0 writes them, the last step's scalars and the volume at the end.  The
+// state buffers alternate as in single steps and are read with coherent loads (no read-only
+// cache: other blocks wrote them earlier in the same launch).
+// The barrier waits are bounded: after ~4 s a block raises DA_ERR_TIMEOUT and returns, and the
+// others give up at their next barrier.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_sync(DevScalars *sc) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = &sc->bar_gen;
+        volatile int *err = &sc->err;
+        const unsigned g = *gen;
+        __threadfence();
+        int good = 1;
+        if (atomicAdd(&sc->bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(&sc->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&sc->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            for (unsigned it = 0; *gen == g; ++it) {
+                if (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > 4000000000ull) {
+                    atomicCAS(&sc->err, 0, DA_ERR_TIMEOUT);
+                    good = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        if (*err == DA_ERR_TIMEOUT) good = 0;
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <class R>
+struct StatePair {
+    R *h[2];
+    R *hu[2];
+    R *hv[2];
+};
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
+                                                  unsigned *active, uint8_t *clean, uint8_t *tile_wet,
+                                                  double *tile_vol, int ntiles, int cull, MatConsts mc,
+                                                  TimeConsts tc, DevScalars *sc) {
+    __shared__ double red[kBlock / 32];
+    __shared__ int list[kBlock];
+    double time = sc->time;
+    long long iter = sc->iter;
+    double dt = sc->dt, ft = sc->frict_tiny, min_dxe = sc->min_dxe, hmax = sc->hmax;
+    for (int s = 0; s < nsteps; ++s) {
+        const int c = (cur + s) & 1, p = s & 1;
+        unsigned long long *acc_min = p ? &sc->acc_alt_min_dxe : &sc->acc_min_dxe;
+        unsigned long long *acc_max = p ? &sc->acc_alt_hmax : &sc->acc_hmax;
+        const StateRef<R> U{S.h[c], S.hu[c], S.hv[c]};
+        const StateOut<R> O{S.h[c ^ 1], S.hu[c ^ 1], S.hv[c ^ 1]};
+        unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
+        coef_phase<R, false>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max);
+        push_minmax(my_min, my_max, acc_min, acc_max);
+        if (!grid_sync(sc)) return;
+        min_dxe = __longlong_as_double(__ldcg(acc_min));
+        hmax = __longlong_as_double(__ldcg(acc_max));
+        step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+        time += dt;
+        iter += 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            // read by every block before this step's first barrier; used again next step
+            *(p ? &sc->acc_min_dxe : &sc->acc_alt_min_dxe) = kMinDxeStart;
+            *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
+        }
+        const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
+        update_phase<R, false>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, R(dt), ftr,
+                               nullptr, nullptr, nullptr, 0, list, red);
+        if (!grid_sync(sc)) return;
+    }
+    if (blockIdx.x == 0) {
+        const double v = volume_sum(tile_vol, ntiles, red);
+        if (threadIdx.x == 0) {
+            sc->volume = v;
+            sc->time = time;
+            sc->iter = iter;
+            sc->dt = dt;
+            sc->frict_tiny = ft;
+            sc->min_dxe = min_dxe;
+            sc->hmax = hmax;
+            sc->acc_min_dxe = sc->acc_alt_min_dxe = kMinDxeStart;
+            sc->acc_hmax = sc->acc_alt_hmax = 0ull;
         }
     }
 }
@@ -328,7 +484,7 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> O{(R *)ctx->U[o][0], (R *)ctx->U[o][1], (R *)ctx->U[o][2]};
     R *kact = (R *)ctx->kact;
-    const int tiles = ctx->ntiles, grid = ctx->nblocks, cull = ctx->p.tile_culling;
+    const int tiles = ctx->ntiles, grid = ctx->grid, cull = ctx->p.tile_culling;
     if (record_mask) {
         // branch recording for the adjoint: codes and flags for every cell of the listed tiles
         ++ctx->rec_id;
@@ -338,8 +494,7 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE_REC);
         k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                            ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part,
-                                                            record_mask, ctx->tile_epoch, ctx->tile_act, ctx->rec_id);
+                                                            ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, record_mask, ctx->tile_epoch, ctx->tile_act, ctx->rec_id);
         trace_end(ctx);
     } else {
         trace_begin(ctx, TR_COEF);
@@ -348,11 +503,50 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE);
         k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                      ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, ctx->vol_part);
+                                                      ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc);
         trace_end(ctx);
     }
     ctx->cur = o;
     return cuda_check(ctx, cudaGetLastError(), "forward step launch");
+}
+
+// nsteps steps in one cooperative launch of k_steps; the grid is capped at the number of blocks
+// that can be resident at once (the launch fails otherwise, it never deadlocks).
+template <class R>
+int launch_steps_t(da_ctx *ctx, int nsteps) {
+    if (nsteps <= 0) return DA_OK;
+    if (ctx->coop_cap[sizeof(R) == 8] <= 0) {
+        int per_sm = 0;
+        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_steps<R>, kBlock, 0),
+                            "occupancy");
+        if (st) return st;
+        ctx->coop_cap[sizeof(R) == 8] = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
+    }
+    const int cap = ctx->coop_cap[sizeof(R) == 8];
+    if (cap <= 0) return set_error(ctx, DA_ERR_UNSUPPORTED, "multi-step kernel cannot be resident");
+    const int grid = ctx->grid < cap ? ctx->grid : cap;
+    MeshArgs m = mesh_args(ctx);
+    StatePair<R> S;
+    for (int b = 0; b < 2; ++b) {
+        S.h[b] = (R *)ctx->U[b][0];
+        S.hu[b] = (R *)ctx->U[b][1];
+        S.hv[b] = (R *)ctx->U[b][2];
+    }
+    int cur = ctx->cur, n = nsteps, ntiles = ctx->ntiles, cull = ctx->p.tile_culling;
+    R *kact = (R *)ctx->kact;
+    unsigned *active = ctx->active;
+    uint8_t *clean = ctx->clean, *tile_wet = ctx->tile_wet;
+    double *tile_vol = ctx->tile_vol;
+    MatConsts mc = ctx->mc;
+    TimeConsts tc = ctx->tc;
+    DevScalars *sc = ctx->dsc;
+    void *args[] = {&m, &S, &cur, &n, &kact, &active, &clean, &tile_wet, &tile_vol, &ntiles, &cull, &mc, &tc, &sc};
+    trace_begin(ctx, TR_STEPS);
+    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_steps<R>, grid, kBlock, args, 0, ctx->stream);
+    trace_end(ctx, nsteps);
+    if (e != cudaSuccess) return cuda_check(ctx, e, "multi-step launch");
+    ctx->cur = (cur + nsteps) & 1;
+    return DA_OK;
 }
 
 }  // namespace

@@ -12,17 +12,17 @@ namespace da {
 namespace fv {
 
 template <class R>
-struct StateRef {
-    const R *__restrict__ h;
-    const R *__restrict__ hu;
-    const R *__restrict__ hv;
+struct StateRef {  // no __restrict__: the multi-step kernel reads what other blocks wrote
+    const R *h;
+    const R *hu;
+    const R *hv;
 };
 
 template <class R>
 struct StateOut {
-    R *__restrict__ h;
-    R *__restrict__ hu;
-    R *__restrict__ hv;
+    R *h;
+    R *hu;
+    R *hv;
 };
 
 // c_sgn (src/header/geoflow.h:90-100): zero inside +-GEOFLOW_TINY
@@ -262,7 +262,7 @@ __device__ __forceinline__ void riemann(const Hfv<R> &l, const Hfv<R> &r, R flux
 
 // State, flux and speeds of neighbour e; only h is read for a dry neighbour.
 template <class R>
-__device__ __forceinline__ void nb_hfv(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact, int e,
+__device__ __forceinline__ void nb_hfv(const MeshArgs &m, const StateRef<R> &U, const R *kact, int e,
                                        int dir, Hfv<R> &o) {
     const R h = U.h[e];
     if (h < R(DA_TINY)) {
@@ -276,7 +276,7 @@ __device__ __forceinline__ void nb_hfv(const MeshArgs &m, const StateRef<R> &U, 
 // Flux on side s of cell i (the value the reference stores on the side's edge-midpoint node):
 // one Riemann flux with a same-size or coarser neighbour, the mean of two with two finer ones.
 template <class R>
-__device__ __forceinline__ void side_flux(const MeshArgs &m, const StateRef<R> &U, const R *__restrict__ kact, int i,
+__device__ __forceinline__ void side_flux(const MeshArgs &m, const StateRef<R> &U, const R *kact, int i,
                                           uint8_t bf, int s, const Hfv<R> &self, R F[3]) {
     const int dir = s & 1;
     const bool plus = s < 2;

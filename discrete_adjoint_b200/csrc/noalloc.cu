@@ -30,8 +30,7 @@ constexpr size_t kOffMat = align256(kOffBflag + kMaxCells);
 constexpr size_t kOffClean = align256(kOffMat + kMaxCells);
 constexpr size_t kOffTileWet = align256(kOffClean + kMaxTiles);
 constexpr size_t kOffTileVol = align256(kOffTileWet + kMaxTiles);
-constexpr size_t kOffVolPart = align256(kOffTileVol + kMaxTiles * sizeof(double));
-constexpr size_t kOffScalars = align256(kOffVolPart + kMaxGrid * sizeof(double));
+constexpr size_t kOffScalars = align256(kOffTileVol + kMaxTiles * sizeof(double));
 constexpr size_t kScratchBytes = align256(kOffScalars + sizeof(DevScalars));
 
 // The scratch of every call.  Host code must not take this name as a device address: the
@@ -69,6 +68,9 @@ __global__ void k_init(DevScalars *sc, double time, long long iter) {
     sc->err = 0;
     sc->blocks_done[0] = sc->blocks_done[1] = 0u;
     sc->pad = 0;
+    sc->acc_alt_min_dxe = __double_as_longlong(10000000.0);
+    sc->acc_alt_hmax = 0ull;
+    sc->bar_count = sc->bar_gen = 0u;
 }
 
 // Boundary / two-neighbour flags and byte materials from the caller's tables; an index out of
@@ -129,7 +131,6 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     uint8_t *clean = base + noalloc::kOffClean;
     uint8_t *tile_wet = base + noalloc::kOffTileWet;
     double *tile_vol = (double *)(base + noalloc::kOffTileVol);
-    double *vol_part = (double *)(base + noalloc::kOffVolPart);
     DevScalars *sc = (DevScalars *)(base + noalloc::kOffScalars);
 
     MatConsts mc{};
@@ -164,7 +165,7 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     // every tile is processed (no culling across independent calls)
     fwd::k_coef<double><<<grid, fwd::kBlock, 0, s>>>(m, U, kact, active, tile_wet, ntiles, 0, mc, tc, sc);
     fwd::k_update<double><<<grid, fwd::kBlock, 0, s>>>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, 0, mc,
-                                                       sc, vol_part);
+                                                       sc);
     if (cudaGetLastError() != cudaSuccess) return DA_ERR_CUDA;
     if (cudaMemcpyAsync(&hs, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess) return DA_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return DA_ERR_CUDA;

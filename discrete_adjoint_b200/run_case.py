@@ -1,0 +1,50 @@
+"""Run one of the synthetic workloads through the C ABI and print a JSON summary.
+
+    python -m discrete_adjoint_b200.run_case --workload 2 --precision fp32 --steps 20 [--full-sweep]
+    python -m discrete_adjoint_b200.run_case --workload 3 --precision fp64 --adjoint 64
+
+A fixed, small command line for profilers (ncu -k <kernel> -s <skip> -c <count> python -m ...):
+the forward steps go through da_forward_run (CUDA graphs), the adjoint through da_adjoint_run.
+Workloads: 1 = 40k-cell plane and runout, 2 = 3.75M-cell adaptive hill + noise, 3 = 1M-cell
+uniform plane (the forward + adjoint workload).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import _ffi, inputs
+from .solver import GeoflowContext, TimeProps, adjoint_run
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--steps", type=int, default=20, help="forward steps (ignored with --adjoint)")
+    ap.add_argument("--full-sweep", action="store_true", help="switch tile culling off")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="HORIZON",
+                    help="run forward + adjoint over HORIZON steps (32 snapshots) instead")
+    ap.add_argument("--device", type=int, default=0)
+    a = ap.parse_args(argv)
+    w = {1: inputs.workload1, 2: inputs.workload2, 3: inputs.workload3}[a.workload]()
+    prec = _ffi.DA_PREC_FP32_SPLIT if a.precision == "fp32" else _ffi.DA_PREC_FP64
+    with GeoflowContext(w.mat, TimeProps(), precision=prec, device=a.device,
+                        tile_culling=not a.full_sweep) as c:
+        c.upload_mesh(w.mesh)
+        c.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
+        out = {"workload": w.name, "cells": w.mesh.n, "precision": a.precision, "culling": not a.full_sweep}
+        if a.adjoint:
+            p0 = w.piles[0]
+            box = inputs.WORKLOAD3_BOX if a.workload == 3 else (p0.xc - 500.0, p0.xc + 500.0, p0.yc - 500.0, p0.yc + 500.0)
+            g = adjoint_run(c, box, a.adjoint, 32, w.mesh.dh0_dpile)
+            out.update({"horizon": a.adjoint, "J": g.J, "dJ_dbedfrict": g.dJ_dbedfrict, "dJ_dpile": g.dJ_dpile,
+                        "forward_steps": g.forward_steps, "device_ms": g.device_ms})
+        else:
+            s, ms = c.run_timed(a.steps)
+            out.update({"steps": a.steps, "device_ms": ms, "volume": s.volume, "iter": s.iter})
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

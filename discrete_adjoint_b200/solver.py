@@ -51,7 +51,7 @@ class TimeProps:
 
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
                 influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                tile_culling: bool = True) -> _ffi.da_params:
+                tile_culling: bool = True, grid_blocks: int = 0) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -72,6 +72,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.influx_dt = influx_dt
     p.fp32_sign_floor = fp32_sign_floor
     p.tile_culling = int(tile_culling)
+    p.grid_blocks = int(grid_blocks)
     return p
 
 
@@ -89,12 +90,13 @@ class GeoflowContext:
 
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
                  device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                 tile_culling: bool = True):
+                 tile_culling: bool = True, grid_blocks: int = 0):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
-        self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling)
+        self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling,
+                                  grid_blocks)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:
@@ -165,15 +167,26 @@ class GeoflowContext:
     def set_tracing(self, on: bool):
         self._check(self.lib.da_set_tracing(self.ctx, int(on)), "da_set_tracing")
 
-    def trace(self) -> dict:
-        """{kernel: (total device ms, launches)} since tracing was switched on."""
+    def trace(self, with_steps: bool = False) -> dict:
+        """{kernel: (total device ms, launches)} since tracing was switched on; with_steps adds
+        the time steps those launches covered as a third entry."""
         out = {}
-        for k in range(9):
-            ms, n = C.c_double(), C.c_int64()
+        for k in range(_ffi.DA_TRACE_KINDS):
+            ms, n, s = C.c_double(), C.c_int64(), C.c_int64()
             self._check(self.lib.da_trace_read(self.ctx, k, C.byref(ms), C.byref(n)), "da_trace_read")
+            self._check(self.lib.da_trace_steps(self.ctx, k, C.byref(s)), "da_trace_steps")
             if n.value:
-                out[self.lib.da_trace_name(k).decode()] = (ms.value, n.value)
+                name = self.lib.da_trace_name(k).decode()
+                out[name] = (ms.value, n.value, s.value) if with_steps else (ms.value, n.value)
         return out
+
+    def autotune(self, nsteps: int = 20) -> dict:
+        """Pick the grid of the tiled kernels by timing nsteps steps per candidate (da_autotune);
+        the state is left where it was.  Returns {"best": grid, "ms_per_step": {grid: ms}}."""
+        r = _ffi.da_tune_result()
+        self._check(self.lib.da_autotune(self.ctx, nsteps, C.byref(r)), "da_autotune")
+        self.params.grid_blocks = r.grid[r.best]
+        return {"best": r.grid[r.best], "ms_per_step": {r.grid[k]: r.ms_per_step[k] for k in range(r.n)}}
 
     def profile(self, nsteps: int) -> dict:
         """Mean device ms per forward kernel over nsteps (events around every launch)."""

@@ -88,7 +88,9 @@ typedef struct da_params {
     int32_t tile_culling;        /* 1: tiles of 256 cells with no wet cell in or next to them are
                                   * not rewritten when both state buffers already hold them
                                   * (results are bit-identical); 0: every cell is rewritten */
-    int32_t reserved0;
+    int32_t grid_blocks;         /* blocks of 256 threads per launch of the tiled step kernels
+                                  * (each block walks a strided list of 256-cell tiles); 0 = 4 per
+                                  * SM.  Results do not depend on it; da_autotune picks it. */
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
@@ -192,12 +194,29 @@ int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms);
 const char *da_forward_kernel_name(int32_t k);
 /* Tracing of every launch of the step and the adjoint (forward runs then skip CUDA graphs):
  * on != 0 starts it with cleared sums, 0 stops it.  da_trace_read returns, for kernel kind k in
- * [0, DA_TRACE_KINDS), the summed device time in ms and the number of launches; da_trace_name
- * names the kind. */
-#define DA_TRACE_KINDS 9
+ * [0, DA_TRACE_KINDS), the summed device time in ms and the number of launches; da_trace_steps
+ * the number of time steps those launches covered (more than the launches only for the
+ * multi-step kernel "k_steps"); da_trace_name names the kind. */
+#define DA_TRACE_KINDS 11
 int da_set_tracing(da_ctx *ctx, int32_t on);
 int da_trace_read(da_ctx *ctx, int32_t k, double *total_ms, int64_t *launches);
+int da_trace_steps(da_ctx *ctx, int32_t k, int64_t *steps);
 const char *da_trace_name(int32_t k);
+
+/* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
+ * Times nsteps forward steps from the current state for each candidate grid of the tiled
+ * kernels (1, 2, 3, 4, 6 and 8 blocks of 256 threads per SM, capped at the tile count), keeps
+ * the fastest as da_params.grid_blocks and puts the state, time and iteration back after every
+ * trial.  Results of later steps do not depend on the choice.  out (optional) receives the
+ * candidates and their mean ms per step. */
+#define DA_TUNE_MAX 8
+typedef struct da_tune_result {
+    int32_t n;                   /* candidates tried */
+    int32_t best;                /* index of the one kept */
+    int32_t grid[DA_TUNE_MAX];
+    double ms_per_step[DA_TUNE_MAX];
+} da_tune_result;
+int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out);
 
 /* ---- one step without any device allocation ------------------------------------------------
  * No counterpart in the reference: an addition for callers that may not allocate device memory

@@ -107,6 +107,31 @@ def test_tile_culling_is_bit_identical(precision):
     assert sa.time == sb.time and sa.volume == sb.volume
 
 
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+def test_grid_size_and_autotune_do_not_change_results(precision):
+    # the tiled kernels' results do not depend on the grid (fixed-order volume sum, min for dt),
+    # and the autotuner puts the state, time and iteration back after its trials
+    w = inputs.workload1()
+    out = []
+    for grid in (1, 7, 148, 0, 4096):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision, grid_blocks=grid) as ctx:
+            ctx.upload_mesh(w.mesh)
+            ctx.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
+            s = ctx.run(120)
+            out.append((ctx.get_state(), s))
+    with gpu_ctx(w, precision=precision) as ctx:
+        ctx.run(40)
+        r = ctx.autotune(10)
+        assert r["best"] in r["ms_per_step"] and all(v > 0 for v in r["ms_per_step"].values())
+        s = ctx.run(80)
+        out.append((ctx.get_state(), s))
+    a, sa = out[0]
+    for b, sb in out[1:]:
+        for u, v in zip(a, b):
+            assert np.array_equal(u, v)
+        assert sa.time == sb.time and sa.volume == sb.volume and sa.iter == sb.iter
+
+
 def test_set_state_resets_culling():
     w = inputs.test_case(seed=2)
     h, hu, hv, dts, st = oracle_run(w, 30)
