@@ -163,7 +163,12 @@ def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dic
                     nbr, statics (dx, dy, g, dg, curv [+ x, y]) and writes A (3 x 8) and B (4 x 8)
                     and updates two FP64 sensitivities
       k_adj_gather  every cell reads its mask byte and lambda and writes lambda; an active cell also
-                    reads h, bflag, nbr, A (3 x 8) and updates two FP64 sensitivities"""
+                    reads h, bflag, nbr, A (3 x 8) and updates two FP64 sensitivities
+    The multi-step kernel k_steps counts coef + update per time step; the fused reverse step
+    k_youturn counts the two recording phases, k_adj_src and k_adj_gather; a snapshot copy
+    reads and writes the state once (3 x r x n each way).
+    These are full-sweep figures: tile culling skips the cells of dry tiles, so a culled launch
+    touches fewer bytes than this (the ncu capture's DRAM traffic shows how many)."""
     r = 8 if precision == "fp64" else 4
     xy = 2 * r if precision == "fp64" else 0
     coef = n * r + n_wet * (2 * r + 1 + 1 + 16 + 2 * r + r + xy + r)
@@ -171,7 +176,8 @@ def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dic
     src = n * r + n_wet * (2 * r + 2 * r + 1 + 1 + 1 + 16 + 2 * r + 7 * r + xy + 24 + 32 + 32)
     gat = n * (1 + 3 * r + 3 * r) + n_act * (r + 1 + 16 + 24 + 32)
     return {"k_coef": coef, "k_update": upd, "k_coef_record": coef + n, "k_update_record": upd + n,
-            "k_adj_src": src, "k_adj_gather": gat}
+            "k_adj_src": src, "k_adj_gather": gat, "k_steps": coef + upd,
+            "k_youturn": coef + upd + 2 * n + src + gat, "snapshot_copy": 2 * 3 * r * n}
 
 
 # DRAM bytes (read + write) per launch from the committed ncu captures of the headline
@@ -269,7 +275,7 @@ def fwdadj(args, ws, local):
         # per-kernel device times of one traced run
         c.set_tracing(True)
         adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
-        res["trace"] = c.trace()
+        res["trace"] = c.trace(with_steps=True)
         c.set_tracing(False)
         # e2e through the C ABI with host buffers: H2D of the initial state, the run, D2H of
         # the gradients and lambda^0
@@ -306,20 +312,32 @@ def fwdadj(args, ws, local):
 
 
 def forward_config2(args, ws, local):
+    """Forward steps alone on the 3.75M-cell adaptive workload, through da_forward_run (the
+    multi-step kernel), with and without tile culling, in both precisions.  The full sweeps
+    (every cell rewritten every step) carry the roofline of the step kernel."""
     from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, inputs
     w = inputs.workload2()
     m = w.mesh
     res = {}
+    hbm, peak_kind = peaks()
     for name, prec, cull in (("fp32", _ffi.DA_PREC_FP32_SPLIT, True),
                              ("fp32_full_sweep", _ffi.DA_PREC_FP32_SPLIT, False),
-                             ("fp64", _ffi.DA_PREC_FP64, True)):
+                             ("fp64", _ffi.DA_PREC_FP64, True),
+                             ("fp64_full_sweep", _ffi.DA_PREC_FP64, False)):
         c = GeoflowContext(w.mat, TimeProps(), precision=prec, device=local, tile_culling=cull)
         c.upload_mesh(m)
         c.set_state(m.h0, m.hu0, m.hv0)
         c.run(5)
         _, ms = c.run_timed(300)
         ms = allmax(ms, ws, local)
-        res[name] = {"value": m.n * 300 * ws / (ms * 1e-3), "ms_per_step": ms / 300, "kernel_ms": c.profile(20)}
+        wv, av = wet_counts(m, c.get_state()[0])
+        r = {"value": m.n * 300 * ws / (ms * 1e-3), "us_per_step": 1e3 * ms / 300, "wet_cells": wv, "active_cells": av}
+        if not cull:
+            bytes_step = algorithmic_bytes("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32", m.n, wv, av)["k_steps"]
+            gbs = bytes_step / (ms * 1e-3 / 300) / 1e9
+            r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step, "achieved": gbs, "peak": hbm,
+                             "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind}
+        res[name] = r
         c.close()
     return w, res
 
@@ -371,14 +389,13 @@ def main():
     alg = algorithmic_bytes(head, m.n, r["n_wet"], r["n_act"])
     hbm, peak_kind = peaks()
     avg_ms = tr[dom][0] / tr[dom][1]
-    achieved = alg.get(dom, 0.0) / (avg_ms * 1e-3) / 1e9
+    steps_per_launch = tr[dom][2] / tr[dom][1]
+    achieved = alg.get(dom, 0.0) * steps_per_launch / (avg_ms * 1e-3) / 1e9
 
     fwd = None
     if not args.no_forward:
         w2, f2 = forward_config2(args, ws, local)
-        fwd = {"workload": w2.name, "cells": w2.mesh.n, "steps": 300,
-               "value_fp32_split": f2["fp32"]["value"], "value_fp32_full_sweep": f2["fp32_full_sweep"]["value"],
-               "value_fp64": f2["fp64"]["value"], "kernel_ms": {k: v["kernel_ms"] for k, v in f2.items()}}
+        fwd = {"workload": w2.name, "cells": w2.mesh.n, "steps": 300, "unit": "cell-updates/s", **f2}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -387,7 +404,7 @@ def main():
                "sample": sample + "; forward steps only (no CPU fwd+adjoint sweep exists)"}
 
     if rank == 0:
-        launches_per_run = sum(n for _, n in tr.values())
+        launches_per_run = sum(v[1] for v in tr.values())
         line = {
             "metric": METRIC, "value": hr["value"], "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": hr["ms"] / args.steps, "higher_is_better": True,
@@ -403,9 +420,11 @@ def main():
                            "over_fp64": r["fp32"]["value"] / r["fp64"]["value"], "rel_err_vs_fp64": errs,
                            "within_tolerance": fp32_ok, "e2e": r["fp32"]["e2e"]["value"]},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": peak_kind, "alg_bytes_per_launch": alg.get(dom),
+                         "frac": achieved / hbm, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg.get(dom, 0.0) * steps_per_launch,
+                         "steps_per_launch": steps_per_launch,
                          "avg_launch_ms": avg_ms, "wet_cells_avg": r["n_wet"], "active_cells_avg": r["n_act"],
-                         "trace_ms_launches": {k: [round(v[0], 4), v[1]] for k, v in tr.items()},
+                         "trace_ms_launches_steps": {k: [round(v[0], 4), v[1], v[2]] for k, v in tr.items()},
                          "traffic": traffic_per_launch(head, dom)},
             "e2e": hr["e2e"],
             "gpu_launches": int(launches_per_run * args.steps),

@@ -337,7 +337,7 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
         }
     }
     // the caller's lambda differs from buffer 1 everywhere
-    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
     if (!st) st = store(ctx, 0);
     if (!st) st = launch_forward_step(ctx, ctx->mask);
     if (!st) st = launch_adjoint_step(ctx, 0, 1, sec2, cos_int);

@@ -38,6 +38,11 @@ __device__ __forceinline__ R kact_of(const MatConsts &mc, int mat, uint8_t code)
     return code == 0 ? R(mc.kact_rest) : R(mc.kact_sgn[mat][code - 1]);
 }
 
+// The 8 one-byte segment flags of tile t as one 8-byte load (flag arrays are padded to tiles).
+__device__ __forceinline__ unsigned long long seg_flags8(const uint8_t *flags, int t) {
+    return *reinterpret_cast<const unsigned long long *>(flags + (size_t)t * 8);
+}
+
 // Mask byte of cell i in the current recording step: tiles the step did not list count as zero.
 __device__ __forceinline__ uint8_t mask_of(const uint8_t *__restrict__ mask, const int *__restrict__ epoch, int rec_id,
                                            int i) {
@@ -238,8 +243,8 @@ __device__ __forceinline__ void riemann_adj(int dir, const Side<R> &L, const Sid
 struct AdjArgs {
     const uint8_t *mask;                // branch codes of the replayed forward step
     const int *tile_epoch;              // recording step that last listed each tile
-    const uint8_t *tile_act;
-    uint8_t *lam_clean;                 // both adjoint buffers hold the same tile
+    const uint8_t *seg_act;             // [nseg] the segment had an active cell in that step
+    uint8_t *lam_clean;                 // [nseg] both adjoint buffers hold the same segment
     int rec_id;
     int ntiles;
     double *A;                          // [3][n] source adjoint of each cell (FP64)
@@ -263,7 +268,7 @@ __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       // a wet cell is active, so its tile was listed by the recording step and had an active cell
-      const bool need = tq < aa.ntiles && aa.tile_epoch[tq] == aa.rec_id && aa.tile_act[tq];
+      const bool need = tq < aa.ntiles && aa.tile_epoch[tq] == aa.rec_id && seg_flags8(aa.seg_act, tq) != 0ull;
       const int cnt = compact_tiles(need, tq, list);
       for (int q = 0; q < cnt; ++q) {
         const int i = list[q] * kBlock + threadIdx.x;
@@ -380,15 +385,18 @@ __device__ __forceinline__ void adj_gather_phase(const MeshArgs &m, const StateR
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       bool need = false;
-      if (tq < aa.ntiles) need = (aa.tile_epoch[tq] == aa.rec_id && aa.tile_act[tq]) || !aa.lam_clean[tq];
+      if (tq < aa.ntiles)
+          need = (aa.tile_epoch[tq] == aa.rec_id && seg_flags8(aa.seg_act, tq) != 0ull) ||
+                 seg_flags8(aa.lam_clean, tq) != 0x0101010101010101ull;
       const int cnt = compact_tiles(need, tq, list);
       for (int q = 0; q < cnt; ++q) {
         const int t = list[q];
-        const bool tile_active = aa.tile_epoch[t] == aa.rec_id && aa.tile_act[t];
-        if (threadIdx.x == 0) aa.lam_clean[t] = tile_active ? 0 : 1;
         const int j = t * kBlock + threadIdx.x;
+        const bool recorded = aa.tile_epoch[t] == aa.rec_id;
+        const bool seg_active = recorded && aa.seg_act[j >> 5];
+        if ((threadIdx.x & 31) == 0) aa.lam_clean[j >> 5] = seg_active ? 0 : 1;
         if (j >= m.n) continue;
-        const uint8_t mj = tile_active ? aa.mask[j] : uint8_t(0);
+        const uint8_t mj = seg_active ? aa.mask[j] : uint8_t(0);
         if (!(mj & 8)) {
             // not active in the forward step: its update was the identity, and no neighbour is wet
             Lout.h[j] = Lnext.h[j];

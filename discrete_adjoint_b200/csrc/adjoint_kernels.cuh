@@ -12,7 +12,7 @@ AdjArgs adj_args(da_ctx *ctx, const double *sec2, double cos_int) {
     AdjArgs a;
     a.mask = ctx->mask;
     a.tile_epoch = ctx->tile_epoch;
-    a.tile_act = ctx->tile_act;
+    a.seg_act = ctx->seg_act;
     a.lam_clean = ctx->lam_clean;
     a.rec_id = ctx->rec_id;
     a.ntiles = ctx->ntiles;
@@ -54,7 +54,7 @@ int seed_t(da_ctx *ctx, int lam_out, const double box[4]) {
     StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
     // lambda^N is written everywhere: the two adjoint buffers differ on every tile
-    cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream);
+    cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream);
     trace_begin(ctx, TR_ADJ_SEED);
     k_adj_seed<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, Lo, box[0], box[1], box[2], box[3], ctx->seed_part,
                                                              ctx->seed_J, ctx->seed_counter);
@@ -80,21 +80,20 @@ int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
 // branch codes recorded (coefficient phase, barrier, dt, update phase), a barrier, the source
 // adjoint, a barrier and the gather, i.e. the four launches of the separate path with grid
 // barriers instead of kernel boundaries.  U^n stays in buffer cur; U^{n+1} goes to cur ^ 1.
-// Block 0 writes the step's scalars and the volume at the end, as the separate kernels do.
+// Block 0 writes the step's scalars at the end, as the separate kernels do.
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
-                                                    uint8_t *clean, uint8_t *tile_wet, double *tile_vol, int ntiles,
+                                                    uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol, int ntiles,
                                                     int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
-                                                    uint8_t *mask, int *tile_epoch, uint8_t *tile_act, int rec_id,
+                                                    uint8_t *mask, int *tile_epoch, uint8_t *seg_act, int rec_id,
                                                     StateRef<R> Ln, StateOut<R> Lo, AdjArgs aa) {
-    __shared__ double red[kBlock / 32];
     __shared__ int list[kBlock];
     const double time = sc->time;
     const long long iter = sc->iter;
     const StateRef<R> U{S.h[cur], S.hu[cur], S.hv[cur]};
     const StateOut<R> O{S.h[cur ^ 1], S.hu[cur ^ 1], S.hv[cur ^ 1]};
     unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-    fwd::coef_phase<R, true>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
+    fwd::coef_phase<R, true>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
     fwd::push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (!fwd::grid_sync(sc)) return;
     const double min_dxe = __longlong_as_double(__ldcg(&sc->acc_min_dxe));
@@ -102,16 +101,14 @@ __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R
     double dt, ft;
     fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-    fwd::update_phase<R, true>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, R(dt), ftr, mask,
-                               tile_epoch, tile_act, rec_id, list, red);
+    fwd::update_phase<R, true>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, R(dt), ftr,
+                               mask, tile_epoch, seg_act, rec_id, list);
     if (!fwd::grid_sync(sc)) return;
     adj_src_phase<R>(m, U, Ln, mc, aa, R(dt), ftr, list);
     if (!fwd::grid_sync(sc)) return;
     adj_gather_phase<R>(m, U, Ln, Lo, mc, aa, R(dt), list);
     if (blockIdx.x == 0) {
-        const double v = fwd::volume_sum(tile_vol, ntiles, red);
         if (threadIdx.x == 0) {
-            sc->volume = v;
             sc->time = time + dt;
             sc->iter = iter + 1;
             sc->dt = dt;
@@ -150,17 +147,17 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     int cur = ctx->cur, ntiles = ctx->ntiles, cull = ctx->p.tile_culling, rec_id = ctx->rec_id;
     R *kact = (R *)ctx->kact;
     unsigned *active = ctx->active;
-    uint8_t *clean = ctx->clean, *tile_wet = ctx->tile_wet, *mask = ctx->mask, *tile_act = ctx->tile_act;
+    uint8_t *seg_clean = ctx->seg_clean, *seg_wet = ctx->seg_wet, *mask = ctx->mask, *seg_act = ctx->seg_act;
     int *tile_epoch = ctx->tile_epoch;
-    double *tile_vol = ctx->tile_vol;
+    double *seg_vol = ctx->seg_vol;
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
     StateRef<R> Ln{(const R *)ctx->lam[lam_in][0], (const R *)ctx->lam[lam_in][1], (const R *)ctx->lam[lam_in][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
     AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
-    void *args[] = {&m,  &S,     &cur,   &kact,       &active,  &clean,  &tile_wet, &tile_vol, &ntiles, &cull,
-                    &mc, &tc,    &sc,    &mask,       &tile_epoch, &tile_act, &rec_id, &Ln, &Lo, &aa};
+    void *args[] = {&m,  &S,  &cur,  &kact, &active,     &seg_clean, &seg_wet, &seg_vol, &ntiles, &cull,
+                    &mc, &tc, &sc,   &mask, &tile_epoch, &seg_act,   &rec_id,  &Ln,      &Lo,     &aa};
     trace_begin(ctx, TR_YOUTURN);
     const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_youturn<R>, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx);

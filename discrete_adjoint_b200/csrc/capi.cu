@@ -129,12 +129,13 @@ static void free_state(da_ctx *ctx) {
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
     dfree(ctx->kact);
-    dfree(ctx->tile_vol);
+    dfree(ctx->seg_vol);
+    dfree(ctx->vol_parts);
     dfree(ctx->active);
-    dfree(ctx->clean);
-    dfree(ctx->tile_wet);
+    dfree(ctx->seg_clean);
+    dfree(ctx->seg_wet);
     dfree(ctx->tile_epoch);
-    dfree(ctx->tile_act);
+    dfree(ctx->seg_act);
     dfree(ctx->lam_clean);
     ctx->have_state = false;
 }
@@ -474,6 +475,7 @@ int da_forward_step(da_ctx *ctx, da_step_stats *out) {
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_step: no state");
     cudaSetDevice(ctx->device);
     int st = launch_forward_step(ctx);
+    if (!st) st = launch_volume(ctx);
     if (!st) st = sync_scalars(ctx);
     fill_stats(ctx, out);
     return st;
@@ -506,6 +508,7 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
+    if (!st) st = launch_volume(ctx);
     if (!st) st = sync_scalars(ctx);
     fill_stats(ctx, last);
     return st;
@@ -529,6 +532,7 @@ int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
     t.on = true;
     for (int s = 0; s < nsteps && !st; ++s) st = launch_forward_step(ctx);
     if (!st) st = trace_flush(ctx);
+    if (!st) st = launch_volume(ctx);
     t.on = was_on;
     if (!st) st = sync_scalars(ctx);
     const int kinds[2] = {TR_COEF, TR_UPDATE};

@@ -112,13 +112,16 @@ struct da_ctx {
     void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     void *kact = nullptr;            // [n] Real
-    double *tile_vol = nullptr;      // [ntiles] cached volume partial of each tile
-    unsigned *active = nullptr;      // [ceil(n/32)] bit per cell: wet or next to a wet cell
-    uint8_t *clean = nullptr;        // [ntiles] 1 when both state buffers hold the same tile
-    uint8_t *tile_wet = nullptr;     // [ntiles] 1 when the tile held a wet cell after the last update
+    // segments: 32 consecutive cells (one warp), 8 per tile; arrays padded to whole tiles
+    int nseg = 0;                    // ntiles * 8
+    double *seg_vol = nullptr;       // [nseg] volume partial of each segment after its last update
+    double *vol_parts = nullptr;     // [256] partial sums of the volume reduction
+    unsigned *active = nullptr;      // [nseg] bit per cell: wet or next to a wet cell
+    uint8_t *seg_clean = nullptr;    // [nseg] 1 when both state buffers hold the same segment
+    uint8_t *seg_wet = nullptr;      // [nseg] 1 when the segment held a wet cell after the last update
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
-    uint8_t *tile_act = nullptr;     // [ntiles] the tile had an active cell in that step
-    uint8_t *lam_clean = nullptr;    // [ntiles] both adjoint buffers hold the same tile
+    uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
+    uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment
     int rec_id = 0;                  // id of the current recording step
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
@@ -166,6 +169,8 @@ void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask = nullptr);
 int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask);
 int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask);
+// the volume (sum dx dy h) of the current state into the device scalars
+int launch_volume(da_ctx *ctx);
 // nsteps whole steps in one cooperative launch (k_steps); same results as nsteps single steps
 int launch_forward_steps(da_ctx *ctx, int nsteps);
 int launch_forward_steps_fp64(da_ctx *ctx, int nsteps);

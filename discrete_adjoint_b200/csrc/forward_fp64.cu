@@ -10,16 +10,18 @@ int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
 }
 int launch_forward_steps_fp64(da_ctx *ctx, int nsteps) { return fwd::launch_steps_t<double>(ctx, nsteps); }
 
+int launch_volume(da_ctx *ctx) { return fwd::launch_volume_t(ctx); }
+
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
     ctx->ntiles = int((n + fwd::kBlock - 1) / fwd::kBlock);
-    // persistent kernels: 4 blocks of 256 threads per SM, never more blocks than tiles
+    ctx->nseg = ctx->ntiles * (fwd::kBlock / 32);
+    // seed kernel grid: 4 blocks of 256 threads per SM, never more blocks than tiles
     const int cap = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
     ctx->nblocks = ctx->ntiles < cap ? ctx->ntiles : cap;
     update_grid(ctx);
-    // the active bitmask is padded to whole tiles (8 words each) for the 16-byte tile tests
-    const size_t words = (size_t)ctx->ntiles * (fwd::kBlock / 32);
+    const size_t nseg = (size_t)ctx->nseg;
     int st = DA_OK;
     for (int b = 0; b < 2 && !st; ++b)
         for (int v = 0; v < 3 && !st; ++v) {
@@ -27,27 +29,29 @@ int forward_alloc(da_ctx *ctx) {
             if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->U[b][v], 0, rs * n, ctx->stream), "memset");
         }
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_wet, ctx->ntiles), "cudaMalloc(tile_wet)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_wet, nseg), "cudaMalloc(seg_wet)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_epoch, sizeof(int) * ctx->ntiles), "cudaMalloc(epoch)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_epoch, 0xff, sizeof(int) * ctx->ntiles, ctx->stream), "memset");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_act, ctx->ntiles), "cudaMalloc(tile_act)");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->lam_clean, ctx->ntiles), "cudaMalloc(lam_clean)");
-    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->ntiles, ctx->stream), "memset");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_vol, sizeof(double) * ctx->ntiles), "cudaMalloc(vol)");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->active, sizeof(unsigned) * words), "cudaMalloc(active)");
-    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * words, ctx->stream), "memset");
-    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->clean, ctx->ntiles), "cudaMalloc(clean)");
-    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->clean, 0, ctx->ntiles, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_act, nseg), "cudaMalloc(seg_act)");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->lam_clean, nseg), "cudaMalloc(lam_clean)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_vol, sizeof(double) * nseg), "cudaMalloc(vol)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_vol, 0, sizeof(double) * nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->vol_parts, sizeof(double) * fwd::kVolParts), "cudaMalloc(vol)");
+    // the active bitmask is padded to whole tiles (8 words each) for the 16-byte tile tests
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->active, sizeof(unsigned) * nseg), "cudaMalloc(active)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_clean, nseg), "cudaMalloc(clean)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_clean, 0, nseg, ctx->stream), "memset");
     return st;
 }
 
 int forward_state_changed(da_ctx *ctx) {
-    // the buffers no longer hold the same tiles, any tile may be wet, no cell is marked active
-    int st = cuda_check(ctx, cudaMemsetAsync(ctx->clean, 0, ctx->ntiles, ctx->stream), "memset");
-    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_wet, 1, ctx->ntiles, ctx->stream), "memset");
-    if (!st)
-        st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * ((ctx->mesh.n + 31) / 32), ctx->stream),
-                        "memset");
+    // the buffers no longer hold the same segments, any segment may be wet, no cell is marked active
+    const size_t nseg = (size_t)ctx->nseg;
+    int st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_clean, 0, nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_wet, 1, nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * nseg, ctx->stream), "memset");
     return st;
 }
 

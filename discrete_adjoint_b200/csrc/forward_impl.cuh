@@ -28,6 +28,13 @@ namespace {  // internal linkage: each precision TU keeps its own copy
 using namespace fv;
 
 constexpr int kBlock = kTileCells;  // one thread per cell of a tile
+constexpr unsigned long long kAllSegs = 0x0101010101010101ull;  // a flag byte set in all 8 segments
+constexpr int kVolParts = 256;  // fixed partition of the volume sum
+
+// The 8 one-byte segment flags of tile t as one 8-byte load (flag arrays are padded to tiles).
+__device__ __forceinline__ unsigned long long seg_flags(const uint8_t *flags, int t) {
+    return *reinterpret_cast<const unsigned long long *>(flags + (size_t)t * 8);
+}
 
 // dt from the reduced CFL bound and hmax (get_coef_and_eigen.C:168-179 with the single-rank
 // MPI_Allreduce(MIN)), then TimeProps::incrtime.  frict_tiny follows hpfem.C:232-235 with the
@@ -84,8 +91,9 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 
 
 // ----------------------------------------------------------------------------- k_coef
-// One thread per cell of each listed tile.  With tile culling, a tile that held no wet cell
-// after the last update is not listed (its depths cannot have changed since).  Wet cells
+// One thread per cell of each listed tile.  With tile culling, a tile none of whose 32-cell
+// segments held a wet cell after the last update is not listed (its depths cannot have changed
+// since).  Wet cells
 // (h >= GEOFLOW_TINY) also mark themselves and their face neighbours in the active bitmask that
 // k_update reads: a cell outside that set has zero fluxes and no sources this step.
 // RECORD: also writes the branch code of every cell of a listed tile into mask (0 dry / at rest,
@@ -93,12 +101,12 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // The thread's CFL min and hmax (bit patterns of positive doubles) accumulate in my_min / my_max.
 template <class R, bool RECORD>
 __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> &U, R *kact, unsigned *active,
-                                           const uint8_t *tile_wet, int ntiles, int cull, const MatConsts &mc,
+                                           const uint8_t *seg_wet, int ntiles, int cull, const MatConsts &mc,
                                            DevScalars *sc, uint8_t *mask, int *list, unsigned long long &my_min,
                                            unsigned long long &my_max) {
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
-        const bool need = tq < ntiles && (!cull || tile_wet[tq]);
+        const bool need = tq < ntiles && (!cull || seg_flags(seg_wet, tq) != 0ull);
         const int cnt = compact_tiles(need, tq, list);
         for (int q = 0; q < cnt; ++q) {
             const int i = list[q] * kBlock + threadIdx.x;
@@ -162,13 +170,13 @@ __device__ __forceinline__ void push_minmax(unsigned long long my_min, unsigned 
 
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
-                                                 unsigned *__restrict__ active, const uint8_t *__restrict__ tile_wet,
+                                                 unsigned *__restrict__ active, const uint8_t *__restrict__ seg_wet,
                                                  int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
                                                  uint8_t *__restrict__ mask = nullptr) {
     __shared__ int list[kBlock];
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
-    coef_phase<R, RECORD>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
+    coef_phase<R, RECORD>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
     push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (last_block(&sc->blocks_done[0])) {
         if (threadIdx.x == 0) {
@@ -261,28 +269,29 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 }
 
 // ---------------------------------------------------------------------------- k_update
-// Tiles of kBlock consecutive cells through the strided tile list.  A tile is listed when it has
-// an active cell, or when its two ping-pong buffers differ (not clean), or when culling is off.
-// In a listed tile, active cells get the full update and the others are copied (their update is
-// the identity).  A tile that is not listed is already identical in both buffers.  Each listed
-// tile stores its volume partial, its clean flag and whether it now holds a wet cell; the volume
-// is the sum of every tile's partial in a fixed order, so it depends neither on culling nor on
-// the grid.
+// Tiles of kBlock consecutive cells through the strided tile list; each warp owns one 32-cell
+// segment of a tile and keeps that segment's flags, so a tile needs no block-wide step.  A tile
+// is listed when a cell of it is active, when a segment's two ping-pong buffers differ (not
+// clean), or when culling is off.  In a listed tile, active cells get the full update and the
+// others are copied (their update is the identity); a tile that is not listed is already
+// identical in both buffers.  Each segment stores its volume partial (the volume is their sum in
+// a fixed order, so it depends neither on culling nor on the grid), its clean flag and whether it
+// now holds a wet cell.
 // RECORD: every cell of a listed tile gets its full mask byte (the k_coef code of a wet cell,
-// bit 3 active, bit 2 depth clamped) and the tile records the step id (tile_epoch) and whether
-// it had an active cell (tile_act); masks of tiles with another epoch count as zero.
+// bit 3 active, bit 2 depth clamped), the tile records the step id (tile_epoch) and each segment
+// whether it had an active cell (seg_act); masks of tiles with another epoch count as zero.
 template <class R, bool RECORD>
 __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R> &U, const StateOut<R> &O,
-                                             const R *kact, unsigned *active, uint8_t *clean, uint8_t *tile_wet,
-                                             double *tile_vol, int ntiles, int cull, const MatConsts &mc,
+                                             const R *kact, unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
+                                             double *seg_vol, int ntiles, int cull, const MatConsts &mc,
                                              DevScalars *sc, R dt, R ft, uint8_t *mask, int *tile_epoch,
-                                             uint8_t *tile_act, int rec_id, int *list, double *red) {
+                                             uint8_t *seg_act, int rec_id, int *list) {
     const int lane = threadIdx.x & 31;
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
         bool need = false;
         if (tq < ntiles) {
-            need = !cull || !clean[tq];
+            need = !cull || seg_flags(seg_clean, tq) != kAllSegs;
             if (!need) {
                 // the tile's 8 bitmask words in two 16-byte loads (the bitmask is padded to
                 // whole tiles)
@@ -295,8 +304,8 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
         for (int q = 0; q < cnt; ++q) {
             const int t = list[q];
             const int i = t * kBlock + threadIdx.x;
-            const unsigned word = (i < m.n) ? active[i >> 5] : 0u;
-            const bool tile_active = __syncthreads_or(word != 0u);
+            const int seg = i >> 5;
+            const unsigned word = active[seg];  // padded: bits of cells >= n are never set
             double vol = 0.0;
             bool wet_after = false;
             if (i < m.n) {
@@ -315,59 +324,59 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
                 vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
             }
-            __syncwarp();
-            if (lane == 0 && word) active[i >> 5] = 0u;
-            const bool any_wet = __syncthreads_or(wet_after);
-            const double tv = block_sum(vol, red);
-            if (threadIdx.x == 0) {
-                tile_vol[t] = tv;
-                clean[t] = tile_active ? 0 : 1;
-                tile_wet[t] = any_wet ? 1 : 0;
-                if (RECORD) {
-                    tile_epoch[t] = rec_id;
-                    tile_act[t] = tile_active ? 1 : 0;
-                }
+            const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
+            vol = warp_sum(vol);
+            if (lane == 0) {
+                if (word) active[seg] = 0u;
+                seg_vol[seg] = vol;
+                seg_clean[seg] = word ? 0 : 1;
+                seg_wet[seg] = wet_bits ? 1 : 0;
+                if (RECORD) seg_act[seg] = word ? 1 : 0;
             }
+            if (RECORD && threadIdx.x == 0) tile_epoch[t] = rec_id;
         }
     }
-}
-
-// Sum of the tiles' volume partials in a fixed order (thread q takes tiles q, q + 256, ... in
-// four interleaved running sums; then the block sum); every thread of the calling block must
-// enter.  Loads go through L2 (the partials were written by other blocks).
-__device__ __forceinline__ double volume_sum(const double *tile_vol, int ntiles, double *red) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int b = threadIdx.x;
-    for (; b + 3 * kBlock < ntiles; b += 4 * kBlock) {
-        a0 += __ldcg(tile_vol + b);
-        a1 += __ldcg(tile_vol + b + kBlock);
-        a2 += __ldcg(tile_vol + b + 2 * kBlock);
-        a3 += __ldcg(tile_vol + b + 3 * kBlock);
-    }
-    for (; b < ntiles; b += kBlock) a0 += __ldcg(tile_vol + b);
-    return block_sum((a0 + a1) + (a2 + a3), red);
 }
 
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
                                                    const R *__restrict__ kact, unsigned *__restrict__ active,
-                                                   uint8_t *__restrict__ clean, uint8_t *__restrict__ tile_wet,
-                                                   double *__restrict__ tile_vol, int ntiles, int cull, MatConsts mc,
+                                                   uint8_t *__restrict__ seg_clean, uint8_t *__restrict__ seg_wet,
+                                                   double *__restrict__ seg_vol, int ntiles, int cull, MatConsts mc,
                                                    DevScalars *sc, uint8_t *__restrict__ mask = nullptr,
                                                    int *__restrict__ tile_epoch = nullptr,
-                                                   uint8_t *__restrict__ tile_act = nullptr, int rec_id = 0) {
-    __shared__ double red[kBlock / 32];
+                                                   uint8_t *__restrict__ seg_act = nullptr, int rec_id = 0) {
     __shared__ int list[kBlock];
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
-    update_phase<R, RECORD>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, dt, ft, mask,
-                            tile_epoch, tile_act, rec_id, list, red);
-    if (last_block(&sc->blocks_done[1])) {
-        const double t = volume_sum(tile_vol, ntiles, red);
-        if (threadIdx.x == 0) {
-            sc->volume = t;
-            sc->blocks_done[1] = 0;
-        }
+    update_phase<R, RECORD>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, dt, ft, mask,
+                            tile_epoch, seg_act, rec_id, list);
+}
+
+// ---------------------------------------------------------------------------- volume
+// sum of dx dy h over the mesh (step.C:205) from the segments' partials, in a fixed order: block
+// b of kVolParts sums a fixed contiguous range of segments, then one block adds the parts.
+// Launched only when the volume is asked for.
+__global__ void __launch_bounds__(kBlock) k_volume_parts(const double *__restrict__ seg_vol, int nseg,
+                                                         double *__restrict__ parts) {
+    __shared__ double red[kBlock / 32];
+    const int per = (nseg + kVolParts - 1) / kVolParts;
+    const int s0 = blockIdx.x * per, s1 = min(nseg, s0 + per);
+    double acc = 0.0;
+    for (int s = s0 + threadIdx.x; s < s1; s += kBlock) acc += seg_vol[s];
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) parts[blockIdx.x] = acc;
+}
+
+__global__ void __launch_bounds__(kVolParts) k_volume_final(const double *__restrict__ parts, DevScalars *sc) {
+    __shared__ double red[kVolParts / 32];
+    const double v = warp_sum(parts[threadIdx.x]);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kVolParts / 32; ++w) t += red[w];
+        sc->volume = t;
     }
 }
 
@@ -376,7 +385,7 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
 // phase, a grid barrier, dt (every block forms the same dt from the same reduced values), the
 // update phase and a second barrier.  Odd and even steps accumulate the CFL min / hmax in two
 // pairs, so block 0 can restart one pair while the other is read.  time and iteration advance
-// in registers; block 0 writes them, the last step's scalars and the volume at the end.  The
+// in registers; block 0 writes them and the last step's scalars at the end.  The
 // state buffers alternate as in single steps and are read with coherent loads (no read-only
 // cache: other blocks wrote them earlier in the same launch).
 // The barrier waits are bounded: after ~4 s a block raises DA_ERR_TIMEOUT and returns, and the
@@ -428,10 +437,9 @@ struct StatePair {
 
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
-                                                  unsigned *active, uint8_t *clean, uint8_t *tile_wet,
-                                                  double *tile_vol, int ntiles, int cull, MatConsts mc,
+                                                  unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
+                                                  double *seg_vol, int ntiles, int cull, MatConsts mc,
                                                   TimeConsts tc, DevScalars *sc) {
-    __shared__ double red[kBlock / 32];
     __shared__ int list[kBlock];
     double time = sc->time;
     long long iter = sc->iter;
@@ -443,7 +451,7 @@ __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, in
         const StateRef<R> U{S.h[c], S.hu[c], S.hv[c]};
         const StateOut<R> O{S.h[c ^ 1], S.hu[c ^ 1], S.hv[c ^ 1]};
         unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-        coef_phase<R, false>(m, U, kact, active, tile_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max);
+        coef_phase<R, false>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max);
         push_minmax(my_min, my_max, acc_min, acc_max);
         if (!grid_sync(sc)) return;
         min_dxe = __longlong_as_double(__ldcg(acc_min));
@@ -457,14 +465,12 @@ __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, in
             *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
         }
         const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-        update_phase<R, false>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, cull, mc, sc, R(dt), ftr,
-                               nullptr, nullptr, nullptr, 0, list, red);
+        update_phase<R, false>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, R(dt), ftr,
+                               nullptr, nullptr, nullptr, 0, list);
         if (!grid_sync(sc)) return;
     }
     if (blockIdx.x == 0) {
-        const double v = volume_sum(tile_vol, ntiles, red);
         if (threadIdx.x == 0) {
-            sc->volume = v;
             sc->time = time;
             sc->iter = iter;
             sc->dt = dt;
@@ -489,21 +495,22 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
         // branch recording for the adjoint: codes and flags for every cell of the listed tiles
         ++ctx->rec_id;
         trace_begin(ctx, TR_COEF_REC);
-        k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull,
+        k_coef<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->seg_wet, tiles, cull,
                                                           ctx->mc, ctx->tc, ctx->dsc, record_mask);
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE_REC);
-        k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                            ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc, record_mask, ctx->tile_epoch, ctx->tile_act, ctx->rec_id);
+        k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->seg_clean, ctx->seg_wet,
+                                                            ctx->seg_vol, tiles, cull, ctx->mc, ctx->dsc, record_mask,
+                                                            ctx->tile_epoch, ctx->seg_act, ctx->rec_id);
         trace_end(ctx);
     } else {
         trace_begin(ctx, TR_COEF);
-        k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->tile_wet, tiles, cull, ctx->mc,
+        k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->seg_wet, tiles, cull, ctx->mc,
                                                     ctx->tc, ctx->dsc);
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE);
-        k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->clean, ctx->tile_wet,
-                                                      ctx->tile_vol, tiles, cull, ctx->mc, ctx->dsc);
+        k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->seg_clean, ctx->seg_wet,
+                                                      ctx->seg_vol, tiles, cull, ctx->mc, ctx->dsc);
         trace_end(ctx);
     }
     ctx->cur = o;
@@ -535,18 +542,25 @@ int launch_steps_t(da_ctx *ctx, int nsteps) {
     int cur = ctx->cur, n = nsteps, ntiles = ctx->ntiles, cull = ctx->p.tile_culling;
     R *kact = (R *)ctx->kact;
     unsigned *active = ctx->active;
-    uint8_t *clean = ctx->clean, *tile_wet = ctx->tile_wet;
-    double *tile_vol = ctx->tile_vol;
+    uint8_t *seg_clean = ctx->seg_clean, *seg_wet = ctx->seg_wet;
+    double *seg_vol = ctx->seg_vol;
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
-    void *args[] = {&m, &S, &cur, &n, &kact, &active, &clean, &tile_wet, &tile_vol, &ntiles, &cull, &mc, &tc, &sc};
+    void *args[] = {&m, &S, &cur, &n, &kact, &active, &seg_clean, &seg_wet, &seg_vol, &ntiles, &cull, &mc, &tc, &sc};
     trace_begin(ctx, TR_STEPS);
     const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_steps<R>, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx, nsteps);
     if (e != cudaSuccess) return cuda_check(ctx, e, "multi-step launch");
     ctx->cur = (cur + nsteps) & 1;
     return DA_OK;
+}
+
+// The volume of the current state into the scalars (two launches, fixed order).
+inline int launch_volume_t(da_ctx *ctx) {
+    k_volume_parts<<<kVolParts, kBlock, 0, ctx->stream>>>(ctx->seg_vol, ctx->nseg, ctx->vol_parts);
+    k_volume_final<<<1, kVolParts, 0, ctx->stream>>>(ctx->vol_parts, ctx->dsc);
+    return cuda_check(ctx, cudaGetLastError(), "volume launch");
 }
 
 }  // namespace

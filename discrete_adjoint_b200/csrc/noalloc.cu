@@ -27,10 +27,12 @@ constexpr size_t kOffKact = 0;
 constexpr size_t kOffActive = align256(kOffKact + kMaxCells * sizeof(double));
 constexpr size_t kOffBflag = align256(kOffActive + (kMaxCells / 32) * sizeof(unsigned));
 constexpr size_t kOffMat = align256(kOffBflag + kMaxCells);
+constexpr size_t kMaxSegs = kMaxTiles * (fwd::kBlock / 32);
 constexpr size_t kOffClean = align256(kOffMat + kMaxCells);
-constexpr size_t kOffTileWet = align256(kOffClean + kMaxTiles);
-constexpr size_t kOffTileVol = align256(kOffTileWet + kMaxTiles);
-constexpr size_t kOffScalars = align256(kOffTileVol + kMaxTiles * sizeof(double));
+constexpr size_t kOffSegWet = align256(kOffClean + kMaxSegs);
+constexpr size_t kOffSegVol = align256(kOffSegWet + kMaxSegs);
+constexpr size_t kOffVolParts = align256(kOffSegVol + kMaxSegs * sizeof(double));
+constexpr size_t kOffScalars = align256(kOffVolParts + fwd::kVolParts * sizeof(double));
 constexpr size_t kScratchBytes = align256(kOffScalars + sizeof(DevScalars));
 
 // The scratch of every call.  Host code must not take this name as a device address: the
@@ -128,9 +130,10 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     unsigned *active = (unsigned *)(base + noalloc::kOffActive);
     uint8_t *bflag = base + noalloc::kOffBflag;
     uint8_t *mat8 = base + noalloc::kOffMat;
-    uint8_t *clean = base + noalloc::kOffClean;
-    uint8_t *tile_wet = base + noalloc::kOffTileWet;
-    double *tile_vol = (double *)(base + noalloc::kOffTileVol);
+    uint8_t *seg_clean = base + noalloc::kOffClean;
+    uint8_t *seg_wet = base + noalloc::kOffSegWet;
+    double *seg_vol = (double *)(base + noalloc::kOffSegVol);
+    double *vol_parts = (double *)(base + noalloc::kOffVolParts);
     DevScalars *sc = (DevScalars *)(base + noalloc::kOffScalars);
 
     MatConsts mc{};
@@ -139,7 +142,8 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
 
     // the array keeps the previous call's contents: zero the active bitmask, reset the scalars
     noalloc::k_init<<<1, 32, 0, s>>>(sc, time, (long long)iter);
-    if (cudaMemsetAsync(active, 0, sizeof(unsigned) * ((n + 31) / 32), s) != cudaSuccess) return DA_ERR_CUDA;
+    if (cudaMemsetAsync(active, 0, sizeof(unsigned) * (size_t)ntiles * (fwd::kBlock / 32), s) != cudaSuccess)
+        return DA_ERR_CUDA;
     noalloc::k_prep<<<grid, fwd::kBlock, 0, s>>>(n, mesh->nbr, mesh->material, p->n_materials, bflag, mat8, sc);
     if (cudaGetLastError() != cudaSuccess) return DA_ERR_CUDA;
     DevScalars hs;
@@ -163,9 +167,11 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     fv::StateRef<double> U{h, hu, hv};
     fv::StateOut<double> O{h_out, hu_out, hv_out};
     // every tile is processed (no culling across independent calls)
-    fwd::k_coef<double><<<grid, fwd::kBlock, 0, s>>>(m, U, kact, active, tile_wet, ntiles, 0, mc, tc, sc);
-    fwd::k_update<double><<<grid, fwd::kBlock, 0, s>>>(m, U, O, kact, active, clean, tile_wet, tile_vol, ntiles, 0, mc,
-                                                       sc);
+    fwd::k_coef<double><<<grid, fwd::kBlock, 0, s>>>(m, U, kact, active, seg_wet, ntiles, 0, mc, tc, sc);
+    fwd::k_update<double><<<grid, fwd::kBlock, 0, s>>>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, 0,
+                                                       mc, sc);
+    fwd::k_volume_parts<<<fwd::kVolParts, fwd::kBlock, 0, s>>>(seg_vol, ntiles * (fwd::kBlock / 32), vol_parts);
+    fwd::k_volume_final<<<1, fwd::kVolParts, 0, s>>>(vol_parts, sc);
     if (cudaGetLastError() != cudaSuccess) return DA_ERR_CUDA;
     if (cudaMemcpyAsync(&hs, sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s) != cudaSuccess) return DA_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return DA_ERR_CUDA;

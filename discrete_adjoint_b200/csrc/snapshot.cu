@@ -1,7 +1,7 @@
 // Checkpoint copies of the adjoint's reverse sweep: one launch per store or restore.
-// A snapshot holds the state (3 arrays), the per-tile wet flags and the step scalars.  A restore
-// writes the state into both ping-pong buffers, so every tile is clean afterwards and the next
-// steps keep their tile culling.
+// A snapshot holds the state (3 arrays), the per-segment wet flags and the step scalars.  A
+// restore writes the state into both ping-pong buffers, so every segment is clean afterwards and
+// the next steps keep their tile culling.
 #include <cuda_runtime.h>
 
 #include "da_internal.h"
@@ -39,8 +39,8 @@ struct SnapArgs {
     size_t flag_bytes;
     const DevScalars *sc_src;
     DevScalars *sc_dst;
-    uint8_t *clean;          // set to 1 for every tile when not null
-    int ntiles;
+    uint8_t *clean;          // set to 1 for every segment when not null
+    int nseg;
 };
 
 __global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs a) {
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs a) {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (a.clean)
-        for (size_t t = tid; t < (size_t)a.ntiles; t += stride) a.clean[t] = 1;
+        for (size_t t = tid; t < (size_t)a.nseg; t += stride) a.clean[t] = 1;
     if (tid == 0) *a.sc_dst = *a.sc_src;
 }
 
@@ -59,7 +59,7 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 size_t snapshot_bytes(const da_ctx *ctx) {
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
-    return 3 * align256(rs * (size_t)ctx->mesh.n) + align256((size_t)ctx->ntiles) + sizeof(DevScalars);
+    return 3 * align256(rs * (size_t)ctx->mesh.n) + align256((size_t)ctx->nseg) + sizeof(DevScalars);
 }
 
 int launch_snapshot(da_ctx *ctx, void *slot, bool store) {
@@ -67,11 +67,11 @@ int launch_snapshot(da_ctx *ctx, void *slot, bool store) {
     const size_t bytes = rs * (size_t)ctx->mesh.n, ab = align256(bytes);
     unsigned char *base = (unsigned char *)slot;
     unsigned char *flags = base + 3 * ab;
-    DevScalars *ssc = (DevScalars *)(flags + align256((size_t)ctx->ntiles));
+    DevScalars *ssc = (DevScalars *)(flags + align256((size_t)ctx->nseg));
     SnapArgs a{};
     a.bytes = bytes;
-    a.flag_bytes = (size_t)ctx->ntiles;
-    a.ntiles = ctx->ntiles;
+    a.flag_bytes = (size_t)ctx->nseg;
+    a.nseg = ctx->nseg;
     for (int v = 0; v < 3; ++v) {
         if (store) {
             a.src[v] = (const unsigned char *)ctx->U[ctx->cur][v];
@@ -84,17 +84,17 @@ int launch_snapshot(da_ctx *ctx, void *slot, bool store) {
         }
     }
     if (store) {
-        a.flags_src = ctx->tile_wet;
+        a.flags_src = ctx->seg_wet;
         a.flags_dst = flags;
         a.sc_src = ctx->dsc;
         a.sc_dst = ssc;
         a.clean = nullptr;
     } else {
         a.flags_src = flags;
-        a.flags_dst = ctx->tile_wet;
+        a.flags_dst = ctx->seg_wet;
         a.sc_src = ssc;
         a.sc_dst = ctx->dsc;
-        a.clean = ctx->clean;
+        a.clean = ctx->seg_clean;
     }
     int grid = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
     trace_begin(ctx, TR_SNAPSHOT);

@@ -224,7 +224,7 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out);
  * GPU's memory, or a real-time loop in which allocating is forbidden.  The caller passes device
  * pointers for the flattened mesh (same layout as da_upload_mesh's, FP64), for the state in and
  * for the state out (in and out must not overlap); the step's temporaries live in one fixed
- * array of about 10.7 MB that every GPU loading this library holds until the process exits.
+ * array of about 11 MB that every GPU loading this library holds until the process exits.
  * Meshes with more than DA_NOALLOC_MAX_CELLS cells are rejected with DA_ERR_UNSUPPORTED, as is
  * any precision but DA_PREC_FP64; a neighbour or material index out of range gives
  * DA_ERR_INVALID before the step runs.  time/iter are TimeProps::time and ::iter before the
