@@ -83,7 +83,8 @@ int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
 // Block 0 writes the step's scalars at the end, as the separate kernels do.
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
-                                                    uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol, int ntiles,
+                                                    uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
+                                                    uint8_t *seg_dirty, int ntiles,
                                                     int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
                                                     uint8_t *mask, int *tile_epoch, uint8_t *seg_act, int rec_id,
                                                     StateRef<R> Ln, StateOut<R> Lo, AdjArgs aa) {
@@ -101,7 +102,8 @@ __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R
     double dt, ft;
     fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-    fwd::update_phase<R, true>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, R(dt), ftr,
+    fwd::update_phase<R, true>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc,
+                               R(dt), ftr,
                                mask, tile_epoch, seg_act, rec_id, list);
     if (!fwd::grid_sync(sc)) return;
     adj_src_phase<R>(m, U, Ln, mc, aa, R(dt), ftr, list);
@@ -150,14 +152,15 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     uint8_t *seg_clean = ctx->seg_clean, *seg_wet = ctx->seg_wet, *mask = ctx->mask, *seg_act = ctx->seg_act;
     int *tile_epoch = ctx->tile_epoch;
     double *seg_vol = ctx->seg_vol;
+    uint8_t *seg_dirty = ctx->seg_dirty;
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
     StateRef<R> Ln{(const R *)ctx->lam[lam_in][0], (const R *)ctx->lam[lam_in][1], (const R *)ctx->lam[lam_in][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
     AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
-    void *args[] = {&m,  &S,  &cur,  &kact, &active,     &seg_clean, &seg_wet, &seg_vol, &ntiles, &cull,
-                    &mc, &tc, &sc,   &mask, &tile_epoch, &seg_act,   &rec_id,  &Ln,      &Lo,     &aa};
+    void *args[] = {&m,  &S,    &cur,  &kact, &active,     &seg_clean, &seg_wet, &seg_vol, &seg_dirty, &ntiles, &cull,
+                    &mc, &tc,   &sc,   &mask, &tile_epoch, &seg_act,   &rec_id,  &Ln,      &Lo,        &aa};
     trace_begin(ctx, TR_YOUTURN);
     const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_youturn<R>, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx);

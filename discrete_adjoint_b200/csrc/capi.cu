@@ -134,6 +134,7 @@ static void free_state(da_ctx *ctx) {
     dfree(ctx->active);
     dfree(ctx->seg_clean);
     dfree(ctx->seg_wet);
+    dfree(ctx->seg_dirty);
     dfree(ctx->tile_epoch);
     dfree(ctx->seg_act);
     dfree(ctx->lam_clean);

@@ -119,6 +119,7 @@ struct da_ctx {
     unsigned *active = nullptr;      // [nseg] bit per cell: wet or next to a wet cell
     uint8_t *seg_clean = nullptr;    // [nseg] 1 when both state buffers hold the same segment
     uint8_t *seg_wet = nullptr;      // [nseg] 1 when the segment held a wet cell after the last update
+    uint8_t *seg_dirty = nullptr;    // [nseg] 1 when the segment may differ from the base checkpoint
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
     uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
     uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment

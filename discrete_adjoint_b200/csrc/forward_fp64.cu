@@ -43,6 +43,8 @@ int forward_alloc(da_ctx *ctx) {
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * nseg, ctx->stream), "memset");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_clean, nseg), "cudaMalloc(clean)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_clean, 0, nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_dirty, nseg), "cudaMalloc(dirty)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_dirty, 1, nseg, ctx->stream), "memset");
     return st;
 }
 
@@ -52,6 +54,7 @@ int forward_state_changed(da_ctx *ctx) {
     int st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_clean, 0, nseg, ctx->stream), "memset");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_wet, 1, nseg, ctx->stream), "memset");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->active, 0, sizeof(unsigned) * nseg, ctx->stream), "memset");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_dirty, 1, nseg, ctx->stream), "memset");
     return st;
 }
 

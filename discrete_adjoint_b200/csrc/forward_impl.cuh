@@ -283,7 +283,8 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 template <class R, bool RECORD>
 __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R> &U, const StateOut<R> &O,
                                              const R *kact, unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
-                                             double *seg_vol, int ntiles, int cull, const MatConsts &mc,
+                                             double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
+                                             const MatConsts &mc,
                                              DevScalars *sc, R dt, R ft, uint8_t *mask, int *tile_epoch,
                                              uint8_t *seg_act, int rec_id, int *list) {
     const int lane = threadIdx.x & 31;
@@ -327,7 +328,10 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
             vol = warp_sum(vol);
             if (lane == 0) {
-                if (word) active[seg] = 0u;
+                if (word) {
+                    active[seg] = 0u;
+                    seg_dirty[seg] = 1;  // changed since the base checkpoint
+                }
                 seg_vol[seg] = vol;
                 seg_clean[seg] = word ? 0 : 1;
                 seg_wet[seg] = wet_bits ? 1 : 0;
@@ -342,14 +346,15 @@ template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, StateOut<R> O,
                                                    const R *__restrict__ kact, unsigned *__restrict__ active,
                                                    uint8_t *__restrict__ seg_clean, uint8_t *__restrict__ seg_wet,
-                                                   double *__restrict__ seg_vol, int ntiles, int cull, MatConsts mc,
+                                                   double *__restrict__ seg_vol, uint8_t *__restrict__ seg_dirty,
+                                                   int ntiles, int cull, MatConsts mc,
                                                    DevScalars *sc, uint8_t *__restrict__ mask = nullptr,
                                                    int *__restrict__ tile_epoch = nullptr,
                                                    uint8_t *__restrict__ seg_act = nullptr, int rec_id = 0) {
     __shared__ int list[kBlock];
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
-    update_phase<R, RECORD>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, dt, ft, mask,
+    update_phase<R, RECORD>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc, dt, ft, mask,
                             tile_epoch, seg_act, rec_id, list);
 }
 
@@ -438,8 +443,8 @@ struct StatePair {
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
-                                                  double *seg_vol, int ntiles, int cull, MatConsts mc,
-                                                  TimeConsts tc, DevScalars *sc) {
+                                                  double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
+                                                  MatConsts mc, TimeConsts tc, DevScalars *sc) {
     __shared__ int list[kBlock];
     double time = sc->time;
     long long iter = sc->iter;
@@ -465,7 +470,8 @@ __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, in
             *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
         }
         const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-        update_phase<R, false>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, cull, mc, sc, R(dt), ftr,
+        update_phase<R, false>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc,
+                               R(dt), ftr,
                                nullptr, nullptr, nullptr, 0, list);
         if (!grid_sync(sc)) return;
     }
@@ -500,7 +506,8 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE_REC);
         k_update<R, true><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->seg_clean, ctx->seg_wet,
-                                                            ctx->seg_vol, tiles, cull, ctx->mc, ctx->dsc, record_mask,
+                                                            ctx->seg_vol, ctx->seg_dirty, tiles, cull, ctx->mc, ctx->dsc,
+                                                            record_mask,
                                                             ctx->tile_epoch, ctx->seg_act, ctx->rec_id);
         trace_end(ctx);
     } else {
@@ -510,7 +517,7 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
         trace_end(ctx);
         trace_begin(ctx, TR_UPDATE);
         k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->seg_clean, ctx->seg_wet,
-                                                      ctx->seg_vol, tiles, cull, ctx->mc, ctx->dsc);
+                                                      ctx->seg_vol, ctx->seg_dirty, tiles, cull, ctx->mc, ctx->dsc);
         trace_end(ctx);
     }
     ctx->cur = o;
@@ -544,10 +551,12 @@ int launch_steps_t(da_ctx *ctx, int nsteps) {
     unsigned *active = ctx->active;
     uint8_t *seg_clean = ctx->seg_clean, *seg_wet = ctx->seg_wet;
     double *seg_vol = ctx->seg_vol;
+    uint8_t *seg_dirty = ctx->seg_dirty;
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
-    void *args[] = {&m, &S, &cur, &n, &kact, &active, &seg_clean, &seg_wet, &seg_vol, &ntiles, &cull, &mc, &tc, &sc};
+    void *args[] = {&m,        &S,       &cur,       &n,     &kact, &active, &seg_clean, &seg_wet,
+                    &seg_vol,  &seg_dirty, &ntiles,  &cull,  &mc,   &tc,     &sc};
     trace_begin(ctx, TR_STEPS);
     const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_steps<R>, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx, nsteps);

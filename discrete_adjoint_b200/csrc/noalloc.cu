@@ -31,7 +31,8 @@ constexpr size_t kMaxSegs = kMaxTiles * (fwd::kBlock / 32);
 constexpr size_t kOffClean = align256(kOffMat + kMaxCells);
 constexpr size_t kOffSegWet = align256(kOffClean + kMaxSegs);
 constexpr size_t kOffSegVol = align256(kOffSegWet + kMaxSegs);
-constexpr size_t kOffVolParts = align256(kOffSegVol + kMaxSegs * sizeof(double));
+constexpr size_t kOffSegDirty = align256(kOffSegVol + kMaxSegs * sizeof(double));
+constexpr size_t kOffVolParts = align256(kOffSegDirty + kMaxSegs);
 constexpr size_t kOffScalars = align256(kOffVolParts + fwd::kVolParts * sizeof(double));
 constexpr size_t kScratchBytes = align256(kOffScalars + sizeof(DevScalars));
 
@@ -134,6 +135,7 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     uint8_t *seg_wet = base + noalloc::kOffSegWet;
     double *seg_vol = (double *)(base + noalloc::kOffSegVol);
     double *vol_parts = (double *)(base + noalloc::kOffVolParts);
+    uint8_t *seg_dirty = base + noalloc::kOffSegDirty;
     DevScalars *sc = (DevScalars *)(base + noalloc::kOffScalars);
 
     MatConsts mc{};
@@ -168,8 +170,8 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
     fv::StateOut<double> O{h_out, hu_out, hv_out};
     // every tile is processed (no culling across independent calls)
     fwd::k_coef<double><<<grid, fwd::kBlock, 0, s>>>(m, U, kact, active, seg_wet, ntiles, 0, mc, tc, sc);
-    fwd::k_update<double><<<grid, fwd::kBlock, 0, s>>>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, ntiles, 0,
-                                                       mc, sc);
+    fwd::k_update<double><<<grid, fwd::kBlock, 0, s>>>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
+                                                       ntiles, 0, mc, sc);
     fwd::k_volume_parts<<<fwd::kVolParts, fwd::kBlock, 0, s>>>(seg_vol, ntiles * (fwd::kBlock / 32), vol_parts);
     fwd::k_volume_final<<<1, fwd::kVolParts, 0, s>>>(vol_parts, sc);
     if (cudaGetLastError() != cudaSuccess) return DA_ERR_CUDA;

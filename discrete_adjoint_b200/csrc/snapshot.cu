@@ -1,59 +1,133 @@
-// Checkpoint copies of the adjoint's reverse sweep: one launch per store or restore.
-// A snapshot holds the state (3 arrays), the per-segment wet flags and the step scalars.  A
-// restore writes the state into both ping-pong buffers, so every segment is clean afterwards and
-// the next steps keep their tile culling.
+// Checkpoint copies of the adjoint's reverse sweep: one launch per store or restore, one warp
+// per 32-cell segment.
+//
+// Slot 0 is the base checkpoint: a full copy of the state.  Every later store copies only the
+// segments that an update has changed since the base ("dirty" segments, seg_dirty), so a flow that
+// covers a small part of the mesh is checkpointed at the cost of its footprint.  A restore writes
+// into both ping-pong buffers the snapshot's dirty segments, and the base copy of the segments
+// that are dirty now but were not at the snapshot; every other segment already holds the base
+// state in both buffers.  Each restored segment gets its wet flag and volume partial recomputed
+// from the restored depths (the same sums as the update), so culling and the volume stay exact.
+// Afterwards every segment is clean and the live dirty flags are the snapshot's.
 #include <cuda_runtime.h>
 
-#include "da_internal.h"
+#include "fv_device.cuh"
 
 namespace da {
 namespace {
 
+using namespace fv;
+
 constexpr int kBlock = 256;
 
-__device__ __forceinline__ void copy_bytes(const unsigned char *__restrict__ src, unsigned char *__restrict__ dst,
-                                           unsigned char *__restrict__ dst2, size_t bytes) {
-    const size_t nv = bytes / 16;
-    const uint4 *s4 = (const uint4 *)src;
-    uint4 *d4 = (uint4 *)dst;
-    uint4 *e4 = (uint4 *)dst2;
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += stride) {
-        const uint4 v = s4[k];
-        d4[k] = v;
-        if (dst2) e4[k] = v;
-    }
-    for (size_t k = nv * 16 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < bytes; k += stride) {
-        dst[k] = src[k];
-        if (dst2) dst2[k] = src[k];
-    }
-}
+enum SnapMode { STORE_BASE = 0, STORE = 1, RESTORE_BASE = 2, RESTORE = 3 };
 
+template <class R>
 struct SnapArgs {
-    const unsigned char *src[3];
-    unsigned char *dst[3];
-    unsigned char *dst2[3];  // second destination (the other ping-pong buffer) or null
-    size_t bytes;            // per state array
-    const unsigned char *flags_src;
-    unsigned char *flags_dst;
-    size_t flag_bytes;
-    const DevScalars *sc_src;
-    DevScalars *sc_dst;
-    uint8_t *clean;          // set to 1 for every segment when not null
+    MeshArgs m;
+    R *buf[2][3];          // the two ping-pong buffers (h, hu, hv)
+    int cur;               // live buffer
+    R *snap[3];            // this slot's state arrays (only dirty segments are valid after STORE)
+    const R *base[3];      // slot 0's state arrays
+    uint8_t *snap_dirty;   // [nseg] the slot's dirty flags
+    DevScalars *snap_sc;   // the slot's step scalars
+    uint8_t *seg_dirty;    // live flags
+    uint8_t *seg_clean;
+    uint8_t *seg_wet;
+    double *seg_vol;
+    DevScalars *sc;
     int nseg;
+    int mode;
 };
 
-__global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs a) {
-    for (int v = 0; v < 3; ++v) copy_bytes(a.src[v], a.dst[v], a.dst2[v], a.bytes);
-    copy_bytes(a.flags_src, a.flags_dst, nullptr, a.flag_bytes);
-    const size_t stride = (size_t)gridDim.x * blockDim.x;
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (a.clean)
-        for (size_t t = tid; t < (size_t)a.nseg; t += stride) a.clean[t] = 1;
-    if (tid == 0) *a.sc_dst = *a.sc_src;
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs<R> a) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.nseg; s += warps) {
+        const int i = s * 32 + lane;
+        const bool in = i < a.m.n;
+        if (a.mode == STORE_BASE || a.mode == STORE) {
+            const bool copy = a.mode == STORE_BASE || a.seg_dirty[s];
+            if (copy && in)
+                for (int v = 0; v < 3; ++v) a.snap[v][i] = a.buf[a.cur][v][i];
+            if (lane == 0) {
+                if (a.mode == STORE_BASE) {
+                    // relative to the new base only segments whose two buffers differ are dirty
+                    a.seg_dirty[s] = a.seg_clean[s] ? 0 : 1;
+                } else {
+                    a.snap_dirty[s] = a.seg_dirty[s];
+                }
+            }
+            continue;
+        }
+        // restores
+        const uint8_t sd = a.mode == RESTORE_BASE ? 0 : a.snap_dirty[s];
+        const uint8_t ld = a.seg_dirty[s];
+        if (sd || ld) {
+            double vol = 0.0;
+            bool wet = false;
+            if (in) {
+                R val[3];
+                for (int v = 0; v < 3; ++v) {
+                    val[v] = sd ? a.snap[v][i] : a.base[v][i];
+                    a.buf[0][v][i] = val[v];
+                    a.buf[1][v][i] = val[v];
+                }
+                vol = double(cell_dx<R>(a.m, i)) * double(cell_dy<R>(a.m, i)) * double(val[0]);
+                wet = val[0] >= R(DA_TINY);
+            }
+            const unsigned wet_bits = __ballot_sync(0xffffffffu, wet);
+            vol = warp_sum(vol);
+            if (lane == 0) {
+                a.seg_vol[s] = vol;
+                a.seg_wet[s] = wet_bits ? 1 : 0;
+            }
+        }
+        if (lane == 0) {
+            a.seg_dirty[s] = sd;
+            a.seg_clean[s] = 1;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (a.mode == STORE_BASE || a.mode == STORE)
+            *a.snap_sc = *a.sc;
+        else
+            *a.sc = *a.snap_sc;
+    }
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <class R>
+int launch_t(da_ctx *ctx, void *slot, bool store) {
+    const size_t n = (size_t)ctx->mesh.n, ab = align256(sizeof(R) * n);
+    const bool is_base = slot == ctx->snaps[0];
+    unsigned char *b = (unsigned char *)slot, *b0 = (unsigned char *)ctx->snaps[0];
+    SnapArgs<R> a{};
+    a.m = mesh_args(ctx);
+    for (int q = 0; q < 2; ++q)
+        for (int v = 0; v < 3; ++v) a.buf[q][v] = (R *)ctx->U[q][v];
+    a.cur = ctx->cur;
+    for (int v = 0; v < 3; ++v) {
+        a.snap[v] = (R *)(b + v * ab);
+        a.base[v] = (const R *)(b0 + v * ab);
+    }
+    a.snap_dirty = b + 3 * ab;
+    a.snap_sc = (DevScalars *)(b + 3 * ab + align256((size_t)ctx->nseg));
+    a.seg_dirty = ctx->seg_dirty;
+    a.seg_clean = ctx->seg_clean;
+    a.seg_wet = ctx->seg_wet;
+    a.seg_vol = ctx->seg_vol;
+    a.sc = ctx->dsc;
+    a.nseg = ctx->nseg;
+    a.mode = store ? (is_base ? STORE_BASE : STORE) : (is_base ? RESTORE_BASE : RESTORE);
+    const int grid = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
+    trace_begin(ctx, TR_SNAPSHOT);
+    k_snapshot<R><<<grid, kBlock, 0, ctx->stream>>>(a);
+    trace_end(ctx);
+    return cuda_check(ctx, cudaGetLastError(), "snapshot copy");
+}
 
 }  // namespace
 
@@ -63,44 +137,7 @@ size_t snapshot_bytes(const da_ctx *ctx) {
 }
 
 int launch_snapshot(da_ctx *ctx, void *slot, bool store) {
-    const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
-    const size_t bytes = rs * (size_t)ctx->mesh.n, ab = align256(bytes);
-    unsigned char *base = (unsigned char *)slot;
-    unsigned char *flags = base + 3 * ab;
-    DevScalars *ssc = (DevScalars *)(flags + align256((size_t)ctx->nseg));
-    SnapArgs a{};
-    a.bytes = bytes;
-    a.flag_bytes = (size_t)ctx->nseg;
-    a.nseg = ctx->nseg;
-    for (int v = 0; v < 3; ++v) {
-        if (store) {
-            a.src[v] = (const unsigned char *)ctx->U[ctx->cur][v];
-            a.dst[v] = base + v * ab;
-            a.dst2[v] = nullptr;
-        } else {
-            a.src[v] = base + v * ab;
-            a.dst[v] = (unsigned char *)ctx->U[ctx->cur][v];
-            a.dst2[v] = (unsigned char *)ctx->U[1 - ctx->cur][v];
-        }
-    }
-    if (store) {
-        a.flags_src = ctx->seg_wet;
-        a.flags_dst = flags;
-        a.sc_src = ctx->dsc;
-        a.sc_dst = ssc;
-        a.clean = nullptr;
-    } else {
-        a.flags_src = flags;
-        a.flags_dst = ctx->seg_wet;
-        a.sc_src = ssc;
-        a.sc_dst = ctx->dsc;
-        a.clean = ctx->seg_clean;
-    }
-    int grid = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
-    trace_begin(ctx, TR_SNAPSHOT);
-    k_snapshot<<<grid, kBlock, 0, ctx->stream>>>(a);
-    trace_end(ctx);
-    return cuda_check(ctx, cudaGetLastError(), "snapshot copy");
+    return ctx->p.precision == DA_PREC_FP64 ? launch_t<double>(ctx, slot, store) : launch_t<float>(ctx, slot, store);
 }
 
 }  // namespace da

@@ -158,12 +158,40 @@ def test_adjoint_run_restores_state_and_time():
         c.run(5)
         before = np.stack(c.get_state())
         adjoint_run(c, box_of(w), 10, 3)
+        assert np.array_equal(np.stack(c.get_state()), before)
         s = c.step()
+        after = np.stack(c.get_state())
         assert s.iter == 6
         c.set_state(*before)
         c.set_time(s.time - s.dt, 5)
         s2 = c.step()
         assert s2.dt == s.dt
+        # the restored checkpoint carries exact culling flags and volume partials
+        assert s2.volume == s.volume
+        assert np.array_equal(np.stack(c.get_state()), after)
+
+
+def test_sparse_checkpoints_on_a_mostly_dry_mesh():
+    # one pile on a large mesh: most segments never change, so stores and restores copy only the
+    # flow's footprint; the result must not depend on the number of checkpoints, and the state
+    # and volume after the run must be the starting ones
+    w = inputs.workload1()
+    m = w.mesh
+    box = (w.piles[0].xc - 300.0, w.piles[0].xc + 300.0, w.piles[0].yc - 300.0, w.piles[0].yc + 300.0)
+    out = []
+    for snaps in (2, 5, 40):
+        with ctx_for(w) as c:
+            c.run(3)
+            start = np.stack(c.get_state())
+            g = adjoint_run(c, box, 40, snaps, m.dh0_dpile, want_lambda0=True)
+            assert np.array_equal(np.stack(c.get_state()), start)
+            s1 = c.step()
+            out.append((g, s1))
+    (g0, s0), rest = out[0], out[1:]
+    for g, s in rest:
+        assert g.J == g0.J and g.dJ_dbedfrict == g0.dJ_dbedfrict and g.dJ_dpile == g0.dJ_dpile
+        assert np.array_equal(g.lambda0, g0.lambda0)
+        assert s.volume == s0.volume and s.time == s0.time
 
 
 def test_fp32_split_adjoint_close_to_fp64():
