@@ -139,6 +139,12 @@ def barrier(ws: int, dev: int):
         torch.cuda.synchronize(dev)
 
 
+def pinned(count: int) -> np.ndarray:
+    """A float64 host array in page-locked memory (torch's pinned allocator)."""
+    import torch
+    return torch.empty(count, dtype=torch.float64, pin_memory=True).numpy()
+
+
 def wet_counts(m, h) -> tuple[int, int]:
     """(cells with h >= GEOFLOW_TINY, cells that are wet or have a wet face neighbour)."""
     wet = h >= 1e-4
@@ -277,15 +283,16 @@ def fwdadj(args, ws, local):
         adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
         res["trace"] = c.trace(with_steps=True)
         c.set_tracing(False)
-        # e2e through the C ABI with host buffers: H2D of the initial state, the run, D2H of
+        # e2e through the C ABI with pinned host buffers: H2D of the initial state, the run, D2H of
         # the gradients and lambda^0
-        h0, hu0, hv0 = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+        h0, hu0, hv0, lam_host = pinned(m.n), pinned(m.n), pinned(m.n), pinned(3 * m.n)
+        h0[:], hu0[:], hv0[:] = m.h0, m.hu0, m.hv0
         barrier(ws, local)
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             c.set_state(h0, hu0, hv0)
             c.set_time(0.0, 0)
-            ge = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, want_lambda0=True)
+            ge = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, lambda0_out=lam_host)
         e2e_s = allmax(time.perf_counter() - t0, ws, local)
         res["e2e"] = {"value": m.n * HORIZON * args.e2e_steps * ws / e2e_s, "unit": "cell-updates/s",
                       "h2d_bytes_per_step": 3 * 8 * m.n, "d2h_bytes_per_step": 3 * 8 * m.n + 8 * 32,
@@ -348,7 +355,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3, help="timed forward+adjoint runs (512 time steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-forward", action="store_true", help="skip the forward-only section")

@@ -248,19 +248,11 @@ int upload_tables(da_ctx *ctx, double *sec2, double *cos_int) {
 int copy_lambda_out(da_ctx *ctx, int buf, double *host) {
     const size_t n = (size_t)ctx->mesh.n;
     int st = DA_OK;
-    if (ctx->p.precision == DA_PREC_FP64) {
-        for (int v = 0; v < 3 && !st; ++v)
-            st = cuda_check(ctx, cudaMemcpyAsync(host + v * n, ctx->lam[buf][v], sizeof(double) * n, cudaMemcpyDeviceToHost,
-                                                 ctx->stream), "copy lambda");
-        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    } else {
-        std::vector<float> tmp(n);
-        for (int v = 0; v < 3 && !st; ++v) {
-            st = cuda_check(ctx, cudaMemcpy(tmp.data(), ctx->lam[buf][v], sizeof(float) * n, cudaMemcpyDeviceToHost),
-                            "copy lambda");
-            for (size_t i = 0; i < n && !st; ++i) host[v * n + i] = tmp[i];
-        }
+    for (int v = 0; v < 3 && !st; ++v) {
+        st = download_real(ctx, host + v * n, ctx->lam[buf][v]);
+        if (!st && ctx->p.precision != DA_PREC_FP64) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     }
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     return st;
 }
 
@@ -322,20 +314,7 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
     if (!st) st = upload_tables(ctx, sec2, &cos_int);
     const size_t n = (size_t)ctx->mesh.n;
     // lambda_next into buffer 0
-    if (!st) {
-        if (ctx->p.precision == DA_PREC_FP64) {
-            for (int v = 0; v < 3 && !st; ++v)
-                st = cuda_check(ctx, cudaMemcpy(ctx->lam[0][v], lambda_next + v * n, sizeof(double) * n,
-                                                cudaMemcpyHostToDevice), "copy lambda");
-        } else {
-            std::vector<float> tmp(n);
-            for (int v = 0; v < 3 && !st; ++v) {
-                for (size_t i = 0; i < n; ++i) tmp[i] = float(lambda_next[v * n + i]);
-                st = cuda_check(ctx, cudaMemcpy(ctx->lam[0][v], tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice),
-                                "copy lambda");
-            }
-        }
-    }
+    for (int v = 0; v < 3 && !st; ++v) st = upload_real(ctx, ctx->lam[0][v], lambda_next + v * n);
     // the caller's lambda differs from buffer 1 everywhere
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
     if (!st) st = store(ctx, 0);

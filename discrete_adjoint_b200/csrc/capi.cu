@@ -135,6 +135,7 @@ static void free_state(da_ctx *ctx) {
     dfree(ctx->seg_clean);
     dfree(ctx->seg_wet);
     dfree(ctx->seg_dirty);
+    dfree(ctx->stage);
     dfree(ctx->tile_epoch);
     dfree(ctx->seg_act);
     dfree(ctx->lam_clean);
@@ -193,6 +194,45 @@ void update_grid(da_ctx *ctx) {
     int g = ctx->p.grid_blocks > 0 ? ctx->p.grid_blocks : per_sm4;
     if (ctx->ntiles > 0 && g > ctx->ntiles) g = ctx->ntiles;
     ctx->grid = g > 0 ? g : 1;
+}
+
+// FP64 host arrays <-> FP32 device arrays through the FP64 staging buffer: the copy is one DMA
+// of the caller's array (fast from pinned memory) and the rounding (to nearest) runs on the device.
+__global__ void k_narrow(const double *__restrict__ s, float *__restrict__ d, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = float(s[i]);
+}
+__global__ void k_widen(const float *__restrict__ s, double *__restrict__ d, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = double(s[i]);
+}
+
+static int stage_alloc(da_ctx *ctx) {
+    if (ctx->stage) return DA_OK;
+    return cuda_check(ctx, cudaMalloc((void **)&ctx->stage, sizeof(double) * (size_t)ctx->mesh.n), "cudaMalloc(stage)");
+}
+
+int upload_real(da_ctx *ctx, void *dev, const double *host) {
+    const int n = ctx->mesh.n;
+    if (ctx->p.precision == DA_PREC_FP64)
+        return cuda_check(ctx, cudaMemcpyAsync(dev, host, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream),
+                          "copy to device");
+    int st = stage_alloc(ctx);
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(ctx->stage, host, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                                  ctx->stream), "copy to device");
+    if (!st) k_narrow<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>(ctx->stage, (float *)dev, n);
+    return st ? st : cuda_check(ctx, cudaGetLastError(), "narrow");
+}
+
+int download_real(da_ctx *ctx, double *host, const void *dev) {
+    const int n = ctx->mesh.n;
+    if (ctx->p.precision == DA_PREC_FP64)
+        return cuda_check(ctx, cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream),
+                          "copy to host");
+    int st = stage_alloc(ctx);
+    if (!st) k_widen<<<ctx->sm_count * 4, 256, 0, ctx->stream>>>((const float *)dev, ctx->stage, n);
+    if (!st) st = cuda_check(ctx, cudaGetLastError(), "widen");
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(host, ctx->stage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                                  ctx->stream), "copy to host");
+    return st;
 }
 
 static void fill_stats(const da_ctx *ctx, da_step_stats *out) {
@@ -424,22 +464,9 @@ int da_set_state(da_ctx *ctx, const double *h, const double *hu, const double *h
     if (!ctx || !h || !hu || !hv) return DA_ERR_INVALID;
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_set_state: no mesh");
     cudaSetDevice(ctx->device);
-    const int n = ctx->mesh.n;
     const double *src[3] = {h, hu, hv};
     int st = DA_OK;
-    if (ctx->p.precision == DA_PREC_FP64) {
-        for (int v = 0; v < 3 && !st; ++v)
-            st = cuda_check(ctx, cudaMemcpyAsync(ctx->U[ctx->cur][v], src[v], sizeof(double) * n,
-                                                 cudaMemcpyHostToDevice, ctx->stream), "copy state");
-        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    } else {
-        std::vector<float> tmp(n);
-        for (int v = 0; v < 3 && !st; ++v) {
-            for (int i = 0; i < n; ++i) tmp[i] = float(src[v][i]);
-            st = cuda_check(ctx, cudaMemcpy(ctx->U[ctx->cur][v], tmp.data(), sizeof(float) * n, cudaMemcpyHostToDevice),
-                            "copy state");
-        }
-    }
+    for (int v = 0; v < 3 && !st; ++v) st = upload_real(ctx, ctx->U[ctx->cur][v], src[v]);
     if (!st) st = forward_state_changed(ctx);
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (!st) ctx->have_state = true;
@@ -450,23 +477,14 @@ int da_get_state(da_ctx *ctx, double *h, double *hu, double *hv) {
     if (!ctx || !h || !hu || !hv) return DA_ERR_INVALID;
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_get_state: no state");
     cudaSetDevice(ctx->device);
-    const int n = ctx->mesh.n;
     double *dst[3] = {h, hu, hv};
     int st = DA_OK;
-    if (ctx->p.precision == DA_PREC_FP64) {
-        for (int v = 0; v < 3 && !st; ++v)
-            st = cuda_check(ctx, cudaMemcpyAsync(dst[v], ctx->U[ctx->cur][v], sizeof(double) * n,
-                                                 cudaMemcpyDeviceToHost, ctx->stream), "copy state");
-        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    } else {
-        std::vector<float> tmp(n);
-        for (int v = 0; v < 3 && !st; ++v) {
-            st = cuda_check(ctx, cudaMemcpyAsync(tmp.data(), ctx->U[ctx->cur][v], sizeof(float) * n,
-                                                 cudaMemcpyDeviceToHost, ctx->stream), "copy state");
-            if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-            for (int i = 0; i < n && !st; ++i) dst[v][i] = double(tmp[i]);
-        }
+    for (int v = 0; v < 3 && !st; ++v) {
+        st = download_real(ctx, dst[v], ctx->U[ctx->cur][v]);
+        // the staging buffer is reused by the next array
+        if (!st && ctx->p.precision != DA_PREC_FP64) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     }
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     return st;
 }
 

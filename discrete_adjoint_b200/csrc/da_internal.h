@@ -120,6 +120,7 @@ struct da_ctx {
     uint8_t *seg_clean = nullptr;    // [nseg] 1 when both state buffers hold the same segment
     uint8_t *seg_wet = nullptr;      // [nseg] 1 when the segment held a wet cell after the last update
     uint8_t *seg_dirty = nullptr;    // [nseg] 1 when the segment may differ from the base checkpoint
+    double *stage = nullptr;         // [n] FP64 staging for host transfers of FP32 arrays
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
     uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
     uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment
@@ -177,6 +178,10 @@ int launch_forward_steps(da_ctx *ctx, int nsteps);
 int launch_forward_steps_fp64(da_ctx *ctx, int nsteps);
 int launch_forward_steps_fp32(da_ctx *ctx, int nsteps);
 int forward_alloc(da_ctx *ctx);
+// capi.cu: one FP64 host array to / from a device array of the context's precision (stream-ordered;
+// an FP32 download must finish before the next one reuses the staging buffer)
+int upload_real(da_ctx *ctx, void *dev, const double *host);
+int download_real(da_ctx *ctx, double *host, const void *dev);
 // capi.cu: grid of the tiled kernels from da_params.grid_blocks, the SM count and the tile count
 void update_grid(da_ctx *ctx);
 // adjoint_fp64.cu / adjoint_fp32.cu

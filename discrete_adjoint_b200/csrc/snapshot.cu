@@ -1,7 +1,9 @@
 // Checkpoint copies of the adjoint's reverse sweep: one launch per store or restore, one warp
 // per 32-cell segment.
 //
-// Slot 0 is the base checkpoint: a full copy of the state.  Every later store copies only the
+// Slot 0 is the base checkpoint: a full copy of the state; storing it also copies the live state
+// into the other ping-pong buffer wherever the two differ, so that afterwards every segment holds
+// the base in both buffers and none is dirty.  Every later store copies only the
 // segments that an update has changed since the base ("dirty" segments, seg_dirty), so a flow that
 // covers a small part of the mesh is checkpointed at the cost of its footprint.  A restore writes
 // into both ping-pong buffers the snapshot's dirty segments, and the base copy of the segments
@@ -47,17 +49,38 @@ __global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs<R> a) {
     for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < a.nseg; s += warps) {
         const int i = s * 32 + lane;
         const bool in = i < a.m.n;
-        if (a.mode == STORE_BASE || a.mode == STORE) {
-            const bool copy = a.mode == STORE_BASE || a.seg_dirty[s];
-            if (copy && in)
+        if (a.mode == STORE) {
+            if (a.seg_dirty[s] && in)
                 for (int v = 0; v < 3; ++v) a.snap[v][i] = a.buf[a.cur][v][i];
-            if (lane == 0) {
-                if (a.mode == STORE_BASE) {
-                    // relative to the new base only segments whose two buffers differ are dirty
-                    a.seg_dirty[s] = a.seg_clean[s] ? 0 : 1;
-                } else {
-                    a.snap_dirty[s] = a.seg_dirty[s];
+            if (lane == 0) a.snap_dirty[s] = a.seg_dirty[s];
+            continue;
+        }
+        if (a.mode == STORE_BASE) {
+            const bool differ = !a.seg_clean[s];
+            double vol = 0.0;
+            bool wet = false;
+            if (in) {
+                R val[3];
+                for (int v = 0; v < 3; ++v) {
+                    val[v] = a.buf[a.cur][v][i];
+                    a.snap[v][i] = val[v];
+                    if (differ) a.buf[a.cur ^ 1][v][i] = val[v];
                 }
+                vol = double(cell_dx<R>(a.m, i)) * double(cell_dy<R>(a.m, i)) * double(val[0]);
+                wet = val[0] >= R(DA_TINY);
+            }
+            if (differ) {
+                // flags of a segment set wholesale by a state change: recompute them
+                const unsigned wet_bits = __ballot_sync(0xffffffffu, wet);
+                vol = warp_sum(vol);
+                if (lane == 0) {
+                    a.seg_vol[s] = vol;
+                    a.seg_wet[s] = wet_bits ? 1 : 0;
+                }
+            }
+            if (lane == 0) {
+                a.seg_dirty[s] = 0;
+                a.seg_clean[s] = 1;
             }
             continue;
         }

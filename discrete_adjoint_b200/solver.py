@@ -214,9 +214,11 @@ def _grad(g: _ffi.da_gradient, n_mat: int, n_piles: int, lam0=None) -> Gradient:
 
 
 def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpile=None,
-                want_lambda0: bool = False) -> Gradient:
+                want_lambda0: bool = False, lambda0_out: np.ndarray | None = None) -> Gradient:
     """dual_solver() of src/adjoint/dual_solver.C:80 over nsteps steps from the current state, for
-    J = sum of h^2 dx dy over the cells whose centre lies in box = (xmin, xmax, ymin, ymax)."""
+    J = sum of h^2 dx dy over the cells whose centre lies in box = (xmin, xmax, ymin, ymax).
+    lambda0_out: a caller-owned contiguous float64 array of 3 n values (e.g. in pinned memory)
+    that receives lambda^0; want_lambda0 allocates one instead."""
     f = _ffi.da_functional(_ffi.DA_FUNC_H2_BOX, 0, (C.c_double * 4)(*box))
     n = ctx.mesh.n
     dh = None
@@ -224,7 +226,12 @@ def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpil
     if dh0_dpile is not None and len(dh0_dpile):
         dh = np.ascontiguousarray(dh0_dpile, dtype=np.float64).reshape(-1, n)
         n_piles = dh.shape[0]
-    lam0 = np.zeros(3 * n) if want_lambda0 else None
+    if lambda0_out is not None:
+        if lambda0_out.dtype != np.float64 or lambda0_out.size != 3 * n or not lambda0_out.flags.c_contiguous:
+            raise ValueError("lambda0_out must be a contiguous float64 array of 3 n values")
+        lam0 = lambda0_out.reshape(3 * n)
+    else:
+        lam0 = np.zeros(3 * n) if want_lambda0 else None
     g = _ffi.da_gradient()
     ctx._check(ctx.lib.da_adjoint_run(ctx.ctx, C.byref(f), nsteps, nsnapshots,
                                       _ffi.dptr(dh) if dh is not None else None, n_piles, C.byref(g),
