@@ -31,6 +31,7 @@ UNITS = [
     ("adjoint_host.cu", []),
     ("noalloc.cu", ["--fmad=false"]),
     ("snapshot.cu", []),
+    ("ensemble.cu", []),
     ("mesh_host.cpp", []),
 ]
 

@@ -160,6 +160,19 @@ class da_gradient(C.Structure):
 
 DA_FUNC_H2_BOX = 1
 
+
+class da_member(C.Structure):
+    _fields_ = [
+        ("mesh", da_mesh_soa),
+        ("h0", PD), ("hu0", PD), ("hv0", PD),
+        ("dh0_dpile", PD),
+        ("n_materials", C.c_int32),
+        ("pad", C.c_int32),
+        ("bedfrict", C.c_double * DA_MAX_MATERIALS),
+        ("intfrict", C.c_double),
+        ("box", C.c_double * 4),
+    ]
+
 # name -> (restype, argtypes) for every symbol the headers declare
 SIGNATURES = {
     "da_abi_version": (C.c_int, []),
@@ -189,6 +202,12 @@ SIGNATURES = {
     "da_trace_name": (C.c_char_p, [C.c_int32]),
     "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
+    "da_ensemble_upload": (C.c_int, [C.c_void_p, C.POINTER(da_member), C.c_int32]),
+    "da_ensemble_restart": (C.c_int, [C.c_void_p]),
+    "da_ensemble_forward": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "da_ensemble_stats": (C.c_int, [C.c_void_p, C.POINTER(da_step_stats)]),
+    "da_ensemble_get_state": (C.c_int, [C.c_void_p, C.c_int32, PD, PD, PD]),
+    "da_ensemble_adjoint": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(da_gradient), C.POINTER(C.c_double)]),
     "da_mesh_build": (C.c_int, [C.POINTER(da_mesh_spec), C.POINTER(da_dem), C.POINTER(da_pile_spec), C.c_int32,
                                 C.c_double, C.c_double, C.POINTER(C.POINTER(da_mesh_host))]),
     "da_mesh_free": (None, [C.POINTER(da_mesh_host)]),

@@ -6,9 +6,15 @@ namespace da {
 int launch_adjoint_step_fp64(da_ctx *ctx, int a, int b, const double *sec2, double c) {
     return adj::step_t<double>(ctx, a, b, sec2, c);
 }
-int launch_adjoint_seed_fp64(da_ctx *ctx, int b, const double box[4]) { return adj::seed_t<double>(ctx, b, box); }
 int launch_adjoint_reduce_fp64(da_ctx *ctx, int a, int np) { return adj::reduce_t<double>(ctx, a, np); }
-int launch_youturn_fp64(da_ctx *ctx, int a, int b, const double *sec2, double c) {
-    return adj::youturn_t<double>(ctx, a, b, sec2, c);
+int launch_youturn_fp64(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box) {
+    return adj::youturn_t<double>(ctx, a, b, sec2, c, seed, box);
 }
+int launch_functional_fp64(da_ctx *ctx, double *out) { return adj::functional_t<double>(ctx, out); }
+// the volume of every ensemble member from the segments' volume parts (fixed order)
+int launch_member_volume(da_ctx *ctx, double *out) {
+    adj::k_inst_sum<<<ctx->ninst, adj::kBlock, 0, ctx->stream>>>(ctx->seg_vol, ctx->ia.seg0, ctx->nseg, out);
+    return cuda_check(ctx, cudaGetLastError(), "member volume launch");
+}
+int launch_adjoint_reduce_inst_fp64(da_ctx *ctx, int a) { return adj::reduce_inst_t<double>(ctx, a); }
 }  // namespace da

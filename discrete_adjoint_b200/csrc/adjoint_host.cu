@@ -21,24 +21,30 @@ namespace da {
 
 int launch_adjoint_step_fp64(da_ctx *, int, int, const double *, double);
 int launch_adjoint_step_fp32(da_ctx *, int, int, const double *, double);
-int launch_adjoint_seed_fp64(da_ctx *, int, const double *);
-int launch_adjoint_seed_fp32(da_ctx *, int, const double *);
 int launch_adjoint_reduce_fp64(da_ctx *, int, int);
 int launch_adjoint_reduce_fp32(da_ctx *, int, int);
+int launch_functional_fp64(da_ctx *, double *);
+int launch_functional_fp32(da_ctx *, double *);
 int forward_state_changed(da_ctx *ctx);
 
-int launch_youturn_fp64(da_ctx *, int, int, const double *, double);
-int launch_youturn_fp32(da_ctx *, int, int, const double *, double);
-int launch_youturn(da_ctx *ctx, int a, int b, const double *sec2, double c) {
-    return ctx->p.precision == DA_PREC_FP64 ? launch_youturn_fp64(ctx, a, b, sec2, c)
-                                            : launch_youturn_fp32(ctx, a, b, sec2, c);
+int launch_youturn_fp64(da_ctx *, int, int, const double *, double, bool, const double *);
+int launch_youturn_fp32(da_ctx *, int, int, const double *, double, bool, const double *);
+int launch_youturn(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_youturn_fp64(ctx, a, b, sec2, c, seed, box)
+                                            : launch_youturn_fp32(ctx, a, b, sec2, c, seed, box);
+}
+int launch_functional(da_ctx *ctx, double *out) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_functional_fp64(ctx, out) : launch_functional_fp32(ctx, out);
+}
+int launch_adjoint_reduce_inst_fp64(da_ctx *, int);
+int launch_adjoint_reduce_inst_fp32(da_ctx *, int);
+int launch_adjoint_reduce_inst(da_ctx *ctx, int lam0) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_reduce_inst_fp64(ctx, lam0)
+                                            : launch_adjoint_reduce_inst_fp32(ctx, lam0);
 }
 int launch_adjoint_step(da_ctx *ctx, int a, int b, const double *sec2, double c) {
     return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_step_fp64(ctx, a, b, sec2, c)
                                             : launch_adjoint_step_fp32(ctx, a, b, sec2, c);
-}
-int launch_adjoint_seed(da_ctx *ctx, int b, const double box[4]) {
-    return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_seed_fp64(ctx, b, box) : launch_adjoint_seed_fp32(ctx, b, box);
 }
 int launch_adjoint_reduce(da_ctx *ctx, int a, int np) {
     return ctx->p.precision == DA_PREC_FP64 ? launch_adjoint_reduce_fp64(ctx, a, np)
@@ -46,8 +52,8 @@ int launch_adjoint_reduce(da_ctx *ctx, int a, int np) {
 }
 
 namespace {
-
 size_t rsize(const da_ctx *ctx) { return ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float); }
+}  // namespace
 
 // d kact / d phi_bed and d phi_int of gmfggetcoef's three signed branches (getcoef.f:19-66):
 // k = (2/c^2)(1 - s sqrt|1 - (1 + t^2) c^2|) - 1 with c = cos phi_int, t = tan phi_bed, times
@@ -74,20 +80,24 @@ void kact_derivatives(const da_params &p, double *dkb, double *dki) {
     }
 }
 
+namespace {
+
 int adj_alloc(da_ctx *ctx, int nsnap) {
     const size_t n = (size_t)ctx->mesh.n;
     const size_t rs = rsize(ctx);
     int st = DA_OK;
-    if (ctx->adj_n != (int)n) {
+    const int nouts = (ctx->ninst > 0 ? ctx->ninst : 1) * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES);
+    if (ctx->adj_n != (int)n || ctx->adj_ninst != ctx->ninst) {
         auto fr = [](void *p) { if (p) cudaFree(p); };
         fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
-        fr(ctx->red_out); fr(ctx->red_part); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter);
+        fr(ctx->red_out); fr(ctx->red_part); fr(ctx->inst_J); fr(ctx->seg_J);
         for (int b = 0; b < 2; ++b)
             for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
         for (void *s : ctx->snaps) fr(s);
         ctx->snaps.clear();
         ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
-        ctx->red_out = ctx->red_part = ctx->seed_part = ctx->seed_J = nullptr; ctx->seed_counter = nullptr;
+        ctx->red_out = ctx->red_part = ctx->inst_J = ctx->seg_J = nullptr;
+        ctx->adj_n = -1;
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->mask, n), "cudaMalloc(mask)");
         for (int b = 0; b < 2 && !st; ++b)
             for (int v = 0; v < 3 && !st; ++v) st = cuda_check(ctx, cudaMalloc(&ctx->lam[b][v], rs * n), "cudaMalloc(lam)");
@@ -96,14 +106,13 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->gbed, sizeof(double) * n), "cudaMalloc(gbed)");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->gint, sizeof(double) * n), "cudaMalloc(gint)");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->dk_tab, sizeof(double) * 2 * DA_MAX_MATERIALS * 3), "cudaMalloc");
-        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_out, sizeof(double) * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_out, sizeof(double) * nouts), "cudaMalloc");
         if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->red_part, sizeof(double) * kAdjReduceParts * (DA_MAX_MATERIALS + 1 + DA_MAX_PILES)), "cudaMalloc");
-        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_part, sizeof(double) * ctx->nblocks), "cudaMalloc");
-        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_J, sizeof(double)), "cudaMalloc");
-        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seed_counter, sizeof(unsigned)), "cudaMalloc");
-        if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seed_counter, 0, sizeof(unsigned), ctx->stream), "memset");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->inst_J, sizeof(double) * (ctx->ninst > 0 ? ctx->ninst : 1)), "cudaMalloc");
+        if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_J, sizeof(double) * ctx->nseg), "cudaMalloc");
         if (st) return st;
         ctx->adj_n = (int)n;
+        ctx->adj_ninst = ctx->ninst;
     }
     while ((int)ctx->snaps.size() < nsnap && !st) {
         void *p = nullptr;
@@ -158,7 +167,7 @@ struct Runner {
     std::vector<int> free_slots;
     int lam_cur = 0;  // buffer holding lambda^{n+1}
     bool seeded = false;
-    double box[4];
+    double box[4] = {0, 0, 0, 0};
     double sec2[DA_MAX_MATERIALS];
     double cos_int;
     long long fsteps = 0;
@@ -177,18 +186,11 @@ struct Runner {
         return st;
     }
     int youturn() {
-        int st = DA_OK;
         ++fsteps;
         pos = -1;  // past the step that is being taken back
-        if (!seeded) {
-            // the last step: replay, seed lambda^N from U^N (the state just produced), reverse
-            st = launch_forward_step(ctx, ctx->mask);
-            if (!st) st = launch_adjoint_seed(ctx, lam_cur, box);
-            seeded = true;
-            if (!st) st = launch_adjoint_step(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
-        } else {
-            st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int);
-        }
+        // the first reverse step (the horizon's last step) also seeds lambda^N from U^N
+        const int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box);
+        seeded = true;
         lam_cur = 1 - lam_cur;
         return st;
     }
@@ -245,6 +247,8 @@ int upload_tables(da_ctx *ctx, double *sec2, double *cos_int) {
     return st;
 }
 
+}  // namespace
+
 int copy_lambda_out(da_ctx *ctx, int buf, double *host) {
     const size_t n = (size_t)ctx->mesh.n;
     int st = DA_OK;
@@ -256,6 +260,8 @@ int copy_lambda_out(da_ctx *ctx, int buf, double *host) {
     return st;
 }
 
+namespace {
+
 int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool reduced = false) {
     int st = reduced ? DA_OK : launch_adjoint_reduce(ctx, lam0, n_piles);
     std::vector<double> red(DA_MAX_MATERIALS + 1 + DA_MAX_PILES, 0.0);
@@ -263,7 +269,7 @@ int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool red
     if (!st) st = cuda_check(ctx, cudaMemcpyAsync(red.data(), ctx->red_out, sizeof(double) * nout, cudaMemcpyDeviceToHost,
                                                   ctx->stream), "read gradient");
     double J = 0.0;
-    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(&J, ctx->seed_J, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(&J, ctx->inst_J, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
                              "read J");
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (st || !out) return st;
@@ -276,6 +282,46 @@ int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool red
 }
 
 }  // namespace
+
+// The reverse sweep shared by da_adjoint_run and da_ensemble_adjoint: checkpointed forward run
+// over nsteps steps from the current state, reverse steps back to step 0, the state put back,
+// J and the gradient sums launched (single: red_out[n_mat + 1 + n_piles]; ensemble: per member).
+// lam0 receives the buffer that holds lambda^0.
+int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
+                  long long *fsteps, float *dev_ms) {
+    int st = adj_alloc(ctx, nsnapshots + 1);
+    Runner r;
+    r.ctx = ctx;
+    if (box)
+        for (int q = 0; q < 4; ++q) r.box[q] = box[q];
+    if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
+    if (st) return st;
+    r.sch.build(nsteps, nsnapshots);
+    for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, ctx->stream);
+    st = store(ctx, 0);
+    r.pos = 0;
+    if (!st) st = r.reverse(0, nsteps, 0);
+    if (!st) st = restore(ctx, 0);
+    // the gradient sums are in the timed region
+    if (!st) st = launch_functional(ctx, ctx->inst_J);
+    if (!st) st = ctx->ninst > 0 ? launch_adjoint_reduce_inst(ctx, r.lam_cur) : launch_adjoint_reduce(ctx, r.lam_cur, n_piles);
+    cudaEventRecord(e1, ctx->stream);
+    if (!st) st = sync_check(ctx);
+    float ms = 0.f;
+    if (!st) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!st) st = trace_flush(ctx);
+    if (lam0) *lam0 = r.lam_cur;
+    if (fsteps) *fsteps = r.fsteps;
+    if (dev_ms) *dev_ms = ms;
+    return st;
+}
+
 }  // namespace da
 
 using namespace da;
@@ -306,6 +352,7 @@ int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0) {
 
 int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, da_gradient *partial) {
     if (!ctx || !lambda_next || !lambda_out) return DA_ERR_INVALID;
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_step: ensemble context");
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_adjoint_step: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_step: no state");
     cudaSetDevice(ctx->device);
@@ -338,14 +385,11 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
         return DA_ERR_INVALID;
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_adjoint_run: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_run: no state");
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_run: ensemble context (da_ensemble_adjoint)");
     cudaSetDevice(ctx->device);
     const size_t n = (size_t)ctx->mesh.n;
-    int st = adj_alloc(ctx, nsnapshots + 1);
-    Runner r;
-    r.ctx = ctx;
-    for (int q = 0; q < 4; ++q) r.box[q] = f->box[q];
-    if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
-    if (!st && n_piles > 0) {
+    int st = DA_OK;
+    if (n_piles > 0) {
         if (ctx->dh0) cudaFree(ctx->dh0);
         ctx->dh0 = nullptr;
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * n * n_piles), "cudaMalloc(dh0)");
@@ -353,29 +397,14 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
             st = cuda_check(ctx, cudaMemcpy(ctx->dh0, dh0_dpile, sizeof(double) * n * n_piles, cudaMemcpyHostToDevice),
                             "copy dh0");
     }
-    if (st) return st;
-    r.sch.build(nsteps, nsnapshots);
-    for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, ctx->stream);
-    st = store(ctx, 0);
-    r.pos = 0;
-    if (!st) st = r.reverse(0, nsteps, 0);
-    if (!st) st = restore(ctx, 0);
-    if (!st) st = launch_adjoint_reduce(ctx, r.lam_cur, n_piles);  // the gradient sums are in the timed region
-    cudaEventRecord(e1, ctx->stream);
-    if (!st) st = sync_check(ctx);
+    int lam0 = 0;
+    long long fsteps = 0;
     float dev_ms = 0.f;
-    if (!st) cudaEventElapsedTime(&dev_ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (!st) st = trace_flush(ctx);
-    if (!st && lambda0) st = copy_lambda_out(ctx, r.lam_cur, lambda0);
-    if (!st) st = fill_gradient(ctx, r.lam_cur, n_piles, out, /*reduced=*/true);
+    if (!st) st = adjoint_sweep(ctx, f->box, nsteps, nsnapshots, n_piles, &lam0, &fsteps, &dev_ms);
+    if (!st && lambda0) st = copy_lambda_out(ctx, lam0, lambda0);
+    if (!st) st = fill_gradient(ctx, lam0, n_piles, out, /*reduced=*/true);
     if (!st && out) {
-        out->forward_steps = r.fsteps;
+        out->forward_steps = fsteps;
         out->snapshots = nsnapshots;
         out->device_ms = dev_ms;
     }

@@ -262,16 +262,36 @@ __device__ __forceinline__ double dk_of(const double *tab, int mat, uint8_t code
 }
 
 // ------------------------------------------------------------------------- k_adj_src
-template <class R>
+// Per-member tables of an ensemble tile (BATCH): material constants, dt and the parameter tables.
+struct InstTables {
+    const double *sec2_bed;
+    double cos_int;
+    const double *dk_dbed, *dk_dint;
+};
+
+template <bool BATCH>
+__device__ __forceinline__ InstTables inst_tables(const AdjArgs &aa, const InstArgs &ia, int inst) {
+    if (!BATCH) return InstTables{aa.sec2_bed, aa.cos_int, aa.dk_dbed, aa.dk_dint};
+    const double *dk = ia.dk_tab + (size_t)inst * 2 * DA_MAX_MATERIALS * 3;
+    return InstTables{ia.sec2_bed + (size_t)inst * DA_MAX_MATERIALS, ia.cos_int[inst], dk, dk + DA_MAX_MATERIALS * 3};
+}
+
+template <class R, bool BATCH = false>
 __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
-                                              const MatConsts &mc, const AdjArgs &aa, R dt, R ft, int *list) {
+                                              const MatConsts &mc0, const AdjArgs &aa, R dt0, R ft, int *list,
+                                              const InstArgs &ia) {
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       // a wet cell is active, so its tile was listed by the recording step and had an active cell
       const bool need = tq < aa.ntiles && aa.tile_epoch[tq] == aa.rec_id && seg_flags8(aa.seg_act, tq) != 0ull;
       const int cnt = compact_tiles(need, tq, list);
       for (int q = 0; q < cnt; ++q) {
-        const int i = list[q] * kBlock + threadIdx.x;
+        const int t = list[q];
+        const int inst = BATCH ? ia.tile_inst[t] : 0;
+        const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+        const R dt = BATCH ? R(ia.dt[inst]) : dt0;
+        const InstTables it = inst_tables<BATCH>(aa, ia, inst);
+        const int i = t * kBlock + threadIdx.x;
         if (i >= m.n) continue;
         double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
         const R h_i = U.h[i];
@@ -333,8 +353,8 @@ __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<
                 const double dJ_dk = double(-nu_u * sg0 * h * wx * sin_int - nu_v * sg1 * h * wy * sin_int);
                 const double dJ_dsin = double(-nu_u * sg0 * h * k * wx - nu_v * sg1 * h * k * wy);
                 const double dJ_dtan = double(-nu_u * sg2 * (Px > R(0) ? Px : R(0)) - nu_v * sg3 * (Py > R(0) ? Py : R(0)));
-                const double gb = dJ_dtan * aa.sec2_bed[mat] + dJ_dk * dk_of(aa.dk_dbed, mat, code);
-                const double gi = dJ_dsin * aa.cos_int + dJ_dk * dk_of(aa.dk_dint, mat, code);
+                const double gb = dJ_dtan * it.sec2_bed[mat] + dJ_dk * dk_of(it.dk_dbed, mat, code);
+                const double gi = dJ_dsin * it.cos_int + dJ_dk * dk_of(it.dk_dint, mat, code);
                 if (gb != 0.0) aa.gbed[i] += gb;
                 if (gi != 0.0) aa.gint[i] += gi;
             }
@@ -354,7 +374,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
     __shared__ int list[kBlock];
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > sign_floor ? R(sc->frict_tiny) : sign_floor;
-    adj_src_phase<R>(m, U, Lnext, mc, aa, dt, ft, list);
+    adj_src_phase<R>(m, U, Lnext, mc, aa, dt, ft, list, InstArgs{});
 }
 
 // Flux weight of cell c for its side s: -dt/dx on a plus side, +dt/dx on a minus side, halved
@@ -378,10 +398,10 @@ __device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &
 }
 
 // ---------------------------------------------------------------------- k_adj_gather
-template <class R>
+template <class R, bool BATCH = false>
 __device__ __forceinline__ void adj_gather_phase(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
-                                                 const StateOut<R> &Lout, const MatConsts &mc, const AdjArgs &aa, R dt,
-                                                 int *list) {
+                                                 const StateOut<R> &Lout, const MatConsts &mc0, const AdjArgs &aa,
+                                                 R dt0, int *list, const InstArgs &ia) {
     for (int round = 0; sched_more(round, aa.ntiles); ++round) {
       const int tq = sched_tile(round);
       bool need = false;
@@ -391,6 +411,9 @@ __device__ __forceinline__ void adj_gather_phase(const MeshArgs &m, const StateR
       const int cnt = compact_tiles(need, tq, list);
       for (int q = 0; q < cnt; ++q) {
         const int t = list[q];
+        const int inst = BATCH ? ia.tile_inst[t] : 0;
+        const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+        const R dt = BATCH ? R(ia.dt[inst]) : dt0;
         const int j = t * kBlock + threadIdx.x;
         const bool recorded = aa.tile_epoch[t] == aa.rec_id;
         const bool seg_active = recorded && aa.seg_act[j >> 5];
@@ -461,8 +484,9 @@ __device__ __forceinline__ void adj_gather_phase(const MeshArgs &m, const StateR
         if (dJ_dkj != 0.0) {
             const uint8_t code = mj & 3;
             const int mat = m.mat[j];
-            aa.gbed[j] += dJ_dkj * dk_of(aa.dk_dbed, mat, code);
-            aa.gint[j] += dJ_dkj * dk_of(aa.dk_dint, mat, code);
+            const InstTables it = inst_tables<BATCH>(aa, ia, inst);
+            aa.gbed[j] += dJ_dkj * dk_of(it.dk_dbed, mat, code);
+            aa.gint[j] += dJ_dkj * dk_of(it.dk_dint, mat, code);
         }
       }
     }
@@ -472,56 +496,56 @@ template <class R>
 __global__ void __launch_bounds__(kBlock) k_adj_gather(MeshArgs m, StateRef<R> U, StateRef<R> Lnext, StateOut<R> Lout,
                                                        MatConsts mc, AdjArgs aa, const DevScalars *__restrict__ sc) {
     __shared__ int list[kBlock];
-    adj_gather_phase<R>(m, U, Lnext, Lout, mc, aa, R(sc->dt), list);
+    adj_gather_phase<R>(m, U, Lnext, Lout, mc, aa, R(sc->dt), list, InstArgs{});
 }
 
-// ------------------------------------------------------------------------ k_adj_seed
-// J = sum over cells with centre in the box of h^2 dx dy; lambda^N = dJ/dU^N.  FP64 partials per
-// block, summed in block order by the last block.
-template <class R>
-__global__ void __launch_bounds__(kBlock) k_adj_seed(MeshArgs m, StateRef<R> U, StateOut<R> L, double x0, double x1,
-                                                     double y0, double y1, double *__restrict__ part,
-                                                     double *__restrict__ J, unsigned *__restrict__ counter) {
-    __shared__ double red[kBlock / 32];
-    double acc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
-        double xc, yc;
-        if constexpr (sizeof(R) == 8) {
-            xc = m.x[i];
-            yc = m.y[i];
-        } else {
-            xc = m.x ? m.x[i] : 0.0;
-            yc = m.y ? m.y[i] : 0.0;
+// ------------------------------------------------------------------------ seed
+// J = sum over the cells whose centre lies in the box of h^2 dx dy (the member's box in an
+// ensemble); lambda^N = dJ/dU^N.  One warp per segment, which stores its part of J; the J of a
+// member is the sum of its segments' parts in order (k_inst_sum).
+struct Box {
+    double v[4];  // xmin, xmax, ymin, ymax
+};
+
+template <class R, bool BATCH>
+__device__ __forceinline__ void seed_phase(const MeshArgs &m, const StateRef<R> &UN, const StateOut<R> &L,
+                                           const Box &box, double *seg_J, int nseg, const InstArgs &ia) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nseg; s += warps) {
+        const double *bx = BATCH ? ia.box + (size_t)4 * ia.tile_inst[s >> 3] : box.v;
+        const int i = s * 32 + lane;
+        double acc = 0.0;
+        if (i < m.n) {
+            const double xc = m.x[i], yc = m.y[i];
+            const bool in = xc >= bx[0] && xc <= bx[1] && yc >= bx[2] && yc <= bx[3];
+            const double h = double(UN.h[i]);
+            const double area = double(cell_dx<R>(m, i)) * double(cell_dy<R>(m, i));
+            L.h[i] = in ? R(2.0 * h * area) : R(0);
+            L.hu[i] = R(0);
+            L.hv[i] = R(0);
+            if (in) acc = h * h * area;
         }
-        const bool in = xc >= x0 && xc <= x1 && yc >= y0 && yc <= y1;
-        const double h = double(U.h[i]);
-        const double area = double(cell_dx<R>(m, i)) * double(cell_dy<R>(m, i));
-        L.h[i] = in ? R(2.0 * h * area) : R(0);
-        L.hu[i] = R(0);
-        L.hv[i] = R(0);
-        if (in) acc += h * h * area;
+        acc = warp_sum(acc);
+        if (lane == 0) seg_J[s] = acc;
     }
+}
+
+// Sum of per-segment values over each member's segment range (seg0 == null: one range over all
+// segments), thread-strided then block-reduced: a fixed order.
+__global__ void __launch_bounds__(kBlock) k_inst_sum(const double *__restrict__ part, const int32_t *__restrict__ seg0,
+                                                     int nseg, double *__restrict__ out) {
+    __shared__ double red[kBlock / 32];
+    const int s0 = seg0 ? seg0[blockIdx.x] : 0, s1 = seg0 ? seg0[blockIdx.x + 1] : nseg;
+    double acc = 0.0;
+    for (int s = s0 + threadIdx.x; s < s1; s += kBlock) acc += part[s];
     acc = warp_sum(acc);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < kBlock / 32; ++w) t += red[w];
-        part[blockIdx.x] = t;
-    }
-    __shared__ bool last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double t = 0.0;
-        for (int b = 0; b < gridDim.x; ++b) t += ((volatile double *)part)[b];
-        *J = t;
-        *counter = 0;
+        out[blockIdx.x] = t;
     }
 }
 
@@ -557,6 +581,37 @@ __global__ void __launch_bounds__(kBlock) k_adj_reduce(MeshArgs m, StateRef<R> L
         double t = 0.0;
         for (int w = 0; w < kBlock / 32; ++w) t += red[w];
         part[(size_t)o * kReduceParts + blockIdx.x] = t;
+    }
+}
+
+// Ensemble: block (k, o) sums output o of member k over the member's cells, in a fixed order:
+// o < n_mat the basal-friction sensitivities of material o, o == n_mat the internal friction,
+// o == n_mat + 1 the member's pile height (lambda_h dh0/dP).
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_adj_reduce_inst(MeshArgs m, StateRef<R> L0, const double *__restrict__ gbed,
+                                                            const double *__restrict__ gint,
+                                                            const double *__restrict__ dh0, int n_mat,
+                                                            const int32_t *__restrict__ seg0, double *__restrict__ out) {
+    __shared__ double red[kBlock / 32];
+    const int k = blockIdx.x, o = blockIdx.y;
+    const int i0 = seg0[k] * 32, i1 = min(m.n, seg0[k + 1] * 32);
+    double acc = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        if (o < n_mat) {
+            if (m.mat[i] == o) acc += gbed[i];
+        } else if (o == n_mat) {
+            acc += gint[i];
+        } else if (dh0) {
+            acc += double(L0.h[i]) * dh0[i];
+        }
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) t += red[w];
+        out[(size_t)k * (n_mat + 2) + o] = t;
     }
 }
 

@@ -48,21 +48,6 @@ int step_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_
 }
 
 template <class R>
-int seed_t(da_ctx *ctx, int lam_out, const double box[4]) {
-    const MeshArgs m = mesh_args(ctx);
-    const int c = ctx->cur;
-    StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
-    StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
-    // lambda^N is written everywhere: the two adjoint buffers differ on every tile
-    cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream);
-    trace_begin(ctx, TR_ADJ_SEED);
-    k_adj_seed<R><<<ctx->nblocks, kBlock, 0, ctx->stream>>>(m, U, Lo, box[0], box[1], box[2], box[3], ctx->seed_part,
-                                                             ctx->seed_J, ctx->seed_counter);
-    trace_end(ctx);
-    return cuda_check(ctx, cudaGetLastError(), "adjoint seed launch");
-}
-
-template <class R>
 int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
     const MeshArgs m = mesh_args(ctx);
     StateRef<R> L{(const R *)ctx->lam[lam0][0], (const R *)ctx->lam[lam0][1], (const R *)ctx->lam[lam0][2]};
@@ -75,46 +60,71 @@ int reduce_t(da_ctx *ctx, int lam0, int n_piles) {
     return cuda_check(ctx, cudaGetLastError(), "adjoint reduce launch");
 }
 
+// Ensemble gradients: (n_mat + 2) outputs per member into red_out, n_mat the largest material
+// count of the members.
+template <class R>
+int reduce_inst_t(da_ctx *ctx, int lam0) {
+    const MeshArgs m = mesh_args(ctx);
+    StateRef<R> L{(const R *)ctx->lam[lam0][0], (const R *)ctx->lam[lam0][1], (const R *)ctx->lam[lam0][2]};
+    trace_begin(ctx, TR_ADJ_REDUCE);
+    k_adj_reduce_inst<R><<<dim3(ctx->ninst, ctx->p.n_materials + 2), kBlock, 0, ctx->stream>>>(
+        m, L, ctx->gbed, ctx->gint, ctx->dh0, ctx->p.n_materials, ctx->ia.seg0, ctx->red_out);
+    trace_end(ctx);
+    return cuda_check(ctx, cudaGetLastError(), "ensemble reduce launch");
+}
+
 // ------------------------------------------------------------------------ k_youturn
 // One whole reverse step in one cooperative launch: the forward step of U^n replayed with its
 // branch codes recorded (coefficient phase, barrier, dt, update phase), a barrier, the source
 // adjoint, a barrier and the gather, i.e. the four launches of the separate path with grid
 // barriers instead of kernel boundaries.  U^n stays in buffer cur; U^{n+1} goes to cur ^ 1.
-// Block 0 writes the step's scalars at the end, as the separate kernels do.
-template <class R>
+// SEED (the last step of the horizon): lambda^N is seeded from the U^N just produced before the
+// adjoint phases, with each segment's part of J.  BATCH: every member with its own constants and
+// dt (the members' dt pass between two barriers).  Block 0 writes the step's scalars at the end,
+// as the separate kernels do.
+template <class R, bool BATCH, bool SEED>
 __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
                                                     uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
-                                                    uint8_t *seg_dirty, int ntiles,
-                                                    int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
-                                                    uint8_t *mask, int *tile_epoch, uint8_t *seg_act, int rec_id,
-                                                    StateRef<R> Ln, StateOut<R> Lo, AdjArgs aa) {
+                                                    uint8_t *seg_dirty, int ntiles, int cull, MatConsts mc,
+                                                    TimeConsts tc, DevScalars *sc, uint8_t *mask, int *tile_epoch,
+                                                    uint8_t *seg_act, int rec_id, StateRef<R> Ln, StateOut<R> Lseed,
+                                                    StateOut<R> Lo, AdjArgs aa, InstArgs ia, Box box, double *seg_J) {
     __shared__ int list[kBlock];
     const double time = sc->time;
     const long long iter = sc->iter;
     const StateRef<R> U{S.h[cur], S.hu[cur], S.hv[cur]};
     const StateOut<R> O{S.h[cur ^ 1], S.hu[cur ^ 1], S.hv[cur ^ 1]};
     unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-    fwd::coef_phase<R, true>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
-    fwd::push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
+    fwd::coef_phase<R, true, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max, ia);
+    if (!BATCH) fwd::push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (!fwd::grid_sync(sc)) return;
-    const double min_dxe = __longlong_as_double(__ldcg(&sc->acc_min_dxe));
-    const double hmax = __longlong_as_double(__ldcg(&sc->acc_hmax));
-    double dt, ft;
-    fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+    double dt = 0.0, ft, min_dxe = 0.0, hmax = 0.0;
+    if (BATCH) {
+        ft = iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
+        fwd::inst_dt_pass(ia, iter, tc);
+        if (!fwd::grid_sync(sc)) return;
+    } else {
+        min_dxe = __longlong_as_double(__ldcg(&sc->acc_min_dxe));
+        hmax = __longlong_as_double(__ldcg(&sc->acc_hmax));
+        fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+    }
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-    fwd::update_phase<R, true>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc,
-                               R(dt), ftr,
-                               mask, tile_epoch, seg_act, rec_id, list);
+    fwd::update_phase<R, true, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc,
+                                      sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id, list, ia);
     if (!fwd::grid_sync(sc)) return;
-    adj_src_phase<R>(m, U, Ln, mc, aa, R(dt), ftr, list);
+    if (SEED) {
+        seed_phase<R, BATCH>(m, StateRef<R>{O.h, O.hu, O.hv}, Lseed, box, seg_J, ntiles * (kBlock / 32), ia);
+        if (!fwd::grid_sync(sc)) return;
+    }
+    adj_src_phase<R, BATCH>(m, U, Ln, mc, aa, R(dt), ftr, list, ia);
     if (!fwd::grid_sync(sc)) return;
-    adj_gather_phase<R>(m, U, Ln, Lo, mc, aa, R(dt), list);
-    if (blockIdx.x == 0) {
-        if (threadIdx.x == 0) {
+    adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->iter = iter + 1;
+        sc->frict_tiny = ft;
+        if (!BATCH) {
             sc->time = time + dt;
-            sc->iter = iter + 1;
             sc->dt = dt;
-            sc->frict_tiny = ft;
             sc->min_dxe = min_dxe;
             sc->hmax = hmax;
             sc->acc_min_dxe = fwd::kMinDxeStart;
@@ -124,18 +134,22 @@ __global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R
 }
 
 // The live state is U^n in buffer cur; afterwards U^{n+1} is (cur flips) and lambda^n is in
-// lam_out.
+// lam_out.  seed: lambda^N goes into lam_in first (from U^{n+1} = U^N) with J's segment parts.
 template <class R>
-int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int) {
+int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int, bool seed,
+              const double *box4) {
     const int pi = sizeof(R) == 8;
-    if (ctx->coop_cap_yt[pi] <= 0) {
+    const bool batch = ctx->ninst > 0;
+    const void *kern = batch ? (seed ? (const void *)k_youturn<R, true, true> : (const void *)k_youturn<R, true, false>)
+                             : (seed ? (const void *)k_youturn<R, false, true> : (const void *)k_youturn<R, false, false>);
+    int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed];
+    if (cap_ref <= 0) {
         int per_sm = 0;
-        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_youturn<R>, kBlock, 0),
-                            "occupancy");
+        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");
         if (st) return st;
-        ctx->coop_cap_yt[pi] = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
+        cap_ref = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
     }
-    const int cap = ctx->coop_cap_yt[pi];
+    const int cap = cap_ref;
     if (cap <= 0) return set_error(ctx, DA_ERR_UNSUPPORTED, "reverse-step kernel cannot be resident");
     const int grid = ctx->grid < cap ? ctx->grid : cap;
     ++ctx->rec_id;
@@ -151,22 +165,43 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     unsigned *active = ctx->active;
     uint8_t *seg_clean = ctx->seg_clean, *seg_wet = ctx->seg_wet, *mask = ctx->mask, *seg_act = ctx->seg_act;
     int *tile_epoch = ctx->tile_epoch;
-    double *seg_vol = ctx->seg_vol;
+    double *seg_vol = ctx->seg_vol, *seg_J = ctx->seg_J;
     uint8_t *seg_dirty = ctx->seg_dirty;
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
     StateRef<R> Ln{(const R *)ctx->lam[lam_in][0], (const R *)ctx->lam[lam_in][1], (const R *)ctx->lam[lam_in][2]};
+    StateOut<R> Ls{(R *)ctx->lam[lam_in][0], (R *)ctx->lam[lam_in][1], (R *)ctx->lam[lam_in][2]};
     StateOut<R> Lo{(R *)ctx->lam[lam_out][0], (R *)ctx->lam[lam_out][1], (R *)ctx->lam[lam_out][2]};
     AdjArgs aa = adj_args<R>(ctx, sec2, cos_int);
-    void *args[] = {&m,  &S,    &cur,  &kact, &active,     &seg_clean, &seg_wet, &seg_vol, &seg_dirty, &ntiles, &cull,
-                    &mc, &tc,   &sc,   &mask, &tile_epoch, &seg_act,   &rec_id,  &Ln,      &Lo,        &aa};
+    InstArgs ia = ctx->ia;
+    Box box{};
+    if (box4)
+        for (int q = 0; q < 4; ++q) box.v[q] = box4[q];
+    if (seed) {
+        // lambda^N is written everywhere: the two adjoint buffers differ on every segment
+        int st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
+        if (st) return st;
+    }
+    void *args[] = {&m,    &S,   &cur,        &kact,    &active, &seg_clean, &seg_wet, &seg_vol, &seg_dirty,
+                    &ntiles, &cull, &mc,      &tc,      &sc,     &mask,      &tile_epoch, &seg_act, &rec_id,
+                    &Ln,   &Ls,  &Lo,         &aa,      &ia,     &box,       &seg_J};
     trace_begin(ctx, TR_YOUTURN);
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_youturn<R>, grid, kBlock, args, 0, ctx->stream);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx);
     if (e != cudaSuccess) return cuda_check(ctx, e, "reverse-step launch");
     ctx->cur = cur ^ 1;
     return DA_OK;
+}
+
+// Per-member J (or the single J) from the segments' parts, fixed order; one block per member.
+template <class R>
+int functional_t(da_ctx *ctx, double *out) {
+    const int nm = ctx->ninst > 0 ? ctx->ninst : 1;
+    trace_begin(ctx, TR_ADJ_SEED);
+    k_inst_sum<<<nm, kBlock, 0, ctx->stream>>>(ctx->seg_J, ctx->ninst > 0 ? ctx->ia.seg0 : nullptr, ctx->nseg, out);
+    trace_end(ctx);
+    return cuda_check(ctx, cudaGetLastError(), "functional launch");
 }
 
 }  // namespace

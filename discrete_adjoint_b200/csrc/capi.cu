@@ -145,14 +145,15 @@ static void free_state(da_ctx *ctx) {
 static void free_adjoint(da_ctx *ctx) {
     auto fr = [](void *p) { if (p) cudaFree(p); };
     fr(ctx->mask); fr(ctx->adjA); fr(ctx->adjB); fr(ctx->gbed); fr(ctx->gint); fr(ctx->dk_tab);
-    fr(ctx->red_out); fr(ctx->red_part); fr(ctx->seed_part); fr(ctx->seed_J); fr(ctx->seed_counter); fr(ctx->dh0);
+    fr(ctx->red_out); fr(ctx->red_part); fr(ctx->inst_J); fr(ctx->seg_J); fr(ctx->dh0);
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
     for (void *s : ctx->snaps) fr(s);
     ctx->snaps.clear();
     ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
-    ctx->red_out = ctx->red_part = ctx->seed_part = ctx->seed_J = ctx->dh0 = nullptr; ctx->seed_counter = nullptr;
+    ctx->red_out = ctx->red_part = ctx->inst_J = ctx->seg_J = ctx->dh0 = nullptr;
     ctx->adj_n = 0;
+    ctx->adj_ninst = -1;
 }
 
 static void drop_graphs(da_ctx *ctx) {
@@ -345,6 +346,7 @@ da_ctx *da_create(const da_params *p, int *err) {
 }
 
 void da_destroy(da_ctx *ctx) {
+    if (ctx) free_members(ctx);
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
@@ -416,6 +418,7 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (st) return st;
     drop_graphs(ctx);
+    free_members(ctx);
     free_mesh(ctx);
     free_state(ctx);
     free_adjoint(ctx);
@@ -490,6 +493,7 @@ int da_get_state(da_ctx *ctx, double *h, double *hu, double *hv) {
 
 int da_forward_step(da_ctx *ctx, da_step_stats *out) {
     if (!ctx) return DA_ERR_INVALID;
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_forward_step: ensemble context (da_ensemble_forward)");
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_step: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_step: no state");
     cudaSetDevice(ctx->device);
@@ -540,6 +544,7 @@ const char *da_forward_kernel_name(int32_t k) {
 
 int da_forward_profile(da_ctx *ctx, int32_t nsteps, double *kernel_ms) {
     if (!ctx || nsteps <= 0 || !kernel_ms) return DA_ERR_INVALID;
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_forward_profile: ensemble context");
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_forward_profile: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_forward_profile: no state");
     cudaSetDevice(ctx->device);
@@ -616,6 +621,11 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     if (st) return st;
     const DevScalars saved_sc = *ctx->hsc;
     const int cur0 = ctx->cur;
+    // ensemble: the members' times too (their accumulators are at rest between steps)
+    std::vector<double> saved_time(ctx->ninst);
+    if (ctx->ninst > 0)
+        st = cuda_check(ctx, cudaMemcpy(saved_time.data(), ctx->ia.time, sizeof(double) * ctx->ninst,
+                                        cudaMemcpyDeviceToHost), "save times");
     void *saved[3] = {nullptr, nullptr, nullptr};
     for (int v = 0; v < 3 && !st; ++v) {
         st = cuda_check(ctx, cudaMalloc(&saved[v], rs * n), "cudaMalloc(autotune)");
@@ -632,6 +642,9 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
         *ctx->hsc = saved_sc;
         if (!s) s = cuda_check(ctx, cudaMemcpyAsync(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice,
                                                     ctx->stream), "restore scalars");
+        if (!s && ctx->ninst > 0)
+            s = cuda_check(ctx, cudaMemcpyAsync(ctx->ia.time, saved_time.data(), sizeof(double) * ctx->ninst,
+                                                cudaMemcpyHostToDevice, ctx->stream), "restore times");
         if (!s) s = forward_state_changed(ctx);
         if (!s) s = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
         return s;
@@ -656,7 +669,7 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
         update_grid(ctx);
         drop_graphs(ctx);
         st = put_back();
-        if (!st) st = launch_forward_step(ctx);  // the first step after a state change sweeps every tile
+        if (!st) st = launch_forward_steps(ctx, 1);  // the first step after a state change sweeps every tile
         double ms = 0.0;
         if (!st) st = da_forward_run_timed(ctx, nsteps, nullptr, &ms);
         r.grid[k] = cand[k];

@@ -62,6 +62,26 @@ struct TimeConsts {
     long long n_replay;
 };
 
+// Ensemble (batched) mode: the mesh is the members' meshes one after another, each padded to
+// whole tiles, and these device tables give each tile its member and each member its constants
+// and step scalars.  All members take the same number of steps (one shared iteration count), each
+// with its own dt.  ninst == 0 in a single-instance context.
+struct InstArgs {
+    int ninst;
+    const int32_t *tile_inst;     // [ntiles] member of each tile
+    const MatConsts *mcs;         // [ninst]
+    double *time;                 // [ninst] TimeProps::time of each member
+    double *dt;                   // [ninst] dt of the current step
+    double *min_dxe, *hmax;       // [ninst] CFL reductions of the current step
+    unsigned long long *acc_min;  // [ninst] running CFL min (bit patterns of positive doubles)
+    unsigned long long *acc_max;  // [ninst] running hmax
+    const double *sec2_bed;       // [ninst][DA_MAX_MATERIALS] 1 + tan^2(phi_bed)
+    const double *cos_int;        // [ninst]
+    const double *dk_tab;         // [ninst][2][DA_MAX_MATERIALS][3] d kact / d phi_bed, d phi_int
+    const double *box;            // [ninst][4] functional box
+    const int32_t *seg0;          // [ninst + 1] first segment of each member
+};
+
 // Device copy of the flattened mesh.  FP64 path reads the double arrays; the FP32-split
 // path reads the float copies.
 struct DevMesh {
@@ -121,6 +141,17 @@ struct da_ctx {
     uint8_t *seg_wet = nullptr;      // [nseg] 1 when the segment held a wet cell after the last update
     uint8_t *seg_dirty = nullptr;    // [nseg] 1 when the segment may differ from the base checkpoint
     double *stage = nullptr;         // [n] FP64 staging for host transfers of FP32 arrays
+    double *seg_J = nullptr;         // [nseg] functional part of each segment at the final step
+    // ensemble mode (ninst > 0): device tables of InstArgs, host copies of the member layout
+    int ninst = 0;
+    da::InstArgs ia{};
+    std::vector<int32_t> inst_cell0;  // [ninst + 1] first cell of each member (multiple of 256)
+    std::vector<int32_t> inst_ncell;  // [ninst] cells of each member before padding
+    std::vector<int32_t> inst_nmat;   // [ninst] materials of each member
+    std::vector<int32_t> inst_npile;  // [ninst] piles of each member (0 or 1)
+    void *inst_mem = nullptr;         // one allocation holding every InstArgs table
+    double *inst_vol = nullptr;       // [ninst] members' volumes (stats)
+    std::vector<double> inst_init;    // [3][n] members' initial states, concatenated (restart)
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
     uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
     uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment
@@ -128,8 +159,8 @@ struct da_ctx {
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
     int grid = 0;                    // grid of the tiled step kernels (da_params.grid_blocks)
-    int coop_cap[2] = {0, 0};        // resident blocks of k_steps (FP32, FP64), 0 = not queried
-    int coop_cap_yt[2] = {0, 0};     // resident blocks of k_youturn
+    int coop_cap[4] = {0, 0, 0, 0};     // resident blocks of k_steps [FP32, FP64] x [single, ensemble]
+    int coop_cap_yt[8] = {};            // of k_youturn [FP32, FP64] x [single, ensemble] x [seed]
     int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror
@@ -147,13 +178,12 @@ struct da_ctx {
     double *dk_tab = nullptr;        // [2][DA_MAX_MATERIALS][3] d kact / d phi_bed, d phi_int
     double *red_out = nullptr;       // [DA_MAX_MATERIALS + 1 + DA_MAX_PILES]
     double *red_part = nullptr;      // [same x kAdjReduceParts] partial sums of the gradient reduction
-    double *seed_part = nullptr;     // [nblocks]
-    double *seed_J = nullptr;
-    unsigned *seed_counter = nullptr;
+    double *inst_J = nullptr;        // [max(ninst, 1)] J of each member
     double *dh0 = nullptr;           // [n_piles][n]
     std::vector<void *> snaps;       // checkpoint slots, 3 state arrays each
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
     int adj_n = 0;
+    int adj_ninst = -1;
     da::TraceState trace;
 };
 
@@ -191,6 +221,16 @@ int launch_youturn(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, dou
 int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
 int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
 int forward_state_changed(da_ctx *ctx);
+// adjoint_host.cu: d kact / d phi_bed and d phi_int of each material's three branches
+void kact_derivatives(const da_params &p, double *dkb, double *dki);
+// adjoint_host.cu: the checkpointed reverse sweep (see there)
+int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
+                  long long *fsteps, float *dev_ms);
+int copy_lambda_out(da_ctx *ctx, int buf, double *host);
+// ensemble.cu: drop the ensemble tables (back to a single-instance layout)
+void free_members(da_ctx *ctx);
+// adjoint_fp64.cu: ensemble members' volumes into out[ninst] (device)
+int launch_member_volume(da_ctx *ctx, double *out);
 // snapshot.cu
 size_t snapshot_bytes(const da_ctx *ctx);
 int launch_snapshot(da_ctx *ctx, void *slot, bool store);

@@ -90,6 +90,17 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 }
 
 
+// Warp-reduced CFL min / hmax into one accumulator pair.
+__device__ __forceinline__ void push_minmax(unsigned long long my_min, unsigned long long my_max,
+                                            unsigned long long *acc_min, unsigned long long *acc_max) {
+    my_min = warp_min_u64(my_min);
+    my_max = warp_max_u64(my_max);
+    if ((threadIdx.x & 31) == 0) {
+        if (my_min != 0x7FF0000000000000ull) atomicMin(acc_min, my_min);
+        if (my_max) atomicMax(acc_max, my_max);
+    }
+}
+
 // ----------------------------------------------------------------------------- k_coef
 // One thread per cell of each listed tile.  With tile culling, a tile none of whose 32-cell
 // segments held a wet cell after the last update is not listed (its depths cannot have changed
@@ -99,17 +110,22 @@ __device__ __forceinline__ bool last_block(unsigned *counter) {
 // RECORD: also writes the branch code of every cell of a listed tile into mask (0 dry / at rest,
 // 1..3 for sgn(vel) = -1, 0, +1 of gmfggetcoef) for the adjoint's replay.
 // The thread's CFL min and hmax (bit patterns of positive doubles) accumulate in my_min / my_max.
-template <class R, bool RECORD>
+// BATCH (ensemble): the tile's member gives the material constants, and the CFL values go to the
+// member's accumulators after every tile.
+template <class R, bool RECORD, bool BATCH = false>
 __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> &U, R *kact, unsigned *active,
-                                           const uint8_t *seg_wet, int ntiles, int cull, const MatConsts &mc,
+                                           const uint8_t *seg_wet, int ntiles, int cull, const MatConsts &mc0,
                                            DevScalars *sc, uint8_t *mask, int *list, unsigned long long &my_min,
-                                           unsigned long long &my_max) {
+                                           unsigned long long &my_max, const InstArgs &ia) {
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
         const bool need = tq < ntiles && (!cull || seg_flags(seg_wet, tq) != 0ull);
         const int cnt = compact_tiles(need, tq, list);
         for (int q = 0; q < cnt; ++q) {
-            const int i = list[q] * kBlock + threadIdx.x;
+            const int t = list[q];
+            const int inst = BATCH ? ia.tile_inst[t] : 0;
+            const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+            const int i = t * kBlock + threadIdx.x;
             bool wet = false;
             if (i < m.n) {
                 const R h = U.h[i];
@@ -153,18 +169,12 @@ __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> 
             }
             const unsigned self = __ballot_sync(0xffffffffu, wet);
             if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
+            if (BATCH) {
+                push_minmax(my_min, my_max, ia.acc_min + inst, ia.acc_max + inst);
+                my_min = 0x7FF0000000000000ull;
+                my_max = 0ull;
+            }
         }
-    }
-}
-
-// Warp-reduced CFL min / hmax into one accumulator pair.
-__device__ __forceinline__ void push_minmax(unsigned long long my_min, unsigned long long my_max,
-                                            unsigned long long *acc_min, unsigned long long *acc_max) {
-    my_min = warp_min_u64(my_min);
-    my_max = warp_max_u64(my_max);
-    if ((threadIdx.x & 31) == 0) {
-        if (my_min != 0x7FF0000000000000ull) atomicMin(acc_min, my_min);
-        if (my_max) atomicMax(acc_max, my_max);
     }
 }
 
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
     __shared__ int list[kBlock];
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
-    coef_phase<R, RECORD>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max);
+    coef_phase<R, RECORD>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max, InstArgs{});
     push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (last_block(&sc->blocks_done[0])) {
         if (threadIdx.x == 0) {
@@ -280,13 +290,13 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 // RECORD: every cell of a listed tile gets its full mask byte (the k_coef code of a wet cell,
 // bit 3 active, bit 2 depth clamped), the tile records the step id (tile_epoch) and each segment
 // whether it had an active cell (seg_act); masks of tiles with another epoch count as zero.
-template <class R, bool RECORD>
+template <class R, bool RECORD, bool BATCH = false>
 __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R> &U, const StateOut<R> &O,
                                              const R *kact, unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                              double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
-                                             const MatConsts &mc,
-                                             DevScalars *sc, R dt, R ft, uint8_t *mask, int *tile_epoch,
-                                             uint8_t *seg_act, int rec_id, int *list) {
+                                             const MatConsts &mc0,
+                                             DevScalars *sc, R dt0, R ft, uint8_t *mask, int *tile_epoch,
+                                             uint8_t *seg_act, int rec_id, int *list, const InstArgs &ia) {
     const int lane = threadIdx.x & 31;
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
@@ -304,6 +314,9 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
         const int cnt = compact_tiles(need, tq, list);
         for (int q = 0; q < cnt; ++q) {
             const int t = list[q];
+            const int inst = BATCH ? ia.tile_inst[t] : 0;
+            const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+            const R dt = BATCH ? R(ia.dt[inst]) : dt0;
             const int i = t * kBlock + threadIdx.x;
             const int seg = i >> 5;
             const unsigned word = active[seg];  // padded: bits of cells >= n are never set
@@ -355,7 +368,7 @@ __global__ void __launch_bounds__(kBlock) k_update(MeshArgs m, StateRef<R> U, St
     const R dt = R(sc->dt);
     const R ft = R(sc->frict_tiny) > R(mc.sign_floor) ? R(sc->frict_tiny) : R(mc.sign_floor);
     update_phase<R, RECORD>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc, dt, ft, mask,
-                            tile_epoch, seg_act, rec_id, list);
+                            tile_epoch, seg_act, rec_id, list, InstArgs{});
 }
 
 // ---------------------------------------------------------------------------- volume
@@ -440,11 +453,31 @@ struct StatePair {
     R *hv[2];
 };
 
-template <class R>
+// Ensemble: the dt of every member from its reduced CFL values (threads over members), its time
+// advanced, its accumulators restarted.  Runs between two grid barriers.
+__device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter, const TimeConsts &tc) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ia.ninst; k += gridDim.x * blockDim.x) {
+        const double mn = __longlong_as_double(__ldcg(ia.acc_min + k));
+        const double hx = __longlong_as_double(__ldcg(ia.acc_max + k));
+        const double time = ia.time[k];
+        double dt, ft;
+        step_dt(mn, hx, time, iter, tc, dt, ft);
+        ia.dt[k] = dt;
+        ia.time[k] = time + dt;
+        ia.min_dxe[k] = mn;
+        ia.hmax[k] = hx;
+        ia.acc_min[k] = kMinDxeStart;
+        ia.acc_max[k] = 0ull;
+    }
+}
+
+// BATCH: every member of the ensemble steps with its own dt (a third barrier per step after the
+// members' dt pass); the shared iteration count lives in the scalars.
+template <class R, bool BATCH = false>
 __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
-                                                  MatConsts mc, TimeConsts tc, DevScalars *sc) {
+                                                  MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia) {
     __shared__ int list[kBlock];
     double time = sc->time;
     long long iter = sc->iter;
@@ -456,31 +489,38 @@ __global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, in
         const StateRef<R> U{S.h[c], S.hu[c], S.hv[c]};
         const StateOut<R> O{S.h[c ^ 1], S.hu[c ^ 1], S.hv[c ^ 1]};
         unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-        coef_phase<R, false>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max);
-        push_minmax(my_min, my_max, acc_min, acc_max);
+        coef_phase<R, false, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max,
+                                    ia);
+        if (!BATCH) push_minmax(my_min, my_max, acc_min, acc_max);
         if (!grid_sync(sc)) return;
-        min_dxe = __longlong_as_double(__ldcg(acc_min));
-        hmax = __longlong_as_double(__ldcg(acc_max));
-        step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
-        time += dt;
-        iter += 1;
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            // read by every block before this step's first barrier; used again next step
-            *(p ? &sc->acc_min_dxe : &sc->acc_alt_min_dxe) = kMinDxeStart;
-            *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
+        if (BATCH) {
+            ft = iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
+            inst_dt_pass(ia, iter, tc);
+            iter += 1;
+            if (!grid_sync(sc)) return;
+        } else {
+            min_dxe = __longlong_as_double(__ldcg(acc_min));
+            hmax = __longlong_as_double(__ldcg(acc_max));
+            step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+            time += dt;
+            iter += 1;
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                // read by every block before this step's first barrier; used again next step
+                *(p ? &sc->acc_min_dxe : &sc->acc_alt_min_dxe) = kMinDxeStart;
+                *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
+            }
         }
         const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-        update_phase<R, false>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc, sc,
-                               R(dt), ftr,
-                               nullptr, nullptr, nullptr, 0, list);
+        update_phase<R, false, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc,
+                                      sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list, ia);
         if (!grid_sync(sc)) return;
     }
-    if (blockIdx.x == 0) {
-        if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->iter = iter;
+        sc->frict_tiny = ft;
+        if (!BATCH) {
             sc->time = time;
-            sc->iter = iter;
             sc->dt = dt;
-            sc->frict_tiny = ft;
             sc->min_dxe = min_dxe;
             sc->hmax = hmax;
             sc->acc_min_dxe = sc->acc_alt_min_dxe = kMinDxeStart;
@@ -529,14 +569,16 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
 template <class R>
 int launch_steps_t(da_ctx *ctx, int nsteps) {
     if (nsteps <= 0) return DA_OK;
-    if (ctx->coop_cap[sizeof(R) == 8] <= 0) {
+    const bool batch = ctx->ninst > 0;
+    const void *kern = batch ? (const void *)k_steps<R, true> : (const void *)k_steps<R, false>;
+    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch];
+    if (cap_ref <= 0) {
         int per_sm = 0;
-        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_steps<R>, kBlock, 0),
-                            "occupancy");
+        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");
         if (st) return st;
-        ctx->coop_cap[sizeof(R) == 8] = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
+        cap_ref = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
     }
-    const int cap = ctx->coop_cap[sizeof(R) == 8];
+    const int cap = cap_ref;
     if (cap <= 0) return set_error(ctx, DA_ERR_UNSUPPORTED, "multi-step kernel cannot be resident");
     const int grid = ctx->grid < cap ? ctx->grid : cap;
     MeshArgs m = mesh_args(ctx);
@@ -555,10 +597,11 @@ int launch_steps_t(da_ctx *ctx, int nsteps) {
     MatConsts mc = ctx->mc;
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
+    InstArgs ia = ctx->ia;
     void *args[] = {&m,        &S,       &cur,       &n,     &kact, &active, &seg_clean, &seg_wet,
-                    &seg_vol,  &seg_dirty, &ntiles,  &cull,  &mc,   &tc,     &sc};
+                    &seg_vol,  &seg_dirty, &ntiles,  &cull,  &mc,   &tc,     &sc,     &ia};
     trace_begin(ctx, TR_STEPS);
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_steps<R>, grid, kBlock, args, 0, ctx->stream);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx, nsteps);
     if (e != cudaSuccess) return cuda_check(ctx, e, "multi-step launch");
     ctx->cur = (cur + nsteps) & 1;

@@ -38,6 +38,9 @@ struct SnapArgs {
     uint8_t *seg_wet;
     double *seg_vol;
     DevScalars *sc;
+    double *times;         // ensemble: the members' times (null in a single context)
+    double *snap_times;
+    int ninst;
     int nseg;
     int mode;
 };
@@ -112,11 +115,20 @@ __global__ void __launch_bounds__(kBlock) k_snapshot(SnapArgs<R> a) {
             a.seg_clean[s] = 1;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (a.mode == STORE_BASE || a.mode == STORE)
-            *a.snap_sc = *a.sc;
-        else
-            *a.sc = *a.snap_sc;
+    if (blockIdx.x == 0) {
+        const bool st = a.mode == STORE_BASE || a.mode == STORE;
+        if (threadIdx.x == 0) {
+            if (st)
+                *a.snap_sc = *a.sc;
+            else
+                *a.sc = *a.snap_sc;
+        }
+        for (int k = threadIdx.x; k < a.ninst; k += blockDim.x) {
+            if (st)
+                a.snap_times[k] = a.times[k];
+            else
+                a.times[k] = a.snap_times[k];
+        }
     }
 }
 
@@ -138,6 +150,9 @@ int launch_t(da_ctx *ctx, void *slot, bool store) {
     }
     a.snap_dirty = b + 3 * ab;
     a.snap_sc = (DevScalars *)(b + 3 * ab + align256((size_t)ctx->nseg));
+    a.snap_times = (double *)(b + 3 * ab + align256((size_t)ctx->nseg) + align256(sizeof(DevScalars)));
+    a.times = ctx->ia.time;
+    a.ninst = ctx->ninst;
     a.seg_dirty = ctx->seg_dirty;
     a.seg_clean = ctx->seg_clean;
     a.seg_wet = ctx->seg_wet;
@@ -156,7 +171,8 @@ int launch_t(da_ctx *ctx, void *slot, bool store) {
 
 size_t snapshot_bytes(const da_ctx *ctx) {
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);
-    return 3 * align256(rs * (size_t)ctx->mesh.n) + align256((size_t)ctx->nseg) + sizeof(DevScalars);
+    return 3 * align256(rs * (size_t)ctx->mesh.n) + align256((size_t)ctx->nseg) + align256(sizeof(DevScalars)) +
+           sizeof(double) * (size_t)ctx->ninst;
 }
 
 int launch_snapshot(da_ctx *ctx, void *slot, bool store) {

@@ -112,6 +112,44 @@ def workload3(cells_per_side: int = 1024, seed: int = 0) -> Workload:
 WORKLOAD3_BOX = (350.0, 850.0, 2250.0, 2750.0)
 
 
+@dataclass
+class MemberSpec:
+    slope_deg: float
+    volume: float      # pile volume, m^3
+    bedfrict_deg: float
+    side: int          # cells across (side^2 cells)
+
+
+def ensemble_specs(n: int, seed: int = 4, min_side: int = 128, max_side: int = 512) -> list:
+    """Seeded draws for an ensemble of inclined-plane runs: slope U(20, 35) deg, pile volume
+    U(1e4, 1e6) m^3, basal friction U(12, 28) deg, uneven meshes of side U{min_side..max_side}
+    (a multiple of 16) cells."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        out.append(MemberSpec(float(rng.uniform(20.0, 35.0)), float(rng.uniform(1.0e4, 1.0e6)),
+                              float(rng.uniform(12.0, 28.0)), int(16 * rng.integers(min_side // 16, max_side // 16 + 1))))
+    return out
+
+
+def ensemble_member(spec: MemberSpec, intfrict_deg: float = 30.0):
+    """(mesh, MatProps, pile, box) of one ensemble member: a plane of the drawn slope meeting a flat
+    runout at mid-domain, a paraboloid pile (height 0.3 R, volume pi/2 H R^2, so R scales with
+    volume^(1/3)) a fifth of the way down, a uniform mesh of side^2 cells over 24 R x 24 R, and the
+    functional box over the start of the runout."""
+    R = (spec.volume / (0.15 * math.pi)) ** (1.0 / 3.0)
+    L = 24.0 * R
+    res = L / spec.side
+    dem = inclined_plane(L, L, res, spec.slope_deg, 0.5 * L)
+    pile = Pile(0.2 * L, 0.5 * L, 0.3 * R, R, R)
+    base = spec.side // 16
+    mesh_spec = MeshSpec(xmin=0.0, ymin=0.0, dx0=L / base, dy0=L / base, nx0=base, ny0=base, max_level=4, uniform=True)
+    mesh = Mesh.build(mesh_spec, dem, [pile])
+    mat = MatProps(intfrict_deg=intfrict_deg, bedfrict_deg=[spec.bedfrict_deg])
+    box = (0.5 * L, 0.7 * L, 0.4 * L, 0.6 * L)
+    return mesh, mat, pile, box
+
+
 def test_case(seed: int = 1, nx0: int = 24, ny0: int = 16, max_level: int = 2, random_frac: float = 0.35,
               n_materials: int = 2) -> Workload:
     """Small seeded case with hanging nodes everywhere: bumpy slope, two piles, two materials."""

@@ -203,6 +203,43 @@ int da_trace_read(da_ctx *ctx, int32_t k, double *total_ms, int64_t *launches);
 int da_trace_steps(da_ctx *ctx, int32_t k, int64_t *steps);
 const char *da_trace_name(int32_t k);
 
+/* ---- ensembles: many instances in one launch ------------------------------------------------
+ * The reference runs the instances of an ensemble (the stochastic module's sampled pile volumes
+ * and friction angles) as separate processes, each through step() and dual_solver().  Here the
+ * members share one context: their flattened meshes are laid one after another (each padded to
+ * whole 256-cell tiles) and every step kernel advances all of them in the same cooperative launch,
+ * each member with its own material constants, dt and time; the iteration count (and so
+ * frict_tiny) is shared.  A member's state after a run equals its single-instance run bit for bit
+ * in FP64 (and its dt and time); J and gradients equal it up to the order of the FP64 sums.  The
+ * context's da_params give the precision and every setting but the friction angles and material
+ * count, which come from each member.  da_upload_mesh and the single-instance run / adjoint
+ * calls are not used on an ensemble context (DA_ERR_INVALID). */
+typedef struct da_member {
+    da_mesh_soa mesh;                   /* the member's flattened mesh (host arrays) */
+    const double *h0, *hu0, *hv0;       /* [n] initial state */
+    const double *dh0_dpile;            /* [n] d h0 / d pile height of the member's pile, or NULL */
+    int32_t n_materials;
+    int32_t pad;
+    double bedfrict[DA_MAX_MATERIALS];  /* radians */
+    double intfrict;                    /* radians */
+    double box[4];                      /* functional box (xmin, xmax, ymin, ymax) */
+} da_member;
+/* Replaces the context's mesh and state with the members'; time 0, iteration 0. */
+int da_ensemble_upload(da_ctx *ctx, const da_member *members, int32_t n_members);
+/* Every member back to its initial state, time 0, iteration 0. */
+int da_ensemble_restart(da_ctx *ctx);
+/* nsteps steps of every member in one cooperative launch; device_ms (optional) its device time. */
+int da_ensemble_forward(da_ctx *ctx, int32_t nsteps, double *device_ms);
+/* Per-member scalars of the last step (out[n_members]): dt, time, volume, hmax, iteration. */
+int da_ensemble_stats(da_ctx *ctx, da_step_stats *out);
+/* One member's current state (FP64 host arrays of its own n cells). */
+int da_ensemble_get_state(da_ctx *ctx, int32_t member, double *h, double *hu, double *hv);
+/* Forward + discrete adjoint of every member over nsteps steps from the current state (binomial
+ * checkpoints shared by all members), J = sum of h^2 dx dy over the member's box; out[n_members]
+ * gets each member's J and gradients (dJ_dpile[0] for its pile); the state is put back.
+ * device_ms (optional): device time of the whole sweep. */
+int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_gradient *out, double *device_ms);
+
 /* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
  * Times nsteps forward steps from the current state for each candidate grid of the tiled
  * kernels (1, 2, 3, 4, 6 and 8 blocks of 256 threads per SM, capped at the tile count), keeps
