@@ -16,11 +16,14 @@ reported beside it with their errors.
 
 Also reported: the FP32-split errors against FP64 (final state, J, gradients, lambda^0),
 the forward step alone on the 3.75M-cell adaptive workload (hill + noise, 3 piles, 4 materials),
-per-kernel device times (tracing), the roofline of the dominant kernel, e2e through the C ABI
-with host buffers, clocks, and a CPU baseline.
+the batched 512-member ensemble (forward + adjoint, 300 steps) against the same members run one
+after another, per-kernel device times (tracing), the roofline of the dominant kernel, e2e
+through the C ABI with pinned host buffers, clocks, and a CPU baseline.
 
-Multi-GPU: the workload is one instance, so N > 1 runs N independent replicas (one per rank,
-"weak" scaling, no data-path collective); barrier and max over ranks stay.
+Multi-GPU: the headline workload is one instance, so N > 1 runs N independent replicas (one per
+rank, "weak" scaling, no data-path collective); the ensemble's members are split over the ranks
+(size-balanced greedy partition) with one gather of the per-member results; barrier and max over
+ranks stay.
 
 --impl reference: the reference's own step() compiled from its sources (oracle/_ref/ref_harness,
 when built) timed on this host, else the oracle restatement; rank 0 only.
@@ -44,6 +47,8 @@ import numpy as np  # noqa: E402
 METRIC = "cell-updates/s fwd+adjoint, FP32-split & batched vs plain FP64 GPU at ≤1e-5 rel err"
 HORIZON = 512
 SNAPSHOTS = 32
+ENS_STEPS = 300
+ENS_SNAPSHOTS = 32
 
 
 def peaks():
@@ -128,6 +133,16 @@ def allmax(x: float, ws: int, dev: int) -> float:
     import torch.distributed as dist
     t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(x: float, ws: int, dev: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -255,6 +270,8 @@ def fwdadj(args, ws, local):
     sampler = ClockSampler(local)
     for name, prec in (("fp64", _ffi.DA_PREC_FP64), ("fp32", _ffi.DA_PREC_FP32_SPLIT)):
         c = fresh(prec)
+        # launch shape of the step kernels picked by the autotuner on this workload
+        tune = c.autotune(10)
         for _ in range(args.warmup):
             adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
         if not args.no_clocks:
@@ -275,7 +292,8 @@ def fwdadj(args, ws, local):
         ms = allmax(ms, ws, local)
         gl = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, want_lambda0=True)
         res = {"ms": ms, "value": m.n * HORIZON * args.steps * ws / (ms * 1e-3), "grad": gl,
-               "forward_steps": g.forward_steps}
+               "forward_steps": g.forward_steps, "launch_shape": {"blocks_per_sm": tune["best"][0],
+                                                                   "grid": tune["best"][1]}}
         res["clocks"] = sampler.stop() if not args.no_clocks else {"sm_mhz": None, "sm_max_mhz": None,
                                                                      "reasons": ["not sampled"]}
         # per-kernel device times of one traced run
@@ -349,6 +367,62 @@ def forward_config2(args, ws, local):
     return w, res
 
 
+def ensemble_config4(args, ws, rank, local):
+    """The batched ensemble: seeded members (plane slope U(20, 35) deg, pile volume U(1e4, 1e6) m^3,
+    basal friction U(12, 28) deg, meshes of 16k-262k cells), forward + adjoint of each member's
+    runout functional over 300 steps with 32 checkpoints, all members in the same launches; the
+    same members run one after another through the plain FP64 single-instance path for the
+    batched-vs-sequential ratio (device time of each run, summed).  With N ranks the members
+    are split by a size-balanced greedy partition and each rank runs its share; the per-member
+    results are gathered once."""
+    from discrete_adjoint_b200 import Ensemble, GeoflowContext, Member, TimeProps, _ffi, adjoint_run, inputs
+    from discrete_adjoint_b200.ensemble import gather_results, shard_members
+    specs = inputs.ensemble_specs(args.members)
+    sizes = [s.side * s.side for s in specs]
+    mine = shard_members(sizes, ws, rank)
+    members = []
+    for k in mine:
+        mesh, mat, _, box = inputs.ensemble_member(specs[k])
+        members.append(Member(mesh, mat, box))
+    cells = sum(mb.mesh.n for mb in members)
+    total_cells = int(allsum(cells, ws, local))
+    out = {"members": args.members, "cells": total_cells, "steps": ENS_STEPS, "snapshots": ENS_SNAPSHOTS,
+           "members_per_rank_max": int(allmax(len(members), ws, local))}
+    grads = {}
+    for name, prec in (("fp64", _ffi.DA_PREC_FP64), ("fp32", _ffi.DA_PREC_FP32_SPLIT)):
+        with Ensemble(members, precision=prec, device=local) as ens:
+            tune = ens.autotune(5)
+            ens.adjoint(ENS_STEPS, ENS_SNAPSHOTS)  # warm-up
+            barrier(ws, local)
+            g, ms = ens.adjoint(ENS_STEPS, ENS_SNAPSHOTS)
+            barrier(ws, local)
+            ms = allmax(ms, ws, local)
+        grads[name] = gather_results({k: (gg.J, gg.dJ_dbedfrict[0], gg.dJ_dpile[0]) for k, gg in zip(mine, g)}, ws)
+        out[name] = {"ms": ms, "value": total_cells * ENS_STEPS / (ms * 1e-3),
+                     "launch_shape": {"blocks_per_sm": tune["best"][0], "grid": tune["best"][1]}}
+    rel = lambda a, b: abs(a - b) / max(abs(b), 1e-300)  # noqa: E731
+    out["fp32_rel_err_vs_fp64_max"] = {
+        q: max(rel(grads["fp32"][k][i], grads["fp64"][k][i]) for k in grads["fp64"])
+        for i, q in enumerate(("J", "dJ_dbedfrict", "dJ_dpile"))}
+    if ws == 1 and not args.no_sequential:
+        seq_ms, worst = 0.0, 0.0
+        for i, mb in enumerate(members):
+            with GeoflowContext(mb.mat, TimeProps(), precision=_ffi.DA_PREC_FP64, device=local) as c:
+                c.upload_mesh(mb.mesh)
+                c.set_state(mb.mesh.h0, mb.mesh.hu0, mb.mesh.hv0)
+                if i == 0:
+                    adjoint_run(c, mb.box, ENS_STEPS, ENS_SNAPSHOTS, mb.mesh.dh0_dpile[0])  # module warm-up
+                gs = adjoint_run(c, mb.box, ENS_STEPS, ENS_SNAPSHOTS, mb.mesh.dh0_dpile[0])
+            seq_ms += gs.device_ms
+            e = grads["fp64"][mine[i]]
+            worst = max(worst, rel(e[0], gs.J), rel(e[1], gs.dJ_dbedfrict[0]), rel(e[2], gs.dJ_dpile[0]))
+        out["sequential_fp64"] = {"ms": seq_ms, "value": total_cells * ENS_STEPS / (seq_ms * 1e-3)}
+        out["batched_fp64_over_sequential"] = seq_ms / out["fp64"]["ms"]
+        out["batched_fp32_over_sequential"] = seq_ms / out["fp32"]["ms"]
+        out["batched_vs_sequential_max_rel_diff"] = worst
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -359,6 +433,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--no-forward", action="store_true", help="skip the forward-only section")
+    ap.add_argument("--members", type=int, default=512, help="ensemble members (0 skips the ensemble section)")
+    ap.add_argument("--no-sequential", action="store_true", help="skip the sequential baseline of the ensemble")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -404,6 +480,8 @@ def main():
         w2, f2 = forward_config2(args, ws, local)
         fwd = {"workload": w2.name, "cells": w2.mesh.n, "steps": 300, "unit": "cell-updates/s", **f2}
 
+    ens = ensemble_config4(args, ws, rank, local) if args.members > 0 else None
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, kind, sample = reference_forward_rate(w, 15.0)
@@ -421,7 +499,7 @@ def main():
                        "precision": "fp64" if head == "fp64" else "fp32-split",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "per-run working set larger than L2 (no flush needed)",
-                       "forward_steps_per_run": hr["forward_steps"]},
+                       "forward_steps_per_run": hr["forward_steps"], "launch_shape": hr["launch_shape"]},
             "fp64": {"value": r["fp64"]["value"], "ms_per_run": r["fp64"]["ms"] / args.steps},
             "fp32_split": {"value": r["fp32"]["value"], "ms_per_run": r["fp32"]["ms"] / args.steps,
                            "over_fp64": r["fp32"]["value"] / r["fp64"]["value"], "rel_err_vs_fp64": errs,
@@ -438,6 +516,7 @@ def main():
             "clocks": hr["clocks"],
             "cpu_baseline": cpu,
             "forward_only": fwd,
+            "ensemble": ens,
         }
         print(json.dumps(line))
     if ws > 1:

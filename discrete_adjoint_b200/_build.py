@@ -63,7 +63,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
-    objs = []
+    objs, jobs = [], []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
@@ -75,7 +75,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 cmd = [nvcc] + NVCC_COMMON + extra + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            jobs.append(cmd)
+    # the translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs)):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB, objs):
         cmd = [nvcc, "-shared", "-Xcompiler", "-fPIC"] + ARCH + objs + ["-o", LIB, "-cudart", "static"]
         if verbose:

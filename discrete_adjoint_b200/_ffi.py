@@ -56,6 +56,8 @@ class da_params(C.Structure):
         ("fp32_sign_floor", C.c_double),
         ("tile_culling", C.c_int32),
         ("grid_blocks", C.c_int32),
+        ("blocks_per_sm", C.c_int32),
+        ("reserved1", C.c_int32),
     ]
 
 
@@ -78,7 +80,7 @@ DA_TRACE_KINDS = 11
 
 class da_tune_result(C.Structure):
     _fields_ = [("n", C.c_int32), ("best", C.c_int32), ("grid", C.c_int32 * DA_TUNE_MAX),
-                ("ms_per_step", C.c_double * DA_TUNE_MAX)]
+                ("blocks_per_sm", C.c_int32 * DA_TUNE_MAX), ("ms_per_step", C.c_double * DA_TUNE_MAX)]
 
 
 class da_step_stats(C.Structure):

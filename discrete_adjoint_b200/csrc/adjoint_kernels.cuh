@@ -82,8 +82,8 @@ int reduce_inst_t(da_ctx *ctx, int lam0) {
 // adjoint phases, with each segment's part of J.  BATCH: every member with its own constants and
 // dt (the members' dt pass between two barriers).  Block 0 writes the step's scalars at the end,
 // as the separate kernels do.
-template <class R, bool BATCH, bool SEED>
-__global__ void __launch_bounds__(kBlock) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
+template <class R, bool BATCH, bool SEED, int OCC>
+__global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
                                                     uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
                                                     uint8_t *seg_dirty, int ntiles, int cull, MatConsts mc,
                                                     TimeConsts tc, DevScalars *sc, uint8_t *mask, int *tile_epoch,
@@ -140,9 +140,15 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
               const double *box4) {
     const int pi = sizeof(R) == 8;
     const bool batch = ctx->ninst > 0;
-    const void *kern = batch ? (seed ? (const void *)k_youturn<R, true, true> : (const void *)k_youturn<R, true, false>)
-                             : (seed ? (const void *)k_youturn<R, false, true> : (const void *)k_youturn<R, false, false>);
-    int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed];
+    const int occ3 = ctx->p.blocks_per_sm == 3;
+    const void *kern;
+    if (occ3)
+        kern = batch ? (seed ? (const void *)k_youturn<R, true, true, 3> : (const void *)k_youturn<R, true, false, 3>)
+                     : (seed ? (const void *)k_youturn<R, false, true, 3> : (const void *)k_youturn<R, false, false, 3>);
+    else
+        kern = batch ? (seed ? (const void *)k_youturn<R, true, true, 2> : (const void *)k_youturn<R, true, false, 2>)
+                     : (seed ? (const void *)k_youturn<R, false, true, 2> : (const void *)k_youturn<R, false, false, 2>);
+    int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed + 8 * occ3];
     if (cap_ref <= 0) {
         int per_sm = 0;
         int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");

@@ -106,6 +106,7 @@ static bool params_ok(const da_params *p) {
     if (p->n_materials < 1 || p->n_materials > DA_MAX_MATERIALS) return false;
     if (!(p->epsilon > 0) || !(p->gravity_scale > 0) || !(p->gamma > 0)) return false;
     if (p->grid_blocks < 0 || p->grid_blocks > (1 << 20)) return false;
+    if (p->blocks_per_sm != 0 && p->blocks_per_sm != 2 && p->blocks_per_sm != 3) return false;
     return true;
 }
 
@@ -291,6 +292,8 @@ void da_params_default(da_params *p) {
     p->fp32_sign_floor = 0.0;
     p->tile_culling = 1;
     p->grid_blocks = 0;
+    p->blocks_per_sm = 0;
+    p->reserved1 = 0;
 }
 
 da_ctx *da_create(const da_params *p, int *err) {
@@ -606,8 +609,9 @@ int da_trace_steps(da_ctx *ctx, int32_t k, int64_t *steps) {
 }  // extern "C"
 
 // ---------------------------------------------------------------------------- autotuner
-// Times nsteps forward steps from the current state for each candidate grid (1, 2, 3, 4, 6 and
-// 8 blocks per SM, capped at the tile count) and keeps the fastest.  The state, time and
+// Times nsteps forward steps from the current state for each candidate launch shape (register
+// budget of 2 or 3 resident blocks per SM x grids of 1..budget blocks per SM) and keeps the
+// fastest.  The state, time and
 // iteration are put back after every trial, so the tuning leaves the run where it was.
 int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     using namespace da;
@@ -650,22 +654,27 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
         return s;
     };
     const int sm = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    const int mult[6] = {1, 2, 3, 4, 6, 8};
-    int cand[DA_TUNE_MAX], nc = 0;
-    for (int k = 0; k < 6; ++k) {
-        int g = mult[k] * sm;
-        if (g > ctx->ntiles) g = ctx->ntiles;
-        bool dup = false;
-        for (int j = 0; j < nc; ++j) dup |= cand[j] == g;
-        if (!dup && nc < DA_TUNE_MAX) cand[nc++] = g;
-    }
-    const int32_t grid0 = ctx->p.grid_blocks;
+    // (blocks per SM of the register budget, grid): grids of 1, 2, 3 blocks per SM up to the budget
+    int cand_occ[DA_TUNE_MAX], cand[DA_TUNE_MAX], nc = 0;
+    for (int occ = 2; occ <= 3; ++occ)
+        for (int mult = 1; mult <= occ; ++mult) {
+            int g = mult * sm;
+            if (g > ctx->ntiles) g = ctx->ntiles;
+            bool dup = false;
+            for (int j = 0; j < nc; ++j) dup |= cand[j] == g && cand_occ[j] == occ;
+            if (!dup && nc < DA_TUNE_MAX) {
+                cand_occ[nc] = occ;
+                cand[nc++] = g;
+            }
+        }
+    const int32_t grid0 = ctx->p.grid_blocks, occ0 = ctx->p.blocks_per_sm;
     double best_ms = HUGE_VAL;
     int best = 0;
     da_tune_result r;
     std::memset(&r, 0, sizeof(r));
     for (int k = 0; k < nc && !st; ++k) {
         ctx->p.grid_blocks = cand[k];
+        ctx->p.blocks_per_sm = cand_occ[k];
         update_grid(ctx);
         drop_graphs(ctx);
         st = put_back();
@@ -673,6 +682,7 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
         double ms = 0.0;
         if (!st) st = da_forward_run_timed(ctx, nsteps, nullptr, &ms);
         r.grid[k] = cand[k];
+        r.blocks_per_sm[k] = cand_occ[k];
         r.ms_per_step[k] = ms / nsteps;
         if (!st && ms < best_ms) {
             best_ms = ms;
@@ -682,6 +692,7 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     r.n = nc;
     r.best = best;
     ctx->p.grid_blocks = st ? grid0 : cand[best];
+    ctx->p.blocks_per_sm = st ? occ0 : cand_occ[best];
     update_grid(ctx);
     drop_graphs(ctx);
     const int st2 = put_back();

@@ -159,8 +159,8 @@ struct da_ctx {
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
     int grid = 0;                    // grid of the tiled step kernels (da_params.grid_blocks)
-    int coop_cap[4] = {0, 0, 0, 0};     // resident blocks of k_steps [FP32, FP64] x [single, ensemble]
-    int coop_cap_yt[8] = {};            // of k_youturn [FP32, FP64] x [single, ensemble] x [seed]
+    int coop_cap[8] = {};     // resident blocks of k_steps [FP32, FP64] x [single, ensemble] x [2, 3 per SM]
+    int coop_cap_yt[16] = {};  // of k_youturn [FP32, FP64] x [single, ensemble] x [seed] x [2, 3 per SM]
     int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror

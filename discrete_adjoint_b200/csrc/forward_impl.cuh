@@ -472,9 +472,10 @@ __device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter,
 }
 
 // BATCH: every member of the ensemble steps with its own dt (a third barrier per step after the
-// members' dt pass); the shared iteration count lives in the scalars.
-template <class R, bool BATCH = false>
-__global__ void __launch_bounds__(kBlock) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
+// members' dt pass); the shared iteration count lives in the scalars.  OCC: resident blocks per
+// SM the register budget is set for (da_params.blocks_per_sm).
+template <class R, bool BATCH = false, int OCC = 2>
+__global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
                                                   MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia) {
@@ -570,8 +571,10 @@ template <class R>
 int launch_steps_t(da_ctx *ctx, int nsteps) {
     if (nsteps <= 0) return DA_OK;
     const bool batch = ctx->ninst > 0;
-    const void *kern = batch ? (const void *)k_steps<R, true> : (const void *)k_steps<R, false>;
-    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch];
+    const int occ3 = ctx->p.blocks_per_sm == 3;
+    const void *kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3> : (const void *)k_steps<R, true, 2>)
+                             : (occ3 ? (const void *)k_steps<R, false, 3> : (const void *)k_steps<R, false, 2>);
+    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch + 4 * occ3];
     if (cap_ref <= 0) {
         int per_sm = 0;
         int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");

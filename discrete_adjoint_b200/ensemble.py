@@ -15,7 +15,7 @@ import numpy as np
 
 from . import _ffi
 from .mesh import Mesh
-from .solver import Gradient, MatProps, StepStats, TimeProps, make_params
+from .solver import Gradient, MatProps, StepStats, TimeProps, make_params, tune_result
 
 
 @dataclass
@@ -29,13 +29,14 @@ class Member:
 
 class Ensemble:
     def __init__(self, members: list[Member], precision: int = _ffi.DA_PREC_FP64, device: int = 0,
-                 tp: TimeProps | None = None, grid_blocks: int = 0):
+                 tp: TimeProps | None = None, grid_blocks: int = 0, blocks_per_sm: int = 0):
         if not members:
             raise ValueError("empty ensemble")
         self.lib = _ffi.load()
         self.members = members
         self.precision = precision
-        self.params = make_params(members[0].mat, tp or TimeProps(), precision, device, grid_blocks=grid_blocks)
+        self.params = make_params(members[0].mat, tp or TimeProps(), precision, device, grid_blocks=grid_blocks,
+                                  blocks_per_sm=blocks_per_sm)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:
@@ -129,5 +130,32 @@ class Ensemble:
     def autotune(self, nsteps: int = 10) -> dict:
         r = _ffi.da_tune_result()
         self._check(self.lib.da_autotune(self.ctx, nsteps, C.byref(r)), "da_autotune")
-        return {"best": r.grid[r.best], "ms_per_step": {r.grid[k]: r.ms_per_step[k] for k in range(r.n)}}
+        return tune_result(r)
 
+
+
+def shard_members(sizes, world: int, rank: int) -> list[int]:
+    """Members of one rank under a size-balanced greedy partition: largest first, each to the rank
+    with the fewest cells so far (ties to the lower rank).  Every rank computes the same
+    partition; the members of a rank keep their ensemble order."""
+    load = [0] * world
+    owner = [0] * len(sizes)
+    for k in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[k] = r
+        load[r] += sizes[k]
+    return [k for k in range(len(sizes)) if owner[k] == rank]
+
+
+def gather_results(local: dict, world: int) -> dict:
+    """Member index -> result over all ranks (torch.distributed all_gather_object; the only
+    exchange of a sharded ensemble, once per run)."""
+    if world == 1:
+        return dict(local)
+    import torch.distributed as dist
+    parts = [None] * world
+    dist.all_gather_object(parts, local)
+    out = {}
+    for p in parts:
+        out.update(p)
+    return out

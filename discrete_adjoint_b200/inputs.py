@@ -136,7 +136,8 @@ def ensemble_member(spec: MemberSpec, intfrict_deg: float = 30.0):
     """(mesh, MatProps, pile, box) of one ensemble member: a plane of the drawn slope meeting a flat
     runout at mid-domain, a paraboloid pile (height 0.3 R, volume pi/2 H R^2, so R scales with
     volume^(1/3)) a fifth of the way down, a uniform mesh of side^2 cells over 24 R x 24 R, and the
-    functional box over the start of the runout."""
+    functional box from the pile's centre to 6 R downslope (where the flow's front is after a few
+    hundred steps), 4.8 R wide."""
     R = (spec.volume / (0.15 * math.pi)) ** (1.0 / 3.0)
     L = 24.0 * R
     res = L / spec.side
@@ -146,7 +147,7 @@ def ensemble_member(spec: MemberSpec, intfrict_deg: float = 30.0):
     mesh_spec = MeshSpec(xmin=0.0, ymin=0.0, dx0=L / base, dy0=L / base, nx0=base, ny0=base, max_level=4, uniform=True)
     mesh = Mesh.build(mesh_spec, dem, [pile])
     mat = MatProps(intfrict_deg=intfrict_deg, bedfrict_deg=[spec.bedfrict_deg])
-    box = (0.5 * L, 0.7 * L, 0.4 * L, 0.6 * L)
+    box = (0.2 * L, 0.45 * L, 0.4 * L, 0.6 * L)
     return mesh, mat, pile, box
 
 

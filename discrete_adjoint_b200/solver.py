@@ -51,7 +51,7 @@ class TimeProps:
 
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
                 influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                tile_culling: bool = True, grid_blocks: int = 0) -> _ffi.da_params:
+                tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -73,6 +73,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.fp32_sign_floor = fp32_sign_floor
     p.tile_culling = int(tile_culling)
     p.grid_blocks = int(grid_blocks)
+    p.blocks_per_sm = int(blocks_per_sm)
     return p
 
 
@@ -90,13 +91,13 @@ class GeoflowContext:
 
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
                  device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                 tile_culling: bool = True, grid_blocks: int = 0):
+                 tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
         self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling,
-                                  grid_blocks)
+                                  grid_blocks, blocks_per_sm)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:
@@ -181,18 +182,25 @@ class GeoflowContext:
         return out
 
     def autotune(self, nsteps: int = 20) -> dict:
-        """Pick the grid of the tiled kernels by timing nsteps steps per candidate (da_autotune);
-        the state is left where it was.  Returns {"best": grid, "ms_per_step": {grid: ms}}."""
+        """Pick the launch shape of the step kernels by timing nsteps steps per candidate
+        (da_autotune); the state is left where it was.  Returns {"best": (blocks_per_sm, grid),
+        "ms_per_step": {(blocks_per_sm, grid): ms}}."""
         r = _ffi.da_tune_result()
         self._check(self.lib.da_autotune(self.ctx, nsteps, C.byref(r)), "da_autotune")
         self.params.grid_blocks = r.grid[r.best]
-        return {"best": r.grid[r.best], "ms_per_step": {r.grid[k]: r.ms_per_step[k] for k in range(r.n)}}
+        self.params.blocks_per_sm = r.blocks_per_sm[r.best]
+        return tune_result(r)
 
     def profile(self, nsteps: int) -> dict:
         """Mean device ms per forward kernel over nsteps (events around every launch)."""
         out = np.zeros(2)
         self._check(self.lib.da_forward_profile(self.ctx, nsteps, _ffi.dptr(out)), "da_forward_profile")
         return {self.lib.da_forward_kernel_name(k).decode(): float(out[k]) for k in range(2)}
+
+
+def tune_result(r: _ffi.da_tune_result) -> dict:
+    keys = [(r.blocks_per_sm[k], r.grid[k]) for k in range(r.n)]
+    return {"best": keys[r.best], "ms_per_step": {keys[k]: r.ms_per_step[k] for k in range(r.n)}}
 
 
 @dataclass

@@ -91,6 +91,11 @@ typedef struct da_params {
     int32_t grid_blocks;         /* blocks of 256 threads per launch of the tiled step kernels
                                   * (each block walks a strided list of 256-cell tiles); 0 = 4 per
                                   * SM.  Results do not depend on it; da_autotune picks it. */
+    int32_t blocks_per_sm;       /* register budget of the multi-step and reverse-step kernels:
+                                  * compiled for 2 or 3 resident blocks per SM (3: fewer registers,
+                                  * more warps to hide latency; pays on dense meshes and ensembles);
+                                  * 0 = 2.  Results do not depend on it; da_autotune picks it. */
+    int32_t reserved1;
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
@@ -241,16 +246,18 @@ int da_ensemble_get_state(da_ctx *ctx, int32_t member, double *h, double *hu, do
 int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_gradient *out, double *device_ms);
 
 /* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
- * Times nsteps forward steps from the current state for each candidate grid of the tiled
- * kernels (1, 2, 3, 4, 6 and 8 blocks of 256 threads per SM, capped at the tile count), keeps
- * the fastest as da_params.grid_blocks and puts the state, time and iteration back after every
+ * Times nsteps forward steps from the current state for each candidate launch shape of the
+ * step kernels (register budget of 2 or 3 resident blocks per SM; 1, 2 or 3 blocks of 256
+ * threads per SM, capped at the resident count and the tile count), keeps the fastest as
+ * da_params.blocks_per_sm / grid_blocks and puts the state, time and iteration back after every
  * trial.  Results of later steps do not depend on the choice.  out (optional) receives the
  * candidates and their mean ms per step. */
 #define DA_TUNE_MAX 8
 typedef struct da_tune_result {
     int32_t n;                   /* candidates tried */
     int32_t best;                /* index of the one kept */
-    int32_t grid[DA_TUNE_MAX];
+    int32_t grid[DA_TUNE_MAX];   /* da_params.grid_blocks of each candidate */
+    int32_t blocks_per_sm[DA_TUNE_MAX];  /* da_params.blocks_per_sm of each candidate */
     double ms_per_step[DA_TUNE_MAX];
 } da_tune_result;
 int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out);

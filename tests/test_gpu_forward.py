@@ -113,8 +113,8 @@ def test_grid_size_and_autotune_do_not_change_results(precision):
     # and the autotuner puts the state, time and iteration back after its trials
     w = inputs.workload1()
     out = []
-    for grid in (1, 7, 148, 0, 4096):
-        with GeoflowContext(w.mat, TimeProps(), precision=precision, grid_blocks=grid) as ctx:
+    for grid, occ in ((1, 2), (7, 3), (148, 0), (0, 3), (4096, 2)):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision, grid_blocks=grid, blocks_per_sm=occ) as ctx:
             ctx.upload_mesh(w.mesh)
             ctx.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
             s = ctx.run(120)
