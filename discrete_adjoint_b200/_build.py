@@ -32,6 +32,7 @@ UNITS = [
     ("noalloc.cu", ["--fmad=false"]),
     ("snapshot.cu", []),
     ("ensemble.cu", []),
+    ("dwr.cu", []),
     ("mesh_host.cpp", []),
 ]
 

@@ -123,6 +123,8 @@ class da_mesh_spec(C.Structure):
         ("boxes", PD),
         ("random_frac", C.c_double),
         ("seed", C.c_uint64),
+        ("extra_level", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -204,6 +206,8 @@ SIGNATURES = {
     "da_trace_name": (C.c_char_p, [C.c_int32]),
     "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
+    "da_dwr_setup": (C.c_int, [C.c_void_p, C.POINTER(da_mesh_soa), PI32, PI32, PD]),
+    "da_dwr_step": (C.c_int, [C.c_void_p, PD, PD, PD, PD]),
     "da_ensemble_upload": (C.c_int, [C.c_void_p, C.POINTER(da_member), C.c_int32]),
     "da_ensemble_restart": (C.c_int, [C.c_void_p]),
     "da_ensemble_forward": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),

@@ -283,6 +283,8 @@ int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool red
 
 }  // namespace
 
+int adj_alloc_for_dwr(da_ctx *ctx) { return adj_alloc(ctx, 1); }
+
 // The reverse sweep shared by da_adjoint_run and da_ensemble_adjoint: checkpointed forward run
 // over nsteps steps from the current state, reverse steps back to step 0, the state put back,
 // J and the gradient sums launched (single: red_out[n_mat + 1 + n_piles]; ensemble: per member).

@@ -349,7 +349,10 @@ da_ctx *da_create(const da_params *p, int *err) {
 }
 
 void da_destroy(da_ctx *ctx) {
-    if (ctx) free_members(ctx);
+    if (ctx) {
+        free_members(ctx);
+        dwr_release(ctx);
+    }
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
@@ -422,6 +425,7 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     if (st) return st;
     drop_graphs(ctx);
     free_members(ctx);
+    dwr_release(ctx);
     free_mesh(ctx);
     free_state(ctx);
     free_adjoint(ctx);

@@ -82,6 +82,24 @@ struct InstArgs {
     const int32_t *seg0;          // [ninst + 1] first segment of each member
 };
 
+// Dual-weighted-residual indicator: the error grid's own context and the device tables (dwr.cu).
+struct DwrState {
+    da_ctx *fine = nullptr;      // context of the error grid (the mesh refined once)
+    int nf = 0;
+    void *mem = nullptr;         // one allocation for the tables below
+    int32_t *parent = nullptr;   // [nf]
+    int32_t *children = nullptr; // [4][n] fine cells of each coarse cell, -1 unused
+    int32_t *interp = nullptr;   // [4][nf] coarse interpolants, -1 unused
+    double *weight = nullptr;    // [4][nf]
+    double *ut_next = nullptr;   // [3][nf] reconstructed U^{n+1}
+    double *lamt = nullptr;      // [3][nf] reconstructed adjoint
+    double *err = nullptr;       // [nf] el_error
+    double *corr = nullptr;      // [nf] correction
+    double *cell = nullptr;      // [n] el_error summed over each coarse cell's children
+    double *parts = nullptr;     // compensated partial sums
+    double *sums = nullptr;      // [2] total el_error, total correction
+};
+
 // Device copy of the flattened mesh.  FP64 path reads the double arrays; the FP32-split
 // path reads the float copies.
 struct DevMesh {
@@ -152,6 +170,7 @@ struct da_ctx {
     void *inst_mem = nullptr;         // one allocation holding every InstArgs table
     double *inst_vol = nullptr;       // [ninst] members' volumes (stats)
     std::vector<double> inst_init;    // [3][n] members' initial states, concatenated (restart)
+    da::DwrState dwr;                 // error grid of the DWR indicator (da_dwr_setup)
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
     uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
     uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment
@@ -227,6 +246,12 @@ void kact_derivatives(const da_params &p, double *dkb, double *dki);
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
                   long long *fsteps, float *dev_ms);
 int copy_lambda_out(da_ctx *ctx, int buf, double *host);
+// dwr.cu: the indicator of the step U[un] -> U[unext] with adjoint lam[lam] (coarse dt, time and
+// iteration before the step); release of the error grid
+int dwr_indicator(da_ctx *ctx, int un, int unext, int lam, double dt, double time0, long long iter0);
+void dwr_release(da_ctx *ctx);
+// adjoint_host.cu: adjoint buffers and one checkpoint slot
+int adj_alloc_for_dwr(da_ctx *ctx);
 // ensemble.cu: drop the ensemble tables (back to a single-instance layout)
 void free_members(da_ctx *ctx);
 // adjoint_fp64.cu: ensemble members' volumes into out[ninst] (device)

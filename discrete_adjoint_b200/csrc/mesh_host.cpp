@@ -226,16 +226,24 @@ extern "C" int da_mesh_build(const da_mesh_spec *spec, const da_dem *dem, const 
         (n_piles > 0 && !piles) || (spec->n_boxes > 0 && !spec->boxes) || length_scale <= 0 ||
         gravity_scale <= 0)
         return DA_ERR_INVALID;
-    if ((int64_t(std::max(spec->nx0, spec->ny0)) << spec->max_level) >= (int64_t(1) << 29)) return DA_ERR_INVALID;
+    if ((int64_t(std::max(spec->nx0, spec->ny0)) << (spec->max_level + (spec->extra_level ? 1 : 0))) >=
+        (int64_t(1) << 29))
+        return DA_ERR_INVALID;
     if (dem && (dem->nrows < 4 || dem->ncols < 4 || !dem->elev || dem->res <= 0)) return DA_ERR_INVALID;
     *out = nullptr;
     da_mesh_host *m = nullptr;
     try {
         MeshBuild mb(*spec);
         mb.build(piles, n_piles);
+        if (spec->extra_level) {
+            // every leaf once more: 2:1 balance is kept, levels go up to max_level + 1
+            std::vector<uint64_t> all(mb.leaves.begin(), mb.leaves.end());
+            for (uint64_t k : all)
+                mb.refine_leaf({int(k >> 58), int64_t((k >> 29) & 0x1FFFFFFFull), int64_t(k & 0x1FFFFFFFull)});
+        }
 
         // ---- Morton order of the leaves (lower-left corner at the finest level)
-        const int L = spec->max_level;
+        const int L = spec->max_level + (spec->extra_level ? 1 : 0);
         std::vector<std::pair<uint64_t, uint64_t>> order;
         order.reserve(mb.leaves.size());
         for (uint64_t k : mb.leaves) {

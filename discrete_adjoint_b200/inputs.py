@@ -81,6 +81,8 @@ class Workload:
     mat: MatProps
     piles: list
     nsteps: int
+    spec: MeshSpec | None = None  # how the mesh was built (the DWR error grid rebuilds it one level finer)
+    dem: DEM | None = None
 
 
 def workload1(seed: int = 0) -> Workload:
@@ -92,7 +94,7 @@ def workload1(seed: int = 0) -> Workload:
                     refine_margin=60.0, boxes=[(0.0, 2000.0, 100.0, 1900.0)])
     mesh = Mesh.build(spec, dem, piles)
     return Workload("inclined-plane 2km x 2km, 1 pile, adaptive (~40k cells)", mesh,
-                    MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 200)
+                    MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 200, spec, dem)
 
 
 def workload3(cells_per_side: int = 1024, seed: int = 0) -> Workload:
@@ -106,7 +108,7 @@ def workload3(cells_per_side: int = 1024, seed: int = 0) -> Workload:
     spec = MeshSpec(xmin=0.0, ymin=0.0, dx0=L / base, dy0=L / base, nx0=base, ny0=base, max_level=4, uniform=True)
     mesh = Mesh.build(spec, dem, piles)
     return Workload(f"inclined-plane 5km x 5km uniform {cells_per_side}^2, 1 pile", mesh,
-                    MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 512)
+                    MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 512, spec, dem)
 
 
 WORKLOAD3_BOX = (350.0, 850.0, 2250.0, 2750.0)
@@ -177,7 +179,7 @@ def test_case(seed: int = 1, nx0: int = 24, ny0: int = 16, max_level: int = 2, r
                     refine_margin=40.0, random_frac=random_frac, seed=seed)
     mesh = Mesh.build(spec, dem, piles)
     bed = [20.0, 16.0][:n_materials]
-    return Workload(f"test case seed {seed}", mesh, MatProps(intfrict_deg=32.0, bedfrict_deg=bed), piles, 50)
+    return Workload(f"test case seed {seed}", mesh, MatProps(intfrict_deg=32.0, bedfrict_deg=bed), piles, 50, spec, dem)
 
 
 def workload2(seed: int = 2, target_cells: float = 4.0e6, res: float = 5.0) -> Workload:
@@ -204,4 +206,4 @@ def workload2(seed: int = 2, target_cells: float = 4.0e6, res: float = 5.0) -> W
     mesh = Mesh.build(spec, dem, piles)
     bed = [float(b) for b in rng.uniform(15.0, 25.0, size=4)]
     return Workload("hill+noise 20km x 20km, 3 piles, 4 materials, adaptive to 5 m", mesh,
-                    MatProps(intfrict_deg=30.0, bedfrict_deg=bed), piles, 1000)
+                    MatProps(intfrict_deg=30.0, bedfrict_deg=bed), piles, 1000, spec, dem)

@@ -54,6 +54,7 @@ class MeshSpec:
     boxes: list = field(default_factory=list)   # [(xmin, xmax, ymin, ymax), ...]
     random_frac: float = 0.0
     seed: int = 0
+    extra_level: bool = False   # split every leaf once more after balancing (DWR error grid)
 
 
 class Mesh:
@@ -90,7 +91,8 @@ class Mesh:
         boxes = np.ascontiguousarray(np.array(spec.boxes, dtype=np.float64).reshape(-1))
         cs = _ffi.da_mesh_spec(spec.xmin, spec.ymin, spec.dx0, spec.dy0, spec.nx0, spec.ny0, spec.max_level,
                                int(spec.uniform), spec.refine_margin, len(spec.boxes),
-                               _ffi.dptr(boxes) if len(spec.boxes) else None, spec.random_frac, spec.seed)
+                               _ffi.dptr(boxes) if len(spec.boxes) else None, spec.random_frac, spec.seed,
+                               int(spec.extra_level), 0)
         cdem = None
         keep = []
         if dem is not None:

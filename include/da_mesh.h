@@ -52,6 +52,9 @@ typedef struct da_mesh_spec {
     const double *boxes;       /* [4*n_boxes] xmin,xmax,ymin,ymax */
     double random_frac;        /* fraction of cells refined at random (tests: hanging nodes everywhere) */
     uint64_t seed;
+    int32_t extra_level;       /* 1: after balancing, every leaf is split once more (the error grid of
+                                * the dual-weighted-residual estimate, uniform_refine.C:24-130) */
+    int32_t pad;
 } da_mesh_spec;
 
 /* Host-owned mesh.  All arrays have n_cells entries per component. */

@@ -245,6 +245,23 @@ int da_ensemble_get_state(da_ctx *ctx, int32_t member, double *h, double *hu, do
  * device_ms (optional): device time of the whole sweep. */
 int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_gradient *out, double *device_ms);
 
+/* ---- dual-weighted-residual error indicator -------------------------------------------------
+ * The reference's estimate (error_compute.C:24-119, called from dual_solver.C:170 and :230):
+ * the residual of one step on the mesh refined once, r = update(U~^n) - U~^{n+1}, weighted by the
+ * adjoint: el_error = sum_j |r_j (lambda_j - lambda~_j)| and correction = sum_j r_j lambda_j per
+ * refined cell, U~ and lambda~ reconstructed from the coarse cell centres (bilinear_interp.C),
+ * lambda the coarse adjoint of the parent cell.
+ * da_dwr_setup takes the refined grid (every cell of the context's mesh split once, e.g. the
+ * mesh builder's extra_level), each fine cell's parent, and the reconstruction as four
+ * (coarse cell, weight) pairs per fine cell ([4][nf], -1 = unused).
+ * da_dwr_step evaluates the indicator of the step from the context's current state U^n, with
+ * lambda_next = dJ/dU^{n+1} (host [3][n]); the coarse step is taken and undone.  Outputs
+ * (optional): el_error per fine cell [nf], its sum over each coarse cell's children [n], and
+ * sums[2] = total el_error and total correction (compensated FP64 sums in a fixed order). */
+int da_dwr_setup(da_ctx *ctx, const da_mesh_soa *fine, const int32_t *parent, const int32_t *interp,
+                 const double *weight);
+int da_dwr_step(da_ctx *ctx, const double *lambda_next, double *el_error, double *cell_error, double *sums);
+
 /* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
  * Times nsteps forward steps from the current state for each candidate launch shape of the
  * step kernels (register budget of 2 or 3 resident blocks per SM; 1, 2 or 3 blocks of 256
