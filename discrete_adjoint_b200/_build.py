@@ -33,6 +33,7 @@ UNITS = [
     ("snapshot.cu", []),
     ("ensemble.cu", []),
     ("dwr.cu", []),
+    ("stats.cu", []),
     ("mesh_host.cpp", []),
 ]
 

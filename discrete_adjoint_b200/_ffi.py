@@ -165,6 +165,23 @@ class da_gradient(C.Structure):
 DA_FUNC_H2_BOX = 1
 
 
+DA_MAX_PLANES = 16
+
+
+class da_stats_props(C.Structure):
+    _fields_ = [("heightifreach", C.c_double), ("xyifreach", C.c_double * 2), ("hxyminmax", C.c_double),
+                ("min_height", C.c_double), ("vslump", C.c_double), ("n_planes", C.c_int32), ("pad", C.c_int32),
+                ("planes", PD)]
+
+
+class da_stats(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("xcen", "ycen", "xvar", "yvar", "rmean", "area", "vmean", "umean",
+                                          "vxmean", "vymean", "slopemean", "statvolume", "piler", "hmax", "vmax",
+                                          "umax", "vstar")] + \
+               [("xyminmax", C.c_double * 4), ("testpoint_reach", C.c_int32), ("pad", C.c_int32),
+                ("energy", C.c_double)]
+
+
 class da_member(C.Structure):
     _fields_ = [
         ("mesh", da_mesh_soa),
@@ -206,6 +223,7 @@ SIGNATURES = {
     "da_trace_name": (C.c_char_p, [C.c_int32]),
     "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
+    "da_compute_stats": (C.c_int, [C.c_void_p, C.POINTER(da_stats_props), C.c_double, C.POINTER(da_stats), PD]),
     "da_dwr_setup": (C.c_int, [C.c_void_p, C.POINTER(da_mesh_soa), PI32, PI32, PD]),
     "da_dwr_step": (C.c_int, [C.c_void_p, PD, PD, PD, PD]),
     "da_ensemble_upload": (C.c_int, [C.c_void_p, C.POINTER(da_member), C.c_int32]),

@@ -176,6 +176,13 @@ int run_t(da_ctx *ctx, DwrState &d, int un, int unext, int lam, double dt, doubl
     return st;
 }
 
+// The context's scalars in stream order (its stream does not synchronise with the legacy stream).
+int read_scalars(da_ctx *ctx) {
+    int st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
+                        "scalars");
+    return st ? st : cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+}
+
 void free_dwr(da_ctx *ctx) {
     DwrState &d = ctx->dwr;
     if (d.fine) da_destroy(d.fine);
@@ -272,11 +279,11 @@ int da_dwr_step(da_ctx *ctx, const double *lambda_next, double *el_error, double
     for (int v = 0; v < 3 && !st; ++v) st = upload_real(ctx, ctx->lam[0][v], lambda_next + v * n);
     // the coarse step n -> n+1 from a base checkpoint, put back afterwards
     if (!st) st = launch_snapshot(ctx, ctx->snaps[0], true);
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "scalars");
+    if (!st) st = read_scalars(ctx);
     const double time0 = ctx->hsc->time;
     const long long iter0 = ctx->hsc->iter;
     if (!st) st = launch_forward_step(ctx);
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "scalars");
+    if (!st) st = read_scalars(ctx);
     if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "da_dwr_step: device error in the coarse step");
     const double dt = ctx->hsc->dt;
     if (!st) st = dwr_indicator(ctx, 1 - ctx->cur, ctx->cur, 0, dt, time0, iter0);

@@ -261,7 +261,10 @@ int da_ensemble_forward(da_ctx *ctx, int32_t nsteps, double *device_ms) {
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "scalars");
+    // in stream order: the context's stream does not synchronise with the legacy stream
+    if (!st) st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost,
+                                                  ctx->stream), "scalars");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "device error during the ensemble run");
     return st;
 }

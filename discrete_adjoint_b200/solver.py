@@ -181,6 +181,26 @@ class GeoflowContext:
                 out[name] = (ms.value, n.value, s.value) if with_steps else (ms.value, n.value)
         return out
 
+    def stats(self, d_time: float = 0.0, test_point=(0.0, 0.0, 0.0), vslump: float = 0.0, planes=(),
+              discharge=None, hxyminmax: float = -1.0, min_height: float = -1.0) -> dict:
+        """calc_stats of the current state (da_compute_stats).  test_point = (heightifreach, x, y);
+        planes = [(xa, xb, ya, yb), ...]; discharge (float64 array, one per plane) accumulates
+        d_time * flux in place.  Returns the StatProps fields by name."""
+        pr = _ffi.da_stats_props()
+        pr.heightifreach, pr.xyifreach[0], pr.xyifreach[1] = test_point
+        pr.hxyminmax, pr.min_height, pr.vslump = hxyminmax, min_height, vslump
+        pl = np.ascontiguousarray(np.asarray(planes, dtype=np.float64).reshape(-1, 4)) if len(planes) else None
+        pr.n_planes = 0 if pl is None else pl.shape[0]
+        pr.planes = _ffi.dptr(pl) if pl is not None else None
+        if pl is not None and (discharge is None or len(discharge) != pl.shape[0]):
+            raise ValueError("discharge must hold one value per plane")
+        out = _ffi.da_stats()
+        self._check(self.lib.da_compute_stats(self.ctx, C.byref(pr), d_time, C.byref(out),
+                                              _ffi.dptr(discharge) if pl is not None else None), "da_compute_stats")
+        res = {k: getattr(out, k) for k, _ in out._fields_ if k not in ("xyminmax", "pad")}
+        res["xmin"], res["xmax"], res["ymin"], res["ymax"] = list(out.xyminmax)
+        return res
+
     def autotune(self, nsteps: int = 20) -> dict:
         """Pick the launch shape of the step kernels by timing nsteps steps per candidate
         (da_autotune); the state is left where it was.  Returns {"best": (blocks_per_sm, grid),

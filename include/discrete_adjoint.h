@@ -245,6 +245,36 @@ int da_ensemble_get_state(da_ctx *ctx, int32_t member, double *h, double *hu, do
  * device_ms (optional): device time of the whole sweep. */
 int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_gradient *out, double *device_ms);
 
+/* ---- flow statistics and discharge planes ---------------------------------------------------
+ * calc_stats (src/geoflow/stats.C:31-360) of the current state, and DISCHARGE::update
+ * (properties.h:964-1133): discharge[k] += d_time * flux of (hu, hv) through plane k (the reference
+ * calls calc_stats after every step with that step's dt).  Lengths, heights and velocities are in
+ * the mesh's units (the reference's LENGTH/HEIGHT scale factors are 1).  Sums are FP64 in a fixed
+ * order (the reference's hash-table order differs, so they agree to rounding).  slopemean uses the
+ * terrain slope recovered from the gravity vector, -(g_x, g_y)/g_z, where the reference samples the
+ * GIS slope grid. */
+#define DA_MAX_PLANES 16
+typedef struct da_stats_props {
+    double heightifreach;        /* StatProps::heightifreach: depth at the test point that counts as reached */
+    double xyifreach[2];         /* StatProps::xyifreach: the test point */
+    double hxyminmax;            /* StatProps::hxyminmax (< 0: 10 x min_height, datread.C:315-316) */
+    double min_height;           /* MatProps::MAX_NEGLIGIBLE_HEIGHT (< 0: epsilon / 1e4, datread.C:210) */
+    double vslump;               /* MatProps::Vslump (vstar = vmean / vslump; 0 gives vstar = 0) */
+    int32_t n_planes;            /* discharge planes, <= DA_MAX_PLANES */
+    int32_t pad;
+    const double *planes;        /* [n_planes][4]: xa, xb, ya, yb */
+} da_stats_props;
+typedef struct da_stats {
+    double xcen, ycen, xvar, yvar, rmean, area;
+    double vmean, umean, vxmean, vymean, slopemean;
+    double statvolume, piler, hmax, vmax, umax, vstar;
+    double xyminmax[4];          /* xmin, xmax, ymin, ymax of the cells with h >= hxyminmax */
+    int32_t testpoint_reach;     /* the wet cell nearest the test point is at least heightifreach deep */
+    int32_t pad;
+    double energy;               /* sum of (g h^2 + h |v|^2) / 2 dA (stats.C's "adjoint" sum) */
+} da_stats;
+int da_compute_stats(da_ctx *ctx, const da_stats_props *props, double d_time, da_stats *out, double *discharge);
+
 /* ---- dual-weighted-residual error indicator -------------------------------------------------
  * The reference's estimate (error_compute.C:24-119, called from dual_solver.C:170 and :230):
  * the residual of one step on the mesh refined once, r = update(U~^n) - U~^{n+1}, weighted by the

@@ -97,8 +97,12 @@ def reference_available() -> bool:
     return os.path.exists(REF_EXE)
 
 
+STAT_FIELDS = ("xcen", "ycen", "xvar", "yvar", "rmean", "area", "vmean", "umean", "vxmean", "vymean", "slopemean",
+               "statvolume", "piler", "hmax", "vmax", "umax", "vstar", "xmin", "xmax", "ymin", "ymax", "timereached")
+
+
 def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf"), ref_static: bool = False,
-                  workdir: str | None = None) -> dict:
+                  workdir: str | None = None, test_point=(0.0, 0.0, 0.0), vslump: float = 1.0, planes=()) -> dict:
     """Runs the reference's own compiled step() (oracle/_ref/ref_harness) nsteps times.
 
     mat: MatProps (degrees, as in frict.data).  Returns dt history, time, final state, and the
@@ -127,6 +131,11 @@ def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf
             for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature,
                       h, hu, hv):
                 f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+            # calc_stats inputs: test point (height, x, y), Vslump, discharge planes (xa, xb, ya, yb)
+            f.write(np.array(list(test_point) + [vslump], dtype="<f8").tobytes())
+            f.write(struct.pack("<i", len(planes)))
+            for pl in planes:
+                f.write(np.array(pl, dtype="<f8").tobytes())
         r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
@@ -154,4 +163,6 @@ def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf
     out["flux"] = take(12 * n).reshape(4, 3, n)
     out["gravity"] = take(3 * n).reshape(3, n)
     out["d_gravity"] = take(2 * n).reshape(2, n)
+    out["stats"] = dict(zip(STAT_FIELDS, take(len(STAT_FIELDS))))
+    out["discharge"] = take(len(planes))
     return out

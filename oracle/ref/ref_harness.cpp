@@ -116,6 +116,14 @@ int main(int argc, char **argv) {
     rd(f, zeta.data(), zeta.size()); rd(f, grav.data(), grav.size()); rd(f, dgrav.data(), dgrav.size());
     rd(f, curv.data(), curv.size());
     rd(f, h.data(), n); rd(f, hu.data(), n); rd(f, hv.data(), n);
+    // statistics inputs (StatProps, properties.h:180-200; DISCHARGE planes): test point height and
+    // position, Vslump, then the discharge planes (xa, xb, ya, yb each)
+    double stat_in[4];
+    rd(f, stat_in, 4);
+    int32_t n_planes = 0;
+    rd(f, &n_planes, 1);
+    std::vector<double> plane_in(4 * (size_t)n_planes);
+    if (n_planes > 0) rd(f, plane_in.data(), plane_in.size());
     std::fclose(f);
 
     // ---- MatProps (properties.h:527-640): material ids are 1-based in the reference
@@ -132,12 +140,22 @@ int main(int argc, char **argv) {
     matprops.LENGTH_SCALE = 1.0;
     matprops.HEIGHT_SCALE = sc[1];
     matprops.gamma = sc[3];
+    matprops.MAX_NEGLIGIBLE_HEIGHT = matprops.HEIGHT_SCALE / 10000.0;  // datread.C:210
+    matprops.Vslump = stat_in[3];
     TimeProps timeprops;
     timeprops.inittime(1 << 30, sc[4], HUGE_VAL, HUGE_VAL, 1.0);
     PileProps pileprops;
     FluxProps fluxprops;
     StatProps statprops;
+    statprops.hxyminmax = matprops.MAX_NEGLIGIBLE_HEIGHT * 10.0;  // datread.C:315-316
+    statprops.heightifreach = stat_in[0];
+    statprops.xyifreach[0] = stat_in[1];
+    statprops.xyifreach[1] = stat_in[2];
+    statprops.timereached = -1.0;
     DISCHARGE discharge;
+    std::vector<double *> plane_rows(n_planes);
+    for (int k = 0; k < n_planes; ++k) plane_rows[k] = &plane_in[4 * (size_t)k];
+    if (n_planes > 0) discharge.init(n_planes, plane_rows.data());
     OutLine outline;
 
     // ---- nodes at integer positions (units of half the finest cell)
@@ -309,6 +327,15 @@ int main(int argc, char **argv) {
         for (int c = 0; c < n; ++c) buf[c] = els[c]->d_gravity[k];
         wr(o, buf.data(), n);
     }
+    // calc_stats of the last step (StatProps) and the discharge through each plane
+    const double st_out[22] = {statprops.xcen,     statprops.ycen,    statprops.xvar,       statprops.yvar,
+                               statprops.rmean,    statprops.area,    statprops.vmean,      statprops.umean,
+                               statprops.vxmean,   statprops.vymean,  statprops.slopemean,  statprops.statvolume,
+                               statprops.piler,    statprops.hmax,    statprops.vmax,       statprops.umax,
+                               statprops.vstar,    statprops.xyminmax[0], statprops.xyminmax[1],
+                               statprops.xyminmax[2], statprops.xyminmax[3], statprops.timereached};
+    wr(o, st_out, 22);
+    for (int k = 0; k < n_planes; ++k) wr(o, &discharge.planes[k][9], 1);
     std::fclose(o);
     return 0;
 }

@@ -11,7 +11,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def fixtures():
-    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+    return sorted(glob.glob(os.path.join(GOLDEN, "fwd_*.npz")))
 
 
 def load(path):
@@ -20,3 +20,11 @@ def load(path):
     ref = {k[4:]: z[k] for k in z.files if k.startswith("ref_")}
     mat = MatProps(intfrict_deg=float(z["intfrict_deg"]), bedfrict_deg=[float(b) for b in z["bedfrict_deg"]])
     return mesh, mat, int(z["nsteps"]), ref
+
+
+def load_stats(path):
+    """(mesh, mat, nsteps, npz) of a stats_* fixture."""
+    z = np.load(path)
+    mesh = Mesh(**{k[5:]: z[k] for k in z.files if k.startswith("mesh_")})
+    mat = MatProps(intfrict_deg=float(z["intfrict_deg"]), bedfrict_deg=[float(b) for b in z["bedfrict_deg"]])
+    return mesh, mat, int(z["nsteps"]), z

@@ -84,3 +84,21 @@ def test_oracle_matches_live_reference_time_clipping():
     rc, dts, st = o.run(h, hu, hv, 40)
     assert np.array_equal(dts, ref["dt"]) and st.time == ref["time"] == 1.7
     assert np.array_equal(h, ref["h"])
+
+
+def test_stats_fixture_matches_a_live_reference_run():
+    # the committed calc_stats / DISCHARGE fixture still matches the reference when it can be run
+    import numpy as np
+    import pytest
+
+    import oracle
+    from golden_util import GOLDEN, load_stats
+    if not oracle.reference_available():
+        pytest.skip("reference harness not built")
+    import os
+    mesh, mat, nsteps, z = load_stats(os.path.join(GOLDEN, "stats_s12_80.npz"))
+    r = oracle.run_reference(mesh, mat, mesh.h0, mesh.hu0, mesh.hv0, nsteps, test_point=tuple(z["test_point"]),
+                             vslump=float(z["vslump"]), planes=[tuple(p) for p in z["planes"]])
+    assert np.array_equal(r["h"], z["ref_h"])
+    assert np.array_equal(np.array([r["stats"][k] for k in oracle.STAT_FIELDS]), z["stat_values"])
+    assert np.array_equal(r["discharge"], z["discharge"])
