@@ -224,6 +224,9 @@ SIGNATURES = {
     "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
     "da_compute_stats": (C.c_int, [C.c_void_p, C.POINTER(da_stats_props), C.c_double, C.POINTER(da_stats), PD]),
+    "da_outline_init": (C.c_int, [C.c_void_p, PD, PD, PD]),
+    "da_outline_update": (C.c_int, [C.c_void_p]),
+    "da_outline_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), PD]),
     "da_dwr_setup": (C.c_int, [C.c_void_p, C.POINTER(da_mesh_soa), PI32, PI32, PD]),
     "da_dwr_step": (C.c_int, [C.c_void_p, PD, PD, PD, PD]),
     "da_ensemble_upload": (C.c_int, [C.c_void_p, C.POINTER(da_member), C.c_int32]),

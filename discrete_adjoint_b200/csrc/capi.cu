@@ -352,6 +352,8 @@ void da_destroy(da_ctx *ctx) {
     if (ctx) {
         free_members(ctx);
         dwr_release(ctx);
+        if (ctx->outline.map) cudaFree(ctx->outline.map);
+        ctx->outline = OutlineGrid{};
     }
     if (!ctx) return;
     cudaSetDevice(ctx->device);

@@ -82,6 +82,13 @@ struct InstArgs {
     const int32_t *seg0;          // [ninst + 1] first segment of each member
 };
 
+// Maximum-depth map (OutLine, properties.h:653-790): depth bit patterns on a regular grid.
+struct OutlineGrid {
+    int nx = 0, ny = 0;
+    double x0 = 0, y0 = 0, dx = 0, dy = 0;
+    unsigned long long *map = nullptr;  // [ny][nx]
+};
+
 // Dual-weighted-residual indicator: the error grid's own context and the device tables (dwr.cu).
 struct DwrState {
     da_ctx *fine = nullptr;      // context of the error grid (the mesh refined once)
@@ -171,6 +178,7 @@ struct da_ctx {
     double *inst_vol = nullptr;       // [ninst] members' volumes (stats)
     std::vector<double> inst_init;    // [3][n] members' initial states, concatenated (restart)
     da::DwrState dwr;                 // error grid of the DWR indicator (da_dwr_setup)
+    da::OutlineGrid outline;          // maximum-depth map (da_outline_init)
     int *tile_epoch = nullptr;       // [ntiles] id of the last recording step that listed the tile
     uint8_t *seg_act = nullptr;      // [nseg] the segment had an active cell in that step
     uint8_t *lam_clean = nullptr;    // [nseg] both adjoint buffers hold the same segment

@@ -258,12 +258,97 @@ int stats_t(da_ctx *ctx, const StatArgs &a, double vslump, double d_time, double
     return cuda_check(ctx, cudaGetLastError(), "stats launch");
 }
 
+// OutLine::update (properties.h:726-790) for every cell: the maximum depth so far over the grid
+// cells its footprint covers (bit patterns of non-negative doubles order like the values, so an
+// integer atomicMax is exact).
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_outline(MeshArgs m, StateRef<R> U, OutlineGrid g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+        const double height = double(U.h[i]);
+        if (!(height > 0.0)) continue;  // the map starts at zero
+        const double x = m.x[i], y = m.y[i], dx = m.dx ? m.dx[i] : double(m.fdx[i]), dy = m.dy ? m.dy[i] : double(m.fdy[i]);
+        const double xstart = x - 0.5 * dx, xstop = x + 0.5 * dx, ystart = y - 0.5 * dy, ystop = y + 0.5 * dy;
+        int ixstart = (int)((xstart - g.x0) / g.dx + 0.5), ixstop = (int)((xstop - g.x0) / g.dx + 0.5);
+        int iystart = (int)((ystart - g.y0) / g.dy + 0.5), iystop = (int)((ystop - g.y0) / g.dy + 0.5);
+        if (ixstart < 0) ixstart = 0;
+        if (ixstop == ixstart) {
+            ixstart = (int)((xstart - g.x0) / g.dx);
+            ixstop = ixstart + 1;
+        }
+        if (ixstop > g.nx) ixstop = g.nx;
+        if (iystart < 0) iystart = 0;
+        if (iystop == iystart) {
+            iystart = (int)((ystart - g.y0) / g.dy);
+            iystop = iystart + 1;
+        }
+        if (iystop > g.ny) iystop = g.ny;
+        const unsigned long long hb = __double_as_longlong(height);
+        for (int iy = iystart; iy < iystop; ++iy)
+            for (int ix = ixstart; ix < ixstop; ++ix)
+                if (ix >= 0 && iy >= 0) atomicMax(g.map + (size_t)iy * g.nx + ix, hb);
+    }
+}
+
 }  // namespace
 }  // namespace da
 
 using namespace da;
 
 extern "C" {
+
+int da_outline_init(da_ctx *ctx, const double dxy[2], const double xrange[2], const double yrange[2]) {
+    if (!ctx || !dxy || !xrange || !yrange || !(dxy[0] > 0) || !(dxy[1] > 0) || !(xrange[1] > xrange[0]) ||
+        !(yrange[1] > yrange[0]))
+        return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    OutlineGrid &g = ctx->outline;
+    if (g.map) cudaFree(g.map);
+    g = OutlineGrid{};
+    // OutLine::init2 (properties.h:702-724)
+    g.dx = dxy[0];
+    g.dy = dxy[1];
+    g.x0 = xrange[0];
+    g.y0 = yrange[0];
+    g.nx = (int)((xrange[1] - xrange[0]) / g.dx + 0.5);
+    g.ny = (int)((yrange[1] - yrange[0]) / g.dy + 0.5);
+    if (g.nx <= 0 || g.ny <= 0 || (long long)g.nx * g.ny > (1ll << 28))
+        return set_error(ctx, DA_ERR_INVALID, "da_outline_init: grid size");
+    int st = cuda_check(ctx, cudaMalloc((void **)&g.map, sizeof(unsigned long long) * (size_t)g.nx * g.ny), "cudaMalloc");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(g.map, 0, sizeof(unsigned long long) * (size_t)g.nx * g.ny, ctx->stream),
+                             "memset");
+    return st;
+}
+
+int da_outline_update(da_ctx *ctx) {
+    if (!ctx) return DA_ERR_INVALID;
+    if (!ctx->outline.map) return set_error(ctx, DA_ERR_INVALID, "da_outline_update: no grid (da_outline_init)");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_outline_update: no state");
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_outline_update: ensemble context");
+    cudaSetDevice(ctx->device);
+    const MeshArgs m = mesh_args(ctx);
+    const int c = ctx->cur, grid = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
+    if (ctx->p.precision == DA_PREC_FP64) {
+        StateRef<double> U{(const double *)ctx->U[c][0], (const double *)ctx->U[c][1], (const double *)ctx->U[c][2]};
+        k_outline<double><<<grid, kBlock, 0, ctx->stream>>>(m, U, ctx->outline);
+    } else {
+        StateRef<float> U{(const float *)ctx->U[c][0], (const float *)ctx->U[c][1], (const float *)ctx->U[c][2]};
+        k_outline<float><<<grid, kBlock, 0, ctx->stream>>>(m, U, ctx->outline);
+    }
+    return cuda_check(ctx, cudaGetLastError(), "outline launch");
+}
+
+int da_outline_read(da_ctx *ctx, int32_t *nx, int32_t *ny, double *map) {
+    if (!ctx) return DA_ERR_INVALID;
+    const OutlineGrid &g = ctx->outline;
+    if (!g.map) return set_error(ctx, DA_ERR_INVALID, "da_outline_read: no grid (da_outline_init)");
+    if (nx) *nx = g.nx;
+    if (ny) *ny = g.ny;
+    if (!map) return DA_OK;
+    cudaSetDevice(ctx->device);
+    int st = cuda_check(ctx, cudaMemcpyAsync(map, g.map, sizeof(double) * (size_t)g.nx * g.ny, cudaMemcpyDeviceToHost,
+                                             ctx->stream), "copy");
+    return st ? st : cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+}
 
 int da_compute_stats(da_ctx *ctx, const da_stats_props *props, double d_time, da_stats *out, double *discharge) {
     if (!ctx || !props || !out || props->n_planes < 0 || props->n_planes > DA_MAX_PLANES ||

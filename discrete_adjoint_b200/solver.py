@@ -201,6 +201,21 @@ class GeoflowContext:
         res["xmin"], res["xmax"], res["ymin"], res["ymax"] = list(out.xyminmax)
         return res
 
+    def outline_init(self, dxy, xrange, yrange):
+        """Maximum-depth map on a regular grid (OutLine::init2)."""
+        a, b, c = (np.ascontiguousarray(v, dtype=np.float64) for v in (dxy, xrange, yrange))
+        self._check(self.lib.da_outline_init(self.ctx, _ffi.dptr(a), _ffi.dptr(b), _ffi.dptr(c)), "da_outline_init")
+
+    def outline_update(self):
+        self._check(self.lib.da_outline_update(self.ctx), "da_outline_update")
+
+    def outline(self) -> np.ndarray:
+        nx, ny = C.c_int32(), C.c_int32()
+        self._check(self.lib.da_outline_read(self.ctx, C.byref(nx), C.byref(ny), None), "da_outline_read")
+        out = np.empty((ny.value, nx.value))
+        self._check(self.lib.da_outline_read(self.ctx, C.byref(nx), C.byref(ny), _ffi.dptr(out)), "da_outline_read")
+        return out
+
     def autotune(self, nsteps: int = 20) -> dict:
         """Pick the launch shape of the step kernels by timing nsteps steps per candidate
         (da_autotune); the state is left where it was.  Returns {"best": (blocks_per_sm, grid),

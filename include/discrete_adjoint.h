@@ -274,6 +274,14 @@ typedef struct da_stats {
     double energy;               /* sum of (g h^2 + h |v|^2) / 2 dA (stats.C's "adjoint" sum) */
 } da_stats;
 int da_compute_stats(da_ctx *ctx, const da_stats_props *props, double d_time, da_stats *out, double *discharge);
+/* Maximum-depth map (OutLine, properties.h:653-790, updated per step at step.C:216-220 under
+ * MAX_DEPTH_MAP): a regular grid of cell size dxy over xrange x yrange (OutLine::init2);
+ * da_outline_update raises every grid cell covered by a mesh cell to that cell's depth if deeper
+ * (call it after each step); da_outline_read gives the grid size and, if map is not NULL, the
+ * map [ny][nx]. */
+int da_outline_init(da_ctx *ctx, const double dxy[2], const double xrange[2], const double yrange[2]);
+int da_outline_update(da_ctx *ctx);
+int da_outline_read(da_ctx *ctx, int32_t *nx, int32_t *ny, double *map);
 
 /* ---- dual-weighted-residual error indicator -------------------------------------------------
  * The reference's estimate (error_compute.C:24-119, called from dual_solver.C:170 and :230):

@@ -163,3 +163,43 @@ def test_errors_are_codes_not_exits():
         ctx.run(3)
     assert e.value.code in (_ffi.DA_ERR_NAN,)
     ctx.close()
+
+
+def outline_host(m, h, g, x0, y0, dx, dy, nx, ny):
+    """OutLine::update (properties.h:726-790) of every cell, numpy loops (reference order)."""
+    for i in range(m.n):
+        xs, xe = m.x[i] - 0.5 * m.dx[i], m.x[i] + 0.5 * m.dx[i]
+        ys, ye = m.y[i] - 0.5 * m.dy[i], m.y[i] + 0.5 * m.dy[i]
+        ix0, ix1 = int((xs - x0) / dx + 0.5), int((xe - x0) / dx + 0.5)
+        iy0, iy1 = int((ys - y0) / dy + 0.5), int((ye - y0) / dy + 0.5)
+        ix0 = max(ix0, 0)
+        if ix1 == ix0:
+            ix0 = int((xs - x0) / dx)
+            ix1 = ix0 + 1
+        ix1 = min(ix1, nx)
+        iy0 = max(iy0, 0)
+        if iy1 == iy0:
+            iy0 = int((ys - y0) / dy)
+            iy1 = iy0 + 1
+        iy1 = min(iy1, ny)
+        blk = g[iy0:iy1, ix0:ix1]
+        np.maximum(blk, h[i], out=blk)
+
+
+def test_max_depth_map_matches_host_restatement():
+    w = inputs.test_case(seed=3)
+    m = w.mesh
+    x0, y0 = 0.0, 0.0
+    xr, yr = (x0, m.x.max() + 20.0), (y0, m.y.max() + 20.0)
+    dxy = (15.0, 12.5)  # not aligned with the cells, so footprints cut grid cells
+    nx, ny = int((xr[1] - xr[0]) / dxy[0] + 0.5), int((yr[1] - yr[0]) / dxy[1] + 0.5)
+    g = np.zeros((ny, nx))
+    with gpu_ctx(w) as ctx:
+        ctx.outline_init(dxy, xr, yr)
+        for _ in range(12):
+            ctx.step()
+            ctx.outline_update()
+            outline_host(m, ctx.get_state()[0], g, x0, y0, dxy[0], dxy[1], nx, ny)
+        dev = ctx.outline()
+    assert dev.shape == (ny, nx)
+    assert np.array_equal(dev, g) and g.max() > 0
