@@ -224,6 +224,7 @@ SIGNATURES = {
     "da_trace_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "da_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_tune_result)]),
     "da_compute_stats": (C.c_int, [C.c_void_p, C.POINTER(da_stats_props), C.c_double, C.POINTER(da_stats), PD]),
+    "da_refine_info": (C.c_int, [C.c_void_p, PD, C.POINTER(C.c_uint8), PD]),
     "da_outline_init": (C.c_int, [C.c_void_p, PD, PD, PD]),
     "da_outline_update": (C.c_int, [C.c_void_p]),
     "da_outline_read": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), PD]),

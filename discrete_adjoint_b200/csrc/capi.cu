@@ -709,3 +709,31 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     return st;
 }
 
+namespace da {
+int launch_refine_info_fp64(da_ctx *, double *, uint8_t *, double *, double *);
+int launch_refine_info_fp32(da_ctx *, double *, uint8_t *, double *, double *);
+}  // namespace da
+
+extern "C" int da_refine_info(da_ctx *ctx, double *el_error, uint8_t *flags, double *geo_target) {
+    if (!ctx) return DA_ERR_INVALID;
+    if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_refine_info: no mesh");
+    if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_refine_info: no state");
+    if (ctx->ninst > 0) return set_error(ctx, DA_ERR_INVALID, "da_refine_info: ensemble context");
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->mesh.n;
+    unsigned char *mem = nullptr;
+    const size_t o_flags = 8 * n, o_parts = (o_flags + n + 255) & ~size_t(255), o_t = o_parts + 8 * 2 * 256;
+    int st = cuda_check(ctx, cudaMalloc((void **)&mem, o_t + 8), "cudaMalloc(refine)");
+    if (!st) st = ctx->p.precision == DA_PREC_FP64
+                      ? launch_refine_info_fp64(ctx, (double *)mem, mem + o_flags, (double *)(mem + o_parts), (double *)(mem + o_t))
+                      : launch_refine_info_fp32(ctx, (double *)mem, mem + o_flags, (double *)(mem + o_parts), (double *)(mem + o_t));
+    if (!st && el_error)
+        st = cuda_check(ctx, cudaMemcpyAsync(el_error, mem, 8 * n, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    if (!st && flags) st = cuda_check(ctx, cudaMemcpyAsync(flags, mem + o_flags, n, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    if (!st && geo_target)
+        st = cuda_check(ctx, cudaMemcpyAsync(geo_target, mem + o_t, 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (mem) cudaFree(mem);
+    return st;
+}
+

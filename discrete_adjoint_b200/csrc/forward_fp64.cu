@@ -9,6 +9,9 @@ int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<double>(ctx, record_mask);
 }
 int launch_forward_steps_fp64(da_ctx *ctx, int nsteps) { return fwd::launch_steps_t<double>(ctx, nsteps); }
+int launch_refine_info_fp64(da_ctx *ctx, double *e, uint8_t *f, double *parts, double *t) {
+    return fwd::refine_info_t<double>(ctx, e, f, parts, t);
+}
 
 int launch_volume(da_ctx *ctx) { return fwd::launch_volume_t(ctx); }
 

@@ -196,15 +196,14 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
     }
 }
 
-// Full corrector update of one active cell (fluxes + sources), reference order.
+// The flux differences F(+side) - F(-side) of one cell in x (div[0]) and y (div[1]): the edge
+// fluxes calc_edge_states leaves on the cell's edge nodes (element2.C:2745-3072, hanging sides
+// averaged on the coarse side), an outflow direction exactly 0 (boundary_flux, :3374-3411).
 template <class R>
-__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *kact,
-                                            const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
-                                            R st[3]) {
-    const uint8_t bf = m.bflag[i];
+__device__ __forceinline__ void flux_div(const MeshArgs &m, const StateRef<R> &U, const R *kact, int i, uint8_t bf,
+                                         const R prev[3], R div[2][3]) {
     const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
     const R gz = grav<R>(m, 2, i);
-    R div[2][3];
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
         if (bf & ((1 << d) | (1 << (d + 2)))) {
@@ -220,6 +219,18 @@ __device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R>
 #pragma unroll
         for (int v = 0; v < 3; ++v) div[d][v] = Fp[v] - Fm[v];
     }
+}
+
+// Full corrector update of one active cell (fluxes + sources), reference order.
+template <class R>
+__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *kact,
+                                            const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
+                                            R st[3]) {
+    const uint8_t bf = m.bflag[i];
+    const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
+    const R gz = grav<R>(m, 2, i);
+    R div[2][3];
+    flux_div<R>(m, U, kact, i, bf, prev, div);
     R dtdx, dtdy;
     if constexpr (sizeof(R) == 8) {
         dtdx = dt / dxc;
@@ -616,6 +627,103 @@ inline int launch_volume_t(da_ctx *ctx) {
     k_volume_parts<<<kVolParts, kBlock, 0, ctx->stream>>>(ctx->seg_vol, ctx->nseg, ctx->vol_parts);
     k_volume_final<<<1, kVolParts, 0, ctx->stream>>>(ctx->vol_parts, ctx->dsc);
     return cuda_check(ctx, cudaGetLastError(), "volume launch");
+}
+
+// ------------------------------------------------------------------------- refinement hand-back
+// After a step: per cell the flux-balance weight el_error[0] = 2 (sum_j |dF_x,j| + |dF_y,j|)^2 /
+// (dx + dy) + WEIGHT_ADJUSTER (Element::calc_flux_balance, element2.C:3705-3745) from the step's
+// edge fluxes (recomputed from the previous state buffer and the step's k act/pass), and the
+// pile-contour tests of H_adapt (Element::if_pile_boundary, element2.C:4020-4065, at GEOFLOW_TINY
+// x 1, 5, 15, 40, hadpt.C:46-48,139-149) on the new state: flag bits 0-3.  Bit 4 (weight above the
+// mean) is set by the second kernel once the mean is known.  Per-block partial sums of the weight
+// over cells with hu > GEOFLOW_TINY (element_weight.C:36-79) in a fixed order.
+__device__ __forceinline__ int pile_boundary(const MeshArgs &m, const double *hnew_d, const float *hnew_f, int i,
+                                             double contour) {
+    auto hv = [&](int k) { return hnew_d ? hnew_d[k] : double(hnew_f[k]); };
+    const uint8_t bf = m.bflag[i];
+    const bool in = hv(i) >= contour;
+    for (int s = 0; s < 4; ++s) {
+        if (bf & (1 << s)) continue;  // outside the map
+        const int ne = (bf & (0x10 << s)) ? 2 : 1;  // a duplicate second slot is skipped
+        for (int q = 0; q < ne; ++q) {
+            const double hk = hv(m.nbr[(size_t)(s + 4 * q) * m.n + i]);
+            if (in && hk < contour) return 2;
+            if (!in && hk >= contour) return 1;
+        }
+    }
+    return 0;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_refine_info(MeshArgs m, StateRef<R> Uprev, StateRef<R> Unew,
+                                                        const R *kact, double *el_error, uint8_t *flags,
+                                                        double *parts) {
+    __shared__ double s_sum[kBlock], s_cnt[kBlock];
+    const int per = (m.n + kVolParts - 1) / kVolParts;
+    const int i0 = blockIdx.x * per, i1 = min(m.n, i0 + per);
+    double sum = 0.0, cnt = 0.0;
+    const double *hd = sizeof(R) == 8 ? (const double *)Unew.h : nullptr;
+    const float *hf = sizeof(R) == 8 ? nullptr : (const float *)Unew.h;
+    for (int i = i0 + threadIdx.x; i < i1; i += kBlock) {
+        const R prev[3] = {Uprev.h[i], Uprev.hu[i], Uprev.hv[i]};
+        R div[2][3];
+        flux_div<R>(m, Uprev, kact, i, m.bflag[i], prev, div);
+        double f = 0.0;
+        for (int v = 0; v < 3; ++v) f += fabs(double(div[0][v])) + fabs(double(div[1][v]));
+        const double dxc = double(cell_dx<R>(m, i)), dyc = double(cell_dy<R>(m, i));
+        const double e = 2. * f * f / (dxc + dyc) + 1.0;  // WEIGHT_ADJUSTER (geoflow.h:22)
+        el_error[i] = e;
+        uint8_t fl = 0;
+        const double contours[4] = {DA_TINY, 5 * DA_TINY, 15 * DA_TINY, 40 * DA_TINY};
+        for (int c = 0; c < 4; ++c)
+            if (pile_boundary(m, hd, hf, i, contours[c]) > 0) fl |= uint8_t(1u << c);
+        flags[i] = fl;
+        if (double(Unew.hu[i]) > DA_TINY) {
+            sum += e;
+            cnt += 1.0;
+        }
+    }
+    s_sum[threadIdx.x] = sum;
+    s_cnt[threadIdx.x] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int t = 0; t < kBlock; ++t) {
+            a += s_sum[t];
+            b += s_cnt[t];
+        }
+        parts[2 * blockIdx.x] = a;
+        parts[2 * blockIdx.x + 1] = b;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_refine_flag(int n, const double *el_error, uint8_t *flags,
+                                                        const double *parts, double *target) {
+    __shared__ double t;
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < kVolParts; ++k) {
+            a += parts[2 * k];
+            b += parts[2 * k + 1];
+        }
+        t = b > 0.0 ? a / b : 1.0;  // element_weight.C:72-76
+        if (blockIdx.x == 0) *target = t;
+    }
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (el_error[i] > t) flags[i] |= uint8_t(16);
+}
+
+template <class R>
+int refine_info_t(da_ctx *ctx, double *el_error, uint8_t *flags, double *parts, double *target) {
+    const MeshArgs m = mesh_args(ctx);
+    const int c = ctx->cur, p = 1 - c;
+    StateRef<R> Un{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
+    StateRef<R> Up{(const R *)ctx->U[p][0], (const R *)ctx->U[p][1], (const R *)ctx->U[p][2]};
+    k_refine_info<R><<<kVolParts, kBlock, 0, ctx->stream>>>(m, Up, Un, (const R *)ctx->kact, el_error, flags, parts);
+    k_refine_flag<<<(ctx->sm_count > 0 ? ctx->sm_count : 148) * 4, kBlock, 0, ctx->stream>>>(m.n, el_error, flags,
+                                                                                            parts, target);
+    return cuda_check(ctx, cudaGetLastError(), "refine info launch");
 }
 
 }  // namespace

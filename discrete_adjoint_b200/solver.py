@@ -201,6 +201,15 @@ class GeoflowContext:
         res["xmin"], res["xmax"], res["ymin"], res["ymax"] = list(out.xyminmax)
         return res
 
+    def refine_info(self):
+        """(flux-balance weight per cell, refinement flags per cell, geo_target) after a step
+        (da_refine_info)."""
+        n = self.mesh.n
+        e, f, t = np.empty(n), np.empty(n, dtype=np.uint8), C.c_double()
+        self._check(self.lib.da_refine_info(self.ctx, _ffi.dptr(e), f.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                            C.byref(t)), "da_refine_info")
+        return e, f, t.value
+
     def outline_init(self, dxy, xrange, yrange):
         """Maximum-depth map on a regular grid (OutLine::init2)."""
         a, b, c = (np.ascontiguousarray(v, dtype=np.float64) for v in (dxy, xrange, yrange))

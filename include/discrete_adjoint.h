@@ -283,6 +283,21 @@ int da_outline_init(da_ctx *ctx, const double dxy[2], const double xrange[2], co
 int da_outline_update(da_ctx *ctx);
 int da_outline_read(da_ctx *ctx, int32_t *nx, int32_t *ny, double *map);
 
+/* ---- adaptation hand-back ---------------------------------------------------------------------
+ * After a forward step, what H_adapt reads to pick the cells to refine (hadpt.C:112-151), so the
+ * host's adapt needs no state download: per cell the flux-balance weight (el_error[0] of
+ * Element::calc_flux_balance, element2.C:3705-3745, from the step's edge fluxes) and flags:
+ * bits 0-3 the pile-contour tests Element::if_pile_boundary (element2.C:4020-4065) at GEOFLOW_TINY
+ * times 1, 5, 15 and 40 (hadpt.C:46-48) on the new state; bit 4 weight above geo_target, the mean
+ * weight of the cells with hu > GEOFLOW_TINY (element_weight.C:36-79; 1 when there is none).  The
+ * generation limit and the flux-source test stay with the host.  Outputs may be NULL. */
+#define DA_REFINE_CONTOUR_1 1
+#define DA_REFINE_CONTOUR_5 2
+#define DA_REFINE_CONTOUR_15 4
+#define DA_REFINE_CONTOUR_40 8
+#define DA_REFINE_WEIGHT 16
+int da_refine_info(da_ctx *ctx, double *el_error, uint8_t *flags, double *geo_target);
+
 /* ---- dual-weighted-residual error indicator -------------------------------------------------
  * The reference's estimate (error_compute.C:24-119, called from dual_solver.C:170 and :230):
  * the residual of one step on the mesh refined once, r = update(U~^n) - U~^{n+1}, weighted by the

@@ -56,3 +56,38 @@ def test_stats_and_discharge_match_the_reference():
         assert abs(st[k] - v) <= tol, (k, st[k], v)
     np.testing.assert_allclose(discharge, z["discharge"], rtol=1e-10)
     assert st["statvolume"] > 0 and st["area"] > 0
+
+
+@pytest.mark.parametrize("path", fixtures(), ids=os.path.basename)
+def test_refine_info_matches_the_reference_edge_fluxes(path):
+    # el_error[0] of calc_flux_balance from the reference's own edge-node fluxes of the last step,
+    # the pile-contour flags from its final depths, geo_target as element_weight forms it
+    mesh, mat, nsteps, ref = load(path)
+    with GeoflowContext(mat, TimeProps()) as c:
+        c.upload_mesh(mesh)
+        c.set_state(mesh.h0, mesh.hu0, mesh.hv0)
+        c.run(nsteps)
+        e, flags, target = c.refine_info()
+        hu = c.get_state()[1]
+    F = ref["flux"]  # [side +x, +y, -x, -y][var][cell]
+    f = np.zeros(mesh.n)
+    for v in range(3):
+        f = f + (np.abs(F[0, v] - F[2, v]) + np.abs(F[1, v] - F[3, v]))
+    e_ref = 2.0 * f * f / (mesh.dx + mesh.dy) + 1.0
+    assert np.array_equal(e, e_ref)
+    h = ref["h"]
+    for bit, c in enumerate((1e-4, 5e-4, 15e-4, 40e-4)):
+        exp = np.zeros(mesh.n, dtype=bool)
+        for s in range(4):
+            for q in (0, 4):
+                k = mesh.nbr[s + q]
+                ok = k >= 0
+                if q == 4:
+                    ok &= mesh.nbr[s + 4] != mesh.nbr[s]
+                kk = np.where(ok, k, 0)
+                exp |= ok & (((h >= c) & (h[kk] < c)) | ((h < c) & (h[kk] >= c)))
+        assert np.array_equal((flags >> bit) & 1 == 1, exp), bit
+    sel = hu > 1e-4
+    t_ref = e_ref[sel].mean() if sel.any() else 1.0
+    assert abs(target - t_ref) <= 1e-12 * t_ref
+    assert np.array_equal((flags >> 4) & 1 == 1, e > target)
