@@ -7,8 +7,9 @@ int launch_adjoint_step_fp64(da_ctx *ctx, int a, int b, const double *sec2, doub
     return adj::step_t<double>(ctx, a, b, sec2, c);
 }
 int launch_adjoint_reduce_fp64(da_ctx *ctx, int a, int np) { return adj::reduce_t<double>(ctx, a, np); }
-int launch_youturn_fp64(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box) {
-    return adj::youturn_t<double>(ctx, a, b, sec2, c, seed, box);
+int launch_youturn_fp64(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box,
+                        void *pre) {
+    return adj::youturn_t<double>(ctx, a, b, sec2, c, seed, box, pre);
 }
 int launch_functional_fp64(da_ctx *ctx, double *out) { return adj::functional_t<double>(ctx, out); }
 // the volume of every ensemble member from the segments' volume parts (fixed order)

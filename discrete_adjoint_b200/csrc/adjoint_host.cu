@@ -27,11 +27,12 @@ int launch_functional_fp64(da_ctx *, double *);
 int launch_functional_fp32(da_ctx *, double *);
 int forward_state_changed(da_ctx *ctx);
 
-int launch_youturn_fp64(da_ctx *, int, int, const double *, double, bool, const double *);
-int launch_youturn_fp32(da_ctx *, int, int, const double *, double, bool, const double *);
-int launch_youturn(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box) {
-    return ctx->p.precision == DA_PREC_FP64 ? launch_youturn_fp64(ctx, a, b, sec2, c, seed, box)
-                                            : launch_youturn_fp32(ctx, a, b, sec2, c, seed, box);
+int launch_youturn_fp64(da_ctx *, int, int, const double *, double, bool, const double *, void *);
+int launch_youturn_fp32(da_ctx *, int, int, const double *, double, bool, const double *, void *);
+int launch_youturn(da_ctx *ctx, int a, int b, const double *sec2, double c, bool seed, const double *box,
+                   void *pre_slot) {
+    return ctx->p.precision == DA_PREC_FP64 ? launch_youturn_fp64(ctx, a, b, sec2, c, seed, box, pre_slot)
+                                            : launch_youturn_fp32(ctx, a, b, sec2, c, seed, box, pre_slot);
 }
 int launch_functional(da_ctx *ctx, double *out) {
     return ctx->p.precision == DA_PREC_FP64 ? launch_functional_fp64(ctx, out) : launch_functional_fp32(ctx, out);
@@ -123,7 +124,8 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
 }
 
 // One launch each (csrc/snapshot.cu): the state, the tile wet flags and the step scalars; a
-// restore fills both state buffers so that tile culling stays valid.
+// restore fills both state buffers so that tile culling stays valid.  Inside the reverse sweep the
+// same copies run as phases of the cooperative step kernels instead (Runner below).
 int store(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], true); }
 int restore(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], false); }
 
@@ -172,24 +174,35 @@ struct Runner {
     double cos_int;
     long long fsteps = 0;
     int pos = -1;  // step index of the live forward state; -1 = not a checkpointed state
+    int pending = -1;  // checkpoint slot the next launch restores first; -1 = none
 
-    // the live state is already the checkpoint right after a store: no copy back
+    // The live state is already the checkpoint right after a store: no copy back.  Otherwise the
+    // restore becomes the first phase of the next step launch (no launch of its own).
     int restore_at(int slot, int step) {
         if (pos == step) return DA_OK;
         pos = step;
-        return restore(ctx, slot);
+        pending = slot;
+        return DA_OK;
     }
-    int advance(int k) {
-        const int st = launch_forward_steps(ctx, k);
+    void *take_pending() {
+        void *p = pending >= 0 ? ctx->snaps[pending] : nullptr;
+        pending = -1;
+        return p;
+    }
+    // k forward steps; store_slot >= 0: the state after them is stored, in the same launch
+    int advance(int k, int store_slot = -1) {
+        if (k == 0) return DA_OK;  // a pending restore waits for the next launch
+        const int st = launch_forward_steps(ctx, k, take_pending(), store_slot >= 0 ? ctx->snaps[store_slot] : nullptr);
         fsteps += k;
         pos += k;
         return st;
     }
+    // every reverse(a, b) ends with a youturn, which takes any restore still pending
     int youturn() {
         ++fsteps;
         pos = -1;  // past the step that is being taken back
         // the first reverse step (the horizon's last step) also seeds lambda^N from U^N
-        const int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box);
+        const int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box, take_pending());
         seeded = true;
         lam_cur = 1 - lam_cur;
         return st;
@@ -211,12 +224,11 @@ struct Runner {
             }
             return st;
         }
-        const int m = a + sch.S(l, c);
+        const int m = a + sch.S(l, c);  // a < m < b
         st = restore_at(slot_a, a);
-        if (!st) st = advance(m - a);
         const int slot_m = free_slots.back();
         free_slots.pop_back();
-        if (!st) st = store(ctx, slot_m);
+        if (!st) st = advance(m - a, slot_m);
         if (!st) st = reverse(m, b, slot_m);
         free_slots.push_back(slot_m);
         if (!st) st = reverse(a, m, slot_a);
@@ -240,8 +252,7 @@ int upload_tables(da_ctx *ctx, double *sec2, double *cos_int) {
         sec2[m] = 1.0 + t * t;
     }
     *cos_int = std::cos(ctx->p.intfrict);
-    int st = cuda_check(ctx, cudaMemcpy(ctx->dk_tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice),
-                        "upload tables");
+    int st = copy_h2d(ctx, ctx->dk_tab, tab.data(), sizeof(double) * tab.size(), "upload tables");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->gbed, 0, sizeof(double) * ctx->mesh.n, ctx->stream), "memset");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->gint, 0, sizeof(double) * ctx->mesh.n, ctx->stream), "memset");
     return st;
@@ -340,7 +351,7 @@ int da_set_dt_replay(da_ctx *ctx, const double *dts, int32_t n, int64_t iter0) {
     ctx->tc.n_replay = 0;
     if (!dts || st) return st;
     st = cuda_check(ctx, cudaMalloc((void **)&ctx->dt_replay, sizeof(double) * n), "cudaMalloc(dt replay)");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->dt_replay, dts, sizeof(double) * n, cudaMemcpyHostToDevice), "copy dts");
+    if (!st) st = copy_h2d(ctx, ctx->dt_replay, dts, sizeof(double) * n, "copy dts");
     if (st) return st;
     ctx->tc.dt_replay = ctx->dt_replay;
     ctx->tc.iter0 = iter0;
@@ -396,8 +407,7 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
         ctx->dh0 = nullptr;
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * n * n_piles), "cudaMalloc(dh0)");
         if (!st)
-            st = cuda_check(ctx, cudaMemcpy(ctx->dh0, dh0_dpile, sizeof(double) * n * n_piles, cudaMemcpyHostToDevice),
-                            "copy dh0");
+            st = copy_h2d(ctx, ctx->dh0, dh0_dpile, sizeof(double) * n * n_piles, "copy dh0");
     }
     int lam0 = 0;
     long long fsteps = 0;

@@ -81,17 +81,24 @@ int reduce_inst_t(da_ctx *ctx, int lam0) {
 // SEED (the last step of the horizon): lambda^N is seeded from the U^N just produced before the
 // adjoint phases, with each segment's part of J.  BATCH: every member with its own constants and
 // dt (the members' dt pass between two barriers).  Block 0 writes the step's scalars at the end,
-// as the separate kernels do.
+// as the separate kernels do.  pre (mode NONE when unused): a checkpoint restore before the step,
+// followed by a barrier.
 template <class R, bool BATCH, bool SEED, int OCC>
 __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
                                                     uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
                                                     uint8_t *seg_dirty, int ntiles, int cull, MatConsts mc,
                                                     TimeConsts tc, DevScalars *sc, uint8_t *mask, int *tile_epoch,
                                                     uint8_t *seg_act, int rec_id, StateRef<R> Ln, StateOut<R> Lseed,
-                                                    StateOut<R> Lo, AdjArgs aa, InstArgs ia, Box box, double *seg_J) {
+                                                    StateOut<R> Lo, AdjArgs aa, InstArgs ia, Box box, double *seg_J,
+                                                    snap::SnapArgs<R> pre) {
     __shared__ int list[kBlock];
-    const double time = sc->time;
-    const long long iter = sc->iter;
+    if (pre.mode != snap::NONE) {
+        snap::snap_segments<R>(pre);
+        snap::snap_scalars<R>(pre);
+        if (!fwd::grid_sync(sc)) return;
+    }
+    const double time = __ldcg(&sc->time);
+    const long long iter = __ldcg(&sc->iter);
     const StateRef<R> U{S.h[cur], S.hu[cur], S.hv[cur]};
     const StateOut<R> O{S.h[cur ^ 1], S.hu[cur ^ 1], S.hv[cur ^ 1]};
     unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
@@ -135,9 +142,11 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
 
 // The live state is U^n in buffer cur; afterwards U^{n+1} is (cur flips) and lambda^n is in
 // lam_out.  seed: lambda^N goes into lam_in first (from U^{n+1} = U^N) with J's segment parts.
+// pre_slot (or null): a checkpoint slot restored first, in the same launch (the live state is then
+// the restored one).
 template <class R>
 int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int, bool seed,
-              const double *box4) {
+              const double *box4, void *pre_slot) {
     const int pi = sizeof(R) == 8;
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
@@ -189,9 +198,10 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
         int st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
         if (st) return st;
     }
+    snap::SnapArgs<R> pre = pre_slot ? snap::snap_args<R>(ctx, pre_slot, false, cur) : snap::no_snap<R>();
     void *args[] = {&m,    &S,   &cur,        &kact,    &active, &seg_clean, &seg_wet, &seg_vol, &seg_dirty,
                     &ntiles, &cull, &mc,      &tc,      &sc,     &mask,      &tile_epoch, &seg_act, &rec_id,
-                    &Ln,   &Ls,  &Lo,         &aa,      &ia,     &box,       &seg_J};
+                    &Ln,   &Ls,  &Lo,         &aa,      &ia,     &box,       &seg_J,   &pre};
     trace_begin(ctx, TR_YOUTURN);
     const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx);

@@ -224,6 +224,16 @@ int upload_real(da_ctx *ctx, void *dev, const double *host) {
     return st ? st : cuda_check(ctx, cudaGetLastError(), "narrow");
 }
 
+int copy_h2d(da_ctx *ctx, void *dev, const void *host, size_t bytes, const char *what) {
+    return cuda_check(ctx, cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream), what);
+}
+
+int copy_d2h(da_ctx *ctx, void *host, const void *dev, size_t bytes, const char *what) {
+    int st = cuda_check(ctx, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream), what);
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), what);
+    return st;
+}
+
 int download_real(da_ctx *ctx, double *host, const void *dev) {
     const int n = ctx->mesh.n;
     if (ctx->p.precision == DA_PREC_FP64)
@@ -338,7 +348,7 @@ da_ctx *da_create(const da_params *p, int *err) {
         std::memcpy(&ctx->hsc->acc_min_dxe, &init, sizeof(init));
         std::memcpy(&ctx->hsc->acc_alt_min_dxe, &init, sizeof(init));
     }
-    st = cuda_check(ctx, cudaMemcpy(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice), "init scalars");
+    st = copy_h2d(ctx, ctx->dsc, ctx->hsc, sizeof(DevScalars), "init scalars");
     if (st) {
         *err = st;
         da_destroy(ctx);
@@ -390,12 +400,12 @@ int da_set_time(da_ctx *ctx, double time, int64_t iter) {
     cudaSetDevice(ctx->device);
     int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (st) return st;
-    st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "read scalars");
+    st = copy_d2h(ctx, ctx->hsc, ctx->dsc, sizeof(DevScalars), "read scalars");
     if (st) return st;
     ctx->hsc->time = time;
     ctx->hsc->iter = iter;
     ctx->hsc->err = 0;
-    return cuda_check(ctx, cudaMemcpy(ctx->dsc, ctx->hsc, sizeof(DevScalars), cudaMemcpyHostToDevice), "write scalars");
+    return copy_h2d(ctx, ctx->dsc, ctx->hsc, sizeof(DevScalars), "write scalars");
 }
 
 int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
@@ -634,8 +644,7 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     // ensemble: the members' times too (their accumulators are at rest between steps)
     std::vector<double> saved_time(ctx->ninst);
     if (ctx->ninst > 0)
-        st = cuda_check(ctx, cudaMemcpy(saved_time.data(), ctx->ia.time, sizeof(double) * ctx->ninst,
-                                        cudaMemcpyDeviceToHost), "save times");
+        st = copy_d2h(ctx, saved_time.data(), ctx->ia.time, sizeof(double) * ctx->ninst, "save times");
     void *saved[3] = {nullptr, nullptr, nullptr};
     for (int v = 0; v < 3 && !st; ++v) {
         st = cuda_check(ctx, cudaMalloc(&saved[v], rs * n), "cudaMalloc(autotune)");

@@ -221,6 +221,13 @@ void trace_begin(da_ctx *ctx, int kind);
 void trace_end(da_ctx *ctx, int steps = 1);
 int trace_flush(da_ctx *ctx);
 int cuda_check(da_ctx *ctx, cudaError_t e, const char *what);
+// Host <-> device copies ordered on the context's stream.  That stream is non-blocking, so a
+// plain cudaMemcpy (legacy stream) would not wait for the kernels queued on it, and a pageable
+// host-to-device cudaMemcpy may return before its data reach the device.  copy_h2d returns once
+// the host buffer may be reused (the copy runs before any later work on the stream); copy_d2h
+// returns once the data are on the host.
+int copy_h2d(da_ctx *ctx, void *dev, const void *host, size_t bytes, const char *what);
+int copy_d2h(da_ctx *ctx, void *host, const void *dev, size_t bytes, const char *what);
 void fill_consts(const da_params &p, MatConsts *mc, TimeConsts *tc);
 
 // forward_fp64.cu / forward_fp32.cu
@@ -231,9 +238,11 @@ int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask);
 // the volume (sum dx dy h) of the current state into the device scalars
 int launch_volume(da_ctx *ctx);
 // nsteps whole steps in one cooperative launch (k_steps); same results as nsteps single steps
-int launch_forward_steps(da_ctx *ctx, int nsteps);
-int launch_forward_steps_fp64(da_ctx *ctx, int nsteps);
-int launch_forward_steps_fp32(da_ctx *ctx, int nsteps);
+// nsteps steps in one cooperative launch; pre_slot / post_slot (checkpoint slots, or null): a
+// restore before the first step and a store after the last one inside the same launch.
+int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot = nullptr, void *post_slot = nullptr);
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot);
+int launch_forward_steps_fp32(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot);
 int forward_alloc(da_ctx *ctx);
 // capi.cu: one FP64 host array to / from a device array of the context's precision (stream-ordered;
 // an FP32 download must finish before the next one reuses the staging buffer)
@@ -244,7 +253,6 @@ void update_grid(da_ctx *ctx);
 // adjoint_fp64.cu / adjoint_fp32.cu
 int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
 // replayed forward step + adjoint step in one cooperative launch (k_youturn)
-int launch_youturn(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
 int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
 int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
 int forward_state_changed(da_ctx *ctx);

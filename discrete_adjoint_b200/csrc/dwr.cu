@@ -261,10 +261,10 @@ int da_dwr_setup(da_ctx *ctx, const da_mesh_soa *fine, const int32_t *parent, co
     d.parts = (double *)(b + o_parts);
     d.sums = (double *)(b + o_sums);
     d.nf = nf;
-    st = cuda_check(ctx, cudaMemcpy(d.parent, parent, 4 * (size_t)nf, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(d.children, children.data(), 4 * (size_t)4 * n, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(d.interp, interp, 4 * (size_t)4 * nf, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(d.weight, weight, 8 * (size_t)4 * nf, cudaMemcpyHostToDevice), "copy");
+    st = copy_h2d(ctx, d.parent, parent, 4 * (size_t)nf, "copy");
+    if (!st) st = copy_h2d(ctx, d.children, children.data(), 4 * (size_t)4 * n, "copy");
+    if (!st) st = copy_h2d(ctx, d.interp, interp, 4 * (size_t)4 * nf, "copy");
+    if (!st) st = copy_h2d(ctx, d.weight, weight, 8 * (size_t)4 * nf, "copy");
     if (st) free_dwr(ctx);
     return st;
 }
@@ -290,9 +290,9 @@ int da_dwr_step(da_ctx *ctx, const double *lambda_next, double *el_error, double
     if (!st) st = launch_snapshot(ctx, ctx->snaps[0], false);
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     const int nf = ctx->dwr.nf;
-    if (!st && el_error) st = cuda_check(ctx, cudaMemcpy(el_error, ctx->dwr.err, 8 * (size_t)nf, cudaMemcpyDeviceToHost), "copy");
-    if (!st && cell_error) st = cuda_check(ctx, cudaMemcpy(cell_error, ctx->dwr.cell, 8 * n, cudaMemcpyDeviceToHost), "copy");
-    if (!st && sums) st = cuda_check(ctx, cudaMemcpy(sums, ctx->dwr.sums, 16, cudaMemcpyDeviceToHost), "copy");
+    if (!st && el_error) st = copy_d2h(ctx, el_error, ctx->dwr.err, 8 * (size_t)nf, "copy");
+    if (!st && cell_error) st = copy_d2h(ctx, cell_error, ctx->dwr.cell, 8 * n, "copy");
+    if (!st && sums) st = copy_d2h(ctx, sums, ctx->dwr.sums, 16, "copy");
     return st;
 }
 

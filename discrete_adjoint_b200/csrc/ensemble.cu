@@ -63,15 +63,13 @@ int upload_member_scalars(da_ctx *ctx) {
     std::vector<double> time(nm);
     std::vector<unsigned long long> amin(nm), amax(nm);
     reset_member_scalars(time, amin, amax);
-    int st = cuda_check(ctx, cudaMemcpy(ctx->ia.time, time.data(), sizeof(double) * nm, cudaMemcpyHostToDevice), "copy");
+    int st = copy_h2d(ctx, ctx->ia.time, time.data(), sizeof(double) * nm, "copy");
     // dt, min_dxe, hmax of a member that has not stepped yet: zero
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->ia.dt, time.data(), sizeof(double) * nm, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->ia.min_dxe, time.data(), sizeof(double) * nm, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->ia.hmax, time.data(), sizeof(double) * nm, cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->ia.acc_min, amin.data(), sizeof(unsigned long long) * nm,
-                                             cudaMemcpyHostToDevice), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->ia.acc_max, amax.data(), sizeof(unsigned long long) * nm,
-                                             cudaMemcpyHostToDevice), "copy");
+    if (!st) st = copy_h2d(ctx, ctx->ia.dt, time.data(), sizeof(double) * nm, "copy");
+    if (!st) st = copy_h2d(ctx, ctx->ia.min_dxe, time.data(), sizeof(double) * nm, "copy");
+    if (!st) st = copy_h2d(ctx, ctx->ia.hmax, time.data(), sizeof(double) * nm, "copy");
+    if (!st) st = copy_h2d(ctx, ctx->ia.acc_min, amin.data(), sizeof(unsigned long long) * nm, "copy");
+    if (!st) st = copy_h2d(ctx, ctx->ia.acc_max, amax.data(), sizeof(unsigned long long) * nm, "copy");
     return st;
 }
 
@@ -192,7 +190,7 @@ int da_ensemble_upload(da_ctx *ctx, const da_member *members, int32_t n_members)
         seg0[k] = cell0[k] / 32;
     }
     seg0[nm] = cell0[nm] / 32;
-    st = cuda_check(ctx, cudaMemcpy(ctx->inst_mem, host.data(), off, cudaMemcpyHostToDevice), "copy member tables");
+    st = copy_h2d(ctx, ctx->inst_mem, host.data(), off, "copy member tables");
     unsigned char *b = (unsigned char *)ctx->inst_mem;
     InstArgs &ia = ctx->ia;
     ia.ninst = nm;
@@ -220,7 +218,7 @@ int da_ensemble_upload(da_ctx *ctx, const da_member *members, int32_t n_members)
     if (!st) st = upload_member_scalars(ctx);
     if (!st && any_pile) {
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * N), "cudaMalloc(dh0)");
-        if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->dh0, dh0.data(), sizeof(double) * N, cudaMemcpyHostToDevice), "copy dh0");
+        if (!st) st = copy_h2d(ctx, ctx->dh0, dh0.data(), sizeof(double) * N, "copy dh0");
     }
     if (!st) st = da_ensemble_restart(ctx);
     if (st) free_members(ctx);
@@ -277,11 +275,11 @@ int da_ensemble_stats(da_ctx *ctx, da_step_stats *out) {
     std::vector<double> dt(nm), time(nm), vol(nm), hmax(nm);
     int st = launch_member_volume(ctx, ctx->inst_vol);
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(dt.data(), ctx->ia.dt, sizeof(double) * nm, cudaMemcpyDeviceToHost), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(time.data(), ctx->ia.time, sizeof(double) * nm, cudaMemcpyDeviceToHost), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(vol.data(), ctx->inst_vol, sizeof(double) * nm, cudaMemcpyDeviceToHost), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(hmax.data(), ctx->ia.hmax, sizeof(double) * nm, cudaMemcpyDeviceToHost), "copy");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost), "scalars");
+    if (!st) st = copy_d2h(ctx, dt.data(), ctx->ia.dt, sizeof(double) * nm, "copy");
+    if (!st) st = copy_d2h(ctx, time.data(), ctx->ia.time, sizeof(double) * nm, "copy");
+    if (!st) st = copy_d2h(ctx, vol.data(), ctx->inst_vol, sizeof(double) * nm, "copy");
+    if (!st) st = copy_d2h(ctx, hmax.data(), ctx->ia.hmax, sizeof(double) * nm, "copy");
+    if (!st) st = copy_d2h(ctx, ctx->hsc, ctx->dsc, sizeof(DevScalars), "scalars");
     if (st) return st;
     for (int k = 0; k < nm; ++k) out[k] = da_step_stats{dt[k], time[k], vol[k], hmax[k], ctx->hsc->iter};
     return DA_OK;
@@ -316,9 +314,8 @@ int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_grad
     float ms = 0.f;
     int st = adjoint_sweep(ctx, nullptr, nsteps, nsnapshots, 1, &lam0, &fsteps, &ms);
     std::vector<double> red((size_t)nm * nout), J(nm);
-    if (!st) st = cuda_check(ctx, cudaMemcpy(red.data(), ctx->red_out, sizeof(double) * red.size(), cudaMemcpyDeviceToHost),
-                             "read gradients");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(J.data(), ctx->inst_J, sizeof(double) * nm, cudaMemcpyDeviceToHost), "read J");
+    if (!st) st = copy_d2h(ctx, red.data(), ctx->red_out, sizeof(double) * red.size(), "read gradients");
+    if (!st) st = copy_d2h(ctx, J.data(), ctx->inst_J, sizeof(double) * nm, "read J");
     if (st) return st;
     for (int k = 0; k < nm; ++k) {
         da_gradient &g = out[k];

@@ -8,7 +8,9 @@ namespace da {
 int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<double>(ctx, record_mask);
 }
-int launch_forward_steps_fp64(da_ctx *ctx, int nsteps) { return fwd::launch_steps_t<double>(ctx, nsteps); }
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre, void *post) {
+    return fwd::launch_steps_t<double>(ctx, nsteps, pre, post);
+}
 int launch_refine_info_fp64(da_ctx *ctx, double *e, uint8_t *f, double *parts, double *t) {
     return fwd::refine_info_t<double>(ctx, e, f, parts, t);
 }
@@ -61,9 +63,9 @@ int forward_state_changed(da_ctx *ctx) {
     return st;
 }
 
-int launch_forward_steps(da_ctx *ctx, int nsteps) {
-    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps);
-    return launch_forward_steps_fp32(ctx, nsteps);
+int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
+    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps, pre_slot, post_slot);
+    return launch_forward_steps_fp32(ctx, nsteps, pre_slot, post_slot);
 }
 
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include "fv_device.cuh"
+#include "snapshot_impl.cuh"
 
 namespace da {
 namespace fwd {
@@ -489,11 +490,19 @@ template <class R, bool BATCH = false, int OCC = 2>
 __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
-                                                  MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia) {
+                                                  MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia,
+                                                  snap::SnapArgs<R> pre, snap::SnapArgs<R> post) {
     __shared__ int list[kBlock];
-    double time = sc->time;
-    long long iter = sc->iter;
-    double dt = sc->dt, ft = sc->frict_tiny, min_dxe = sc->min_dxe, hmax = sc->hmax;
+    if (pre.mode != snap::NONE) {
+        // a checkpoint restore first (both buffers, flags, scalars), then a barrier
+        snap::snap_segments<R>(pre);
+        snap::snap_scalars<R>(pre);
+        if (!grid_sync(sc)) return;
+    }
+    double time = __ldcg(&sc->time);
+    long long iter = __ldcg(&sc->iter);
+    double dt = __ldcg(&sc->dt), ft = __ldcg(&sc->frict_tiny), min_dxe = __ldcg(&sc->min_dxe),
+           hmax = __ldcg(&sc->hmax);
     for (int s = 0; s < nsteps; ++s) {
         const int c = (cur + s) & 1, p = s & 1;
         unsigned long long *acc_min = p ? &sc->acc_alt_min_dxe : &sc->acc_min_dxe;
@@ -539,6 +548,12 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
             sc->acc_hmax = sc->acc_alt_hmax = 0ull;
         }
     }
+    if (post.mode != snap::NONE) {
+        // a checkpoint store of the state after the last step (every block has passed the last
+        // barrier; block 0's thread 0 has just written the scalars it copies)
+        snap::snap_segments<R>(post);
+        snap::snap_scalars<R>(post);
+    }
 }
 
 template <class R>
@@ -578,8 +593,10 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
 
 // nsteps steps in one cooperative launch of k_steps; the grid is capped at the number of blocks
 // that can be resident at once (the launch fails otherwise, it never deadlocks).
+// pre_slot / post_slot (or null): a checkpoint slot restored before the first step / stored after
+// the last one, in the same launch.
 template <class R>
-int launch_steps_t(da_ctx *ctx, int nsteps) {
+int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
     if (nsteps <= 0) return DA_OK;
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
@@ -612,8 +629,11 @@ int launch_steps_t(da_ctx *ctx, int nsteps) {
     TimeConsts tc = ctx->tc;
     DevScalars *sc = ctx->dsc;
     InstArgs ia = ctx->ia;
-    void *args[] = {&m,        &S,       &cur,       &n,     &kact, &active, &seg_clean, &seg_wet,
-                    &seg_vol,  &seg_dirty, &ntiles,  &cull,  &mc,   &tc,     &sc,     &ia};
+    snap::SnapArgs<R> pre = pre_slot ? snap::snap_args<R>(ctx, pre_slot, false, cur) : snap::no_snap<R>();
+    snap::SnapArgs<R> post =
+        post_slot ? snap::snap_args<R>(ctx, post_slot, true, (cur + nsteps) & 1) : snap::no_snap<R>();
+    void *args[] = {&m,       &S,        &cur,    &n,    &kact, &active, &seg_clean, &seg_wet, &seg_vol,
+                    &seg_dirty, &ntiles, &cull,   &mc,   &tc,   &sc,     &ia,        &pre,     &post};
     trace_begin(ctx, TR_STEPS);
     const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
     trace_end(ctx, nsteps);

@@ -388,15 +388,15 @@ int da_compute_stats(da_ctx *ctx, const da_stats_props *props, double d_time, da
     // the state the statistics read may still be in flight on the context's stream
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
     if (!st && props->n_planes > 0)
-        st = cuda_check(ctx, cudaMemcpy(dis, discharge, sizeof(double) * props->n_planes, cudaMemcpyHostToDevice), "copy");
+        st = copy_h2d(ctx, dis, discharge, sizeof(double) * props->n_planes, "copy");
     if (!st) st = ctx->p.precision == DA_PREC_FP64 ? stats_t<double>(ctx, a, props->vslump, d_time, dev)
                                                    : stats_t<float>(ctx, a, props->vslump, d_time, dev);
     double res[32];
     // the context's stream does not synchronise with the legacy stream of cudaMemcpy
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    if (!st) st = cuda_check(ctx, cudaMemcpy(res, dev + (size_t)kParts * kPartLen, sizeof(res), cudaMemcpyDeviceToHost), "copy");
+    if (!st) st = copy_d2h(ctx, res, dev + (size_t)kParts * kPartLen, sizeof(res), "copy");
     if (!st && props->n_planes > 0)
-        st = cuda_check(ctx, cudaMemcpy(discharge, dis, sizeof(double) * props->n_planes, cudaMemcpyDeviceToHost), "copy");
+        st = copy_d2h(ctx, discharge, dis, sizeof(double) * props->n_planes, "copy");
     if (dev) cudaFree(dev);
     if (st) return st;
     out->xcen = res[0];
