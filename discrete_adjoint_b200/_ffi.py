@@ -57,7 +57,7 @@ class da_params(C.Structure):
         ("tile_culling", C.c_int32),
         ("grid_blocks", C.c_int32),
         ("blocks_per_sm", C.c_int32),
-        ("reserved1", C.c_int32),
+        ("tile_staging", C.c_int32),
     ]
 
 

@@ -309,7 +309,7 @@ __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<
                 const uint8_t code = mi & 3;
                 const R k = kact_of<R>(mc, mat, code);
                 R s[6];
-                cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
+                cell_slopes<R>(global_view<R>(m, U, (const R *)nullptr), i, bf, R(mc.gamma), prev, s);
                 R vel0, vel1, h_inv;
                 if constexpr (sizeof(R) == 8) {
                     vel0 = prev[1] / prev[0];

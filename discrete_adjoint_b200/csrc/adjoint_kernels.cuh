@@ -82,16 +82,19 @@ int reduce_inst_t(da_ctx *ctx, int lam0) {
 // adjoint phases, with each segment's part of J.  BATCH: every member with its own constants and
 // dt (the members' dt pass between two barriers).  Block 0 writes the step's scalars at the end,
 // as the separate kernels do.  pre (mode NONE when unused): a checkpoint restore before the step,
-// followed by a barrier.
-template <class R, bool BATCH, bool SEED, int OCC>
+// followed by a barrier.  STAGED: the replayed forward phases stage tiles and halos in shared
+// memory (staged_impl.cuh).
+template <class R, bool BATCH, bool SEED, int OCC, bool STAGED>
 __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StatePair<R> S, int cur, R *kact, unsigned *active,
                                                     uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
                                                     uint8_t *seg_dirty, int ntiles, int cull, MatConsts mc,
                                                     TimeConsts tc, DevScalars *sc, uint8_t *mask, int *tile_epoch,
                                                     uint8_t *seg_act, int rec_id, StateRef<R> Ln, StateOut<R> Lseed,
                                                     StateOut<R> Lo, AdjArgs aa, InstArgs ia, Box box, double *seg_J,
-                                                    snap::SnapArgs<R> pre) {
+                                                    snap::SnapArgs<R> pre, fwd::HaloArgs ha) {
     __shared__ int list[kBlock];
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    fwd::StageSmem<R> &stg = *reinterpret_cast<fwd::StageSmem<R> *>(dyn_smem);
     if (pre.mode != snap::NONE) {
         snap::snap_segments<R>(pre);
         snap::snap_scalars<R>(pre);
@@ -102,7 +105,12 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     const StateRef<R> U{S.h[cur], S.hu[cur], S.hv[cur]};
     const StateOut<R> O{S.h[cur ^ 1], S.hu[cur ^ 1], S.hv[cur ^ 1]};
     unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-    fwd::coef_phase<R, true, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max, ia);
+    if (STAGED)
+        fwd::coef_phase_staged<R, true, BATCH>(m, ha, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min,
+                                               my_max, ia, stg);
+    else
+        fwd::coef_phase<R, true, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, mask, list, my_min, my_max,
+                                        ia);
     if (!BATCH) fwd::push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (!fwd::grid_sync(sc)) return;
     double dt = 0.0, ft, min_dxe = 0.0, hmax = 0.0;
@@ -116,8 +124,13 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
         fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
     }
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-    fwd::update_phase<R, true, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc,
-                                      sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id, list, ia);
+    if (STAGED)
+        fwd::update_phase_staged<R, true, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
+                                                 ntiles, cull, mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id,
+                                                 list, ia, stg);
+    else
+        fwd::update_phase<R, true, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull,
+                                          mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id, list, ia);
     if (!fwd::grid_sync(sc)) return;
     if (SEED) {
         seed_phase<R, BATCH>(m, StateRef<R>{O.h, O.hu, O.hv}, Lseed, box, seg_J, ntiles * (kBlock / 32), ia);
@@ -140,6 +153,20 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     }
 }
 
+// The k_youturn instantiation for the launch's flags.
+template <class R>
+const void *youturn_kernel(bool batch, bool seed, bool occ3, bool staged) {
+#define DA_YT(B, S, O, G) (const void *)k_youturn<R, B, S, O, G>
+#define DA_YT_OCC(B, S, G) (occ3 ? DA_YT(B, S, 3, G) : DA_YT(B, S, 2, G))
+#define DA_YT_SEED(B, G) (seed ? DA_YT_OCC(B, true, G) : DA_YT_OCC(B, false, G))
+#define DA_YT_BATCH(G) (batch ? DA_YT_SEED(true, G) : DA_YT_SEED(false, G))
+    return staged ? DA_YT_BATCH(true) : DA_YT_BATCH(false);
+#undef DA_YT_BATCH
+#undef DA_YT_SEED
+#undef DA_YT_OCC
+#undef DA_YT
+}
+
 // The live state is U^n in buffer cur; afterwards U^{n+1} is (cur flips) and lambda^n is in
 // lam_out.  seed: lambda^N goes into lam_in first (from U^{n+1} = U^N) with J's segment parts.
 // pre_slot (or null): a checkpoint slot restored first, in the same launch (the live state is then
@@ -150,17 +177,19 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     const int pi = sizeof(R) == 8;
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
-    const void *kern;
-    if (occ3)
-        kern = batch ? (seed ? (const void *)k_youturn<R, true, true, 3> : (const void *)k_youturn<R, true, false, 3>)
-                     : (seed ? (const void *)k_youturn<R, false, true, 3> : (const void *)k_youturn<R, false, false, 3>);
-    else
-        kern = batch ? (seed ? (const void *)k_youturn<R, true, true, 2> : (const void *)k_youturn<R, true, false, 2>)
-                     : (seed ? (const void *)k_youturn<R, false, true, 2> : (const void *)k_youturn<R, false, false, 2>);
-    int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed + 8 * occ3];
+    const bool staged = fwd::staged_ok(ctx);
+    const void *kern = youturn_kernel<R>(batch, seed, occ3, staged);
+    const size_t smem = staged ? fwd::stage_smem_bytes<R>() : 0;
+    int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed + 8 * occ3 + 16 * staged];
     if (cap_ref <= 0) {
+        int st = DA_OK;
+        if (staged)
+            st = cuda_check(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "shared memory attribute");
         int per_sm = 0;
-        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");
+        if (!st)
+            st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem),
+                            "occupancy");
         if (st) return st;
         cap_ref = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
     }
@@ -199,11 +228,12 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
         if (st) return st;
     }
     snap::SnapArgs<R> pre = pre_slot ? snap::snap_args<R>(ctx, pre_slot, false, cur) : snap::no_snap<R>();
-    void *args[] = {&m,    &S,   &cur,        &kact,    &active, &seg_clean, &seg_wet, &seg_vol, &seg_dirty,
-                    &ntiles, &cull, &mc,      &tc,      &sc,     &mask,      &tile_epoch, &seg_act, &rec_id,
-                    &Ln,   &Ls,  &Lo,         &aa,      &ia,     &box,       &seg_J,   &pre};
+    fwd::HaloArgs ha = fwd::halo_args(ctx);
+    void *args[] = {&m,      &S,    &cur, &kact, &active, &seg_clean, &seg_wet,    &seg_vol, &seg_dirty,
+                    &ntiles, &cull, &mc,  &tc,   &sc,     &mask,      &tile_epoch, &seg_act, &rec_id,
+                    &Ln,     &Ls,   &Lo,  &aa,   &ia,     &box,       &seg_J,      &pre,     &ha};
     trace_begin(ctx, TR_YOUTURN);
-    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, smem, ctx->stream);
     trace_end(ctx);
     if (e != cudaSuccess) return cuda_check(ctx, e, "reverse-step launch");
     ctx->cur = cur ^ 1;

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <vector>
 
@@ -107,6 +108,7 @@ static bool params_ok(const da_params *p) {
     if (!(p->epsilon > 0) || !(p->gravity_scale > 0) || !(p->gamma > 0)) return false;
     if (p->grid_blocks < 0 || p->grid_blocks > (1 << 20)) return false;
     if (p->blocks_per_sm != 0 && p->blocks_per_sm != 2 && p->blocks_per_sm != 3) return false;
+    if (p->tile_staging != 0 && p->tile_staging != 1) return false;
     return true;
 }
 
@@ -122,6 +124,8 @@ static void free_mesh(da_ctx *ctx) {
     dfree(d.x); dfree(d.y); dfree(d.dx); dfree(d.dy);
     dfree(d.g); dfree(d.dg); dfree(d.curv);
     dfree(d.fdx); dfree(d.fdy); dfree(d.fg); dfree(d.fdg); dfree(d.fcurv);
+    dfree(d.halo_off); dfree(d.halo_idx); dfree(d.nloc);
+    d.halo_max = 0;
     d.n = 0;
     d.epoch = -1;
 }
@@ -170,6 +174,54 @@ static int upload(da_ctx *ctx, T **dst, const T *src, size_t count) {
     if (st) return st;
     return cuda_check(ctx, cudaMemcpyAsync(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, ctx->stream),
                       "copy mesh");
+}
+
+// Halo tables of the staged step phases.  For tile t (cells 256 t ... 256 t + 255): its halo, the
+// cells outside the tile that its cells name as neighbours (sorted, each once), at
+// idx[off[t] .. off[t+1]); for every cell its eight neighbour entries as tile-local slots in
+// nloc[i][s]: 0..255 a cell of the same tile, 256 + k the tile's k-th halo cell, -1 no neighbour.
+// Built on the host once per mesh; not uploaded when a tile's halo exceeds kHaloMax (the step
+// kernels then read neighbours from global memory).
+static int build_halo(da_ctx *ctx, const int32_t *nbr, int n) {
+    const int nt = (n + kTileCells - 1) / kTileCells;
+    std::vector<int32_t> off((size_t)nt + 1), idx, h;
+    std::vector<int16_t> nloc((size_t)8 * n);
+    idx.reserve((size_t)nt * 96);
+    int hmax = 0;
+    for (int t = 0; t < nt; ++t) {
+        const int a = t * kTileCells, b = std::min(n, a + kTileCells);
+        h.clear();
+        for (int s = 0; s < 8; ++s)
+            for (int i = a; i < b; ++i) {
+                const int e = nbr[(size_t)s * n + i];
+                if (e >= 0 && (e < a || e >= b)) h.push_back(e);
+            }
+        std::sort(h.begin(), h.end());
+        h.erase(std::unique(h.begin(), h.end()), h.end());
+        off[t] = (int32_t)idx.size();
+        idx.insert(idx.end(), h.begin(), h.end());
+        hmax = std::max(hmax, (int)h.size());
+        for (int i = a; i < b; ++i)
+            for (int s = 0; s < 8; ++s) {
+                const int e = nbr[(size_t)s * n + i];
+                int slot = -1;
+                if (e >= a && e < b)
+                    slot = e - a;
+                else if (e >= 0)
+                    slot = kTileCells + int(std::lower_bound(h.begin(), h.end(), e) - h.begin());
+                nloc[(size_t)i * 8 + s] = (int16_t)slot;
+            }
+    }
+    off[nt] = (int32_t)idx.size();
+    DevMesh &d = ctx->mesh;
+    d.halo_max = hmax;
+    if (hmax > kHaloMax) return DA_OK;
+    int st = upload(ctx, &d.halo_off, off.data(), off.size());
+    if (!st) st = upload(ctx, &d.halo_idx, idx.data(), idx.size());
+    if (!st) st = upload(ctx, &d.nloc, nloc.data(), nloc.size());
+    // the host vectors are released on return: the copies must have left them
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    return st;
 }
 
 static int sync_scalars(da_ctx *ctx) {
@@ -303,7 +355,7 @@ void da_params_default(da_params *p) {
     p->tile_culling = 1;
     p->grid_blocks = 0;
     p->blocks_per_sm = 0;
-    p->reserved1 = 0;
+    p->tile_staging = 1;
 }
 
 da_ctx *da_create(const da_params *p, int *err) {
@@ -448,6 +500,7 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     if (!st) st = upload(ctx, &d.nbr, m->nbr, (size_t)8 * n);
     if (!st) st = upload(ctx, &d.bflag, bflag.data(), (size_t)n);
     if (!st) st = upload(ctx, &d.mat, mat.data(), (size_t)n);
+    if (!st) st = build_halo(ctx, m->nbr, n);
     // centres: the FP64 step uses them; both precisions test functional boxes with them
     if (!st) st = upload(ctx, &d.x, m->x, (size_t)n);
     if (!st) st = upload(ctx, &d.y, m->y, (size_t)n);

@@ -13,6 +13,9 @@
 
 namespace da {
 
+constexpr int kTileCells = 256;  // cells per tile (Morton-consecutive): one thread each
+constexpr int kHaloMax = 192;    // halo cells a staged tile holds in shared memory
+
 // Per-material constants formed on the host once per parameter change (host libm, so the
 // device never evaluates a transcendental and the FP64 path matches the CPU bit for bit).
 //   kact_sgn[m][s+1]: gmfggetcoef's K_act/pass for sgn(vel) = s, clamped at 0, times epsilon
@@ -121,6 +124,11 @@ struct DevMesh {
     double *curv = nullptr;         // [2][n]
     float *fdx = nullptr, *fdy = nullptr;
     float *fg = nullptr, *fdg = nullptr, *fcurv = nullptr;
+    // staged step phases (capi.cu build_halo); null when a tile's halo exceeds kHaloMax
+    int32_t *halo_off = nullptr;    // [ntiles + 1]
+    int32_t *halo_idx = nullptr;    // halo cells of every tile, tile after tile
+    int16_t *nloc = nullptr;        // [n][8] tile-local slot of each neighbour entry
+    int32_t halo_max = 0;           // largest halo of a tile
 };
 
 // Tracing: CUDA events around every launch of the step and the adjoint, summed per kernel
@@ -186,8 +194,10 @@ struct da_ctx {
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
     int grid = 0;                    // grid of the tiled step kernels (da_params.grid_blocks)
-    int coop_cap[8] = {};     // resident blocks of k_steps [FP32, FP64] x [single, ensemble] x [2, 3 per SM]
-    int coop_cap_yt[16] = {};  // of k_youturn [FP32, FP64] x [single, ensemble] x [seed] x [2, 3 per SM]
+    // resident blocks of k_steps [FP32, FP64] x [single, ensemble] x [2, 3 per SM] x [staged]
+    int coop_cap[16] = {};
+    // of k_youturn [FP32, FP64] x [single, ensemble] x [seed] x [2, 3 per SM] x [staged]
+    int coop_cap_yt[32] = {};
     int sm_count = 0;
     da::DevScalars *dsc = nullptr;   // device scalars
     da::DevScalars *hsc = nullptr;   // pinned host mirror

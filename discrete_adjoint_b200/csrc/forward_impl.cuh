@@ -150,7 +150,7 @@ __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> 
                     } else {
                         const R ui[3] = {h, U.hu[i], U.hv[i]};
                         R s[6];
-                        cell_slopes<R>(m, U, i, bf, R(mc.gamma), ui, s);
+                        cell_slopes<R>(global_view<R>(m, U, kact), i, bf, R(mc.gamma), ui, s);
                         const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
                         kact[i] = k;
                         const R gz = grav<R>(m, 2, i);
@@ -200,11 +200,10 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
 // The flux differences F(+side) - F(-side) of one cell in x (div[0]) and y (div[1]): the edge
 // fluxes calc_edge_states leaves on the cell's edge nodes (element2.C:2745-3072, hanging sides
 // averaged on the coarse side), an outflow direction exactly 0 (boundary_flux, :3374-3411).
-template <class R>
-__device__ __forceinline__ void flux_div(const MeshArgs &m, const StateRef<R> &U, const R *kact, int i, uint8_t bf,
-                                         const R prev[3], R div[2][3]) {
-    const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
-    const R gz = grav<R>(m, 2, i);
+template <class R, class V>
+__device__ __forceinline__ void flux_div(const V &v, int i, uint8_t bf, const R prev[3], R div[2][3]) {
+    const R ki = prev[0] >= R(DA_TINY) ? v.k(i) : R(0);
+    const R gz = v.gz(i);
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
         if (bf & ((1 << d) | (1 << (d + 2)))) {
@@ -215,23 +214,23 @@ __device__ __forceinline__ void flux_div(const MeshArgs &m, const StateRef<R> &U
         Hfv<R> self;
         dirflux<R>(d, prev[0], prev[1], prev[2], ki, gz, self);
         R Fm[3], Fp[3];
-        side_flux<R>(m, U, kact, i, bf, d + 2, self, Fm);
-        side_flux<R>(m, U, kact, i, bf, d, self, Fp);
+        side_flux<R>(v, i, bf, d + 2, self, Fm);
+        side_flux<R>(v, i, bf, d, self, Fp);
 #pragma unroll
         for (int v = 0; v < 3; ++v) div[d][v] = Fp[v] - Fm[v];
     }
 }
 
-// Full corrector update of one active cell (fluxes + sources), reference order.
-template <class R>
-__device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R> &U, const R *kact,
-                                            const MatConsts &mc, int i, R dt, R ft, const R prev[3], R dxc, R dyc,
+// Full corrector update of one active cell (fluxes + sources), reference order.  c is the cell in
+// the view, gi its global index (the per-cell source coefficients are read from the mesh arrays).
+template <class R, class V>
+__device__ __forceinline__ bool update_cell(const V &v, const MeshArgs &m, int gi, int c, uint8_t bf,
+                                            const MatConsts &mc, R dt, R ft, const R prev[3], R dxc, R dyc,
                                             R st[3]) {
-    const uint8_t bf = m.bflag[i];
-    const R ki = prev[0] >= R(DA_TINY) ? kact[i] : R(0);
-    const R gz = grav<R>(m, 2, i);
+    const R ki = prev[0] >= R(DA_TINY) ? v.k(c) : R(0);
+    const R gz = v.gz(c);
     R div[2][3];
-    flux_div<R>(m, U, kact, i, bf, prev, div);
+    flux_div<R>(v, c, bf, prev, div);
     R dtdx, dtdy;
     if constexpr (sizeof(R) == 8) {
         dtdx = dt / dxc;
@@ -246,7 +245,7 @@ __device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R>
     if (clamped) st[0] = R(0);
     if (prev[0] > R(DA_TINY)) {
         R s[6];
-        cell_slopes<R>(m, U, i, bf, R(mc.gamma), prev, s);
+        cell_slopes<R>(v, c, bf, R(mc.gamma), prev, s);
         R vel0, vel1, h_inv;
         if constexpr (sizeof(R) == 8) {
             vel0 = prev[1] / prev[0];
@@ -264,14 +263,14 @@ __device__ __forceinline__ bool update_cell(const MeshArgs &m, const StateRef<R>
         const R sg1 = tiny_sgn(tmp, ft);
         const R sg3 = tiny_sgn(vel1, ft);
         const R sin_int = R(mc.sin_int);
-        const R tan_bed = R(mc.tan_bed[m.mat[i]]);
-        R s1 = grav<R>(m, 0, i) * prev[0];
-        R s2 = sg0 * prev[0] * ki * (gz * s[3] + dgrav<R>(m, 1, i) * prev[0]) * sin_int;
-        R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * curvat<R>(m, 0, i), R(0.0)) * tan_bed;
+        const R tan_bed = R(mc.tan_bed[m.mat[gi]]);
+        R s1 = grav<R>(m, 0, gi) * prev[0];
+        R s2 = sg0 * prev[0] * ki * (gz * s[3] + dgrav<R>(m, 1, gi) * prev[0]) * sin_int;
+        R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * curvat<R>(m, 0, gi), R(0.0)) * tan_bed;
         st[1] += dt * (s1 - s2 - s3);
-        s1 = grav<R>(m, 1, i) * prev[0];
-        s2 = sg1 * prev[0] * ki * (gz * s[0] + dgrav<R>(m, 0, i) * prev[0]) * sin_int;
-        s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, i), R(0.0)) * tan_bed;
+        s1 = grav<R>(m, 1, gi) * prev[0];
+        s2 = sg1 * prev[0] * ki * (gz * s[0] + dgrav<R>(m, 0, gi) * prev[0]) * sin_int;
+        s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, gi), R(0.0)) * tan_bed;
         st[2] += dt * (s1 - s2 - s3);
     }
     return clamped;
@@ -340,7 +339,9 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
                 R st[3] = {prev[0], prev[1], prev[2]};
                 const bool act = word & (1u << lane);
                 bool clamped = false;
-                if (act) clamped = update_cell<R>(m, U, kact, mc, i, dt, ft, prev, dxc, dyc, st);
+                if (act)
+                    clamped = update_cell<R>(global_view<R>(m, U, kact), m, i, i, m.bflag[i], mc, dt, ft, prev, dxc,
+                                             dyc, st);
                 if (RECORD)
                     mask[i] = uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0));
                 if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
@@ -409,6 +410,16 @@ __global__ void __launch_bounds__(kVolParts) k_volume_final(const double *__rest
         sc->volume = t;
     }
 }
+
+}  // namespace
+}  // namespace fwd
+}  // namespace da
+
+#include "staged_impl.cuh"
+
+namespace da {
+namespace fwd {
+namespace {
 
 // ---------------------------------------------------------------------------- k_steps
 // nsteps whole steps in one cooperative launch (all blocks resident): per step the coefficient
@@ -485,14 +496,17 @@ __device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter,
 
 // BATCH: every member of the ensemble steps with its own dt (a third barrier per step after the
 // members' dt pass); the shared iteration count lives in the scalars.  OCC: resident blocks per
-// SM the register budget is set for (da_params.blocks_per_sm).
-template <class R, bool BATCH = false, int OCC = 2>
+// SM the register budget is set for (da_params.blocks_per_sm).  STAGED: the phases stage each
+// tile and its halo in dynamic shared memory (staged_impl.cuh).
+template <class R, bool BATCH = false, int OCC = 2, bool STAGED = false>
 __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
                                                   MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia,
-                                                  snap::SnapArgs<R> pre, snap::SnapArgs<R> post) {
+                                                  snap::SnapArgs<R> pre, snap::SnapArgs<R> post, HaloArgs ha) {
     __shared__ int list[kBlock];
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    StageSmem<R> &stg = *reinterpret_cast<StageSmem<R> *>(dyn_smem);
     if (pre.mode != snap::NONE) {
         // a checkpoint restore first (both buffers, flags, scalars), then a barrier
         snap::snap_segments<R>(pre);
@@ -510,8 +524,12 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
         const StateRef<R> U{S.h[c], S.hu[c], S.hv[c]};
         const StateOut<R> O{S.h[c ^ 1], S.hu[c ^ 1], S.hv[c ^ 1]};
         unsigned long long my_min = 0x7FF0000000000000ull, my_max = 0ull;
-        coef_phase<R, false, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list, my_min, my_max,
-                                    ia);
+        if (STAGED)
+            coef_phase_staged<R, false, BATCH>(m, ha, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list,
+                                               my_min, my_max, ia, stg);
+        else
+            coef_phase<R, false, BATCH>(m, U, kact, active, seg_wet, ntiles, cull, mc, sc, nullptr, list, my_min,
+                                        my_max, ia);
         if (!BATCH) push_minmax(my_min, my_max, acc_min, acc_max);
         if (!grid_sync(sc)) return;
         if (BATCH) {
@@ -532,8 +550,13 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
             }
         }
         const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
-        update_phase<R, false, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull, mc,
-                                      sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list, ia);
+        if (STAGED)
+            update_phase_staged<R, false, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
+                                                 ntiles, cull, mc, sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list,
+                                                 ia, stg);
+        else
+            update_phase<R, false, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull,
+                                          mc, sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list, ia);
         if (!grid_sync(sc)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -600,12 +623,25 @@ int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
     if (nsteps <= 0) return DA_OK;
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
-    const void *kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3> : (const void *)k_steps<R, true, 2>)
-                             : (occ3 ? (const void *)k_steps<R, false, 3> : (const void *)k_steps<R, false, 2>);
-    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch + 4 * occ3];
+    const bool staged = staged_ok(ctx);
+    const void *kern;
+    if (staged)
+        kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3, true> : (const void *)k_steps<R, true, 2, true>)
+                     : (occ3 ? (const void *)k_steps<R, false, 3, true> : (const void *)k_steps<R, false, 2, true>);
+    else
+        kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3> : (const void *)k_steps<R, true, 2>)
+                     : (occ3 ? (const void *)k_steps<R, false, 3> : (const void *)k_steps<R, false, 2>);
+    const size_t smem = staged ? stage_smem_bytes<R>() : 0;
+    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch + 4 * occ3 + 8 * staged];
     if (cap_ref <= 0) {
+        int st = DA_OK;
+        if (staged)
+            st = cuda_check(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                            "shared memory attribute");
         int per_sm = 0;
-        int st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, 0), "occupancy");
+        if (!st)
+            st = cuda_check(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem),
+                            "occupancy");
         if (st) return st;
         cap_ref = per_sm * (ctx->sm_count > 0 ? ctx->sm_count : 1);
     }
@@ -632,10 +668,11 @@ int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
     snap::SnapArgs<R> pre = pre_slot ? snap::snap_args<R>(ctx, pre_slot, false, cur) : snap::no_snap<R>();
     snap::SnapArgs<R> post =
         post_slot ? snap::snap_args<R>(ctx, post_slot, true, (cur + nsteps) & 1) : snap::no_snap<R>();
-    void *args[] = {&m,       &S,        &cur,    &n,    &kact, &active, &seg_clean, &seg_wet, &seg_vol,
-                    &seg_dirty, &ntiles, &cull,   &mc,   &tc,   &sc,     &ia,        &pre,     &post};
+    HaloArgs ha = halo_args(ctx);
+    void *args[] = {&m,         &S,      &cur,  &n,  &kact, &active, &seg_clean, &seg_wet, &seg_vol,
+                    &seg_dirty, &ntiles, &cull, &mc, &tc,   &sc,     &ia,        &pre,     &post, &ha};
     trace_begin(ctx, TR_STEPS);
-    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, 0, ctx->stream);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, smem, ctx->stream);
     trace_end(ctx, nsteps);
     if (e != cudaSuccess) return cuda_check(ctx, e, "multi-step launch");
     ctx->cur = (cur + nsteps) & 1;
@@ -687,7 +724,7 @@ __global__ void __launch_bounds__(kBlock) k_refine_info(MeshArgs m, StateRef<R> 
     for (int i = i0 + threadIdx.x; i < i1; i += kBlock) {
         const R prev[3] = {Uprev.h[i], Uprev.hu[i], Uprev.hv[i]};
         R div[2][3];
-        flux_div<R>(m, Uprev, kact, i, m.bflag[i], prev, div);
+        flux_div<R>(global_view<R>(m, Uprev, kact), i, m.bflag[i], prev, div);
         double f = 0.0;
         for (int v = 0; v < 3; ++v) f += fabs(double(div[0][v])) + fabs(double(div[1][v]));
         const double dxc = double(cell_dx<R>(m, i)), dyc = double(cell_dy<R>(m, i));

@@ -104,14 +104,37 @@ __device__ __forceinline__ R curvat(const MeshArgs &m, int c, int i) {
     if constexpr (sizeof(R) == 8) return m.curv[(size_t)c * m.n + i]; else return m.fcurv[(size_t)c * m.n + i];
 }
 
+// What the per-cell numerics read about a cell and its neighbours goes through a view: nb(s, c)
+// the cell across neighbour entry s of cell c, and the values of a cell.  GlobalView reads the
+// mesh table and the global arrays (c, e = cell indices); the step kernels' staged view reads a
+// tile and its halo from shared memory (tile-local slots).  The arithmetic is the same either way.
+template <class R>
+struct GlobalView {
+    const MeshArgs &m;
+    StateRef<R> U;
+    const R *kact;
+    __device__ __forceinline__ int nb(int s, int c) const { return m.nbr[(size_t)s * m.n + c]; }
+    __device__ __forceinline__ R h(int e) const { return U.h[e]; }
+    __device__ __forceinline__ R hu(int e) const { return U.hu[e]; }
+    __device__ __forceinline__ R hv(int e) const { return U.hv[e]; }
+    __device__ __forceinline__ R k(int e) const { return kact[e]; }
+    __device__ __forceinline__ R gz(int e) const { return grav<R>(m, 2, e); }
+    __device__ __forceinline__ double coord(int dir, int e) const { return (dir == 0 ? m.x : m.y)[e]; }
+    __device__ __forceinline__ float size(int dir, int e) const { return (dir == 0 ? m.fdx : m.fdy)[e]; }
+};
+
+template <class R>
+__device__ __forceinline__ GlobalView<R> global_view(const MeshArgs &m, const StateRef<R> &U, const R *kact) {
+    return GlobalView<R>{m, U, kact};
+}
+
 // Element::get_slopes for one interior cell (element2.C:830-939); out[0..2] d/dx, out[3..5] d/dy.
 // Boundary cells (any side on the domain edge) have zero slopes.
 // FP64: the centre distances are differences of stored centres (ep->coord - coord) and every
 // quotient is a true division, as in the reference.  FP32: distances are half sums of cell
 // sizes (exact for quadtree geometry) and the three divisors of a direction are inverted once.
-template <class R>
-__device__ __forceinline__ void cell_slopes(const MeshArgs &m, const StateRef<R> &U, int i, uint8_t bf, R gamma,
-                                            const R ui[3], R out[6]) {
+template <class R, class V>
+__device__ __forceinline__ void cell_slopes(const V &v, int i, uint8_t bf, R gamma, const R ui[3], R out[6]) {
     if (bf & 0x0F) {
 #pragma unroll
         for (int j = 0; j < 6; ++j) out[j] = R(0);
@@ -119,24 +142,24 @@ __device__ __forceinline__ void cell_slopes(const MeshArgs &m, const StateRef<R>
     }
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
-        const int ep = m.nbr[(size_t)dir * m.n + i];
-        const int em = m.nbr[(size_t)(dir + 2) * m.n + i];
+        const int ep = v.nb(dir, i);
+        const int em = v.nb(dir + 2, i);
         const bool two_p = bf & (0x10 << dir), two_m = bf & (0x10 << (dir + 2));
-        const R up[3] = {U.h[ep], U.hu[ep], U.hv[ep]};
-        const R um[3] = {U.h[em], U.hu[em], U.hv[em]};
+        const R up[3] = {v.h(ep), v.hu(ep), v.hv(ep)};
+        const R um[3] = {v.h(em), v.hu(em), v.hv(em)};
         R up2[3] = {0, 0, 0}, um2[3] = {0, 0, 0};
         if (two_p) {
-            const int e = m.nbr[(size_t)(dir + 4) * m.n + i];
-            up2[0] = U.h[e]; up2[1] = U.hu[e]; up2[2] = U.hv[e];
+            const int e = v.nb(dir + 4, i);
+            up2[0] = v.h(e); up2[1] = v.hu(e); up2[2] = v.hv(e);
         }
         if (two_m) {
-            const int e = m.nbr[(size_t)(dir + 6) * m.n + i];
-            um2[0] = U.h[e]; um2[1] = U.hu[e]; um2[2] = U.hv[e];
+            const int e = v.nb(dir + 6, i);
+            um2[0] = v.h(e); um2[1] = v.hu(e); um2[2] = v.hv(e);
         }
         if constexpr (sizeof(R) == 8) {
-            const double *co = dir == 0 ? m.x : m.y;
-            const double dxp = co[ep] - co[i];
-            const double dxm = co[i] - co[em];
+            const double ci = v.coord(dir, i);
+            const double dxp = v.coord(dir, ep) - ci;
+            const double dxm = ci - v.coord(dir, em);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
                 double dp = (up[j] - ui[j]) / dxp;
@@ -151,9 +174,8 @@ __device__ __forceinline__ void cell_slopes(const MeshArgs &m, const StateRef<R>
                 out[j + 3 * dir] = .5 * (c_sgn(dp) + c_sgn(dm)) * mn;
             }
         } else {
-            const float *sz = dir == 0 ? m.fdx : m.fdy;
-            const float si = sz[i];
-            const float dxp = 0.5f * (sz[ep] + si), dxm = 0.5f * (sz[em] + si);
+            const float si = v.size(dir, i);
+            const float dxp = 0.5f * (v.size(dir, ep) + si), dxm = 0.5f * (v.size(dir, em) + si);
             const float ip = 1.0f / dxp, im = 1.0f / dxm, isum = 1.0f / (dxm + dxp);
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
@@ -261,32 +283,30 @@ __device__ __forceinline__ void riemann(const Hfv<R> &l, const Hfv<R> &r, R flux
 }
 
 // State, flux and speeds of neighbour e; only h is read for a dry neighbour.
-template <class R>
-__device__ __forceinline__ void nb_hfv(const MeshArgs &m, const StateRef<R> &U, const R *kact, int e,
-                                       int dir, Hfv<R> &o) {
-    const R h = U.h[e];
+template <class R, class V>
+__device__ __forceinline__ void nb_hfv(const V &v, int e, int dir, Hfv<R> &o) {
+    const R h = v.h(e);
     if (h < R(DA_TINY)) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) o.u[a] = o.f[a] = o.s[a] = R(0);
         return;
     }
-    dirflux<R>(dir, h, U.hu[e], U.hv[e], kact[e], grav<R>(m, 2, e), o);
+    dirflux<R>(dir, h, v.hu(e), v.hv(e), v.k(e), v.gz(e), o);
 }
 
 // Flux on side s of cell i (the value the reference stores on the side's edge-midpoint node):
 // one Riemann flux with a same-size or coarser neighbour, the mean of two with two finer ones.
-template <class R>
-__device__ __forceinline__ void side_flux(const MeshArgs &m, const StateRef<R> &U, const R *kact, int i,
-                                          uint8_t bf, int s, const Hfv<R> &self, R F[3]) {
+template <class R, class V>
+__device__ __forceinline__ void side_flux(const V &v, int i, uint8_t bf, int s, const Hfv<R> &self, R F[3]) {
     const int dir = s & 1;
     const bool plus = s < 2;
     Hfv<R> nb;
-    nb_hfv<R>(m, U, kact, m.nbr[(size_t)s * m.n + i], dir, nb);
+    nb_hfv<R>(v, v.nb(s, i), dir, nb);
     if (plus) riemann<R>(self, nb, F);
     else riemann<R>(nb, self, F);
     if (bf & (0x10 << s)) {
         R f2[3];
-        nb_hfv<R>(m, U, kact, m.nbr[(size_t)(s + 4) * m.n + i], dir, nb);
+        nb_hfv<R>(v, v.nb(s + 4, i), dir, nb);
         if (plus) riemann<R>(self, nb, f2);
         else riemann<R>(nb, self, f2);
 #pragma unroll
@@ -324,8 +344,6 @@ __device__ __forceinline__ void raise_err(DevScalars *sc, int code) { atomicCAS(
 // consecutive tiles go to consecutive blocks, so the few wet tiles of a compact flow spread over
 // the grid instead of queueing in one block.  The tiles that need work are compacted into
 // shared memory (increasing order) and processed one after another by the whole block.
-constexpr int kTileCells = 256;
-
 __device__ __forceinline__ int sched_tile(int round) {
     return (round * kTileCells + (int)threadIdx.x) * (int)gridDim.x + (int)blockIdx.x;
 }

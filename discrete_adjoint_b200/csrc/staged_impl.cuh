@@ -1,0 +1,324 @@
+// Staged coefficient and update phases of the cooperative step kernels (included by
+// forward_impl.cuh).
+//
+// A block works through its listed tiles one after another.  The values a tile's cells read at
+// their neighbours (depth, momenta, k act/pass, g_z and the centres or sizes) are copied, for the
+// tile's 256 cells and its halo (the outside cells they name as neighbours, at most kHaloMax),
+// into a shared-memory buffer by asynchronous copies (cp.async) one tile ahead: while the block
+// computes tile q, the copies of tile q + 1 and the halo list of tile q + 2 are in flight.  The
+// per-cell arithmetic is the global path's (the same helpers through StagedView), so results are
+// identical; only where the operands come from changes.  Each cell's neighbour entries come from
+// the host-built table of tile-local slots (one 16-byte load per cell).
+//
+// Activity: a cell is updated when it or a face neighbour is wet.  The global path marks every
+// neighbour of a wet cell in the active bitmask with atomics; here the update phase recomputes
+// that set from the staged depths of the tile and its halo, and the coefficient phase only marks
+// neighbours in other tiles (and each warp's own wet cells), which the tile listing needs.
+#pragma once
+
+namespace da {
+namespace fwd {
+namespace {
+
+constexpr int kSlots = kTileCells + kHaloMax;  // slot s < 256: cell 256 t + s; 256 + k: halo cell k
+
+template <class R>
+struct StageBuf {
+    R h[kSlots], hu[kSlots], hv[kSlots];
+    R k[kSlots];   // k act/pass (update phase)
+    R gz[kSlots];  // g_z
+    R c0[kSlots];  // FP64: x centre; FP32: dx
+    R c1[kSlots];  // FP64: y centre; FP32: dy
+};
+
+template <class R>
+struct StageSmem {
+    StageBuf<R> buf[2];
+    int hidx[3][kHaloMax];  // halo cells of three tiles in flight
+    int hoff[kTileCells];   // halo range of each listed tile of the round
+    int hcnt[kTileCells];
+};
+
+template <class R>
+constexpr size_t stage_smem_bytes() {
+    return sizeof(StageSmem<R>);
+}
+
+struct HaloArgs {
+    const int32_t *off;   // [ntiles + 1]
+    const int32_t *idx;   // halo cells, tile after tile
+    const int16_t *nloc;  // [n][8] tile-local neighbour slots
+};
+
+inline HaloArgs halo_args(const da_ctx *ctx) { return HaloArgs{ctx->mesh.halo_off, ctx->mesh.halo_idx, ctx->mesh.nloc}; }
+
+// The staged phases run when the parameters ask for them and the mesh's halo tables exist.
+inline bool staged_ok(const da_ctx *ctx) { return ctx->p.tile_staging == 1 && ctx->mesh.nloc != nullptr; }
+
+// cp.async of BYTES (4 or 8) from global to shared memory; completes at the group's wait.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <class R>
+struct StagedView {
+    const StageBuf<R> &b;
+    int nl[8];  // the cell's neighbour slots
+    __device__ __forceinline__ int nb(int s, int) const { return nl[s]; }
+    __device__ __forceinline__ R h(int e) const { return b.h[e]; }
+    __device__ __forceinline__ R hu(int e) const { return b.hu[e]; }
+    __device__ __forceinline__ R hv(int e) const { return b.hv[e]; }
+    __device__ __forceinline__ R k(int e) const { return b.k[e]; }
+    __device__ __forceinline__ R gz(int e) const { return b.gz[e]; }
+    __device__ __forceinline__ double coord(int dir, int e) const { return double(dir == 0 ? b.c0[e] : b.c1[e]); }
+    __device__ __forceinline__ float size(int dir, int e) const { return float(dir == 0 ? b.c0[e] : b.c1[e]); }
+};
+
+// The eight neighbour slots of cell i (one 16-byte load).
+__device__ __forceinline__ void load_slots(const int16_t *nloc, int i, int nl[8]) {
+    const uint4 w = *reinterpret_cast<const uint4 *>(nloc + (size_t)i * 8);
+    const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        nl[2 * q] = int(int16_t(u[q] & 0xffffu));
+        nl[2 * q + 1] = int(int16_t(u[q] >> 16));
+    }
+}
+
+// Copies of one slot's values.  UPD: also k act/pass and g_z (the update phase reads them at
+// neighbours; the coefficient phase reads g_z at the cell itself only).
+template <class R, bool UPD>
+__device__ __forceinline__ void stage_slot(StageBuf<R> &b, int s, int e, bool own, const MeshArgs &m,
+                                           const StateRef<R> &U, const R *kact) {
+    constexpr int B = sizeof(R);
+    cp_async<B>(&b.h[s], U.h + e);
+    cp_async<B>(&b.hu[s], U.hu + e);
+    cp_async<B>(&b.hv[s], U.hv + e);
+    if (UPD) cp_async<B>(&b.k[s], kact + e);
+    if constexpr (sizeof(R) == 8) {
+        if (UPD || own) cp_async<B>(&b.gz[s], m.g + (size_t)2 * m.n + e);
+        cp_async<B>(&b.c0[s], m.x + e);
+        cp_async<B>(&b.c1[s], m.y + e);
+    } else {
+        if (UPD || own) cp_async<B>(&b.gz[s], m.fg + (size_t)2 * m.n + e);
+        cp_async<B>(&b.c0[s], m.fdx + e);
+        cp_async<B>(&b.c1[s], m.fdy + e);
+    }
+}
+
+// Tile t's own cells and its halo (halo list already in shared memory) into buffer b.
+template <class R, bool UPD>
+__device__ __forceinline__ void stage_tile(StageBuf<R> &b, int t, const int *hidx, int hcnt, const MeshArgs &m,
+                                           const StateRef<R> &U, const R *kact) {
+    const int i = t * kTileCells + (int)threadIdx.x;
+    if (i < m.n) stage_slot<R, UPD>(b, threadIdx.x, i, true, m, U, kact);
+    for (int k = threadIdx.x; k < hcnt; k += kTileCells) stage_slot<R, UPD>(b, kTileCells + k, hidx[k], false, m, U, kact);
+}
+
+__device__ __forceinline__ void stage_halo_list(int *dst, const int32_t *src, int cnt) {
+    for (int k = threadIdx.x; k < cnt; k += kTileCells) cp_async<4>(dst + k, src + k);
+}
+
+// The listed tiles of a round, pipelined: fn(t, buffer, halo list) computes tile t from shared
+// memory.  Needs blockDim.x == kTileCells; every thread of the block calls it with the same cnt.
+template <class R, bool UPD, class F>
+__device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
+                                             const R *kact, int cnt, const int *list, StageSmem<R> &S, F &&fn) {
+    if ((int)threadIdx.x < cnt) {
+        const int t = list[threadIdx.x];
+        const int o = ha.off[t];
+        S.hoff[threadIdx.x] = o;
+        S.hcnt[threadIdx.x] = ha.off[t + 1] - o;
+    }
+    __syncthreads();
+    stage_halo_list(S.hidx[0], ha.idx + S.hoff[0], S.hcnt[0]);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    stage_tile<R, UPD>(S.buf[0], list[0], S.hidx[0], S.hcnt[0], m, U, kact);
+    if (cnt > 1) stage_halo_list(S.hidx[1], ha.idx + S.hoff[1], S.hcnt[1]);
+    cp_async_commit();
+    for (int q = 0; q < cnt; ++q) {
+        // tile q's values and tile q + 1's halo list have landed; every thread is past tile q - 1
+        cp_async_wait_all();
+        __syncthreads();
+        if (q + 1 < cnt) {
+            stage_tile<R, UPD>(S.buf[(q + 1) & 1], list[q + 1], S.hidx[(q + 1) % 3], S.hcnt[q + 1], m, U, kact);
+            if (q + 2 < cnt) stage_halo_list(S.hidx[(q + 2) % 3], ha.idx + S.hoff[q + 2], S.hcnt[q + 2]);
+        }
+        cp_async_commit();
+        fn(list[q], S.buf[q & 1], S.hidx[q % 3]);
+    }
+    __syncthreads();
+}
+
+// Coefficient phase (see coef_phase) with the tile and its halo staged.
+template <class R, bool RECORD, bool BATCH = false>
+__device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
+                                                  R *kact, unsigned *active, const uint8_t *seg_wet, int ntiles,
+                                                  int cull, const MatConsts &mc0, DevScalars *sc, uint8_t *mask,
+                                                  int *list, unsigned long long &my_min, unsigned long long &my_max,
+                                                  const InstArgs &ia, StageSmem<R> &S) {
+    for (int round = 0; sched_more(round, ntiles); ++round) {
+        const int tq = sched_tile(round);
+        const bool need = tq < ntiles && (!cull || seg_flags(seg_wet, tq) != 0ull);
+        const int cnt = compact_tiles(need, tq, list);
+        if (cnt == 0) continue;
+        staged_tiles<R, false>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *hidx) {
+            const int inst = BATCH ? ia.tile_inst[t] : 0;
+            const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+            const int c = threadIdx.x;
+            const int i = t * kTileCells + c;
+            bool wet = false;
+            if (i < m.n) {
+                const R h = b.h[c];
+                if (!(h == h)) raise_err(sc, DA_ERR_NAN);
+                wet = h >= R(DA_TINY);
+                uint8_t code = 0;
+                if (wet) {
+                    const uint8_t bf = m.bflag[i];
+                    StagedView<R> v{b};
+                    load_slots(ha.nloc, i, v.nl);
+                    // neighbours in other tiles: mark them for the tile listing of the update
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) {
+                        if (bf & (1 << s)) continue;
+                        const int ne = (bf & (0x10 << s)) ? 2 : 1;
+                        for (int q = 0; q < ne; ++q) {
+                            const int sl = v.nl[s + 4 * q];
+                            if (sl >= kTileCells) {
+                                const int e = hidx[sl - kTileCells];
+                                atomicOr(&active[e >> 5], 1u << (e & 31));
+                            }
+                        }
+                    }
+                    if (!(h > R(DA_TINY))) {  // h == GEOFLOW_TINY: dry for get_coef_and_eigen, wet for the fluxes
+                        kact[i] = R(mc.kact_rest);
+                    } else {
+                        const R ui[3] = {h, b.hu[c], b.hv[c]};
+                        R s[6];
+                        cell_slopes<R>(v, c, bf, R(mc.gamma), ui, s);
+                        const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
+                        kact[i] = k;
+                        const R gz = b.gz[c];
+                        const R vx = ui[1] / h, vy = ui[2] / h;
+                        const R cc = sqrt(k * gz * h);
+                        const R evx = dabs(vx) + cc, evy = dabs(vy) + cc;
+                        const R ev = evx > evy ? evx : evy;
+                        if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
+                        R dxm, dym;
+                        if constexpr (sizeof(R) == 8) {
+                            dxm = m.dx[i];
+                            dym = m.dy[i];
+                        } else {
+                            dxm = b.c0[c];
+                            dym = b.c1[c];
+                        }
+                        const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
+                        const unsigned long long hb = __double_as_longlong(double(h));
+                        my_min = rb < my_min ? rb : my_min;
+                        my_max = hb > my_max ? hb : my_max;
+                    }
+                }
+                if (RECORD) mask[i] = code;
+            }
+            const unsigned self = __ballot_sync(0xffffffffu, wet);
+            if (self && (threadIdx.x & 31) == 0) atomicOr(&active[i >> 5], self);
+            if (BATCH) {
+                push_minmax(my_min, my_max, ia.acc_min + inst, ia.acc_max + inst);
+                my_min = 0x7FF0000000000000ull;
+                my_max = 0ull;
+            }
+        });
+    }
+}
+
+// Update phase (see update_phase) with the tile and its halo staged.  A listed tile's cells
+// recompute their activity from the staged depths; the segment flags follow it.
+template <class R, bool RECORD, bool BATCH = false>
+__device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
+                                                    const StateOut<R> &O, const R *kact, unsigned *active,
+                                                    uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
+                                                    uint8_t *seg_dirty, int ntiles, int cull, const MatConsts &mc0,
+                                                    DevScalars *sc, R dt0, R ft, uint8_t *mask, int *tile_epoch,
+                                                    uint8_t *seg_act, int rec_id, int *list, const InstArgs &ia,
+                                                    StageSmem<R> &S) {
+    const int lane = threadIdx.x & 31;
+    for (int round = 0; sched_more(round, ntiles); ++round) {
+        const int tq = sched_tile(round);
+        bool need = false;
+        if (tq < ntiles) {
+            need = !cull || seg_flags(seg_clean, tq) != kAllSegs;
+            if (!need) {
+                const uint4 *w4 = reinterpret_cast<const uint4 *>(active + (size_t)tq * (kTileCells / 32));
+                const uint4 a = w4[0], b = w4[1];
+                need = (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
+            }
+        }
+        const int cnt = compact_tiles(need, tq, list);
+        if (cnt == 0) continue;
+        staged_tiles<R, true>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *) {
+            const int inst = BATCH ? ia.tile_inst[t] : 0;
+            const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
+            const R dt = BATCH ? R(ia.dt[inst]) : dt0;
+            const int c = threadIdx.x;
+            const int i = t * kTileCells + c;
+            const int seg = i >> 5;
+            const unsigned word = active[seg];  // marks to clear (padded: bits of cells >= n never set)
+            double vol = 0.0;
+            bool wet_after = false, act = false;
+            if (i < m.n) {
+                const R prev[3] = {b.h[c], b.hu[c], b.hv[c]};
+                const uint8_t bf = m.bflag[i];
+                StagedView<R> v{b};
+                load_slots(ha.nloc, i, v.nl);
+                act = prev[0] >= R(DA_TINY);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    if (bf & (1 << s)) continue;
+                    act |= b.h[v.nl[s]] >= R(DA_TINY);
+                    if (bf & (0x10 << s)) act |= b.h[v.nl[s + 4]] >= R(DA_TINY);
+                }
+                R dxc, dyc;
+                if constexpr (sizeof(R) == 8) {
+                    dxc = m.dx[i];
+                    dyc = m.dy[i];
+                } else {
+                    dxc = b.c0[c];
+                    dyc = b.c1[c];
+                }
+                R st[3] = {prev[0], prev[1], prev[2]};
+                bool clamped = false;
+                if (act) clamped = update_cell<R>(v, m, i, c, bf, mc, dt, ft, prev, dxc, dyc, st);
+                if (RECORD)
+                    mask[i] = uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0));
+                if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
+                O.h[i] = st[0];
+                O.hu[i] = st[1];
+                O.hv[i] = st[2];
+                vol = double(dxc) * double(dyc) * double(st[0]);
+                wet_after = st[0] >= R(DA_TINY);
+            }
+            const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
+            const unsigned act_bits = __ballot_sync(0xffffffffu, act);
+            vol = warp_sum(vol);
+            if (lane == 0) {
+                if (word) active[seg] = 0u;
+                if (act_bits) seg_dirty[seg] = 1;  // changed since the base checkpoint
+                seg_vol[seg] = vol;
+                seg_clean[seg] = act_bits ? 0 : 1;
+                seg_wet[seg] = wet_bits ? 1 : 0;
+                if (RECORD) seg_act[seg] = act_bits ? 1 : 0;
+            }
+            if (RECORD && threadIdx.x == 0) tile_epoch[t] = rec_id;
+        });
+    }
+}
+
+}  // namespace
+}  // namespace fwd
+}  // namespace da

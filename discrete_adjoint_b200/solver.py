@@ -51,7 +51,8 @@ class TimeProps:
 
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
                 influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0) -> _ffi.da_params:
+                tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
+                tile_staging: bool = True) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -74,6 +75,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.tile_culling = int(tile_culling)
     p.grid_blocks = int(grid_blocks)
     p.blocks_per_sm = int(blocks_per_sm)
+    p.tile_staging = int(tile_staging)
     return p
 
 
@@ -91,13 +93,14 @@ class GeoflowContext:
 
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
                  device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
-                 tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0):
+                 tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
+                 tile_staging: bool = True):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
         self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling,
-                                  grid_blocks, blocks_per_sm)
+                                  grid_blocks, blocks_per_sm, tile_staging)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:

@@ -95,7 +95,11 @@ typedef struct da_params {
                                   * compiled for 2 or 3 resident blocks per SM (3: fewer registers,
                                   * more warps to hide latency; pays on dense meshes and ensembles);
                                   * 0 = 2.  Results do not depend on it; da_autotune picks it. */
-    int32_t reserved1;
+    int32_t tile_staging;        /* 1: the multi-step and reverse-step kernels copy each 256-cell
+                                  * tile and its halo (the outside cells its cells name as
+                                  * neighbours) into shared memory one tile ahead, when no tile's
+                                  * halo exceeds 192 cells; 0: they read neighbours from global
+                                  * memory.  Results do not depend on it.  Default 1. */
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */

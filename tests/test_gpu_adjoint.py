@@ -152,6 +152,25 @@ def test_checkpoint_schedule_does_not_change_the_result():
     assert out[3].forward_steps == 16 + 15 or out[3].forward_steps >= 16
 
 
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+def test_tile_staging_does_not_change_the_adjoint(precision):
+    # the replayed forward steps of the reverse sweep (and its recomputation) with tiles and halos
+    # staged in shared memory, against neighbour reads from global memory: same lambda^0 and
+    # gradients bit for bit
+    w = inputs.test_case(seed=3)
+    m = w.mesh
+    out = []
+    for staging in (False, True):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision, tile_staging=staging) as c:
+            c.upload_mesh(m)
+            c.set_state(m.h0, m.hu0, m.hv0)
+            out.append(adjoint_run(c, box_of(w), 24, 4, m.dh0_dpile, want_lambda0=True))
+    a, b = out
+    assert np.array_equal(a.lambda0, b.lambda0)
+    assert a.J == b.J and a.dJ_dintfrict == b.dJ_dintfrict
+    assert np.array_equal(a.dJ_dbedfrict, b.dJ_dbedfrict) and np.array_equal(a.dJ_dpile, b.dJ_dpile)
+
+
 def test_adjoint_run_restores_state_and_time():
     w = inputs.test_case(seed=1)
     with ctx_for(w) as c:

@@ -108,6 +108,27 @@ def test_tile_culling_is_bit_identical(precision):
 
 
 @pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+@pytest.mark.parametrize("layer", [0.0, 0.5])
+def test_tile_staging_is_bit_identical(precision, layer):
+    # the staged phases (tile and halo in shared memory, activity recomputed from the staged
+    # depths) against the phases that read neighbours from global memory: the adaptive mesh with
+    # hanging nodes, with its piles alone (culled, sparse) and with a layer on every cell (dense)
+    w = inputs.workload1()
+    out = []
+    for staging in (False, True):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision, tile_staging=staging,
+                            blocks_per_sm=3 if staging else 0) as ctx:
+            ctx.upload_mesh(w.mesh)
+            ctx.set_state(w.mesh.h0 + layer, w.mesh.hu0, w.mesh.hv0)
+            s = ctx.run(90)
+            out.append((ctx.get_state(), s))
+    (a, sa), (b, sb) = out
+    for u, v in zip(a, b):
+        assert np.array_equal(u, v)
+    assert sa.time == sb.time and sa.volume == sb.volume and sa.dt == sb.dt
+
+
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
 def test_grid_size_and_autotune_do_not_change_results(precision):
     # the tiled kernels' results do not depend on the grid (fixed-order volume sum, min for dt),
     # and the autotuner puts the state, time and iteration back after its trials
