@@ -201,9 +201,15 @@ def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dic
             "k_youturn": coef + upd + 2 * n + src + gat, "snapshot_copy": 2 * 3 * r * n}
 
 
-# DRAM bytes (read + write) per launch from the committed ncu captures of the headline
-# workload (profiles/), keyed by (precision, kernel); None where no capture exists.
-TRAFFIC = {}
+# DRAM bytes (read + write) per launch from the committed ncu captures (profiles/), keyed by
+# (precision, kernel); None where no capture exists.  k_youturn: one reverse step of the
+# headline workload (k_youturn_fwd_adjoint_1M_fp64.md); k_steps_dense_per_step: the dense
+# 3.75M-cell case, per time step (k_steps_dense_hill_3.75M_staged.md).
+TRAFFIC = {
+    ("fp64", "k_youturn"): 2.284288e6 + 2.048e3,
+    ("fp32", "k_steps_dense_per_step"): (4.346160e9 + 0.615296e9) / 10,
+    ("fp64", "k_steps_dense_per_step"): (8.427677e9 + 1.226889e9) / 10,
+}
 
 
 def traffic_per_launch(precision: str, kernel: str):
@@ -336,32 +342,42 @@ def fwdadj(args, ws, local):
     return w, out
 
 
+DENSE_LAYER = 1.0  # m of material added on every cell for the dense forward case
+
+
 def forward_config2(args, ws, local):
     """Forward steps alone on the 3.75M-cell adaptive workload, through da_forward_run (the
-    multi-step kernel), with and without tile culling, in both precisions.  The full sweeps
-    (every cell rewritten every step) carry the roofline of the step kernel."""
+    multi-step kernel), in both precisions: the workload as specified (three piles on a 20 km
+    hill: a sparse flow, tile culling skips the dry tiles) and a dense case on the same mesh with
+    a layer of DENSE_LAYER m added on every cell, so that every cell is wet and updated every
+    step.  The dense case carries the roofline of the step kernel; the launch shape of each run
+    is the autotuner's."""
     from discrete_adjoint_b200 import GeoflowContext, TimeProps, _ffi, inputs
     w = inputs.workload2()
     m = w.mesh
     res = {}
     hbm, peak_kind = peaks()
-    for name, prec, cull in (("fp32", _ffi.DA_PREC_FP32_SPLIT, True),
-                             ("fp32_full_sweep", _ffi.DA_PREC_FP32_SPLIT, False),
-                             ("fp64", _ffi.DA_PREC_FP64, True),
-                             ("fp64_full_sweep", _ffi.DA_PREC_FP64, False)):
-        c = GeoflowContext(w.mat, TimeProps(), precision=prec, device=local, tile_culling=cull)
+    for name, prec, layer in (("fp32", _ffi.DA_PREC_FP32_SPLIT, 0.0),
+                              ("fp32_dense", _ffi.DA_PREC_FP32_SPLIT, DENSE_LAYER),
+                              ("fp64", _ffi.DA_PREC_FP64, 0.0),
+                              ("fp64_dense", _ffi.DA_PREC_FP64, DENSE_LAYER)):
+        c = GeoflowContext(w.mat, TimeProps(), precision=prec, device=local)
         c.upload_mesh(m)
-        c.set_state(m.h0, m.hu0, m.hv0)
+        c.set_state(m.h0 + layer, m.hu0, m.hv0)
         c.run(5)
+        tune = c.autotune(5)
         _, ms = c.run_timed(300)
         ms = allmax(ms, ws, local)
         wv, av = wet_counts(m, c.get_state()[0])
-        r = {"value": m.n * 300 * ws / (ms * 1e-3), "us_per_step": 1e3 * ms / 300, "wet_cells": wv, "active_cells": av}
-        if not cull:
+        r = {"value": m.n * 300 * ws / (ms * 1e-3), "us_per_step": 1e3 * ms / 300, "wet_cells": wv,
+             "active_cells": av, "launch_shape": {"blocks_per_sm": tune["best"][0], "grid": tune["best"][1]}}
+        if layer > 0:
             bytes_step = algorithmic_bytes("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32", m.n, wv, av)["k_steps"]
             gbs = bytes_step / (ms * 1e-3 / 300) / 1e9
             r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step, "achieved": gbs, "peak": hbm,
-                             "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind}
+                             "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind,
+                             "traffic": traffic_per_launch("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32",
+                                                           "k_steps_dense_per_step")}
         res[name] = r
         c.close()
     return w, res

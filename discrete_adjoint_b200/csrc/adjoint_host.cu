@@ -163,8 +163,40 @@ struct Schedule {
     }
 };
 
+// DWR indicator along the reverse sweep (da_adjoint_run_dwr): after the reverse step of n -> n+1
+// (U^n, U^{n+1} and lambda^{n+1} all resident) the indicator of that step, as the reference's
+// dual_solver calls error_compute after each adjoint step (dual_solver.C:206-230).
+struct DwrAcc {
+    double *cell = nullptr;       // [n] device: el_error per coarse cell, summed over the steps
+    double *step_sums = nullptr;  // host [nsteps][2]: total el_error and correction of each step
+    long long iter_begin = 0;     // iteration of U^0
+    int nsteps = 0;
+};
+
+__global__ void k_accumulate(int n, const double *__restrict__ a, double *__restrict__ acc) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[i] += a[i];
+}
+
+int dwr_after_reverse_step(da_ctx *ctx, DwrAcc &d, int lam_next) {
+    // the reverse step wrote the step's dt, time and iteration like a forward step
+    int st = copy_d2h(ctx, ctx->hsc, ctx->dsc, sizeof(DevScalars), "read scalars");
+    if (st) return st;
+    const double dt = ctx->hsc->dt;
+    const long long iter0 = ctx->hsc->iter - 1;
+    const double time0 = ctx->hsc->time - dt;  // enters the error grid's step only through clipping
+    st = dwr_indicator(ctx, ctx->cur ^ 1, ctx->cur, lam_next, dt, time0, iter0);
+    if (st) return st;
+    const int n = ctx->mesh.n, grid = (ctx->sm_count > 0 ? ctx->sm_count : 148) * 4;
+    k_accumulate<<<grid, 256, 0, ctx->stream>>>(n, ctx->dwr.cell, d.cell);
+    st = cuda_check(ctx, cudaGetLastError(), "dwr accumulate");
+    const long long k = iter0 - d.iter_begin;
+    if (!st && k >= 0 && k < d.nsteps) st = copy_d2h(ctx, d.step_sums + 2 * k, ctx->dwr.sums, 16, "dwr sums");
+    return st;
+}
+
 struct Runner {
     da_ctx *ctx;
+    DwrAcc *dwr = nullptr;
     Schedule sch;
     std::vector<int> free_slots;
     int lam_cur = 0;  // buffer holding lambda^{n+1}
@@ -202,7 +234,8 @@ struct Runner {
         ++fsteps;
         pos = -1;  // past the step that is being taken back
         // the first reverse step (the horizon's last step) also seeds lambda^N from U^N
-        const int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box, take_pending());
+        int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box, take_pending());
+        if (!st && dwr) st = dwr_after_reverse_step(ctx, *dwr, lam_cur);
         seeded = true;
         lam_cur = 1 - lam_cur;
         return st;
@@ -301,10 +334,11 @@ int adj_alloc_for_dwr(da_ctx *ctx) { return adj_alloc(ctx, 1); }
 // J and the gradient sums launched (single: red_out[n_mat + 1 + n_piles]; ensemble: per member).
 // lam0 receives the buffer that holds lambda^0.
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
-                  long long *fsteps, float *dev_ms) {
+                  long long *fsteps, float *dev_ms, void *dwr_acc) {
     int st = adj_alloc(ctx, nsnapshots + 1);
     Runner r;
     r.ctx = ctx;
+    r.dwr = (DwrAcc *)dwr_acc;
     if (box)
         for (int q = 0; q < 4; ++q) r.box[q] = box[q];
     if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
@@ -391,8 +425,12 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
     return st;
 }
 
-int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
-                   int32_t n_piles, da_gradient *out, double *lambda0) {
+}  // extern "C"
+
+namespace {
+
+int adjoint_run_impl(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
+                     int32_t n_piles, da_gradient *out, double *lambda0, DwrAcc *dwr) {
     if (!ctx || !f || nsteps <= 0 || nsnapshots < 0 || n_piles < 0 || n_piles > DA_MAX_PILES ||
         (n_piles > 0 && !dh0_dpile) || f->kind != DA_FUNC_H2_BOX)
         return DA_ERR_INVALID;
@@ -412,7 +450,7 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
     int lam0 = 0;
     long long fsteps = 0;
     float dev_ms = 0.f;
-    if (!st) st = adjoint_sweep(ctx, f->box, nsteps, nsnapshots, n_piles, &lam0, &fsteps, &dev_ms);
+    if (!st) st = adjoint_sweep(ctx, f->box, nsteps, nsnapshots, n_piles, &lam0, &fsteps, &dev_ms, dwr);
     if (!st && lambda0) st = copy_lambda_out(ctx, lam0, lambda0);
     if (!st) st = fill_gradient(ctx, lam0, n_piles, out, /*reduced=*/true);
     if (!st && out) {
@@ -420,6 +458,38 @@ int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t 
         out->snapshots = nsnapshots;
         out->device_ms = dev_ms;
     }
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
+                   int32_t n_piles, da_gradient *out, double *lambda0) {
+    return adjoint_run_impl(ctx, f, nsteps, nsnapshots, dh0_dpile, n_piles, out, lambda0, nullptr);
+}
+
+int da_adjoint_run_dwr(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots,
+                       const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0,
+                       double *cell_error, double *step_sums) {
+    if (!ctx || !cell_error || !step_sums) return DA_ERR_INVALID;
+    if (!ctx->dwr.fine) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_run_dwr: no error grid (da_dwr_setup)");
+    if (ctx->mesh.n <= 0 || nsteps <= 0) return da_adjoint_run(ctx, f, nsteps, nsnapshots, dh0_dpile, n_piles, out, lambda0);
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)ctx->mesh.n;
+    DwrAcc acc;
+    acc.step_sums = step_sums;
+    acc.nsteps = nsteps;
+    for (int k = 0; k < 2 * nsteps; ++k) step_sums[k] = 0.0;
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (!st) st = copy_d2h(ctx, ctx->hsc, ctx->dsc, sizeof(DevScalars), "read scalars");
+    acc.iter_begin = ctx->hsc->iter;
+    if (!st) st = cuda_check(ctx, cudaMalloc((void **)&acc.cell, sizeof(double) * n), "cudaMalloc(dwr cells)");
+    if (!st) st = cuda_check(ctx, cudaMemsetAsync(acc.cell, 0, sizeof(double) * n, ctx->stream), "memset");
+    if (!st) st = adjoint_run_impl(ctx, f, nsteps, nsnapshots, dh0_dpile, n_piles, out, lambda0, &acc);
+    if (!st) st = copy_d2h(ctx, cell_error, acc.cell, sizeof(double) * n, "copy dwr cells");
+    if (acc.cell) cudaFree(acc.cell);
     return st;
 }
 

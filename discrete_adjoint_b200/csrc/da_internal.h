@@ -269,8 +269,9 @@ int forward_state_changed(da_ctx *ctx);
 // adjoint_host.cu: d kact / d phi_bed and d phi_int of each material's three branches
 void kact_derivatives(const da_params &p, double *dkb, double *dki);
 // adjoint_host.cu: the checkpointed reverse sweep (see there)
+// dwr_acc (or null): accumulate the DWR indicator of every reverse step (adjoint_host.cu DwrAcc)
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
-                  long long *fsteps, float *dev_ms);
+                  long long *fsteps, float *dev_ms, void *dwr_acc = nullptr);
 int copy_lambda_out(da_ctx *ctx, int buf, double *host);
 // dwr.cu: the indicator of the step U[un] -> U[unext] with adjoint lam[lam] (coarse dt, time and
 // iteration before the step); release of the error grid

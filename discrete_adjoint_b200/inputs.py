@@ -67,9 +67,11 @@ def hill_noise(lx: float, ly: float, res: float, relief: float, noise_rms: float
 
 
 def fractal(lx: float, ly: float, res: float, hurst: float, relief: float, seed: int) -> DEM:
+    """Seeded fractal (fractional Brownian) surface of Hurst exponent hurst: power spectrum
+    ~ 1/f^(2H + 2), scaled to the given relief."""
     rng = np.random.default_rng(seed)
-    X, _ = _posts(0.0, 0.0, lx, ly, res)
-    z = spectral_noise(X.shape, 2.0 * hurst + 2.0, 1.0, rng)
+    shape = (int(round(ly / res)) + 1, int(round(lx / res)) + 1)
+    z = spectral_noise(shape, 2.0 * hurst + 2.0, 1.0, rng)
     z = (z - z.min()) / max(np.ptp(z), 1e-30) * relief
     return DEM(elev=z.astype(np.float32), xmin=0.0, ymin=0.0, res=res)
 
@@ -207,3 +209,49 @@ def workload2(seed: int = 2, target_cells: float = 4.0e6, res: float = 5.0) -> W
     bed = [float(b) for b in rng.uniform(15.0, 25.0, size=4)]
     return Workload("hill+noise 20km x 20km, 3 piles, 4 materials, adaptive to 5 m", mesh,
                     MatProps(intfrict_deg=30.0, bedfrict_deg=bed), piles, 1000, spec, dem)
+
+
+WORKLOAD5_SIDE = 8192
+
+
+def workload5(seed: int = 5, crop: int | None = None, dem: DEM | None = None) -> Workload:
+    """Large single instance: 40 km x 40 km of seeded fractal terrain (H = 0.8, 2 km relief) at
+    5 m posts, uniform at the finest level (8192^2 = 67M cells of 4.88 m); two paraboloid piles
+    near the centre (seeded heights and radii); phi_bed 20, phi_int 30; 2000 steps.  The flux
+    source of the workload (1e3 m^3/s for 60 s) does not change the state in the reference
+    (corrector.C:136-140) and enters dt only while no cell is wet, which never happens with two
+    piles: it is carried as influx_dt (influx5_dt).
+
+    crop: build only the crop x crop cells centred on the domain (same cell positions, same
+    terrain, same piles).  Away from its edges a crop's cells have the same static fields as the
+    full mesh's, so a flow that stays inside evolves identically on both.  dem: the terrain of an
+    earlier call with the same seed (it takes a while to generate)."""
+    rng = np.random.default_rng(seed)
+    L = 40000.0
+    if dem is None:
+        dem = fractal(L, L, 5.0, 0.8, 2000.0, seed)
+    d = L / WORKLOAD5_SIDE
+    piles = []
+    for k in range(2):
+        ang = math.pi * k + rng.uniform(-0.4, 0.4)
+        r = rng.uniform(80.0, 300.0)
+        piles.append(Pile(0.5 * L + 900.0 * math.cos(ang), 0.5 * L + 900.0 * math.sin(ang), rng.uniform(20.0, 60.0),
+                          r, r))
+    side = WORKLOAD5_SIDE if crop is None else int(crop)
+    if side % 16 or side > WORKLOAD5_SIDE:
+        raise ValueError("crop must be a multiple of 16 up to the full side")
+    x0 = 0.5 * L - 0.5 * side * d
+    spec = MeshSpec(xmin=x0, ymin=x0, dx0=16 * d, dy0=16 * d, nx0=side // 16, ny0=side // 16, max_level=4,
+                    uniform=True)
+    mesh = Mesh.build(spec, dem, piles)
+    name = f"fractal 40km x 40km (H 0.8, 2 km relief), uniform {side}^2" + ("" if crop is None else " crop")
+    return Workload(name, mesh, MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0]), piles, 2000, spec, dem)
+
+
+def influx5_dt(mesh: Mesh, gravity_scale: float = 1.0, epsilon: float = 1.0, rate_m3s: float = 1.0e3,
+               area_m2: float = 1.0e4) -> float:
+    """dt[2] of get_coef_and_eigen.C:48-77 for the large workload's flux source while it is active:
+    min(min_dx / influx, 0.81 influx g_s / 9.8) with influx = rate / area * epsilon (m/s)."""
+    influx = rate_m3s / area_m2 * epsilon
+    mindx = float(min(mesh.dx.min(), mesh.dy.min()))
+    return min(mindx / influx, 0.81 * influx * gravity_scale / 9.8)

@@ -2,11 +2,13 @@
 
     python -m discrete_adjoint_b200.run_case --workload 2 --precision fp32 --steps 20 [--full-sweep]
     python -m discrete_adjoint_b200.run_case --workload 3 --precision fp64 --adjoint 64
+    python -m discrete_adjoint_b200.run_case --workload 2 --precision fp64 --layer 1 --steps 10
 
 A fixed, small command line for profilers (ncu -k <kernel> -s <skip> -c <count> python -m ...):
 the forward steps go through da_forward_run (CUDA graphs), the adjoint through da_adjoint_run.
 Workloads: 1 = 40k-cell plane and runout, 2 = 3.75M-cell adaptive hill + noise, 3 = 1M-cell
-uniform plane (the forward + adjoint workload).
+uniform plane (the forward + adjoint workload).  --layer adds that many metres of material on
+every cell (the dense case: every cell wet and updated every step).
 """
 from __future__ import annotations
 
@@ -23,6 +25,7 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--steps", type=int, default=20, help="forward steps (ignored with --adjoint)")
     ap.add_argument("--full-sweep", action="store_true", help="switch tile culling off")
+    ap.add_argument("--layer", type=float, default=0.0, help="metres of material added on every cell")
     ap.add_argument("--adjoint", type=int, default=0, metavar="HORIZON",
                     help="run forward + adjoint over HORIZON steps (32 snapshots) instead")
     ap.add_argument("--device", type=int, default=0)
@@ -32,8 +35,9 @@ def main(argv=None):
     with GeoflowContext(w.mat, TimeProps(), precision=prec, device=a.device,
                         tile_culling=not a.full_sweep) as c:
         c.upload_mesh(w.mesh)
-        c.set_state(w.mesh.h0, w.mesh.hu0, w.mesh.hv0)
-        out = {"workload": w.name, "cells": w.mesh.n, "precision": a.precision, "culling": not a.full_sweep}
+        c.set_state(w.mesh.h0 + a.layer, w.mesh.hu0, w.mesh.hv0)
+        out = {"workload": w.name, "cells": w.mesh.n, "precision": a.precision, "culling": not a.full_sweep,
+               "layer": a.layer}
         if a.adjoint:
             p0 = w.piles[0]
             box = inputs.WORKLOAD3_BOX if a.workload == 3 else (p0.xc - 500.0, p0.xc + 500.0, p0.yc - 500.0, p0.yc + 500.0)

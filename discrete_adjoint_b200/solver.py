@@ -261,6 +261,8 @@ class Gradient:
     snapshots: int
     device_ms: float = 0.0
     lambda0: np.ndarray | None = None
+    dwr_cell: np.ndarray | None = None   # DWR el_error per coarse cell, summed over the steps
+    dwr_steps: np.ndarray | None = None  # [nsteps][2] total el_error and correction per step
 
 
 def _grad(g: _ffi.da_gradient, n_mat: int, n_piles: int, lam0=None) -> Gradient:
@@ -269,11 +271,14 @@ def _grad(g: _ffi.da_gradient, n_mat: int, n_piles: int, lam0=None) -> Gradient:
 
 
 def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpile=None,
-                want_lambda0: bool = False, lambda0_out: np.ndarray | None = None) -> Gradient:
+                want_lambda0: bool = False, lambda0_out: np.ndarray | None = None, dwr: bool = False) -> Gradient:
     """dual_solver() of src/adjoint/dual_solver.C:80 over nsteps steps from the current state, for
     J = sum of h^2 dx dy over the cells whose centre lies in box = (xmin, xmax, ymin, ymax).
     lambda0_out: a caller-owned contiguous float64 array of 3 n values (e.g. in pinned memory)
-    that receives lambda^0; want_lambda0 allocates one instead."""
+    that receives lambda^0; want_lambda0 allocates one instead.  dwr: also the DWR indicator of
+    every step (da_adjoint_run_dwr; needs dwr.Indicator set up on the context): the Gradient's
+    dwr_cell (per coarse cell, summed over the steps) and dwr_steps ([nsteps][2] el_error and
+    correction of each step)."""
     f = _ffi.da_functional(_ffi.DA_FUNC_H2_BOX, 0, (C.c_double * 4)(*box))
     n = ctx.mesh.n
     dh = None
@@ -288,6 +293,15 @@ def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpil
     else:
         lam0 = np.zeros(3 * n) if want_lambda0 else None
     g = _ffi.da_gradient()
+    if dwr:
+        cell, steps = np.zeros(n), np.zeros((nsteps, 2))
+        ctx._check(ctx.lib.da_adjoint_run_dwr(ctx.ctx, C.byref(f), nsteps, nsnapshots,
+                                              _ffi.dptr(dh) if dh is not None else None, n_piles, C.byref(g),
+                                              _ffi.dptr(lam0) if lam0 is not None else None, _ffi.dptr(cell),
+                                              _ffi.dptr(steps)), "da_adjoint_run_dwr")
+        out = _grad(g, len(ctx.mat.bedfrict_deg), n_piles, None if lam0 is None else lam0.reshape(3, n))
+        out.dwr_cell, out.dwr_steps = cell, steps
+        return out
     ctx._check(ctx.lib.da_adjoint_run(ctx.ctx, C.byref(f), nsteps, nsnapshots,
                                       _ffi.dptr(dh) if dh is not None else None, n_piles, C.byref(g),
                                       _ffi.dptr(lam0) if lam0 is not None else None), "da_adjoint_run")

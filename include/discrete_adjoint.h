@@ -318,6 +318,15 @@ int da_refine_info(da_ctx *ctx, double *el_error, uint8_t *flags, double *geo_ta
 int da_dwr_setup(da_ctx *ctx, const da_mesh_soa *fine, const int32_t *parent, const int32_t *interp,
                  const double *weight);
 int da_dwr_step(da_ctx *ctx, const double *lambda_next, double *el_error, double *cell_error, double *sums);
+/* da_adjoint_run with the DWR indicator of every reverse step, as dual_solver computes
+ * error_compute after each adjoint step (src/adjoint/dual_solver.C:206-230): the step n -> n+1 is
+ * evaluated right after its reverse step, from U^n, U^{n+1} and lambda^{n+1}.  Needs
+ * da_dwr_setup.  cell_error [n]: el_error per coarse cell summed over the steps; step_sums
+ * [nsteps][2]: total el_error and total correction of step k (k = 0 the first step of the
+ * horizon).  Synchronises with the host once per step. */
+int da_adjoint_run_dwr(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots,
+                       const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0,
+                       double *cell_error, double *step_sums);
 
 /* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
  * Times nsteps forward steps from the current state for each candidate launch shape of the

@@ -90,3 +90,40 @@ def test_indicator_vanishes_for_a_lake_at_rest():
     inner = (fx > 100.0) & (fx < 540.0) & (fy > 100.0) & (fy < 540.0)
     # rounding only: the reconstruction weights at hanging nodes sum to one within 1e-16
     assert el[inner].max() < 1e-25 and el[inner].max() >= 0.0
+
+
+def test_adjoint_run_accumulates_the_step_indicators():
+    # the indicator of every reverse step of the checkpointed sweep (da_adjoint_run_dwr) against the
+    # same steps one by one: forward states U^n, lambda^N = dJ/dU^N, lambda^n by single reverse
+    # steps, and da_dwr_step at each U^n with lambda^{n+1}
+    from discrete_adjoint_b200 import adjoint_run
+    w = inputs.test_case(seed=1)
+    m = w.mesh
+    g = error_grid(w)
+    N = 6
+    wet = m.h0 > 1.0
+    box = (0.5 * (m.x[wet].min() + m.x[wet].max()), m.x[wet].max() + 100.0, m.y[wet].min(), m.y[wet].max())
+    with ctx_for(w) as c:
+        Indicator(c, g)
+        res = adjoint_run(c, box, N, 2, dwr=True)
+    with ctx_for(w) as c:
+        states, times = [np.stack(c.get_state())], [(0.0, 0)]
+        for k in range(N):
+            s = c.step()
+            states.append(np.stack(c.get_state()))
+            times.append((s.time, s.iter))
+        hN = states[N][0]
+        inb = (m.x >= box[0]) & (m.x <= box[1]) & (m.y >= box[2]) & (m.y <= box[3])
+        lam = np.stack([np.where(inb, 2.0 * hN * (m.dx * m.dy), 0.0), np.zeros(m.n), np.zeros(m.n)])
+        ind = Indicator(c, g)
+        sums, cells = np.zeros((N, 2)), np.zeros(m.n)
+        for k in range(N - 1, -1, -1):
+            c.set_state(*states[k])
+            c.set_time(*times[k])
+            _, cell, sk = ind.step(lam)
+            sums[k] = sk
+            cells += cell
+            lam, _ = adjoint_step(c, lam)
+    assert np.all(sums[:, 0] > 0)
+    np.testing.assert_allclose(res.dwr_steps, sums, rtol=1e-12, atol=1e-14 * np.abs(sums).max())
+    np.testing.assert_allclose(res.dwr_cell, cells, rtol=1e-12, atol=1e-14 * cells.max())
