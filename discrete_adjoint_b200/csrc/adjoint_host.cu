@@ -129,17 +129,28 @@ int adj_alloc(da_ctx *ctx, int nsnap) {
 int store(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], true); }
 int restore(da_ctx *ctx, int slot) { return launch_snapshot(ctx, ctx->snaps[slot], false); }
 
+// The placement is kept in the context and rebuilt only when the horizon or the slot count
+// changes (the dynamic programme is O(N^2 C)).
 struct Schedule {
     int N = 0, C = 0;
     std::vector<long long> cost;  // [(N+1) x (C+1)]
-    std::vector<int> split;
+    std::vector<int> *split = nullptr;
     long long &T(int l, int c) { return cost[(size_t)l * (C + 1) + c]; }
-    int &S(int l, int c) { return split[(size_t)l * (C + 1) + c]; }
+    int &S(int l, int c) { return (*split)[(size_t)l * (C + 1) + c]; }
+    void use(da_ctx *ctx, int n, int c) {
+        split = &ctx->sched_split;
+        N = n;
+        C = c;
+        if (ctx->sched_n == n && ctx->sched_c == c) return;
+        build(n, c);
+        ctx->sched_n = n;
+        ctx->sched_c = c;
+    }
     void build(int n, int c) {
         N = n;
         C = c;
         cost.assign((size_t)(N + 1) * (C + 1), 0);
-        split.assign((size_t)(N + 1) * (C + 1), 0);
+        split->assign((size_t)(N + 1) * (C + 1), 0);
         for (int l = 1; l <= N; ++l) {
             T(l, 0) = (long long)l * (l - 1) / 2;
             for (int cc = 1; cc <= C; ++cc) {
@@ -343,7 +354,7 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
         for (int q = 0; q < 4; ++q) r.box[q] = box[q];
     if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
     if (st) return st;
-    r.sch.build(nsteps, nsnapshots);
+    r.sch.use(ctx, nsteps, nsnapshots);
     for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
@@ -441,11 +452,16 @@ int adjoint_run_impl(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_
     const size_t n = (size_t)ctx->mesh.n;
     int st = DA_OK;
     if (n_piles > 0) {
-        if (ctx->dh0) cudaFree(ctx->dh0);
-        ctx->dh0 = nullptr;
-        st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * n * n_piles), "cudaMalloc(dh0)");
-        if (!st)
-            st = copy_h2d(ctx, ctx->dh0, dh0_dpile, sizeof(double) * n * n_piles, "copy dh0");
+        // kept between runs (a free synchronises the device)
+        const size_t bytes = sizeof(double) * n * n_piles;
+        if (ctx->dh0_bytes < bytes) {
+            if (ctx->dh0) cudaFree(ctx->dh0);
+            ctx->dh0 = nullptr;
+            ctx->dh0_bytes = 0;
+            st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, bytes), "cudaMalloc(dh0)");
+            if (!st) ctx->dh0_bytes = bytes;
+        }
+        if (!st) st = copy_h2d(ctx, ctx->dh0, dh0_dpile, bytes, "copy dh0");
     }
     int lam0 = 0;
     long long fsteps = 0;

@@ -157,6 +157,7 @@ static void free_adjoint(da_ctx *ctx) {
     ctx->snaps.clear();
     ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
     ctx->red_out = ctx->red_part = ctx->inst_J = ctx->seg_J = ctx->dh0 = nullptr;
+    ctx->dh0_bytes = 0;
     ctx->adj_n = 0;
     ctx->adj_ninst = -1;
 }

@@ -217,6 +217,10 @@ struct da_ctx {
     double *red_part = nullptr;      // [same x kAdjReduceParts] partial sums of the gradient reduction
     double *inst_J = nullptr;        // [max(ninst, 1)] J of each member
     double *dh0 = nullptr;           // [n_piles][n]
+    size_t dh0_bytes = 0;            // its allocation
+    // the binomial checkpoint placement of the last horizon / slot count (adjoint_host.cu)
+    std::vector<int> sched_split;
+    int sched_n = -1, sched_c = -1;
     std::vector<void *> snaps;       // checkpoint slots, 3 state arrays each
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
     int adj_n = 0;

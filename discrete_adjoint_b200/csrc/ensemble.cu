@@ -218,6 +218,7 @@ int da_ensemble_upload(da_ctx *ctx, const da_member *members, int32_t n_members)
     if (!st) st = upload_member_scalars(ctx);
     if (!st && any_pile) {
         st = cuda_check(ctx, cudaMalloc((void **)&ctx->dh0, sizeof(double) * N), "cudaMalloc(dh0)");
+        if (!st) ctx->dh0_bytes = sizeof(double) * N;
         if (!st) st = copy_h2d(ctx, ctx->dh0, dh0.data(), sizeof(double) * N, "copy dh0");
     }
     if (!st) st = da_ensemble_restart(ctx);
