@@ -212,6 +212,8 @@ SIGNATURES = {
     "da_forward_run_timed": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(da_step_stats), PD]),
     "da_adjoint_run": (C.c_int, [C.c_void_p, C.POINTER(da_functional), C.c_int32, C.c_int32, PD, C.c_int32,
                                  C.POINTER(da_gradient), PD]),
+    "da_adjoint_run_seeded": (C.c_int, [C.c_void_p, PD, C.c_int32, C.c_int32, PD, C.c_int32,
+                                        C.POINTER(da_gradient), PD]),
     "da_adjoint_run_dwr": (C.c_int, [C.c_void_p, C.POINTER(da_functional), C.c_int32, C.c_int32, PD, C.c_int32,
                                      C.POINTER(da_gradient), PD, PD, PD]),
     "da_adjoint_step": (C.c_int, [C.c_void_p, PD, PD, C.POINTER(da_gradient)]),

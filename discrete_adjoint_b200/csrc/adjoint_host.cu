@@ -345,7 +345,7 @@ int adj_alloc_for_dwr(da_ctx *ctx) { return adj_alloc(ctx, 1); }
 // J and the gradient sums launched (single: red_out[n_mat + 1 + n_piles]; ensemble: per member).
 // lam0 receives the buffer that holds lambda^0.
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
-                  long long *fsteps, float *dev_ms, void *dwr_acc) {
+                  long long *fsteps, float *dev_ms, void *dwr_acc, const double *lambda_end) {
     int st = adj_alloc(ctx, nsnapshots + 1);
     Runner r;
     r.ctx = ctx;
@@ -353,6 +353,17 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
     if (box)
         for (int q = 0; q < 4; ++q) r.box[q] = box[q];
     if (!st) st = upload_tables(ctx, r.sec2, &r.cos_int);
+    if (!st && lambda_end) {
+        // lambda^N given (the adjoint carried back across a later mesh epoch): no functional seed,
+        // J = 0 here; the two adjoint buffers differ everywhere
+        const size_t n = (size_t)ctx->mesh.n;
+        for (int v = 0; v < 3 && !st; ++v) st = upload_real(ctx, ctx->lam[0][v], lambda_end + v * n);
+        if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
+        if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->seg_J, 0, sizeof(double) * ctx->nseg, ctx->stream), "memset");
+        if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+        r.lam_cur = 0;
+        r.seeded = true;
+    }
     if (st) return st;
     r.sch.use(ctx, nsteps, nsnapshots);
     for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
@@ -441,9 +452,10 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
 namespace {
 
 int adjoint_run_impl(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
-                     int32_t n_piles, da_gradient *out, double *lambda0, DwrAcc *dwr) {
-    if (!ctx || !f || nsteps <= 0 || nsnapshots < 0 || n_piles < 0 || n_piles > DA_MAX_PILES ||
-        (n_piles > 0 && !dh0_dpile) || f->kind != DA_FUNC_H2_BOX)
+                     int32_t n_piles, da_gradient *out, double *lambda0, DwrAcc *dwr,
+                     const double *lambda_end = nullptr) {
+    if (!ctx || (!f && !lambda_end) || nsteps <= 0 || nsnapshots < 0 || n_piles < 0 || n_piles > DA_MAX_PILES ||
+        (n_piles > 0 && !dh0_dpile) || (f && f->kind != DA_FUNC_H2_BOX))
         return DA_ERR_INVALID;
     if (ctx->mesh.n <= 0) return set_error(ctx, DA_ERR_NO_MESH, "da_adjoint_run: no mesh");
     if (!ctx->have_state) return set_error(ctx, DA_ERR_INVALID, "da_adjoint_run: no state");
@@ -466,7 +478,9 @@ int adjoint_run_impl(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_
     int lam0 = 0;
     long long fsteps = 0;
     float dev_ms = 0.f;
-    if (!st) st = adjoint_sweep(ctx, f->box, nsteps, nsnapshots, n_piles, &lam0, &fsteps, &dev_ms, dwr);
+    if (!st)
+        st = adjoint_sweep(ctx, f ? f->box : nullptr, nsteps, nsnapshots, n_piles, &lam0, &fsteps, &dev_ms, dwr,
+                           lambda_end);
     if (!st && lambda0) st = copy_lambda_out(ctx, lam0, lambda0);
     if (!st) st = fill_gradient(ctx, lam0, n_piles, out, /*reduced=*/true);
     if (!st && out) {
@@ -484,6 +498,12 @@ extern "C" {
 int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots, const double *dh0_dpile,
                    int32_t n_piles, da_gradient *out, double *lambda0) {
     return adjoint_run_impl(ctx, f, nsteps, nsnapshots, dh0_dpile, n_piles, out, lambda0, nullptr);
+}
+
+int da_adjoint_run_seeded(da_ctx *ctx, const double *lambda_end, int32_t nsteps, int32_t nsnapshots,
+                          const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0) {
+    if (!lambda_end) return DA_ERR_INVALID;
+    return adjoint_run_impl(ctx, nullptr, nsteps, nsnapshots, dh0_dpile, n_piles, out, lambda0, nullptr, lambda_end);
 }
 
 int da_adjoint_run_dwr(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots,

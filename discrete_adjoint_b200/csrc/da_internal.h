@@ -274,8 +274,9 @@ int forward_state_changed(da_ctx *ctx);
 void kact_derivatives(const da_params &p, double *dkb, double *dki);
 // adjoint_host.cu: the checkpointed reverse sweep (see there)
 // dwr_acc (or null): accumulate the DWR indicator of every reverse step (adjoint_host.cu DwrAcc)
+// lambda_end (or null): lambda^N given instead of the functional's seed (host [3][n])
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
-                  long long *fsteps, float *dev_ms, void *dwr_acc = nullptr);
+                  long long *fsteps, float *dev_ms, void *dwr_acc = nullptr, const double *lambda_end = nullptr);
 int copy_lambda_out(da_ctx *ctx, int buf, double *host);
 // dwr.cu: the indicator of the step U[un] -> U[unext] with adjoint lam[lam] (coarse dt, time and
 // iteration before the step); release of the error grid

@@ -308,6 +308,25 @@ def adjoint_run(ctx: GeoflowContext, box, nsteps: int, nsnapshots: int, dh0_dpil
     return _grad(g, len(ctx.mat.bedfrict_deg), n_piles, None if lam0 is None else lam0.reshape(3, n))
 
 
+def adjoint_run_seeded(ctx: GeoflowContext, lambda_end, nsteps: int, nsnapshots: int, dh0_dpile=None) -> Gradient:
+    """The reverse sweep over nsteps steps from the current state with lambda^N = lambda_end given
+    ([3][n], da_adjoint_run_seeded): one mesh epoch of an adjoint across adaptation.  J is 0; the
+    gradient is this epoch's part; lambda0 is returned."""
+    n = ctx.mesh.n
+    le = np.ascontiguousarray(lambda_end, dtype=np.float64).reshape(3 * n)
+    dh = None
+    n_piles = 0
+    if dh0_dpile is not None and len(dh0_dpile):
+        dh = np.ascontiguousarray(dh0_dpile, dtype=np.float64).reshape(-1, n)
+        n_piles = dh.shape[0]
+    lam0 = np.zeros(3 * n)
+    g = _ffi.da_gradient()
+    ctx._check(ctx.lib.da_adjoint_run_seeded(ctx.ctx, _ffi.dptr(le), nsteps, nsnapshots,
+                                             _ffi.dptr(dh) if dh is not None else None, n_piles, C.byref(g),
+                                             _ffi.dptr(lam0)), "da_adjoint_run_seeded")
+    return _grad(g, len(ctx.mat.bedfrict_deg), n_piles, lam0.reshape(3, n))
+
+
 def adjoint_step(ctx: GeoflowContext, lam_next) -> tuple:
     """(lambda^n, parameter parts) for one reverse step at the context's current state."""
     n = ctx.mesh.n

@@ -186,6 +186,13 @@ typedef struct da_gradient {
  * The context's state and time are restored to the start on return. */
 int da_adjoint_run(da_ctx *ctx, const da_functional *f, int32_t nsteps, int32_t nsnapshots,
                    const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0);
+/* da_adjoint_run from a given lambda^N = dJ/dU^N (host [3][n]) instead of a functional: the
+ * reverse sweep of one mesh epoch when the mesh adapts during the horizon (the adjoint of the later
+ * epochs carried back through the transpose of the state transfer, as dual_solver moves the adjoint
+ * across refinement, dualmesh.C:700-712, 980-995).  out->J is 0; the parameter sums are this
+ * epoch's part. */
+int da_adjoint_run_seeded(da_ctx *ctx, const double *lambda_end, int32_t nsteps, int32_t nsnapshots,
+                          const double *dh0_dpile, int32_t n_piles, da_gradient *out, double *lambda0);
 /* One reverse step at the current state U^n: lambda_out = (dU^{n+1}/dU^n)^T lambda_next (host
  * arrays [3][n]).  Replays the forward step to record its branches and time step, then restores
  * the state and time.  The parameter parts of this step are returned in partial (may be NULL). */
