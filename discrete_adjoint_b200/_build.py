@@ -35,6 +35,7 @@ UNITS = [
     ("dwr.cu", []),
     ("stats.cu", []),
     ("mesh_host.cpp", []),
+    ("solution_io.cpp", []),
 ]
 
 
@@ -86,7 +87,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 sys.stderr.write(r.stdout + r.stderr)
                 raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB, objs):
-        cmd = [nvcc, "-shared", "-Xcompiler", "-fPIC"] + ARCH + objs + ["-o", LIB, "-cudart", "static"]
+        cmd = [nvcc, "-shared", "-Xcompiler", "-fPIC"] + ARCH + objs + ["-o", LIB, "-cudart", "static", "-lz"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -244,6 +244,10 @@ SIGNATURES = {
                                 C.c_double, C.c_double, C.POINTER(C.POINTER(da_mesh_host))]),
     "da_mesh_free": (None, [C.POINTER(da_mesh_host)]),
     "da_mesh_view": (C.c_int, [C.POINTER(da_mesh_host), C.POINTER(da_mesh_soa)]),
+    "da_cell_keys": (C.c_int, [C.c_int32, PD, PD, PD, PD, C.POINTER(C.c_uint32)]),
+    "da_write_solution": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_uint32), PD, PD, PD]),
+    "da_read_solution": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_uint32), PD, PD, PD,
+                                   C.POINTER(C.c_int32)]),
 }
 
 _lib = None

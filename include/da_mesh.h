@@ -84,6 +84,22 @@ void da_mesh_free(da_mesh_host *m);
 /* Fills a da_mesh_soa view whose pointers alias the host mesh. */
 int da_mesh_view(const da_mesh_host *m, da_mesh_soa *view);
 
+/* ---- the reference's element keys and forward solution records (host) ---------------------
+ * da_cell_keys: the key TITAN2D gives an element with centre (x, y) in a table spanning xrange x
+ * yrange (Element::gen_my_sons_key, src/datstr/element2.C:4360-4420, through fhsfc2d_ of
+ * src/main/hilbert.C): the 2-D Hilbert code of the normalised centre, 2 x uint32 per cell.
+ * da_write_solution / da_read_solution: the dual solver's gz record of one step's forward state,
+ * solution_<rank>_<step> (SolRec::wrtie_sol_to_disk / read_sol_from_disk, src/datstr/dualmesh.C:
+ * 82-147, 234-297): zero records (depth not positive) by key, then key + (h, hu, hv).  Reading maps
+ * records to cells by key (an unknown key is DA_ERR_INVALID); cells without a record get a zero
+ * state and are counted in n_missing (may be NULL). */
+int da_cell_keys(int32_t n, const double *x, const double *y, const double xrange[2], const double yrange[2],
+                 uint32_t *keys);
+int da_write_solution(const char *path, int32_t n, const uint32_t *keys, const double *h, const double *hu,
+                      const double *hv);
+int da_read_solution(const char *path, int32_t n, const uint32_t *keys, double *h, double *hu, double *hv,
+                     int32_t *n_missing);
+
 #ifdef __cplusplus
 }
 #endif

@@ -166,3 +166,51 @@ def run_reference(mesh, mat, h, hu, hv, nsteps: int, maxtime: float = float("inf
     out["stats"] = dict(zip(STAT_FIELDS, take(len(STAT_FIELDS))))
     out["discharge"] = take(len(planes))
     return out
+
+
+def _harness(payload: bytes, cwd: str) -> bytes:
+    import subprocess
+    fin, fout = os.path.join(cwd, "in.bin"), os.path.join(cwd, "out.bin")
+    with open(fin, "wb") as f:
+        f.write(payload)
+    r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True, cwd=cwd)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
+    return open(fout, "rb").read()
+
+
+def ref_hilbert_keys(u, v) -> np.ndarray:
+    """The reference's own fhsfc2d_ (src/main/hilbert.C) of normalised points: [n][2] uint32."""
+    import struct
+    import tempfile
+    u = np.ascontiguousarray(u, dtype="<f8")
+    v = np.ascontiguousarray(v, dtype="<f8")
+    with tempfile.TemporaryDirectory() as td:
+        raw = _harness(struct.pack("<2i", 0x314B4144, len(u)) + u.tobytes() + v.tobytes(), td)
+    magic, n = struct.unpack_from("<2i", raw, 0)
+    assert magic == 0x324B4144 and n == len(u)
+    return np.frombuffer(raw, dtype="<u4", offset=8).reshape(n, 2).copy()
+
+
+def ref_write_solution(directory: str, rank: int, step: int, keys, h, hu, hv):
+    """The reference's SolRec writes solution_<rank>_<step> into directory (wrtie_sol_to_disk)."""
+    import struct
+    k = np.ascontiguousarray(keys, dtype="<u4")
+    payload = struct.pack("<4i", 0x31574144, rank, step, len(k)) + k.tobytes()
+    for a in (h, hu, hv):
+        payload += np.ascontiguousarray(a, dtype="<f8").tobytes()
+    raw = _harness(payload, directory)
+    assert struct.unpack_from("<i", raw, 0)[0] == 0x32574144
+
+
+def ref_read_solution(directory: str, rank: int, step: int, keys):
+    """The reference's SolRec reads solution_<rank>_<step> from directory (read_sol_from_disk):
+    (found [n]: 0 none, 1 zero record, 2 state record; state [n][3])."""
+    import struct
+    k = np.ascontiguousarray(keys, dtype="<u4")
+    raw = _harness(struct.pack("<4i", 0x31524144, rank, step, len(k)) + k.tobytes(), directory)
+    magic, n = struct.unpack_from("<2i", raw, 0)
+    assert magic == 0x32524144 and n == len(k)
+    found = np.frombuffer(raw, dtype="<i4", offset=8, count=n).copy()
+    state = np.frombuffer(raw, dtype="<f8", offset=8 + 4 * n).reshape(n, 3).copy()
+    return found, state

@@ -21,6 +21,16 @@
 //   double h[n] hu[n] hv[n] slopes[6n] kact[n] flux[4][3][n] gravity[3n] d_gravity[2n]
 // ref_static = 1 recomputes gravity with Element::calc_gravity_vector and d_gravity with
 // Element::calc_d_gravity instead of taking the input's.
+//
+// Other modes, chosen by the first word of the input:
+//   'DAK1' n, double u[n], v[n]  ->  'DAK2' n, uint32 key[2n]: fhsfc2d_ (src/main/hilbert.C) of
+//       each normalised point, the element key of Element::gen_my_sons_key.
+//   'DAW1' rank, step, n, uint32 key[2n], double h[n], hu[n], hv[n]  ->  'DAW2': the reference's
+//       SolRec writes the file solution_<rank>_<step> in the working directory
+//       (record_solution's zero / non-zero split, wrtie_sol_to_disk).
+//   'DAR1' rank, step, n, uint32 key[2n]  ->  'DAR2' n, int32 found[n] (0 none, 1 zero record,
+//       2 state record), double state[3n]: the reference's SolRec reads solution_<rank>_<step>
+//       (read_sol_from_disk) and each key is looked up.
 #include <sys/sysinfo.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -90,6 +100,94 @@ int priority(int info) {
 
 }  // namespace
 
+namespace {
+
+SolRec *make_solrec() {
+    double dkr[2] = {4294967296.0, 4294967296.0}, XR[2] = {0.0, 1.0}, YR[2] = {0.0, 1.0};
+    return new SolRec(dkr, 4099, 2017, XR, YR, 0);
+}
+
+int keys_mode(FILE *f, const char *out) {
+    int32_t n;
+    rd(f, &n, 1);
+    std::vector<double> u(n), v(n);
+    rd(f, u.data(), n);
+    rd(f, v.data(), n);
+    std::vector<unsigned> k(2 * (size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+        double c[2] = {u[i], v[i]};
+        unsigned nkey = 2;
+        fhsfc2d_(c, &nkey, &k[2 * (size_t)i]);
+    }
+    FILE *o = std::fopen(out, "wb");
+    const int32_t m = 0x324B4144;
+    wr(o, &m, 1);
+    wr(o, &n, 1);
+    wr(o, k.data(), k.size());
+    std::fclose(o);
+    return 0;
+}
+
+int write_mode(FILE *f, const char *out) {
+    int32_t h3[3];
+    rd(f, h3, 3);
+    const int rank = h3[0], stp = h3[1], n = h3[2];
+    std::vector<unsigned> k(2 * (size_t)n);
+    std::vector<double> h(n), hu(n), hv(n);
+    rd(f, k.data(), k.size());
+    rd(f, h.data(), n);
+    rd(f, hu.data(), n);
+    rd(f, hv.data(), n);
+    SolRec *sr = make_solrec();
+    for (int32_t i = 0; i < n; ++i) {
+        Jacobian *j = new Jacobian(&k[2 * (size_t)i]);
+        sr->add(j->get_key(), j);
+        if (h[i] > 0.) {
+            double s[3] = {h[i], hu[i], hv[i]};
+            j->put_solution(new Solution(s), stp);
+        } else {
+            j->put_solution(&(Solution::solution_zero), stp);
+        }
+    }
+    sr->update_first_sol_time(stp);
+    sr->update_last_sol_time(stp + 1);
+    sr->wrtie_sol_to_disk(rank);
+    FILE *o = std::fopen(out, "wb");
+    const int32_t m = 0x32574144;
+    wr(o, &m, 1);
+    std::fclose(o);
+    return 0;
+}
+
+int read_mode(FILE *f, const char *out) {
+    int32_t h3[3];
+    rd(f, h3, 3);
+    const int rank = h3[0], stp = h3[1], n = h3[2];
+    std::vector<unsigned> k(2 * (size_t)n);
+    rd(f, k.data(), k.size());
+    SolRec *sr = make_solrec();
+    sr->read_sol_from_disk(rank, stp);
+    std::vector<int32_t> found(n, 0);
+    std::vector<double> st(3 * (size_t)n, 0.0);
+    for (int32_t i = 0; i < n; ++i) {
+        Jacobian *j = (Jacobian *)sr->lookup(&k[2 * (size_t)i]);
+        Solution *s = j ? j->get_solution(stp) : nullptr;
+        if (!s) continue;
+        found[i] = s == &(Solution::solution_zero) ? 1 : 2;
+        for (int v = 0; v < 3; ++v) st[3 * (size_t)i + v] = s->get_solution()[v];
+    }
+    FILE *o = std::fopen(out, "wb");
+    const int32_t m = 0x32524144;
+    wr(o, &m, 1);
+    wr(o, &n, 1);
+    wr(o, found.data(), n);
+    wr(o, st.data(), st.size());
+    std::fclose(o);
+    return 0;
+}
+
+}  // namespace
+
 int main(int argc, char **argv) {
     if (argc != 3) {
         std::fprintf(stderr, "usage: ref_harness in.bin out.bin\n");
@@ -97,8 +195,14 @@ int main(int argc, char **argv) {
     }
     FILE *f = std::fopen(argv[1], "rb");
     if (!f) return 2;
+    int32_t magic;
+    rd(f, &magic, 1);
+    if (magic == 0x314B4144) return keys_mode(f, argv[2]);
+    if (magic == 0x31574144) return write_mode(f, argv[2]);
+    if (magic == 0x31524144) return read_mode(f, argv[2]);
     int32_t hdr[6];
-    rd(f, hdr, 6);
+    hdr[0] = magic;
+    rd(f, hdr + 1, 5);
     if (hdr[0] != 0x31484144) return 3;
     const int n = hdr[1], L = hdr[2], nmat = hdr[3], nsteps = hdr[4], ref_static = hdr[5];
     double sc[5], bed[16];

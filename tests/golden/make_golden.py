@@ -64,8 +64,20 @@ def stats_case(name, seed, nsteps):
     print(p, m.n, "cells", os.path.getsize(p) // 1024, "KiB")
 
 
+def hilbert_keys():
+    """Element keys of the reference's fhsfc2d_ (src/main/hilbert.C) for seeded points of the unit
+    square and its edges."""
+    rng = np.random.default_rng(11)
+    u = np.concatenate([rng.random(1000), [0.0, 1.0, -0.5, 1.5, 0.5, 1e-12, 1 - 1e-12, 0.25, 0.75]])
+    v = np.concatenate([rng.random(1000), [0.0, 1.0, 0.3, 2.0, 0.5, 1 - 1e-12, 1e-12, 0.75, 0.25]])
+    p = os.path.join(HERE, "hilbert_keys.npz")
+    np.savez_compressed(p, u=u, v=v, keys=oracle.ref_hilbert_keys(u, v))
+    print(p)
+
+
 def main():
     ref_build.build()
+    hilbert_keys()
     for case in STATS_CASES:
         stats_case(*case)
     for name, seed, nx0, ny0, L, frac, nsteps in CASES:

@@ -93,3 +93,25 @@ def test_refine_info_matches_the_reference_edge_fluxes(path):
     t_ref = e_ref[sel].mean() if sel.any() else 1.0
     assert abs(target - t_ref) <= 1e-12 * t_ref
     assert np.array_equal((flags >> 4) & 1 == 1, e > target)
+
+
+def test_forward_records_hold_each_steps_state(tmp_path):
+    # the reference's dual-solver records of a device run: file k holds U^k, read back by key
+    from discrete_adjoint_b200 import records
+    mesh, mat, nsteps, ref = load(fixtures()[0])
+    keys = records.mesh_keys(mesh)
+    states = []
+    with GeoflowContext(mat, TimeProps()) as c:
+        c.upload_mesh(mesh)
+        c.set_state(mesh.h0, mesh.hu0, mesh.hv0)
+        records.record_forward(c, 4, str(tmp_path), keys)
+        c.set_state(mesh.h0, mesh.hu0, mesh.hv0)
+        c.set_time(0.0, 0)
+        for _ in range(4):
+            states.append(c.get_state())
+            c.step()
+    for k, (h, hu, hv) in enumerate(states):
+        h2, hu2, hv2, miss = records.read_solution(str(tmp_path / records.solution_name(0, k)), keys)
+        pos = h > 0
+        assert miss == 0 and np.array_equal(h2, np.where(pos, h, 0.0))
+        assert np.array_equal(hu2, np.where(pos, hu, 0.0)) and np.array_equal(hv2, np.where(pos, hv, 0.0))
