@@ -276,6 +276,87 @@ __device__ __forceinline__ InstTables inst_tables(const AdjArgs &aa, const InstA
     return InstTables{ia.sec2_bed + (size_t)inst * DA_MAX_MATERIALS, ia.cos_int[inst], dk, dk + DA_MAX_MATERIALS * 3};
 }
 
+// The source adjoint of one cell (the body of the source phase): for a wet cell of U^n the
+// adjoint of its sources (A), the slope coefficients it passes to its neighbours (B) and its
+// parameter sensitivities, from its own recorded branches (mask) and lambda^{n+1}.  Reads U^n
+// at the cell and its neighbours; writes only the cell's own entries.
+template <class R>
+__device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
+                                             const MatConsts &mc, const AdjArgs &aa, const InstTables &it, R dt,
+                                             R ft, int i) {
+    double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
+    const R h_i = U.h[i];
+    // A and B exist for wet cells only; k_adj_gather reads them only there
+    if (!(h_i > R(DA_TINY))) return;
+    const R prev[3] = {h_i, U.hu[i], U.hv[i]};
+    {
+        R le[3];
+        const uint8_t mi = aa.mask[i];
+        lam_eff<R>(Lnext, mi, i, le);
+        const R nu_u = dt * le[1], nu_v = dt * le[2];
+        if (nu_u != R(0) || nu_v != R(0)) {
+            const uint8_t bf = m.bflag[i];
+            const int mat = m.mat[i];
+            const uint8_t code = mi & 3;
+            const R k = kact_of<R>(mc, mat, code);
+            R s[6];
+            cell_slopes<R>(global_view<R>(m, U, (const R *)nullptr), i, bf, R(mc.gamma), prev, s);
+            R vel0, vel1, h_inv;
+            if constexpr (sizeof(R) == 8) {
+                vel0 = prev[1] / prev[0];
+                vel1 = prev[2] / prev[0];
+                h_inv = 1. / prev[0];
+            } else {
+                h_inv = 1.0f / prev[0];
+                vel0 = prev[1] * h_inv;
+                vel1 = prev[2] * h_inv;
+            }
+            const R sg0 = tiny_sgn(h_inv * (s[4] - vel0 * s[3]), ft);
+            const R sg2 = tiny_sgn(vel0, ft);
+            const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
+            const R sg3 = tiny_sgn(vel1, ft);
+            const R h = prev[0];
+            const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i), gz = grav<R>(m, 2, i);
+            const R dgx = dgrav<R>(m, 0, i), dgy = dgrav<R>(m, 1, i);
+            const R kx = curvat<R>(m, 0, i), ky = curvat<R>(m, 1, i);
+            const R sin_int = R(mc.sin_int), tan_bed = R(mc.tan_bed[mat]);
+            const R Px = gz * h + vel0 * prev[1] * kx, Py = gz * h + vel1 * prev[2] * ky;
+            const R px = Px > R(0) ? R(1) : R(0), py = Py > R(0) ? R(1) : R(0);
+            const R wx = gz * s[3] + dgy * h, wy = gz * s[0] + dgx * h;
+            A[0] = double(nu_u * (gx - sg0 * k * sin_int * (wx + dgy * h) - sg2 * tan_bed * px * (gz - vel0 * vel0 * kx)) +
+                          nu_v * (gy - sg1 * k * sin_int * (wy + dgx * h) - sg3 * tan_bed * py * (gz - vel1 * vel1 * ky)));
+            A[1] = double(nu_u * (-sg2 * tan_bed * px * R(2) * vel0 * kx));
+            A[2] = double(nu_v * (-sg3 * tan_bed * py * R(2) * vel1 * ky));
+            // the limited depth slopes of this cell (zero on boundary cells)
+            if (!(bf & 0x0F)) {
+                SlopeD<R> sd[2];
+                h_slope_deriv<R>(m, U.h, i, bf, R(mc.gamma), h, sd);
+                const R cx = -nu_v * sg1 * h * k * gz * sin_int;  // on d h / dx
+                const R cy = -nu_u * sg0 * h * k * gz * sin_int;  // on d h / dy
+                A[0] += double(cx * (-sd[0].g_dp / sd[0].dxp + sd[0].g_dm / sd[0].dxm) +
+                               cy * (-sd[1].g_dp / sd[1].dxp + sd[1].g_dm / sd[1].dxm));
+                B[0] = double(cx * sd[0].g_dp / sd[0].dxp);
+                B[2] = double(-cx * sd[0].g_dm / sd[0].dxm);
+                B[1] = double(cy * sd[1].g_dp / sd[1].dxp);
+                B[3] = double(-cy * sd[1].g_dm / sd[1].dxm);
+            }
+            // parameter sensitivities of the sources
+            const double dJ_dk = double(-nu_u * sg0 * h * wx * sin_int - nu_v * sg1 * h * wy * sin_int);
+            const double dJ_dsin = double(-nu_u * sg0 * h * k * wx - nu_v * sg1 * h * k * wy);
+            const double dJ_dtan = double(-nu_u * sg2 * (Px > R(0) ? Px : R(0)) - nu_v * sg3 * (Py > R(0) ? Py : R(0)));
+            const double gb = dJ_dtan * it.sec2_bed[mat] + dJ_dk * dk_of(it.dk_dbed, mat, code);
+            const double gi = dJ_dsin * it.cos_int + dJ_dk * dk_of(it.dk_dint, mat, code);
+            if (gb != 0.0) aa.gbed[i] += gb;
+            if (gi != 0.0) aa.gint[i] += gi;
+        }
+    }
+    aa.A[i] = A[0];
+    aa.A[(size_t)m.n + i] = A[1];
+    aa.A[(size_t)2 * m.n + i] = A[2];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) aa.B[(size_t)s * m.n + i] = B[s];
+}
+
 template <class R, bool BATCH = false>
 __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
                                               const MatConsts &mc0, const AdjArgs &aa, R dt0, R ft, int *list,
@@ -293,77 +374,7 @@ __device__ __forceinline__ void adj_src_phase(const MeshArgs &m, const StateRef<
         const InstTables it = inst_tables<BATCH>(aa, ia, inst);
         const int i = t * kBlock + threadIdx.x;
         if (i >= m.n) continue;
-        double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
-        const R h_i = U.h[i];
-        // A and B exist for wet cells only; k_adj_gather reads them only there
-        if (!(h_i > R(DA_TINY))) continue;
-        const R prev[3] = {h_i, U.hu[i], U.hv[i]};
-        {
-            R le[3];
-            const uint8_t mi = aa.mask[i];
-            lam_eff<R>(Lnext, mi, i, le);
-            const R nu_u = dt * le[1], nu_v = dt * le[2];
-            if (nu_u != R(0) || nu_v != R(0)) {
-                const uint8_t bf = m.bflag[i];
-                const int mat = m.mat[i];
-                const uint8_t code = mi & 3;
-                const R k = kact_of<R>(mc, mat, code);
-                R s[6];
-                cell_slopes<R>(global_view<R>(m, U, (const R *)nullptr), i, bf, R(mc.gamma), prev, s);
-                R vel0, vel1, h_inv;
-                if constexpr (sizeof(R) == 8) {
-                    vel0 = prev[1] / prev[0];
-                    vel1 = prev[2] / prev[0];
-                    h_inv = 1. / prev[0];
-                } else {
-                    h_inv = 1.0f / prev[0];
-                    vel0 = prev[1] * h_inv;
-                    vel1 = prev[2] * h_inv;
-                }
-                const R sg0 = tiny_sgn(h_inv * (s[4] - vel0 * s[3]), ft);
-                const R sg2 = tiny_sgn(vel0, ft);
-                const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
-                const R sg3 = tiny_sgn(vel1, ft);
-                const R h = prev[0];
-                const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i), gz = grav<R>(m, 2, i);
-                const R dgx = dgrav<R>(m, 0, i), dgy = dgrav<R>(m, 1, i);
-                const R kx = curvat<R>(m, 0, i), ky = curvat<R>(m, 1, i);
-                const R sin_int = R(mc.sin_int), tan_bed = R(mc.tan_bed[mat]);
-                const R Px = gz * h + vel0 * prev[1] * kx, Py = gz * h + vel1 * prev[2] * ky;
-                const R px = Px > R(0) ? R(1) : R(0), py = Py > R(0) ? R(1) : R(0);
-                const R wx = gz * s[3] + dgy * h, wy = gz * s[0] + dgx * h;
-                A[0] = double(nu_u * (gx - sg0 * k * sin_int * (wx + dgy * h) - sg2 * tan_bed * px * (gz - vel0 * vel0 * kx)) +
-                              nu_v * (gy - sg1 * k * sin_int * (wy + dgx * h) - sg3 * tan_bed * py * (gz - vel1 * vel1 * ky)));
-                A[1] = double(nu_u * (-sg2 * tan_bed * px * R(2) * vel0 * kx));
-                A[2] = double(nu_v * (-sg3 * tan_bed * py * R(2) * vel1 * ky));
-                // the limited depth slopes of this cell (zero on boundary cells)
-                if (!(bf & 0x0F)) {
-                    SlopeD<R> sd[2];
-                    h_slope_deriv<R>(m, U.h, i, bf, R(mc.gamma), h, sd);
-                    const R cx = -nu_v * sg1 * h * k * gz * sin_int;  // on d h / dx
-                    const R cy = -nu_u * sg0 * h * k * gz * sin_int;  // on d h / dy
-                    A[0] += double(cx * (-sd[0].g_dp / sd[0].dxp + sd[0].g_dm / sd[0].dxm) +
-                                   cy * (-sd[1].g_dp / sd[1].dxp + sd[1].g_dm / sd[1].dxm));
-                    B[0] = double(cx * sd[0].g_dp / sd[0].dxp);
-                    B[2] = double(-cx * sd[0].g_dm / sd[0].dxm);
-                    B[1] = double(cy * sd[1].g_dp / sd[1].dxp);
-                    B[3] = double(-cy * sd[1].g_dm / sd[1].dxm);
-                }
-                // parameter sensitivities of the sources
-                const double dJ_dk = double(-nu_u * sg0 * h * wx * sin_int - nu_v * sg1 * h * wy * sin_int);
-                const double dJ_dsin = double(-nu_u * sg0 * h * k * wx - nu_v * sg1 * h * k * wy);
-                const double dJ_dtan = double(-nu_u * sg2 * (Px > R(0) ? Px : R(0)) - nu_v * sg3 * (Py > R(0) ? Py : R(0)));
-                const double gb = dJ_dtan * it.sec2_bed[mat] + dJ_dk * dk_of(it.dk_dbed, mat, code);
-                const double gi = dJ_dsin * it.cos_int + dJ_dk * dk_of(it.dk_dint, mat, code);
-                if (gb != 0.0) aa.gbed[i] += gb;
-                if (gi != 0.0) aa.gint[i] += gi;
-            }
-        }
-        aa.A[i] = A[0];
-        aa.A[(size_t)m.n + i] = A[1];
-        aa.A[(size_t)2 * m.n + i] = A[2];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) aa.B[(size_t)s * m.n + i] = B[s];
+        adj_src_cell<R>(m, U, Lnext, mc, aa, it, dt, ft, i);
       }
     }
 }

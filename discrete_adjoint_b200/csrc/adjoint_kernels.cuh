@@ -124,6 +124,36 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
         fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
     }
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
+    if (STAGED && !SEED) {
+        // the source adjoint of each wet cell right after its update (its own branches and
+        // lambda^{n+1}, U^n around it: nothing another cell writes in this phase), so the reverse
+        // step needs no source phase of its own
+        const R dtr = R(dt);
+        auto src = [&](int t, int i) {
+            const int inst = BATCH ? ia.tile_inst[t] : 0;
+            const MatConsts &mci = BATCH ? ia.mcs[inst] : mc;
+            const R dti = BATCH ? R(ia.dt[inst]) : dtr;
+            adj_src_cell<R>(m, U, Ln, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ftr, i);
+        };
+        fwd::update_phase_staged<R, true, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
+                                                 ntiles, cull, mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id,
+                                                 list, ia, stg, src);
+        if (!fwd::grid_sync(sc)) return;
+        adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sc->iter = iter + 1;
+            sc->frict_tiny = ft;
+            if (!BATCH) {
+                sc->time = time + dt;
+                sc->dt = dt;
+                sc->min_dxe = min_dxe;
+                sc->hmax = hmax;
+                sc->acc_min_dxe = fwd::kMinDxeStart;
+                sc->acc_hmax = 0ull;
+            }
+        }
+        return;
+    }
     if (STAGED)
         fwd::update_phase_staged<R, true, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
                                                  ntiles, cull, mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id,

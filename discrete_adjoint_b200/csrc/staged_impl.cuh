@@ -237,16 +237,22 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
     }
 }
 
+// No per-cell epilogue.
+struct NoEpilogue {
+    __device__ __forceinline__ void operator()(int, int) const {}
+};
+
 // Update phase (see update_phase) with the tile and its halo staged.  A listed tile's cells
-// recompute their activity from the staged depths; the segment flags follow it.
-template <class R, bool RECORD, bool BATCH = false>
+// recompute their activity from the staged depths; the segment flags follow it.  epi(t, i) runs
+// for every cell i < n of a listed tile t after its update (the reverse step's source adjoint).
+template <class R, bool RECORD, bool BATCH = false, class Epi = NoEpilogue>
 __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                                     const StateOut<R> &O, const R *kact, unsigned *active,
                                                     uint8_t *seg_clean, uint8_t *seg_wet, double *seg_vol,
                                                     uint8_t *seg_dirty, int ntiles, int cull, const MatConsts &mc0,
                                                     DevScalars *sc, R dt0, R ft, uint8_t *mask, int *tile_epoch,
                                                     uint8_t *seg_act, int rec_id, int *list, const InstArgs &ia,
-                                                    StageSmem<R> &S) {
+                                                    StageSmem<R> &S, const Epi &epi = Epi{}) {
     const int lane = threadIdx.x & 31;
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
@@ -302,6 +308,7 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 O.hv[i] = st[2];
                 vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
+                epi(t, i);
             }
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
             const unsigned act_bits = __ballot_sync(0xffffffffu, act);
