@@ -233,7 +233,7 @@ static int sync_scalars(da_ctx *ctx) {
     if (st) return st;
     if (ctx->hsc->err == DA_ERR_TIMEOUT) {
         // a multi-step launch gave up at a grid barrier: restart its arrival count
-        cudaMemsetAsync(&ctx->dsc->bar_count, 0, sizeof(unsigned), ctx->stream);
+        cudaMemsetAsync(&ctx->dsc->bar, 0, sizeof(unsigned), ctx->stream);  // the arrivals (low half)
         cudaStreamSynchronize(ctx->stream);
     }
     if (ctx->hsc->err) {

@@ -49,8 +49,8 @@ struct DevScalars {
     int pad;
     unsigned long long acc_alt_min_dxe;  // the multi-step kernel's second accumulator pair
     unsigned long long acc_alt_hmax;     // (odd steps of a launch), same start values
-    unsigned bar_count;   // grid barrier of the multi-step kernel: blocks arrived
-    unsigned bar_gen;     // and barrier generation
+    unsigned long long bar;  // grid barrier of the cooperative kernels: blocks arrived (low 32 bits),
+                             // generation (high 32 bits)
 };
 
 // Time-clipping targets (TimeProps::ndnextoutput / ndnextsave / ndmaxtime) and the

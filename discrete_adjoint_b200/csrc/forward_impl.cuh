@@ -429,8 +429,11 @@ namespace {
 // in registers; block 0 writes them and the last step's scalars at the end.  The
 // state buffers alternate as in single steps and are read with coherent loads (no read-only
 // cache: other blocks wrote them earlier in the same launch).
-// The barrier waits are bounded: after ~4 s a block raises DA_ERR_TIMEOUT and returns, and the
-// others give up at their next barrier.
+// The barrier is one 64-bit word (arrivals in the low half, generation in the high half): a block
+// arrives with one atomic add; the last one to arrive moves the word to the next generation with
+// zero arrivals in one more add; the others poll the word.  The waits are bounded: after ~4 s a
+// block raises DA_ERR_TIMEOUT and returns, and the others give up when they see the error (checked
+// on arrival and every 256 polls).
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -441,19 +444,20 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = &sc->bar_gen;
+        volatile unsigned long long *bar = &sc->bar;
         volatile int *err = &sc->err;
-        const unsigned g = *gen;
+        const int err0 = *err;  // in flight with the arrival
         __threadfence();
-        int good = 1;
-        if (atomicAdd(&sc->bar_count, 1u) == gridDim.x - 1) {
-            atomicExch(&sc->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&sc->bar_gen, 1u);
+        int good = err0 != DA_ERR_TIMEOUT;
+        const unsigned long long old = atomicAdd(&sc->bar, 1ull);
+        const unsigned gen = unsigned(old >> 32);
+        if (unsigned(old) == gridDim.x - 1) {
+            atomicAdd(&sc->bar, (1ull << 32) - gridDim.x);  // all arrived: next generation, no arrivals
         } else {
             const unsigned long long t0 = global_ns();
-            for (unsigned it = 0; *gen == g; ++it) {
-                if (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > 4000000000ull) {
+            for (unsigned it = 1; unsigned(*bar >> 32) == gen; ++it) {
+                if ((it & 255u) == 0 &&
+                    (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > 4000000000ull)) {
                     atomicCAS(&sc->err, 0, DA_ERR_TIMEOUT);
                     good = 0;
                     break;
@@ -462,7 +466,6 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc) {
             }
         }
         __threadfence();
-        if (*err == DA_ERR_TIMEOUT) good = 0;
         ok = good;
     }
     __syncthreads();

@@ -73,7 +73,7 @@ __global__ void k_init(DevScalars *sc, double time, long long iter) {
     sc->pad = 0;
     sc->acc_alt_min_dxe = __double_as_longlong(10000000.0);
     sc->acc_alt_hmax = 0ull;
-    sc->bar_count = sc->bar_gen = 0u;
+    sc->bar = 0ull;
 }
 
 // Boundary / two-neighbour flags and byte materials from the caller's tables; an index out of
