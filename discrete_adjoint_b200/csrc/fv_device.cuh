@@ -353,7 +353,9 @@ __device__ __forceinline__ bool sched_more(int round, int ntiles) {
 }
 
 // Needs blockDim.x == kTileCells; returns the number of tiles listed.
-__device__ __forceinline__ int compact_tiles(bool need, int tile, int *list) {
+// pa, pb (optional): two values per listed tile stored beside it (pa[k], pb[k] for list[k]).
+__device__ __forceinline__ int compact_tiles(bool need, int tile, int *list, int a = 0, int b2 = 0,
+                                             int *pa = nullptr, int *pb = nullptr) {
     __shared__ int warp_count[kTileCells / 32];
     __shared__ int total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -370,7 +372,14 @@ __device__ __forceinline__ int compact_tiles(bool need, int tile, int *list) {
         total = acc;
     }
     __syncthreads();
-    if (need) list[warp_count[warp] + __popc(b & ((1u << lane) - 1u))] = tile;
+    if (need) {
+        const int k = warp_count[warp] + __popc(b & ((1u << lane) - 1u));
+        list[k] = tile;
+        if (pa) {
+            pa[k] = a;
+            pb[k] = b2;
+        }
+    }
     __syncthreads();
     return total;
 }

@@ -123,23 +123,35 @@ __device__ __forceinline__ void stage_halo_list(int *dst, const int32_t *src, in
     for (int k = threadIdx.x; k < cnt; k += kTileCells) cp_async<4>(dst + k, src + k);
 }
 
+// The halo range of tile tq (or nothing past the last tile), loaded beside its flags by the scan
+// and kept with the tile by compact_tiles.
+__device__ __forceinline__ void halo_range(const HaloArgs &ha, int tq, int ntiles, int &off, int &cnt) {
+    off = 0;
+    cnt = 0;
+    if (tq < ntiles) {
+        off = ha.off[tq];
+        cnt = ha.off[tq + 1] - off;
+    }
+}
+
 // The listed tiles of a round, pipelined: fn(t, buffer, halo list) computes tile t from shared
-// memory.  Needs blockDim.x == kTileCells; every thread of the block calls it with the same cnt.
+// memory.  Needs blockDim.x == kTileCells; every thread of the block calls it with the same cnt;
+// S.hoff / S.hcnt hold the listed tiles' halo ranges (compact_tiles).  The first tile's halo
+// cells are read by the threads that copy them; later tiles' lists arrive two tiles ahead.
 template <class R, bool UPD, class F>
 __device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                              const R *kact, int cnt, const int *list, StageSmem<R> &S, F &&fn) {
-    if ((int)threadIdx.x < cnt) {
-        const int t = list[threadIdx.x];
-        const int o = ha.off[t];
-        S.hoff[threadIdx.x] = o;
-        S.hcnt[threadIdx.x] = ha.off[t + 1] - o;
+    {
+        const int t0 = list[0], hc = S.hcnt[0];
+        const int32_t *src = ha.idx + S.hoff[0];
+        const int i = t0 * kTileCells + (int)threadIdx.x;
+        if (i < m.n) stage_slot<R, UPD>(S.buf[0], threadIdx.x, i, true, m, U, kact);
+        for (int k = threadIdx.x; k < hc; k += kTileCells) {
+            const int e = src[k];
+            S.hidx[0][k] = e;
+            stage_slot<R, UPD>(S.buf[0], kTileCells + k, e, false, m, U, kact);
+        }
     }
-    __syncthreads();
-    stage_halo_list(S.hidx[0], ha.idx + S.hoff[0], S.hcnt[0]);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    stage_tile<R, UPD>(S.buf[0], list[0], S.hidx[0], S.hcnt[0], m, U, kact);
     if (cnt > 1) stage_halo_list(S.hidx[1], ha.idx + S.hoff[1], S.hcnt[1]);
     cp_async_commit();
     for (int q = 0; q < cnt; ++q) {
@@ -166,7 +178,9 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
     for (int round = 0; sched_more(round, ntiles); ++round) {
         const int tq = sched_tile(round);
         const bool need = tq < ntiles && (!cull || seg_flags(seg_wet, tq) != 0ull);
-        const int cnt = compact_tiles(need, tq, list);
+        int ho, hc;
+        halo_range(ha, tq, ntiles, ho, hc);
+        const int cnt = compact_tiles(need, tq, list, ho, hc, S.hoff, S.hcnt);
         if (cnt == 0) continue;
         staged_tiles<R, false>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *hidx) {
             const int inst = BATCH ? ia.tile_inst[t] : 0;
@@ -265,7 +279,9 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 need = (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
             }
         }
-        const int cnt = compact_tiles(need, tq, list);
+        int ho, hc;
+        halo_range(ha, tq, ntiles, ho, hc);
+        const int cnt = compact_tiles(need, tq, list, ho, hc, S.hoff, S.hcnt);
         if (cnt == 0) continue;
         staged_tiles<R, true>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *) {
             const int inst = BATCH ? ia.tile_inst[t] : 0;
