@@ -229,6 +229,18 @@ __device__ __forceinline__ bool update_cell(const V &v, const MeshArgs &m, int g
                                             R st[3]) {
     const R ki = prev[0] >= R(DA_TINY) ? v.k(c) : R(0);
     const R gz = v.gz(c);
+    // the cell's source coefficients, read before the fluxes so that the loads overlap them
+    R g0 = R(0), g1 = R(0), dg0 = R(0), dg1 = R(0), cv0 = R(0), cv1 = R(0);
+    int mat = 0;
+    if (prev[0] > R(DA_TINY)) {
+        g0 = grav<R>(m, 0, gi);
+        g1 = grav<R>(m, 1, gi);
+        dg0 = dgrav<R>(m, 0, gi);
+        dg1 = dgrav<R>(m, 1, gi);
+        cv0 = curvat<R>(m, 0, gi);
+        cv1 = curvat<R>(m, 1, gi);
+        mat = m.mat[gi];
+    }
     R div[2][3];
     flux_div<R>(v, c, bf, prev, div);
     R dtdx, dtdy;
@@ -263,14 +275,14 @@ __device__ __forceinline__ bool update_cell(const V &v, const MeshArgs &m, int g
         const R sg1 = tiny_sgn(tmp, ft);
         const R sg3 = tiny_sgn(vel1, ft);
         const R sin_int = R(mc.sin_int);
-        const R tan_bed = R(mc.tan_bed[m.mat[gi]]);
-        R s1 = grav<R>(m, 0, gi) * prev[0];
-        R s2 = sg0 * prev[0] * ki * (gz * s[3] + dgrav<R>(m, 1, gi) * prev[0]) * sin_int;
-        R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * curvat<R>(m, 0, gi), R(0.0)) * tan_bed;
+        const R tan_bed = R(mc.tan_bed[mat]);
+        R s1 = g0 * prev[0];
+        R s2 = sg0 * prev[0] * ki * (gz * s[3] + dg1 * prev[0]) * sin_int;
+        R s3 = sg2 * rmax(gz * prev[0] + vel0 * prev[1] * cv0, R(0.0)) * tan_bed;
         st[1] += dt * (s1 - s2 - s3);
-        s1 = grav<R>(m, 1, gi) * prev[0];
-        s2 = sg1 * prev[0] * ki * (gz * s[0] + dgrav<R>(m, 0, gi) * prev[0]) * sin_int;
-        s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * curvat<R>(m, 1, gi), R(0.0)) * tan_bed;
+        s1 = g1 * prev[0];
+        s2 = sg1 * prev[0] * ki * (gz * s[0] + dg0 * prev[0]) * sin_int;
+        s3 = sg3 * rmax(gz * prev[0] + vel1 * prev[2] * cv1, R(0.0)) * tan_bed;
         st[2] += dt * (s1 - s2 - s3);
     }
     return clamped;

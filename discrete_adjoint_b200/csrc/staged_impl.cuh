@@ -195,6 +195,16 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
                 uint8_t code = 0;
                 if (wet) {
                     const uint8_t bf = m.bflag[i];
+                    const int mat = m.mat[i];
+                    // the cell sizes, read before the neighbour marks so that the loads overlap them
+                    R dxm, dym;
+                    if constexpr (sizeof(R) == 8) {
+                        dxm = m.dx[i];
+                        dym = m.dy[i];
+                    } else {
+                        dxm = b.c0[c];
+                        dym = b.c1[c];
+                    }
                     StagedView<R> v{b};
                     load_slots(ha.nloc, i, v.nl);
                     // neighbours in other tiles: mark them for the tile listing of the update
@@ -216,7 +226,7 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
                         const R ui[3] = {h, b.hu[c], b.hv[c]};
                         R s[6];
                         cell_slopes<R>(v, c, bf, R(mc.gamma), ui, s);
-                        const R k = cell_kact<R>(mc, m.mat[i], h, ui[1], ui[2], s, &code);
+                        const R k = cell_kact<R>(mc, mat, h, ui[1], ui[2], s, &code);
                         kact[i] = k;
                         const R gz = b.gz[c];
                         const R vx = ui[1] / h, vy = ui[2] / h;
@@ -224,14 +234,6 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
                         const R evx = dabs(vx) + cc, evy = dabs(vy) + cc;
                         const R ev = evx > evy ? evx : evy;
                         if (ev > R(1000000000.)) raise_err(sc, DA_ERR_EIGEN);
-                        R dxm, dym;
-                        if constexpr (sizeof(R) == 8) {
-                            dxm = m.dx[i];
-                            dym = m.dy[i];
-                        } else {
-                            dxm = b.c0[c];
-                            dym = b.c1[c];
-                        }
                         const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
                         const unsigned long long hb = __double_as_longlong(double(h));
                         my_min = rb < my_min ? rb : my_min;
@@ -272,12 +274,11 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
         const int tq = sched_tile(round);
         bool need = false;
         if (tq < ntiles) {
-            need = !cull || seg_flags(seg_clean, tq) != kAllSegs;
-            if (!need) {
-                const uint4 *w4 = reinterpret_cast<const uint4 *>(active + (size_t)tq * (kTileCells / 32));
-                const uint4 a = w4[0], b = w4[1];
-                need = (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
-            }
+            // the clean flags and the bitmask words of the tile, loaded together
+            const unsigned long long cf = seg_flags(seg_clean, tq);
+            const uint4 *w4 = reinterpret_cast<const uint4 *>(active + (size_t)tq * (kTileCells / 32));
+            const uint4 a = w4[0], b = w4[1];
+            need = !cull || cf != kAllSegs || (a.x | a.y | a.z | a.w | b.x | b.y | b.z | b.w) != 0u;
         }
         int ho, hc;
         halo_range(ha, tq, ntiles, ho, hc);
