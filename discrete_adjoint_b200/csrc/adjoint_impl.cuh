@@ -64,33 +64,33 @@ struct SlopeD {
     R g_dp, g_dm, dxp, dxm;
 };
 
-template <class R>
-__device__ __forceinline__ void h_slope_deriv(const MeshArgs &m, const R *__restrict__ H, int i, uint8_t bf, R gamma,
-                                              R hi, SlopeD<R> out[2]) {
+// v: where the depths, neighbours and centres / sizes come from (global arrays, or a tile staged
+// in shared memory with i the cell's slot); the arithmetic is the same either way.
+template <class R, class V>
+__device__ __forceinline__ void h_slope_deriv(const V &v, int i, uint8_t bf, R gamma, R hi, SlopeD<R> out[2]) {
 #pragma unroll
     for (int dir = 0; dir < 2; ++dir) {
-        const int ep = m.nbr[(size_t)dir * m.n + i];
-        const int em = m.nbr[(size_t)(dir + 2) * m.n + i];
+        const int ep = v.nb(dir, i);
+        const int em = v.nb(dir + 2, i);
         const bool two_p = bf & (0x10 << dir), two_m = bf & (0x10 << (dir + 2));
         R dxp, dxm, dp, dm;
         if constexpr (sizeof(R) == 8) {
-            const double *co = dir == 0 ? m.x : m.y;
-            dxp = co[ep] - co[i];
-            dxm = co[i] - co[em];
-            dp = (H[ep] - hi) / dxp;
-            if (two_p) dp = .5 * (dp + (H[m.nbr[(size_t)(dir + 4) * m.n + i]] - hi) / dxp);
-            dm = (hi - H[em]) / dxm;
-            if (two_m) dm = .5 * (dm + (hi - H[m.nbr[(size_t)(dir + 6) * m.n + i]]) / dxm);
+            const double ci = v.coord(dir, i);
+            dxp = v.coord(dir, ep) - ci;
+            dxm = ci - v.coord(dir, em);
+            dp = (v.h(ep) - hi) / dxp;
+            if (two_p) dp = .5 * (dp + (v.h(v.nb(dir + 4, i)) - hi) / dxp);
+            dm = (hi - v.h(em)) / dxm;
+            if (two_m) dm = .5 * (dm + (hi - v.h(v.nb(dir + 6, i))) / dxm);
         } else {
-            const float *sz = dir == 0 ? m.fdx : m.fdy;
-            const float si = sz[i];
-            dxp = 0.5f * (sz[ep] + si);
-            dxm = 0.5f * (sz[em] + si);
+            const float si = v.size(dir, i);
+            dxp = 0.5f * (v.size(dir, ep) + si);
+            dxm = 0.5f * (v.size(dir, em) + si);
             const float ip = 1.0f / dxp, im = 1.0f / dxm;
-            dp = (H[ep] - hi) * ip;
-            if (two_p) dp = 0.5f * (dp + (H[m.nbr[(size_t)(dir + 4) * m.n + i]] - hi) * ip);
-            dm = (hi - H[em]) * im;
-            if (two_m) dm = 0.5f * (dm + (hi - H[m.nbr[(size_t)(dir + 6) * m.n + i]]) * im);
+            dp = (v.h(ep) - hi) * ip;
+            if (two_p) dp = 0.5f * (dp + (v.h(v.nb(dir + 4, i)) - hi) * ip);
+            dm = (hi - v.h(em)) * im;
+            if (two_m) dm = 0.5f * (dm + (hi - v.h(v.nb(dir + 6, i))) * im);
         }
         const R dc = (dp * dxm + dm * dxp) / (dxm + dxp);
         const R fac = R(.5) * (c_sgn(dp) + c_sgn(dm));
@@ -280,27 +280,24 @@ __device__ __forceinline__ InstTables inst_tables(const AdjArgs &aa, const InstA
 // adjoint of its sources (A), the slope coefficients it passes to its neighbours (B) and its
 // parameter sensitivities, from its own recorded branches (mask) and lambda^{n+1}.  Reads U^n
 // at the cell and its neighbours; writes only the cell's own entries.
-template <class R>
-__device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
-                                             const MatConsts &mc, const AdjArgs &aa, const InstTables &it, R dt,
-                                             R ft, int i) {
+// adj_src_wet: wet cell i with U^n = prev, g_z, branch byte mi and boundary flags bf; v and vi
+// give the neighbour values of the slopes (global arrays with vi = i, or the tile staged in
+// shared memory with vi the cell's slot).
+template <class R, class V>
+__device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &m, const R prev[3], R gz,
+                                            uint8_t mi, uint8_t bf, const StateRef<R> &Lnext, const MatConsts &mc,
+                                            const AdjArgs &aa, const InstTables &it, R dt, R ft, int i) {
     double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
-    const R h_i = U.h[i];
-    // A and B exist for wet cells only; k_adj_gather reads them only there
-    if (!(h_i > R(DA_TINY))) return;
-    const R prev[3] = {h_i, U.hu[i], U.hv[i]};
     {
         R le[3];
-        const uint8_t mi = aa.mask[i];
         lam_eff<R>(Lnext, mi, i, le);
         const R nu_u = dt * le[1], nu_v = dt * le[2];
         if (nu_u != R(0) || nu_v != R(0)) {
-            const uint8_t bf = m.bflag[i];
             const int mat = m.mat[i];
             const uint8_t code = mi & 3;
             const R k = kact_of<R>(mc, mat, code);
             R s[6];
-            cell_slopes<R>(global_view<R>(m, U, (const R *)nullptr), i, bf, R(mc.gamma), prev, s);
+            cell_slopes<R>(v, vi, bf, R(mc.gamma), prev, s);
             R vel0, vel1, h_inv;
             if constexpr (sizeof(R) == 8) {
                 vel0 = prev[1] / prev[0];
@@ -316,7 +313,7 @@ __device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R
             const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
             const R sg3 = tiny_sgn(vel1, ft);
             const R h = prev[0];
-            const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i), gz = grav<R>(m, 2, i);
+            const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i);
             const R dgx = dgrav<R>(m, 0, i), dgy = dgrav<R>(m, 1, i);
             const R kx = curvat<R>(m, 0, i), ky = curvat<R>(m, 1, i);
             const R sin_int = R(mc.sin_int), tan_bed = R(mc.tan_bed[mat]);
@@ -330,7 +327,7 @@ __device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R
             // the limited depth slopes of this cell (zero on boundary cells)
             if (!(bf & 0x0F)) {
                 SlopeD<R> sd[2];
-                h_slope_deriv<R>(m, U.h, i, bf, R(mc.gamma), h, sd);
+                h_slope_deriv<R>(v, vi, bf, R(mc.gamma), h, sd);
                 const R cx = -nu_v * sg1 * h * k * gz * sin_int;  // on d h / dx
                 const R cy = -nu_u * sg0 * h * k * gz * sin_int;  // on d h / dy
                 A[0] += double(cx * (-sd[0].g_dp / sd[0].dxp + sd[0].g_dm / sd[0].dxm) +
@@ -355,6 +352,19 @@ __device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R
     aa.A[(size_t)2 * m.n + i] = A[2];
 #pragma unroll
     for (int s = 0; s < 4; ++s) aa.B[(size_t)s * m.n + i] = B[s];
+}
+
+// adj_src_cell: cell i of U^n from global memory (nothing for a dry cell).
+template <class R>
+__device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R> &U, const StateRef<R> &Lnext,
+                                             const MatConsts &mc, const AdjArgs &aa, const InstTables &it, R dt,
+                                             R ft, int i) {
+    const R h_i = U.h[i];
+    // A and B exist for wet cells only; k_adj_gather reads them only there
+    if (!(h_i > R(DA_TINY))) return;
+    const R prev[3] = {h_i, U.hu[i], U.hv[i]};
+    adj_src_wet<R>(global_view<R>(m, U, (const R *)nullptr), i, m, prev, grav<R>(m, 2, i), aa.mask[i], m.bflag[i],
+                   Lnext, mc, aa, it, dt, ft, i);
 }
 
 template <class R, bool BATCH = false>
@@ -391,21 +401,35 @@ __global__ void __launch_bounds__(kBlock) k_adj_src(MeshArgs m, StateRef<R> U, S
 // Flux weight of cell c for its side s: -dt/dx on a plus side, +dt/dx on a minus side, halved
 // when the side carries two finer neighbours, zero when c's direction has an outflow side.
 template <class R>
-__device__ __forceinline__ R side_weight(const MeshArgs &m, int c, uint8_t bf, int s, R dt) {
+__device__ __forceinline__ bool side_outflow(uint8_t bf, int s) {
     const int d = s & 1;
-    if (bf & ((1 << d) | (1 << (d + 2)))) return R(0);
-    const R dxc = d == 0 ? cell_dx<R>(m, c) : cell_dy<R>(m, c);
+    return (bf & ((1 << d) | (1 << (d + 2)))) != 0;
+}
+// the weight of a side that is not an outflow direction, with dxc the cell's size across it
+template <class R>
+__device__ __forceinline__ R side_weight_of(R dxc, uint8_t bf, int s, R dt) {
     R w = (s < 2 ? -dt : dt) / dxc;
     if (bf & (0x10 << s)) w = R(0.5) * w;
     return w;
 }
+template <class R>
+__device__ __forceinline__ R side_weight(const MeshArgs &m, int c, uint8_t bf, int s, R dt) {
+    if (side_outflow<R>(bf, s)) return R(0);
+    const int d = s & 1;
+    return side_weight_of<R>(d == 0 ? cell_dx<R>(m, c) : cell_dy<R>(m, c), bf, s, dt);
+}
 
+// A side from the cell's values: k act/pass from its material and branch code where it is wet.
+template <class R>
+__device__ __forceinline__ void side_of(const MatConsts &mc, int dir, R h, R hu, R hv, R gz, int mat, uint8_t mk,
+                                        Side<R> &s) {
+    const R k = h >= R(DA_TINY) ? kact_of<R>(mc, mat, mk & 3) : R(0);
+    make_side<R>(dir, h, hu, hv, k, gz, s);
+}
 template <class R>
 __device__ __forceinline__ void load_side(const MeshArgs &m, const StateRef<R> &U, const MatConsts &mc, uint8_t mk,
                                           int c, int dir, Side<R> &s) {
-    const R h = U.h[c];
-    const R k = h >= R(DA_TINY) ? kact_of<R>(mc, m.mat[c], mk & 3) : R(0);
-    make_side<R>(dir, h, U.hu[c], U.hv[c], k, grav<R>(m, 2, c), s);
+    side_of<R>(mc, dir, U.h[c], U.hu[c], U.hv[c], grav<R>(m, 2, c), m.mat[c], mk, s);
 }
 
 // ---------------------------------------------------------------------- k_adj_gather

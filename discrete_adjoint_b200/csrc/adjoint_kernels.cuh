@@ -1,7 +1,10 @@
 // Launchers of the adjoint kernels for one precision (included by adjoint_fp64.cu / _fp32.cu).
 #pragma once
+#include <algorithm>
+
 #include "adjoint_impl.cuh"
 #include "forward_impl.cuh"
+#include "adjoint_staged.cuh"
 
 namespace da {
 namespace adj {
@@ -125,21 +128,24 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     }
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
     if (STAGED && !SEED) {
-        // the source adjoint of each wet cell right after its update (its own branches and
-        // lambda^{n+1}, U^n around it: nothing another cell writes in this phase), so the reverse
-        // step needs no source phase of its own
+        // the source adjoint of each wet cell right after its update, from the tile and halo
+        // staged for it (its own branches and lambda^{n+1}, U^n around it: nothing another cell
+        // writes in this phase), so the reverse step needs no source phase of its own
         const R dtr = R(dt);
-        auto src = [&](int t, int i) {
+        auto src = [&](int t, int i, const fwd::StagedView<R> &v, int c, const R *prev, uint8_t bf, uint8_t code,
+                       R gz) {
+            if (!(prev[0] > R(DA_TINY))) return;  // A and B exist for wet cells only
             const int inst = BATCH ? ia.tile_inst[t] : 0;
             const MatConsts &mci = BATCH ? ia.mcs[inst] : mc;
             const R dti = BATCH ? R(ia.dt[inst]) : dtr;
-            adj_src_cell<R>(m, U, Ln, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ftr, i);
+            adj_src_wet<R>(v, c, m, prev, gz, code, bf, Ln, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ftr, i);
         };
         fwd::update_phase_staged<R, true, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
                                                  ntiles, cull, mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id,
                                                  list, ia, stg, src);
         if (!fwd::grid_sync(sc)) return;
-        adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
+        adj_gather_phase_staged<R, BATCH>(m, ha, U, Ln, Lo, mc, aa, R(dt), list, ia,
+                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem));
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             sc->iter = iter + 1;
             sc->frict_tiny = ft;
@@ -168,7 +174,11 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     }
     adj_src_phase<R, BATCH>(m, U, Ln, mc, aa, R(dt), ftr, list, ia);
     if (!fwd::grid_sync(sc)) return;
-    adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
+    if (STAGED)
+        adj_gather_phase_staged<R, BATCH>(m, ha, U, Ln, Lo, mc, aa, R(dt), list, ia,
+                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem));
+    else
+        adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->iter = iter + 1;
         sc->frict_tiny = ft;
@@ -209,7 +219,8 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     const int occ3 = ctx->p.blocks_per_sm == 3;
     const bool staged = fwd::staged_ok(ctx);
     const void *kern = youturn_kernel<R>(batch, seed, occ3, staged);
-    const size_t smem = staged ? fwd::stage_smem_bytes<R>() : 0;
+    // the staged phases and the staged gather use the same dynamic shared memory in turn
+    const size_t smem = staged ? std::max(fwd::stage_smem_bytes<R>(), gather_smem_bytes<R>()) : 0;
     int &cap_ref = ctx->coop_cap_yt[pi + 2 * batch + 4 * seed + 8 * occ3 + 16 * staged];
     if (cap_ref <= 0) {
         int st = DA_OK;

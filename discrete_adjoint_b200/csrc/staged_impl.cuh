@@ -255,12 +255,15 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
 
 // No per-cell epilogue.
 struct NoEpilogue {
-    __device__ __forceinline__ void operator()(int, int) const {}
+    template <class... A>
+    __device__ __forceinline__ void operator()(A &&...) const {}
 };
 
 // Update phase (see update_phase) with the tile and its halo staged.  A listed tile's cells
-// recompute their activity from the staged depths; the segment flags follow it.  epi(t, i) runs
-// for every cell i < n of a listed tile t after its update (the reverse step's source adjoint).
+// recompute their activity from the staged depths; the segment flags follow it.
+// epi(t, i, v, c, prev, bf, code, gz) runs for every cell i < n of a listed tile t after its
+// update (the reverse step's source adjoint), with the staged view v of the cell (slot c), its
+// U^n, boundary flags, recorded branch byte and g_z.
 template <class R, bool RECORD, bool BATCH = false, class Epi = NoEpilogue>
 __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                                     const StateOut<R> &O, const R *kact, unsigned *active,
@@ -317,15 +320,16 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 R st[3] = {prev[0], prev[1], prev[2]};
                 bool clamped = false;
                 if (act) clamped = update_cell<R>(v, m, i, c, bf, mc, dt, ft, prev, dxc, dyc, st);
-                if (RECORD)
-                    mask[i] = uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0));
+                const uint8_t code =
+                    RECORD ? uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0)) : 0;
+                if (RECORD) mask[i] = code;
                 if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
                 O.h[i] = st[0];
                 O.hu[i] = st[1];
                 O.hv[i] = st[2];
                 vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
-                epi(t, i);
+                epi(t, i, v, c, prev, bf, code, b.gz[c]);
             }
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
             const unsigned act_bits = __ballot_sync(0xffffffffu, act);
