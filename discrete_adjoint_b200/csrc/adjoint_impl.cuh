@@ -280,20 +280,21 @@ __device__ __forceinline__ InstTables inst_tables(const AdjArgs &aa, const InstA
 // adjoint of its sources (A), the slope coefficients it passes to its neighbours (B) and its
 // parameter sensitivities, from its own recorded branches (mask) and lambda^{n+1}.  Reads U^n
 // at the cell and its neighbours; writes only the cell's own entries.
-// adj_src_wet: wet cell i with U^n = prev, g_z, branch byte mi and boundary flags bf; v and vi
-// give the neighbour values of the slopes (global arrays with vi = i, or the tile staged in
-// shared memory with vi the cell's slot).
+// adj_src_wet: wet cell i with U^n = prev, g_z, branch byte mi, boundary flags bf, lambda^{n+1}
+// = lnext and source coefficients cs; v and vi give the neighbour values of the slopes (global
+// arrays with vi = i, or the tile staged in shared memory with vi the cell's slot).
 template <class R, class V>
 __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &m, const R prev[3], R gz,
-                                            uint8_t mi, uint8_t bf, const StateRef<R> &Lnext, const MatConsts &mc,
-                                            const AdjArgs &aa, const InstTables &it, R dt, R ft, int i) {
+                                            uint8_t mi, uint8_t bf, const R lnext[3], const CellSrc<R> &cs,
+                                            const MatConsts &mc, const AdjArgs &aa, const InstTables &it, R dt, R ft,
+                                            int i) {
     double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
     {
-        R le[3];
-        lam_eff<R>(Lnext, mi, i, le);
+        // lambda_eff: the depth row dropped where the forward step clamped h at zero
+        const R le[3] = {(mi & 4) ? R(0) : lnext[0], lnext[1], lnext[2]};
         const R nu_u = dt * le[1], nu_v = dt * le[2];
         if (nu_u != R(0) || nu_v != R(0)) {
-            const int mat = m.mat[i];
+            const int mat = cs.mat;
             const uint8_t code = mi & 3;
             const R k = kact_of<R>(mc, mat, code);
             R s[6];
@@ -313,9 +314,9 @@ __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &
             const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
             const R sg3 = tiny_sgn(vel1, ft);
             const R h = prev[0];
-            const R gx = grav<R>(m, 0, i), gy = grav<R>(m, 1, i);
-            const R dgx = dgrav<R>(m, 0, i), dgy = dgrav<R>(m, 1, i);
-            const R kx = curvat<R>(m, 0, i), ky = curvat<R>(m, 1, i);
+            const R gx = cs.g[0], gy = cs.g[1];
+            const R dgx = cs.dg[0], dgy = cs.dg[1];
+            const R kx = cs.cv[0], ky = cs.cv[1];
             const R sin_int = R(mc.sin_int), tan_bed = R(mc.tan_bed[mat]);
             const R Px = gz * h + vel0 * prev[1] * kx, Py = gz * h + vel1 * prev[2] * ky;
             const R px = Px > R(0) ? R(1) : R(0), py = Py > R(0) ? R(1) : R(0);
@@ -363,8 +364,9 @@ __device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R
     // A and B exist for wet cells only; k_adj_gather reads them only there
     if (!(h_i > R(DA_TINY))) return;
     const R prev[3] = {h_i, U.hu[i], U.hv[i]};
+    const R lnext[3] = {Lnext.h[i], Lnext.hu[i], Lnext.hv[i]};
     adj_src_wet<R>(global_view<R>(m, U, (const R *)nullptr), i, m, prev, grav<R>(m, 2, i), aa.mask[i], m.bflag[i],
-                   Lnext, mc, aa, it, dt, ft, i);
+                   lnext, cell_src<R>(m, i), mc, aa, it, dt, ft, i);
 }
 
 template <class R, bool BATCH = false>

@@ -131,15 +131,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
         // the source adjoint of each wet cell right after its update, from the tile and halo
         // staged for it (its own branches and lambda^{n+1}, U^n around it: nothing another cell
         // writes in this phase), so the reverse step needs no source phase of its own
-        const R dtr = R(dt);
-        auto src = [&](int t, int i, const fwd::StagedView<R> &v, int c, const R *prev, uint8_t bf, uint8_t code,
-                       R gz) {
-            if (!(prev[0] > R(DA_TINY))) return;  // A and B exist for wet cells only
-            const int inst = BATCH ? ia.tile_inst[t] : 0;
-            const MatConsts &mci = BATCH ? ia.mcs[inst] : mc;
-            const R dti = BATCH ? R(ia.dt[inst]) : dtr;
-            adj_src_wet<R>(v, c, m, prev, gz, code, bf, Ln, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ftr, i);
-        };
+        const SrcEpilogue<R, BATCH> src{m, Ln, mc, aa, ia, R(dt), ftr};
         fwd::update_phase_staged<R, true, BATCH>(m, ha, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty,
                                                  ntiles, cull, mc, sc, R(dt), ftr, mask, tile_epoch, seg_act, rec_id,
                                                  list, ia, stg, src);

@@ -242,6 +242,39 @@ __device__ __forceinline__ void adj_gather_phase_staged(const MeshArgs &m, const
     }
 }
 
+// The reverse step's source adjoint as the epilogue of its staged update phase: lambda^{n+1} of
+// a wet cell is loaded before its update, the rest comes from the update's staged tile.
+template <class R, bool BATCH>
+struct SrcEpilogue {
+    const MeshArgs &m;
+    const StateRef<R> &Ln;
+    const MatConsts &mc;
+    const AdjArgs &aa;
+    const InstArgs &ia;
+    R dt, ft;
+    struct Pre {
+        R l[3];
+    };
+    __device__ __forceinline__ Pre pre(int i, bool wet) const {
+        Pre p{};
+        if (wet) {
+            p.l[0] = Ln.h[i];
+            p.l[1] = Ln.hu[i];
+            p.l[2] = Ln.hv[i];
+        }
+        return p;
+    }
+    __device__ __forceinline__ void operator()(int t, int i, const fwd::StagedView<R> &v, int c, const R *prev,
+                                               uint8_t bf, uint8_t code, R gz, const CellSrc<R> &cs,
+                                               const Pre &p) const {
+        if (!(prev[0] > R(DA_TINY))) return;  // A and B exist for wet cells only
+        const int inst = BATCH ? ia.tile_inst[t] : 0;
+        const MatConsts &mci = BATCH ? ia.mcs[inst] : mc;
+        const R dti = BATCH ? R(ia.dt[inst]) : dt;
+        adj_src_wet<R>(v, c, m, prev, gz, code, bf, p.l, cs, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ft, i);
+    }
+};
+
 }  // namespace
 }  // namespace adj
 }  // namespace da

@@ -467,8 +467,11 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
         !m->curvature || !m->material)
         return set_error(ctx, DA_ERR_INVALID, "da_upload_mesh: missing array");
     const int n = m->n_cells;
-    // host-side validation: neighbour indices in range, materials in range
-    std::vector<uint8_t> bflag(n), mat(n);
+    // host-side validation: neighbour indices in range, materials in range.  The flag and
+    // material bytes are padded with zeros to whole tiles (the staged phases copy a tile's bytes in
+    // 16-byte pieces).
+    const size_t npad = ((size_t)n + kTileCells - 1) / kTileCells * kTileCells;
+    std::vector<uint8_t> bflag(npad, 0), mat(npad, 0);
     for (int i = 0; i < n; ++i) {
         uint8_t b = 0;
         for (int s = 0; s < 4; ++s) {
@@ -499,8 +502,8 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     d.epoch = epoch;
     const bool fp64 = ctx->p.precision == DA_PREC_FP64;
     if (!st) st = upload(ctx, &d.nbr, m->nbr, (size_t)8 * n);
-    if (!st) st = upload(ctx, &d.bflag, bflag.data(), (size_t)n);
-    if (!st) st = upload(ctx, &d.mat, mat.data(), (size_t)n);
+    if (!st) st = upload(ctx, &d.bflag, bflag.data(), npad);
+    if (!st) st = upload(ctx, &d.mat, mat.data(), npad);
     if (!st) st = build_halo(ctx, m->nbr, n);
     // centres: the FP64 step uses them; both precisions test functional boxes with them
     if (!st) st = upload(ctx, &d.x, m->x, (size_t)n);

@@ -116,8 +116,8 @@ struct DevMesh {
     int32_t n = 0;
     int32_t epoch = -1;
     int32_t *nbr = nullptr;         // [8][n]
-    uint8_t *mat = nullptr;         // [n]
-    uint8_t *bflag = nullptr;       // [n] bit s: side s is a domain boundary; bit 4+s: side s has 2 neighbours
+    uint8_t *mat = nullptr;         // [n], zero-padded to whole tiles
+    uint8_t *bflag = nullptr;       // [n], zero-padded to whole tiles; bit s: side s is a domain boundary; bit 4+s: side s has 2 neighbours
     double *x = nullptr, *y = nullptr, *dx = nullptr, *dy = nullptr;
     double *g = nullptr;            // [3][n]
     double *dg = nullptr;           // [2][n]

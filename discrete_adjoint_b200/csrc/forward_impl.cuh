@@ -222,25 +222,14 @@ __device__ __forceinline__ void flux_div(const V &v, int i, uint8_t bf, const R 
 }
 
 // Full corrector update of one active cell (fluxes + sources), reference order.  c is the cell in
-// the view, gi its global index (the per-cell source coefficients are read from the mesh arrays).
+// the view; cs its source coefficients (read only for a wet cell, h > GEOFLOW_TINY).
 template <class R, class V>
-__device__ __forceinline__ bool update_cell(const V &v, const MeshArgs &m, int gi, int c, uint8_t bf,
-                                            const MatConsts &mc, R dt, R ft, const R prev[3], R dxc, R dyc,
-                                            R st[3]) {
+__device__ __forceinline__ bool update_cell(const V &v, int c, uint8_t bf, const CellSrc<R> &cs, const MatConsts &mc,
+                                            R dt, R ft, const R prev[3], R dxc, R dyc, R st[3]) {
     const R ki = prev[0] >= R(DA_TINY) ? v.k(c) : R(0);
     const R gz = v.gz(c);
-    // the cell's source coefficients, read before the fluxes so that the loads overlap them
-    R g0 = R(0), g1 = R(0), dg0 = R(0), dg1 = R(0), cv0 = R(0), cv1 = R(0);
-    int mat = 0;
-    if (prev[0] > R(DA_TINY)) {
-        g0 = grav<R>(m, 0, gi);
-        g1 = grav<R>(m, 1, gi);
-        dg0 = dgrav<R>(m, 0, gi);
-        dg1 = dgrav<R>(m, 1, gi);
-        cv0 = curvat<R>(m, 0, gi);
-        cv1 = curvat<R>(m, 1, gi);
-        mat = m.mat[gi];
-    }
+    const R g0 = cs.g[0], g1 = cs.g[1], dg0 = cs.dg[0], dg1 = cs.dg[1], cv0 = cs.cv[0], cv1 = cs.cv[1];
+    const int mat = cs.mat;
     R div[2][3];
     flux_div<R>(v, c, bf, prev, div);
     R dtdx, dtdy;
@@ -351,9 +340,11 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
                 R st[3] = {prev[0], prev[1], prev[2]};
                 const bool act = word & (1u << lane);
                 bool clamped = false;
-                if (act)
-                    clamped = update_cell<R>(global_view<R>(m, U, kact), m, i, i, m.bflag[i], mc, dt, ft, prev, dxc,
-                                             dyc, st);
+                if (act) {
+                    const CellSrc<R> cs = prev[0] > R(DA_TINY) ? cell_src<R>(m, i) : CellSrc<R>{};
+                    clamped = update_cell<R>(global_view<R>(m, U, kact), i, m.bflag[i], cs, mc, dt, ft, prev, dxc, dyc,
+                                             st);
+                }
                 if (RECORD)
                     mask[i] = uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0));
                 if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);

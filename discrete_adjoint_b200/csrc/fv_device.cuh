@@ -104,6 +104,26 @@ __device__ __forceinline__ R curvat(const MeshArgs &m, int c, int i) {
     if constexpr (sizeof(R) == 8) return m.curv[(size_t)c * m.n + i]; else return m.fcurv[(size_t)c * m.n + i];
 }
 
+// A cell's source coefficients: g_x, g_y, the two stored gravity derivatives, the two
+// curvatures, and its material.
+template <class R>
+struct CellSrc {
+    R g[2], dg[2], cv[2];
+    int mat;
+};
+template <class R>
+__device__ __forceinline__ CellSrc<R> cell_src(const MeshArgs &m, int i) {
+    CellSrc<R> s;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        s.g[q] = grav<R>(m, q, i);
+        s.dg[q] = dgrav<R>(m, q, i);
+        s.cv[q] = curvat<R>(m, q, i);
+    }
+    s.mat = m.mat[i];
+    return s;
+}
+
 // What the per-cell numerics read about a cell and its neighbours goes through a view: nb(s, c)
 // the cell across neighbour entry s of cell c, and the values of a cell.  GlobalView reads the
 // mesh table and the global arrays (c, e = cell indices); the step kernels' staged view reads a

@@ -24,6 +24,12 @@ constexpr int kSlots = kTileCells + kHaloMax;  // slot s < 256: cell 256 t + s; 
 
 template <class R>
 struct StageBuf {
+    // the tile's own cells
+    uint4 nl[kTileCells];                      // neighbour slots (8 x int16)
+    uint8_t bf[kTileCells], mat[kTileCells];   // boundary flags, material
+    R sz[2][sizeof(R) == 8 ? kTileCells : 1];  // FP64: dx, dy (FP32: c0, c1 below)
+    R src[6][kTileCells];                      // update phase: g_x, g_y, the gravity derivatives, curvatures
+    // every slot
     R h[kSlots], hu[kSlots], hv[kSlots];
     R k[kSlots];   // k act/pass (update phase)
     R gz[kSlots];  // g_z
@@ -110,12 +116,70 @@ __device__ __forceinline__ void stage_slot(StageBuf<R> &b, int s, int e, bool ow
     }
 }
 
+// What only the tile's own cells need: neighbour slots, sizes (FP64), source coefficients (UPD),
+// and the tile's flag and material bytes in 16-byte pieces (the byte arrays are padded to tiles).
+template <class R, bool UPD>
+__device__ __forceinline__ void stage_own(StageBuf<R> &b, int t, const MeshArgs &m, const int16_t *nloc) {
+    constexpr int B = sizeof(R);
+    const int c = threadIdx.x;
+    const int i = t * kTileCells + c;
+    if (i < m.n) {
+        cp_async<16>(&b.nl[c], nloc + (size_t)i * 8);
+        if constexpr (sizeof(R) == 8) {
+            cp_async<8>(&b.sz[0][c], m.dx + i);
+            cp_async<8>(&b.sz[1][c], m.dy + i);
+        }
+        if (UPD) {
+            const R *g = sizeof(R) == 8 ? (const R *)m.g : (const R *)m.fg;
+            const R *dg = sizeof(R) == 8 ? (const R *)m.dg : (const R *)m.fdg;
+            const R *cv = sizeof(R) == 8 ? (const R *)m.curv : (const R *)m.fcurv;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                cp_async<B>(&b.src[q][c], g + (size_t)q * m.n + i);
+                cp_async<B>(&b.src[2 + q][c], dg + (size_t)q * m.n + i);
+                cp_async<B>(&b.src[4 + q][c], cv + (size_t)q * m.n + i);
+            }
+        }
+    }
+    if (c < kTileCells / 16)
+        cp_async<16>(&b.bf[16 * c], m.bflag + (size_t)t * kTileCells + 16 * c);
+    else if (c < kTileCells / 8)
+        cp_async<16>(&b.mat[16 * (c - kTileCells / 16)], m.mat + (size_t)t * kTileCells + 16 * (c - kTileCells / 16));
+}
+
+// The staged source coefficients of own cell c.
+template <class R>
+__device__ __forceinline__ CellSrc<R> staged_src(const StageBuf<R> &b, int c) {
+    CellSrc<R> s;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        s.g[q] = b.src[q][c];
+        s.dg[q] = b.src[2 + q][c];
+        s.cv[q] = b.src[4 + q][c];
+    }
+    s.mat = b.mat[c];
+    return s;
+}
+
+// The eight neighbour slots of own cell c from the staged table.
+template <class R>
+__device__ __forceinline__ void staged_slots(const StageBuf<R> &b, int c, int nl[8]) {
+    const uint4 w = b.nl[c];
+    const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        nl[2 * q] = int(int16_t(u[q] & 0xffffu));
+        nl[2 * q + 1] = int(int16_t(u[q] >> 16));
+    }
+}
+
 // Tile t's own cells and its halo (halo list already in shared memory) into buffer b.
 template <class R, bool UPD>
 __device__ __forceinline__ void stage_tile(StageBuf<R> &b, int t, const int *hidx, int hcnt, const MeshArgs &m,
-                                           const StateRef<R> &U, const R *kact) {
+                                           const StateRef<R> &U, const R *kact, const int16_t *nloc) {
     const int i = t * kTileCells + (int)threadIdx.x;
     if (i < m.n) stage_slot<R, UPD>(b, threadIdx.x, i, true, m, U, kact);
+    stage_own<R, UPD>(b, t, m, nloc);
     for (int k = threadIdx.x; k < hcnt; k += kTileCells) stage_slot<R, UPD>(b, kTileCells + k, hidx[k], false, m, U, kact);
 }
 
@@ -146,6 +210,7 @@ __device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &
         const int32_t *src = ha.idx + S.hoff[0];
         const int i = t0 * kTileCells + (int)threadIdx.x;
         if (i < m.n) stage_slot<R, UPD>(S.buf[0], threadIdx.x, i, true, m, U, kact);
+        stage_own<R, UPD>(S.buf[0], t0, m, ha.nloc);
         for (int k = threadIdx.x; k < hc; k += kTileCells) {
             const int e = src[k];
             S.hidx[0][k] = e;
@@ -159,7 +224,8 @@ __device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &
         cp_async_wait_all();
         __syncthreads();
         if (q + 1 < cnt) {
-            stage_tile<R, UPD>(S.buf[(q + 1) & 1], list[q + 1], S.hidx[(q + 1) % 3], S.hcnt[q + 1], m, U, kact);
+            stage_tile<R, UPD>(S.buf[(q + 1) & 1], list[q + 1], S.hidx[(q + 1) % 3], S.hcnt[q + 1], m, U, kact,
+                               ha.nloc);
             if (q + 2 < cnt) stage_halo_list(S.hidx[(q + 2) % 3], ha.idx + S.hoff[q + 2], S.hcnt[q + 2]);
         }
         cp_async_commit();
@@ -194,19 +260,18 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
                 wet = h >= R(DA_TINY);
                 uint8_t code = 0;
                 if (wet) {
-                    const uint8_t bf = m.bflag[i];
-                    const int mat = m.mat[i];
-                    // the cell sizes, read before the neighbour marks so that the loads overlap them
+                    const uint8_t bf = b.bf[c];
+                    const int mat = b.mat[c];
                     R dxm, dym;
                     if constexpr (sizeof(R) == 8) {
-                        dxm = m.dx[i];
-                        dym = m.dy[i];
+                        dxm = b.sz[0][c];
+                        dym = b.sz[1][c];
                     } else {
                         dxm = b.c0[c];
                         dym = b.c1[c];
                     }
                     StagedView<R> v{b};
-                    load_slots(ha.nloc, i, v.nl);
+                    staged_slots(b, c, v.nl);
                     // neighbours in other tiles: mark them for the tile listing of the update
 #pragma unroll
                     for (int s = 0; s < 4; ++s) {
@@ -255,15 +320,18 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
 
 // No per-cell epilogue.
 struct NoEpilogue {
+    struct Pre {};
+    __device__ __forceinline__ Pre pre(int, bool) const { return Pre{}; }
     template <class... A>
     __device__ __forceinline__ void operator()(A &&...) const {}
 };
 
 // Update phase (see update_phase) with the tile and its halo staged.  A listed tile's cells
 // recompute their activity from the staged depths; the segment flags follow it.
-// epi(t, i, v, c, prev, bf, code, gz) runs for every cell i < n of a listed tile t after its
-// update (the reverse step's source adjoint), with the staged view v of the cell (slot c), its
-// U^n, boundary flags, recorded branch byte and g_z.
+// epi(t, i, v, c, prev, bf, code, gz, cs, pre) runs for every cell i < n of a listed tile t after
+// its update (the reverse step's source adjoint), with the staged view v of the cell (slot c), its
+// U^n, boundary flags, recorded branch byte, g_z and source coefficients, and what epi.pre(i, wet)
+// loaded before the update (so that those loads overlap it).
 template <class R, bool RECORD, bool BATCH = false, class Epi = NoEpilogue>
 __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                                     const StateOut<R> &O, const R *kact, unsigned *active,
@@ -299,9 +367,10 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
             bool wet_after = false, act = false;
             if (i < m.n) {
                 const R prev[3] = {b.h[c], b.hu[c], b.hv[c]};
-                const uint8_t bf = m.bflag[i];
+                const auto pre = epi.pre(i, prev[0] > R(DA_TINY));
+                const uint8_t bf = b.bf[c];
                 StagedView<R> v{b};
-                load_slots(ha.nloc, i, v.nl);
+                staged_slots(b, c, v.nl);
                 act = prev[0] >= R(DA_TINY);
 #pragma unroll
                 for (int s = 0; s < 4; ++s) {
@@ -311,15 +380,16 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 }
                 R dxc, dyc;
                 if constexpr (sizeof(R) == 8) {
-                    dxc = m.dx[i];
-                    dyc = m.dy[i];
+                    dxc = b.sz[0][c];
+                    dyc = b.sz[1][c];
                 } else {
                     dxc = b.c0[c];
                     dyc = b.c1[c];
                 }
                 R st[3] = {prev[0], prev[1], prev[2]};
                 bool clamped = false;
-                if (act) clamped = update_cell<R>(v, m, i, c, bf, mc, dt, ft, prev, dxc, dyc, st);
+                const CellSrc<R> cs = staged_src(b, c);
+                if (act) clamped = update_cell<R>(v, c, bf, cs, mc, dt, ft, prev, dxc, dyc, st);
                 const uint8_t code =
                     RECORD ? uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0)) : 0;
                 if (RECORD) mask[i] = code;
@@ -329,7 +399,7 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 O.hv[i] = st[2];
                 vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
-                epi(t, i, v, c, prev, bf, code, b.gz[c]);
+                epi(t, i, v, c, prev, bf, code, b.gz[c], cs, pre);
             }
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
             const unsigned act_bits = __ballot_sync(0xffffffffu, act);
