@@ -142,24 +142,26 @@ __device__ __forceinline__ void dirflux_adj(int dir, const Side<R> &s, const R a
         gk = R(0);
         return;
     }
+    // derivatives only (no branch depends on them): one reciprocal of h serves all quotients
     const R vel = s.vel, a = s.a, h = s.h;
-    const R da_dh = a > R(0) ? R(0.5) * a / h : R(0);
+    const R ih = R(1) / h;
+    const R da_dh = a > R(0) ? R(0.5) * a * ih : R(0);
     const R da_dk = (a > R(0) && s.k > R(0)) ? R(0.5) * a / s.k : R(0);
     const R avel_s = as[0] + as[1] + as[2];
     const R aa = -as[0] + as[2];
     if (dir == 0) {
         const R avel = af[1] * s.hu + af[2] * s.hv + avel_s;
         const R aaa = aa + af[1] * a * h;
-        g[0] = au[0] + af[1] * R(0.5) * a * a - avel * vel / h + aaa * da_dh;
-        g[1] = au[1] + af[0] + af[1] * vel + avel / h;
+        g[0] = au[0] + af[1] * R(0.5) * a * a - avel * vel * ih + aaa * da_dh;
+        g[1] = au[1] + af[0] + af[1] * vel + avel * ih;
         g[2] = au[2] + af[2] * vel;
         gk = aaa * da_dk;
     } else {
         const R avel = af[1] * s.hu + af[2] * s.hv + avel_s;
         const R aaa = aa + af[2] * a * h;
-        g[0] = au[0] + af[2] * R(0.5) * a * a - avel * vel / h + aaa * da_dh;
+        g[0] = au[0] + af[2] * R(0.5) * a * a - avel * vel * ih + aaa * da_dh;
         g[1] = au[1] + af[1] * vel;
-        g[2] = au[2] + af[0] + af[2] * vel + avel / h;
+        g[2] = au[2] + af[0] + af[2] * vel + avel * ih;
         gk = aaa * da_dk;
     }
 }
@@ -208,18 +210,19 @@ __device__ __forceinline__ void riemann_adj(int dir, const Side<R> &L, const Sid
     } else if (sr <= R(0)) {
         afr[0] = mu[0]; afr[1] = mu[1]; afr[2] = mu[2];
     } else {
-        const R D = sr - sl;
+        // derivatives of F = (sr fl - sl fr + sl sr du) / D: one reciprocal of D serves them all
+        const R iD = R(1) / (sr - sl);
         R a_sr = 0, a_sl = 0;
 #pragma unroll
         for (int v = 0; v < 3; ++v) {
             const R du = r.u[v] - l.u[v];
-            const R F = (sr * l.f[v] - sl * r.f[v] + sl * sr * du) / D;
-            afl[v] = mu[v] * sr / D;
-            afr[v] = -mu[v] * sl / D;
-            aur[v] = mu[v] * sl * sr / D;
+            const R F = (sr * l.f[v] - sl * r.f[v] + sl * sr * du) * iD;
+            afl[v] = mu[v] * sr * iD;
+            afr[v] = -mu[v] * sl * iD;
+            aur[v] = mu[v] * sl * sr * iD;
             aul[v] = -aur[v];
-            a_sr += mu[v] * (l.f[v] + sl * du - F) / D;
-            a_sl += mu[v] * (-r.f[v] + sr * du + F) / D;
+            a_sr += mu[v] * (l.f[v] + sl * du - F) * iD;
+            a_sl += mu[v] * (-r.f[v] + sr * du + F) * iD;
         }
         // route d/dsl, d/dsr to the Davis speeds they were taken from
         if (which_l == 1) {
@@ -297,6 +300,9 @@ __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &
             const int mat = cs.mat;
             const uint8_t code = mi & 3;
             const R k = kact_of<R>(mc, mat, code);
+            // the parameter tables of the cell's branch, loaded ahead of the arithmetic
+            const double sec2 = it.sec2_bed[mat], dkb = dk_of(it.dk_dbed, mat, code),
+                         dki = dk_of(it.dk_dint, mat, code);
             R s[6];
             cell_slopes<R>(v, vi, bf, R(mc.gamma), prev, s);
             R vel0, vel1, h_inv;
@@ -331,19 +337,21 @@ __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &
                 h_slope_deriv<R>(v, vi, bf, R(mc.gamma), h, sd);
                 const R cx = -nu_v * sg1 * h * k * gz * sin_int;  // on d h / dx
                 const R cy = -nu_u * sg0 * h * k * gz * sin_int;  // on d h / dy
-                A[0] += double(cx * (-sd[0].g_dp / sd[0].dxp + sd[0].g_dm / sd[0].dxm) +
-                               cy * (-sd[1].g_dp / sd[1].dxp + sd[1].g_dm / sd[1].dxm));
-                B[0] = double(cx * sd[0].g_dp / sd[0].dxp);
-                B[2] = double(-cx * sd[0].g_dm / sd[0].dxm);
-                B[1] = double(cy * sd[1].g_dp / sd[1].dxp);
-                B[3] = double(-cy * sd[1].g_dm / sd[1].dxm);
+                // d slope / d h at the neighbours: g / (centre distance)
+                const R qp0 = sd[0].g_dp / sd[0].dxp, qm0 = sd[0].g_dm / sd[0].dxm;
+                const R qp1 = sd[1].g_dp / sd[1].dxp, qm1 = sd[1].g_dm / sd[1].dxm;
+                A[0] += double(cx * (-qp0 + qm0) + cy * (-qp1 + qm1));
+                B[0] = double(cx * qp0);
+                B[2] = double(-cx * qm0);
+                B[1] = double(cy * qp1);
+                B[3] = double(-cy * qm1);
             }
             // parameter sensitivities of the sources
             const double dJ_dk = double(-nu_u * sg0 * h * wx * sin_int - nu_v * sg1 * h * wy * sin_int);
             const double dJ_dsin = double(-nu_u * sg0 * h * k * wx - nu_v * sg1 * h * k * wy);
             const double dJ_dtan = double(-nu_u * sg2 * (Px > R(0) ? Px : R(0)) - nu_v * sg3 * (Py > R(0) ? Py : R(0)));
-            const double gb = dJ_dtan * it.sec2_bed[mat] + dJ_dk * dk_of(it.dk_dbed, mat, code);
-            const double gi = dJ_dsin * it.cos_int + dJ_dk * dk_of(it.dk_dint, mat, code);
+            const double gb = dJ_dtan * sec2 + dJ_dk * dkb;
+            const double gi = dJ_dsin * it.cos_int + dJ_dk * dki;
             if (gb != 0.0) aa.gbed[i] += gb;
             if (gi != 0.0) aa.gint[i] += gi;
         }

@@ -172,68 +172,61 @@ __device__ __forceinline__ void adj_gather_phase_staged(const MeshArgs &m, const
                         out[2] += g.a[2][c];
                     }
                     const uint8_t bf = g.bf[c];
-                    int nl[8];
-                    {
-                        const uint4 w = g.nl[c];
-                        const unsigned u[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-                        for (int p = 0; p < 4; ++p) {
-                            nl[2 * p] = int(int16_t(u[p] & 0xffffu));
-                            nl[2 * p + 1] = int(int16_t(u[p] >> 16));
-                        }
-                    }
+                    // the branch's parameter derivatives, loaded ahead of the faces
+                    const uint8_t code = mj & 3;
+                    const int mat = g.mat[c];
+                    const InstTables it = inst_tables<BATCH>(aa, ia, inst);
+                    const double dkb = dk_of(it.dk_dbed, mat, code), dki = dk_of(it.dk_dint, mat, code);
+                    const int16_t *nl = reinterpret_cast<const int16_t *>(&g.nl[c]);
                     double dJ_dkj = 0.0;
-#pragma unroll
-                    for (int s = 0; s < 4; ++s) {
+                    // faces f = 2 s + q in the order side s = 0..3, neighbour q = 0 (1 on a hanging
+                    // side); in FP64 one loop body for all of them keeps the code small
+#pragma unroll(sizeof(R) == 8 ? 1 : 8)
+                    for (int f = 0; f < 8; ++f) {
+                        const int s = f >> 1, qq = f & 1;
                         if (bf & (1 << s)) continue;
+                        if (qq && !(bf & (0x10 << s))) continue;
                         const int d = s & 1;
                         const bool plus = s < 2;
-                        const int ne = (bf & (0x10 << s)) ? 2 : 1;
-                        for (int qq = 0; qq < ne; ++qq) {
-                            const int sl = nl[s + 4 * qq];
-                            const uint8_t bk = g.bf[sl];
-                            const R h_k = g.h[sl];
-                            if (h_k > R(DA_TINY)) {
-                                // slope coefficient of neighbour k for j (k's side s^2 faces j)
-                                double bk_s = g.b[s ^ 2][sl];
-                                if (bk & (0x10 << (s ^ 2))) bk_s *= 0.5;
-                                out[0] += bk_s;
-                            }
-                            if (!(h_k >= R(DA_TINY) || h_j >= R(DA_TINY))) continue;
-                            const R wj = side_outflow<R>(bf, s) ? R(0)
-                                                                : side_weight_of<R>(d == 0 ? g.sx[c] : g.sy[c], bf, s, dt);
-                            const R wk = side_outflow<R>(bk, s ^ 2)
-                                             ? R(0)
-                                             : side_weight_of<R>(d == 0 ? g.sx[sl] : g.sy[sl], bk, s ^ 2, dt);
-                            if (wj == R(0) && wk == R(0)) continue;
-                            const uint8_t mk = g.mask[sl];
-                            const R lk[3] = {(mk & 4) ? R(0) : g.lh[sl], g.lhu[sl], g.lhv[sl]};
-                            const R mu[3] = {wj * lj[0] + wk * lk[0], wj * lj[1] + wk * lk[1], wj * lj[2] + wk * lk[2]};
-                            if (mu[0] == R(0) && mu[1] == R(0) && mu[2] == R(0)) continue;
-                            Side<R> sj, sk;
-                            side_of<R>(mc, d, h_j, g.hu[c], g.hv[c], g.gz[c], g.mat[c], mj, sj);
-                            side_of<R>(mc, d, h_k, g.hu[sl], g.hv[sl], g.gz[sl], g.mat[sl], mk, sk);
-                            R gL[3], gR[3], gkL, gkR;
-                            if (plus) {
-                                riemann_adj<R>(d, sj, sk, mu, gL, gR, gkL, gkR);
-                                out[0] += double(gL[0]); out[1] += double(gL[1]); out[2] += double(gL[2]);
-                                dJ_dkj += double(gkL);
-                            } else {
-                                riemann_adj<R>(d, sk, sj, mu, gL, gR, gkL, gkR);
-                                out[0] += double(gR[0]); out[1] += double(gR[1]); out[2] += double(gR[2]);
-                                dJ_dkj += double(gkR);
-                            }
+                        const int sl = nl[s + 4 * qq];
+                        const uint8_t bk = g.bf[sl];
+                        const R h_k = g.h[sl];
+                        if (h_k > R(DA_TINY)) {
+                            // slope coefficient of neighbour k for j (k's side s^2 faces j)
+                            double bk_s = g.b[s ^ 2][sl];
+                            if (bk & (0x10 << (s ^ 2))) bk_s *= 0.5;
+                            out[0] += bk_s;
                         }
+                        if (!(h_k >= R(DA_TINY) || h_j >= R(DA_TINY))) continue;
+                        const R wj = side_outflow<R>(bf, s) ? R(0)
+                                                            : side_weight_of<R>(d == 0 ? g.sx[c] : g.sy[c], bf, s, dt);
+                        const R wk = side_outflow<R>(bk, s ^ 2)
+                                         ? R(0)
+                                         : side_weight_of<R>(d == 0 ? g.sx[sl] : g.sy[sl], bk, s ^ 2, dt);
+                        if (wj == R(0) && wk == R(0)) continue;
+                        const uint8_t mk = g.mask[sl];
+                        const R lk[3] = {(mk & 4) ? R(0) : g.lh[sl], g.lhu[sl], g.lhv[sl]};
+                        const R mu[3] = {wj * lj[0] + wk * lk[0], wj * lj[1] + wk * lk[1], wj * lj[2] + wk * lk[2]};
+                        if (mu[0] == R(0) && mu[1] == R(0) && mu[2] == R(0)) continue;
+                        // the edge's left and right sides: j then k on a plus side, k then j on a minus side
+                        const int eL = plus ? c : sl, eR = plus ? sl : c;
+                        const uint8_t mL = plus ? mj : mk, mR = plus ? mk : mj;
+                        Side<R> sL, sR;
+                        side_of<R>(mc, d, g.h[eL], g.hu[eL], g.hv[eL], g.gz[eL], g.mat[eL], mL, sL);
+                        side_of<R>(mc, d, g.h[eR], g.hu[eR], g.hv[eR], g.gz[eR], g.mat[eR], mR, sR);
+                        R gL[3], gR[3], gkL, gkR;
+                        riemann_adj<R>(d, sL, sR, mu, gL, gR, gkL, gkR);
+                        out[0] += double(plus ? gL[0] : gR[0]);
+                        out[1] += double(plus ? gL[1] : gR[1]);
+                        out[2] += double(plus ? gL[2] : gR[2]);
+                        dJ_dkj += double(plus ? gkL : gkR);
                     }
                     Lout.h[j] = R(out[0]);
                     Lout.hu[j] = R(out[1]);
                     Lout.hv[j] = R(out[2]);
                     if (dJ_dkj != 0.0) {
-                        const uint8_t code = mj & 3;
-                        const int mat = g.mat[c];
-                        const InstTables it = inst_tables<BATCH>(aa, ia, inst);
-                        aa.gbed[j] = g.gb[c] + dJ_dkj * dk_of(it.dk_dbed, mat, code);
-                        aa.gint[j] = g.gi[c] + dJ_dkj * dk_of(it.dk_dint, mat, code);
+                        aa.gbed[j] = g.gb[c] + dJ_dkj * dkb;
+                        aa.gint[j] = g.gi[c] + dJ_dkj * dki;
                     }
                 }
             }
