@@ -433,32 +433,41 @@ namespace {
 // state buffers alternate as in single steps and are read with coherent loads (no read-only
 // cache: other blocks wrote them earlier in the same launch).
 // The barrier is one 64-bit word (arrivals in the low half, generation in the high half): a block
-// arrives with one atomic add; the last one to arrive moves the word to the next generation with
-// zero arrivals in one more add; the others poll the word.  The waits are bounded: after ~4 s a
-// block raises DA_ERR_TIMEOUT and returns, and the others give up when they see the error (checked
-// on arrival and every 256 polls).
+// arrives with one atomic add (acquire-release at GPU scope, after the block's own barrier, so that
+// every write of the block before it is released); the last one to arrive moves the word to the
+// next generation with zero arrivals in one more such add; the others poll the word with acquire
+// loads.  The waits are bounded: after ~4 s a block raises DA_ERR_TIMEOUT and returns, and the
+// others give up when they see the error (checked on arrival and every 256 polls).
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
 
+__device__ __forceinline__ unsigned long long bar_add(unsigned long long *p, unsigned long long v) {
+    unsigned long long old;
+    asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned long long bar_load(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool grid_sync(DevScalars *sc) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned long long *bar = &sc->bar;
         volatile int *err = &sc->err;
-        const int err0 = *err;  // in flight with the arrival
-        __threadfence();
-        int good = err0 != DA_ERR_TIMEOUT;
-        const unsigned long long old = atomicAdd(&sc->bar, 1ull);
+        int good = *err != DA_ERR_TIMEOUT;
+        const unsigned long long old = bar_add(&sc->bar, 1ull);
         const unsigned gen = unsigned(old >> 32);
         if (unsigned(old) == gridDim.x - 1) {
-            atomicAdd(&sc->bar, (1ull << 32) - gridDim.x);  // all arrived: next generation, no arrivals
+            bar_add(&sc->bar, (1ull << 32) - gridDim.x);  // all arrived: next generation, no arrivals
         } else {
             const unsigned long long t0 = global_ns();
-            for (unsigned it = 1; unsigned(*bar >> 32) == gen; ++it) {
+            for (unsigned it = 1; unsigned(bar_load(&sc->bar) >> 32) == gen; ++it) {
                 if ((it & 255u) == 0 &&
                     (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > 4000000000ull)) {
                     atomicCAS(&sc->err, 0, DA_ERR_TIMEOUT);
@@ -468,7 +477,6 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc) {
                 __nanosleep(32);
             }
         }
-        __threadfence();
         ok = good;
     }
     __syncthreads();
