@@ -76,6 +76,15 @@ int reduce_inst_t(da_ctx *ctx, int lam0) {
     return cuda_check(ctx, cudaGetLastError(), "ensemble reduce launch");
 }
 
+// The gather shares its work out by quarter tiles when four times the tiles the recording update
+// listed fit in the grid (a flow over few tiles), else by tiles; every block reads the same count
+// after the barrier that ends the update.
+// split: 0 by that rule, 1 tiles, 2 quarters (da_params.tile_staging 1, 2, 3).
+__device__ __forceinline__ bool gather_quarters(const DevScalars *sc, int split) {
+    if (split) return split == 2;
+    return 4ull * __ldcg(&sc->listed) <= gridDim.x;
+}
+
 // ------------------------------------------------------------------------ k_youturn
 // One whole reverse step in one cooperative launch: the forward step of U^n replayed with its
 // branch codes recorded (coefficient phase, barrier, dt, update phase), a barrier, the source
@@ -94,10 +103,12 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
                                                     TimeConsts tc, DevScalars *sc, uint8_t *mask, int *tile_epoch,
                                                     uint8_t *seg_act, int rec_id, StateRef<R> Ln, StateOut<R> Lseed,
                                                     StateOut<R> Lo, AdjArgs aa, InstArgs ia, Box box, double *seg_J,
-                                                    snap::SnapArgs<R> pre, fwd::HaloArgs ha) {
+                                                    snap::SnapArgs<R> pre, fwd::HaloArgs ha, int gsplit) {
     __shared__ int list[kBlock];
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     fwd::StageSmem<R> &stg = *reinterpret_cast<fwd::StageSmem<R> *>(dyn_smem);
+    // the recording update counts its listed tiles from zero (the adds follow a barrier)
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->listed = 0u;
     if (pre.mode != snap::NONE) {
         snap::snap_segments<R>(pre);
         snap::snap_scalars<R>(pre);
@@ -137,7 +148,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
                                                  list, ia, stg, src);
         if (!fwd::grid_sync(sc)) return;
         adj_gather_phase_staged<R, BATCH>(m, ha, U, Ln, Lo, mc, aa, R(dt), list, ia,
-                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem));
+                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem), gather_quarters(sc, gsplit));
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             sc->iter = iter + 1;
             sc->frict_tiny = ft;
@@ -168,7 +179,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     if (!fwd::grid_sync(sc)) return;
     if (STAGED)
         adj_gather_phase_staged<R, BATCH>(m, ha, U, Ln, Lo, mc, aa, R(dt), list, ia,
-                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem));
+                                          *reinterpret_cast<GatherSmem<R> *>(dyn_smem), gather_quarters(sc, gsplit));
     else
         adj_gather_phase<R, BATCH>(m, U, Ln, Lo, mc, aa, R(dt), list, ia);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -262,9 +273,10 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     }
     snap::SnapArgs<R> pre = pre_slot ? snap::snap_args<R>(ctx, pre_slot, false, cur) : snap::no_snap<R>();
     fwd::HaloArgs ha = fwd::halo_args(ctx);
+    int gsplit = ctx->p.tile_staging >= 2 ? ctx->p.tile_staging - 1 : 0;
     void *args[] = {&m,      &S,    &cur, &kact, &active, &seg_clean, &seg_wet,    &seg_vol, &seg_dirty,
                     &ntiles, &cull, &mc,  &tc,   &sc,     &mask,      &tile_epoch, &seg_act, &rec_id,
-                    &Ln,     &Ls,   &Lo,  &aa,   &ia,     &box,       &seg_J,      &pre,     &ha};
+                    &Ln,     &Ls,   &Lo,  &aa,   &ia,     &box,       &seg_J,      &pre,     &ha,      &gsplit};
     trace_begin(ctx, TR_YOUTURN);
     const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, smem, ctx->stream);
     trace_end(ctx);

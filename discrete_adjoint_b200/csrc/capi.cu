@@ -108,7 +108,7 @@ static bool params_ok(const da_params *p) {
     if (!(p->epsilon > 0) || !(p->gravity_scale > 0) || !(p->gamma > 0)) return false;
     if (p->grid_blocks < 0 || p->grid_blocks > (1 << 20)) return false;
     if (p->blocks_per_sm != 0 && p->blocks_per_sm != 2 && p->blocks_per_sm != 3) return false;
-    if (p->tile_staging != 0 && p->tile_staging != 1) return false;
+    if (p->tile_staging < 0 || p->tile_staging > 3) return false;
     return true;
 }
 

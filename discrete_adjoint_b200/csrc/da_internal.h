@@ -46,7 +46,7 @@ struct DevScalars {
     unsigned long long acc_hmax;     // running max, bit pattern of a non-negative double
     int err;              // sticky DA_ERR_* raised on the device
     unsigned blocks_done[2];  // last-block counters of the coefficient and update kernels
-    int pad;
+    unsigned listed;      // tiles the reverse step's recording update listed (sets the gather's work split)
     unsigned long long acc_alt_min_dxe;  // the multi-step kernel's second accumulator pair
     unsigned long long acc_alt_hmax;     // (odd steps of a launch), same start values
     unsigned long long bar;  // grid barrier of the cooperative kernels: blocks arrived (low 32 bits),

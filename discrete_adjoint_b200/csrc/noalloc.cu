@@ -70,7 +70,7 @@ __global__ void k_init(DevScalars *sc, double time, long long iter) {
     sc->acc_hmax = 0ull;
     sc->err = 0;
     sc->blocks_done[0] = sc->blocks_done[1] = 0u;
-    sc->pad = 0;
+    sc->listed = 0;
     sc->acc_alt_min_dxe = __double_as_longlong(10000000.0);
     sc->acc_alt_hmax = 0ull;
     sc->bar = 0ull;

@@ -59,7 +59,7 @@ struct HaloArgs {
 inline HaloArgs halo_args(const da_ctx *ctx) { return HaloArgs{ctx->mesh.halo_off, ctx->mesh.halo_idx, ctx->mesh.nloc}; }
 
 // The staged phases run when the parameters ask for them and the mesh's halo tables exist.
-inline bool staged_ok(const da_ctx *ctx) { return ctx->p.tile_staging == 1 && ctx->mesh.nloc != nullptr; }
+inline bool staged_ok(const da_ctx *ctx) { return ctx->p.tile_staging >= 1 && ctx->mesh.nloc != nullptr; }
 
 // cp.async of BYTES (4 or 8) from global to shared memory; completes at the group's wait.
 template <int BYTES>
@@ -355,6 +355,7 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
         halo_range(ha, tq, ntiles, ho, hc);
         const int cnt = compact_tiles(need, tq, list, ho, hc, S.hoff, S.hcnt);
         if (cnt == 0) continue;
+        if (RECORD && threadIdx.x == 0) atomicAdd(&sc->listed, (unsigned)cnt);
         staged_tiles<R, true>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *) {
             const int inst = BATCH ? ia.tile_inst[t] : 0;
             const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;

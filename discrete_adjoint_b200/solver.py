@@ -52,7 +52,7 @@ class TimeProps:
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
                 influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
                 tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
-                tile_staging: bool = True) -> _ffi.da_params:
+                tile_staging: int = 1) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -94,7 +94,7 @@ class GeoflowContext:
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
                  device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
                  tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
-                 tile_staging: bool = True):
+                 tile_staging: int = 1):
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()

@@ -99,7 +99,10 @@ typedef struct da_params {
                                   * tile and its halo (the outside cells its cells name as
                                   * neighbours) into shared memory one tile ahead, when no tile's
                                   * halo exceeds 192 cells; 0: they read neighbours from global
-                                  * memory.  Results do not depend on it.  Default 1. */
+                                  * memory.  With 1 the reverse step's gather takes a block per
+                                  * quarter tile and a thread per cell side when the flow covers
+                                  * few tiles, else a block per tile; 2 and 3 fix it to tiles and to
+                                  * quarters.  Results do not depend on it.  Default 1. */
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
