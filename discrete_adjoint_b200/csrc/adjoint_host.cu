@@ -340,10 +340,49 @@ int fill_gradient(da_ctx *ctx, int lam0, int n_piles, da_gradient *out, bool red
 
 int adj_alloc_for_dwr(da_ctx *ctx) { return adj_alloc(ctx, 1); }
 
+// Everything the sweep's launches take as arguments, byte for byte: a graph captured from them is
+// replayed only for the same key (a different mesh, parameter, buffer, checkpoint slot, horizon,
+// launch shape or starting buffer gives a new capture).
+std::vector<unsigned char> sweep_key(const da_ctx *ctx, const double *box, int nsteps, int nsnap, int n_piles,
+                                     bool seeded, const double *sec2, double cos_int) {
+    std::vector<unsigned char> k;
+    auto put = [&](const void *p, size_t b) {
+        const unsigned char *c = (const unsigned char *)p;
+        k.insert(k.end(), c, c + b);
+    };
+    const int ints[] = {nsteps, nsnap, n_piles, seeded ? 1 : 0, ctx->cur, ctx->grid, ctx->ntiles, ctx->nseg,
+                        ctx->ninst, ctx->mesh.n, ctx->sm_count};
+    put(ints, sizeof(ints));
+    double b4[4] = {0, 0, 0, 0};
+    if (box) std::memcpy(b4, box, sizeof(b4));
+    put(b4, sizeof(b4));
+    put(sec2, sizeof(double) * DA_MAX_MATERIALS);
+    put(&cos_int, sizeof(cos_int));
+    put(&ctx->p, sizeof(ctx->p));
+    put(&ctx->mc, sizeof(ctx->mc));
+    put(&ctx->tc, sizeof(ctx->tc));
+    put(&ctx->mesh, sizeof(ctx->mesh));
+    put(&ctx->ia, sizeof(ctx->ia));
+    const void *ptrs[] = {ctx->U[0][0], ctx->U[0][1], ctx->U[0][2], ctx->U[1][0], ctx->U[1][1], ctx->U[1][2],
+                          ctx->lam[0][0], ctx->lam[0][1], ctx->lam[0][2], ctx->lam[1][0], ctx->lam[1][1],
+                          ctx->lam[1][2], ctx->kact, ctx->active, ctx->seg_clean, ctx->seg_wet, ctx->seg_vol,
+                          ctx->seg_dirty, ctx->mask, ctx->tile_epoch, ctx->seg_act, ctx->lam_clean, ctx->adjA,
+                          ctx->adjB, ctx->gbed, ctx->gint, ctx->dk_tab, ctx->red_out, ctx->red_part, ctx->inst_J,
+                          ctx->seg_J, ctx->dh0, ctx->dsc};
+    put(ptrs, sizeof(ptrs));
+    put(ctx->snaps.data(), sizeof(void *) * ctx->snaps.size());
+    return k;
+}
+
 // The reverse sweep shared by da_adjoint_run and da_ensemble_adjoint: checkpointed forward run
 // over nsteps steps from the current state, reverse steps back to step 0, the state put back,
 // J and the gradient sums launched (single: red_out[n_mat + 1 + n_piles]; ensemble: per member).
 // lam0 receives the buffer that holds lambda^0.
+// Without the DWR indicator (which reads every reverse step on the host) and without tracing, the
+// sweep's thousand or so launches are captured once as a CUDA graph and replayed while nothing
+// they depend on changes: a graph starts its cooperative kernels back to back, without the few
+// microseconds of idle GPU between stream launches.  The recording ids the capture gave the
+// reverse steps repeat on a replay, so the graph first clears the tiles' recording ids.
 int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnapshots, int32_t n_piles, int *lam0,
                   long long *fsteps, float *dev_ms, void *dwr_acc, const double *lambda_end) {
     int st = adj_alloc(ctx, nsnapshots + 1);
@@ -367,17 +406,68 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
     if (st) return st;
     r.sch.use(ctx, nsteps, nsnapshots);
     for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
+    // the launches of the sweep, from the base checkpoint to the gradient sums
+    auto sweep = [&]() -> int {
+        int s = store(ctx, 0);
+        r.pos = 0;
+        if (!s) s = r.reverse(0, nsteps, 0);
+        if (!s) s = restore(ctx, 0);
+        if (!s) s = launch_functional(ctx, ctx->inst_J);
+        if (!s) s = ctx->ninst > 0 ? launch_adjoint_reduce_inst(ctx, r.lam_cur) : launch_adjoint_reduce(ctx, r.lam_cur, n_piles);
+        return s;
+    };
+    bool graph = !r.dwr && !ctx->trace.on;
+    if (graph) {
+        std::vector<unsigned char> key = sweep_key(ctx, box, nsteps, nsnapshots, n_piles, r.seeded, r.sec2, r.cos_int);
+        if (!ctx->sweep_graph || key != ctx->sweep_key) {
+            if (ctx->sweep_graph) cudaGraphExecDestroy(ctx->sweep_graph);
+            ctx->sweep_graph = nullptr;
+            ctx->sweep_key.clear();
+            // capture: nothing runs; the host-side state the launches leave is kept for replays
+            const Runner r0 = r;
+            const int cur0 = ctx->cur;
+            cudaGraph_t g = nullptr;
+            int s = cuda_check(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal),
+                               "begin capture");
+            if (!s) {
+                int s2 = cuda_check(ctx, cudaMemsetAsync(ctx->tile_epoch, 0xff, sizeof(int) * ctx->ntiles, ctx->stream),
+                                    "memset");
+                if (!s2) s2 = sweep();
+                const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+                s = s2 ? s2 : cuda_check(ctx, e, "end capture");
+            }
+            if (!s) s = cuda_check(ctx, cudaGraphInstantiate(&ctx->sweep_graph, g, 0), "instantiate");
+            if (g) cudaGraphDestroy(g);
+            if (!s) {
+                ctx->sweep_key = key;
+                ctx->sweep_cur = ctx->cur;
+                ctx->sweep_lam = r.lam_cur;
+                ctx->sweep_fsteps = r.fsteps;
+            } else {
+                // the launches one by one instead
+                if (ctx->sweep_graph) cudaGraphExecDestroy(ctx->sweep_graph);
+                ctx->sweep_graph = nullptr;
+                cudaGetLastError();
+                ctx->err.clear();
+                graph = false;
+            }
+            ctx->cur = cur0;
+            r = r0;
+        }
+    }
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, ctx->stream);
-    st = store(ctx, 0);
-    r.pos = 0;
-    if (!st) st = r.reverse(0, nsteps, 0);
-    if (!st) st = restore(ctx, 0);
-    // the gradient sums are in the timed region
-    if (!st) st = launch_functional(ctx, ctx->inst_J);
-    if (!st) st = ctx->ninst > 0 ? launch_adjoint_reduce_inst(ctx, r.lam_cur) : launch_adjoint_reduce(ctx, r.lam_cur, n_piles);
+    if (graph) {
+        // the gradient sums are in the timed region
+        st = cuda_check(ctx, cudaGraphLaunch(ctx->sweep_graph, ctx->stream), "sweep graph launch");
+        ctx->cur = ctx->sweep_cur;
+        r.lam_cur = ctx->sweep_lam;
+        r.fsteps = ctx->sweep_fsteps;
+    } else {
+        st = sweep();
+    }
     cudaEventRecord(e1, ctx->stream);
     if (!st) st = sync_check(ctx);
     float ms = 0.f;

@@ -155,6 +155,9 @@ static void free_adjoint(da_ctx *ctx) {
         for (int v = 0; v < 3; ++v) { fr(ctx->lam[b][v]); ctx->lam[b][v] = nullptr; }
     for (void *s : ctx->snaps) fr(s);
     ctx->snaps.clear();
+    if (ctx->sweep_graph) cudaGraphExecDestroy(ctx->sweep_graph);
+    ctx->sweep_graph = nullptr;
+    ctx->sweep_key.clear();
     ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
     ctx->red_out = ctx->red_part = ctx->inst_J = ctx->seg_J = ctx->dh0 = nullptr;
     ctx->dh0_bytes = 0;

@@ -222,6 +222,12 @@ struct da_ctx {
     std::vector<int> sched_split;
     int sched_n = -1, sched_c = -1;
     std::vector<void *> snaps;       // checkpoint slots, 3 state arrays each
+    // the reverse sweep's launches captured as a CUDA graph (adjoint_host.cu), with the inputs its
+    // kernels were given (sweep_key) and the host-side results of building it
+    cudaGraphExec_t sweep_graph = nullptr;
+    std::vector<unsigned char> sweep_key;
+    int sweep_cur = 0, sweep_lam = 0;
+    long long sweep_fsteps = 0;
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
     int adj_n = 0;
     int adj_ninst = -1;

@@ -172,6 +172,35 @@ def test_tile_staging_does_not_change_the_adjoint(precision):
         assert np.array_equal(a.dJ_dbedfrict, b.dJ_dbedfrict) and np.array_equal(a.dJ_dpile, b.dJ_dpile)
 
 
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+def test_sweep_graph_replays_match_stream_launches(precision):
+    # the sweep captured as a CUDA graph (first run), replayed (second run), recaptured for another
+    # horizon and again for the first one, against the same sweeps launched one kernel at a time
+    # (tracing on): same lambda^0, J and gradients bit for bit, and the state and time put back
+    w = inputs.test_case(seed=6)
+    m = w.mesh
+    box = box_of(w)
+    runs = {}
+    for traced in (True, False):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision) as c:
+            c.upload_mesh(m)
+            c.set_state(m.h0, m.hu0, m.hv0)
+            c.run(2)
+            start = np.stack(c.get_state())
+            c.set_tracing(traced)
+            out = []
+            for horizon in (36, 36, 30, 36):
+                out.append(adjoint_run(c, box, horizon, 5, m.dh0_dpile, want_lambda0=True))
+                assert np.array_equal(np.stack(c.get_state()), start)
+            runs[traced] = out
+    for a, b in zip(runs[True], runs[False]):
+        assert np.array_equal(a.lambda0, b.lambda0)
+        assert a.J == b.J and a.dJ_dintfrict == b.dJ_dintfrict and a.forward_steps == b.forward_steps
+        assert np.array_equal(a.dJ_dbedfrict, b.dJ_dbedfrict) and np.array_equal(a.dJ_dpile, b.dJ_dpile)
+    assert runs[False][0].J == runs[False][1].J == runs[False][3].J != runs[False][2].J
+    assert runs[False][2].forward_steps != runs[False][0].forward_steps
+
+
 def test_adjoint_run_restores_state_and_time():
     w = inputs.test_case(seed=1)
     with ctx_for(w) as c:
