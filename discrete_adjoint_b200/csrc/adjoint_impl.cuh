@@ -286,11 +286,33 @@ __device__ __forceinline__ InstTables inst_tables(const AdjArgs &aa, const InstA
 // adj_src_wet: wet cell i with U^n = prev, g_z, branch byte mi, boundary flags bf, lambda^{n+1}
 // = lnext and source coefficients cs; v and vi give the neighbour values of the slopes (global
 // arrays with vi = i, or the tile staged in shared memory with vi the cell's slot).
+// The forward's slopes, velocities and friction signs of wet cell vi (update_cell's arithmetic).
 template <class R, class V>
+__device__ __forceinline__ SrcFwd<R> src_fwd(const V &v, int vi, uint8_t bf, const R prev[3], R gamma, R ft) {
+    SrcFwd<R> f;
+    cell_slopes<R>(v, vi, bf, gamma, prev, f.s);
+    if constexpr (sizeof(R) == 8) {
+        f.vel0 = prev[1] / prev[0];
+        f.vel1 = prev[2] / prev[0];
+        f.h_inv = 1. / prev[0];
+    } else {
+        f.h_inv = 1.0f / prev[0];
+        f.vel0 = prev[1] * f.h_inv;
+        f.vel1 = prev[2] * f.h_inv;
+    }
+    f.sg0 = tiny_sgn(f.h_inv * (f.s[4] - f.vel0 * f.s[3]), ft);
+    f.sg2 = tiny_sgn(f.vel0, ft);
+    f.sg1 = tiny_sgn(f.h_inv * (f.s[2] - f.vel1 * f.s[0]), ft);
+    f.sg3 = tiny_sgn(f.vel1, ft);
+    return f;
+}
+
+// get_f() gives the forward's quantities of the cell (computed, or handed over by the update).
+template <class R, class V, class GetF>
 __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &m, const R prev[3], R gz,
                                             uint8_t mi, uint8_t bf, const R lnext[3], const CellSrc<R> &cs,
                                             const MatConsts &mc, const AdjArgs &aa, const InstTables &it, R dt, R ft,
-                                            int i) {
+                                            int i, const GetF &get_f) {
     double A[3] = {0, 0, 0}, B[4] = {0, 0, 0, 0};
     {
         // lambda_eff: the depth row dropped where the forward step clamped h at zero
@@ -303,22 +325,10 @@ __device__ __forceinline__ void adj_src_wet(const V &v, int vi, const MeshArgs &
             // the parameter tables of the cell's branch, loaded ahead of the arithmetic
             const double sec2 = it.sec2_bed[mat], dkb = dk_of(it.dk_dbed, mat, code),
                          dki = dk_of(it.dk_dint, mat, code);
-            R s[6];
-            cell_slopes<R>(v, vi, bf, R(mc.gamma), prev, s);
-            R vel0, vel1, h_inv;
-            if constexpr (sizeof(R) == 8) {
-                vel0 = prev[1] / prev[0];
-                vel1 = prev[2] / prev[0];
-                h_inv = 1. / prev[0];
-            } else {
-                h_inv = 1.0f / prev[0];
-                vel0 = prev[1] * h_inv;
-                vel1 = prev[2] * h_inv;
-            }
-            const R sg0 = tiny_sgn(h_inv * (s[4] - vel0 * s[3]), ft);
-            const R sg2 = tiny_sgn(vel0, ft);
-            const R sg1 = tiny_sgn(h_inv * (s[2] - vel1 * s[0]), ft);
-            const R sg3 = tiny_sgn(vel1, ft);
+            const SrcFwd<R> f = get_f();
+            const R *s = f.s;
+            const R vel0 = f.vel0, vel1 = f.vel1;
+            const R sg0 = f.sg0, sg1 = f.sg1, sg2 = f.sg2, sg3 = f.sg3;
             const R h = prev[0];
             const R gx = cs.g[0], gy = cs.g[1];
             const R dgx = cs.dg[0], dgy = cs.dg[1];
@@ -373,8 +383,10 @@ __device__ __forceinline__ void adj_src_cell(const MeshArgs &m, const StateRef<R
     if (!(h_i > R(DA_TINY))) return;
     const R prev[3] = {h_i, U.hu[i], U.hv[i]};
     const R lnext[3] = {Lnext.h[i], Lnext.hu[i], Lnext.hv[i]};
-    adj_src_wet<R>(global_view<R>(m, U, (const R *)nullptr), i, m, prev, grav<R>(m, 2, i), aa.mask[i], m.bflag[i],
-                   lnext, cell_src<R>(m, i), mc, aa, it, dt, ft, i);
+    const GlobalView<R> v = global_view<R>(m, U, (const R *)nullptr);
+    const uint8_t bf = m.bflag[i];
+    adj_src_wet<R>(v, i, m, prev, grav<R>(m, 2, i), aa.mask[i], bf, lnext, cell_src<R>(m, i), mc, aa, it, dt, ft, i,
+                   [&]() { return src_fwd<R>(v, i, bf, prev, R(mc.gamma), ft); });
 }
 
 template <class R, bool BATCH = false>

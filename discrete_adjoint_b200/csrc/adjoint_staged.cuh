@@ -323,8 +323,9 @@ __device__ __forceinline__ void adj_gather_phase_staged(const MeshArgs &m, const
     }
 }
 
-// The reverse step's source adjoint as the epilogue of its staged update phase: lambda^{n+1} of
-// a wet cell is loaded before its update, the rest comes from the update's staged tile.
+// The reverse step's source adjoint inside its staged update phase: lambda^{n+1} of a wet cell is
+// loaded before its update, the slopes, velocities and friction signs are the update's own, the
+// rest comes from the update's staged tile.
 template <class R, bool BATCH>
 struct SrcEpilogue {
     const MeshArgs &m;
@@ -345,14 +346,15 @@ struct SrcEpilogue {
         }
         return p;
     }
+    // inside the update of wet cell i (h > GEOFLOW_TINY), with the forward's source quantities f
     __device__ __forceinline__ void operator()(int t, int i, const fwd::StagedView<R> &v, int c, const R *prev,
-                                               uint8_t bf, uint8_t code, R gz, const CellSrc<R> &cs,
-                                               const Pre &p) const {
-        if (!(prev[0] > R(DA_TINY))) return;  // A and B exist for wet cells only
+                                               uint8_t bf, uint8_t code, R gz, const CellSrc<R> &cs, const Pre &p,
+                                               const SrcFwd<R> &f) const {
         const int inst = BATCH ? ia.tile_inst[t] : 0;
         const MatConsts &mci = BATCH ? ia.mcs[inst] : mc;
         const R dti = BATCH ? R(ia.dt[inst]) : dt;
-        adj_src_wet<R>(v, c, m, prev, gz, code, bf, p.l, cs, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ft, i);
+        adj_src_wet<R>(v, c, m, prev, gz, code, bf, p.l, cs, mci, aa, inst_tables<BATCH>(aa, ia, inst), dti, ft, i,
+                       [&]() -> const SrcFwd<R> & { return f; });
     }
 };
 

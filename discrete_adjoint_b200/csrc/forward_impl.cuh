@@ -222,10 +222,12 @@ __device__ __forceinline__ void flux_div(const V &v, int i, uint8_t bf, const R 
 }
 
 // Full corrector update of one active cell (fluxes + sources), reference order.  c is the cell in
-// the view; cs its source coefficients (read only for a wet cell, h > GEOFLOW_TINY).
-template <class R, class V>
+// the view; cs its source coefficients (read only for a wet cell, h > GEOFLOW_TINY); hook(f,
+// clamped) runs for a wet cell with the slopes, velocities and friction signs of its sources.
+template <class R, class V, class Hook = NoSrcHook>
 __device__ __forceinline__ bool update_cell(const V &v, int c, uint8_t bf, const CellSrc<R> &cs, const MatConsts &mc,
-                                            R dt, R ft, const R prev[3], R dxc, R dyc, R st[3]) {
+                                            R dt, R ft, const R prev[3], R dxc, R dyc, R st[3],
+                                            const Hook &hook = Hook{}) {
     const R ki = prev[0] >= R(DA_TINY) ? v.k(c) : R(0);
     const R gz = v.gz(c);
     const R g0 = cs.g[0], g1 = cs.g[1], dg0 = cs.dg[0], dg1 = cs.dg[1], cv0 = cs.cv[0], cv1 = cs.cv[1];
@@ -263,6 +265,8 @@ __device__ __forceinline__ bool update_cell(const V &v, int c, uint8_t bf, const
         tmp = h_inv * (s[2] - vel1 * s[0]);
         const R sg1 = tiny_sgn(tmp, ft);
         const R sg3 = tiny_sgn(vel1, ft);
+        // the reverse step's source adjoint of this cell, from these same values (its branches)
+        hook(SrcFwd<R>{{s[0], s[1], s[2], s[3], s[4], s[5]}, vel0, vel1, h_inv, sg0, sg1, sg2, sg3}, clamped);
         const R sin_int = R(mc.sin_int);
         const R tan_bed = R(mc.tan_bed[mat]);
         R s1 = g0 * prev[0];

@@ -124,6 +124,21 @@ __device__ __forceinline__ CellSrc<R> cell_src(const MeshArgs &m, int i) {
     return s;
 }
 
+// What the corrector's source terms form for a wet cell before using them: the limited slopes, the
+// velocities, 1/h and the four friction signs (also what the source adjoint needs of the forward).
+template <class R>
+struct SrcFwd {
+    R s[6];
+    R vel0, vel1, h_inv;
+    R sg0, sg1, sg2, sg3;
+};
+
+// No hook (the forward alone).
+struct NoSrcHook {
+    template <class... A>
+    __device__ __forceinline__ void operator()(A &&...) const {}
+};
+
 // What the per-cell numerics read about a cell and its neighbours goes through a view: nb(s, c)
 // the cell across neighbour entry s of cell c, and the values of a cell.  GlobalView reads the
 // mesh table and the global arrays (c, e = cell indices); the step kernels' staged view reads a

@@ -328,10 +328,11 @@ struct NoEpilogue {
 
 // Update phase (see update_phase) with the tile and its halo staged.  A listed tile's cells
 // recompute their activity from the staged depths; the segment flags follow it.
-// epi(t, i, v, c, prev, bf, code, gz, cs, pre) runs for every cell i < n of a listed tile t after
-// its update (the reverse step's source adjoint), with the staged view v of the cell (slot c), its
-// U^n, boundary flags, recorded branch byte, g_z and source coefficients, and what epi.pre(i, wet)
-// loaded before the update (so that those loads overlap it).
+// epi(t, i, v, c, prev, bf, code, gz, cs, pre, f) runs for every wet cell i of a listed tile t inside
+// its update, where the corrector has formed the source terms' slopes, velocities and friction
+// signs f (the reverse step's source adjoint, which needs exactly these), with the staged view v
+// of the cell (slot c), its U^n, boundary flags, recorded branch byte, g_z and source coefficients,
+// and what epi.pre(i, wet) loaded before the update (so that those loads overlap it).
 template <class R, bool RECORD, bool BATCH = false, class Epi = NoEpilogue>
 __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                                     const StateOut<R> &O, const R *kact, unsigned *active,
@@ -390,9 +391,16 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 R st[3] = {prev[0], prev[1], prev[2]};
                 bool clamped = false;
                 const CellSrc<R> cs = staged_src(b, c);
-                if (act) clamped = update_cell<R>(v, c, bf, cs, mc, dt, ft, prev, dxc, dyc, st);
-                const uint8_t code =
-                    RECORD ? uint8_t((prev[0] >= R(DA_TINY) ? (mask[i] & 3) : 0) | (act ? 8 : 0) | (clamped ? 4 : 0)) : 0;
+                // the k act/pass code the coefficient phase recorded
+                const uint8_t kcode = RECORD && prev[0] >= R(DA_TINY) ? uint8_t(mask[i] & 3) : uint8_t(0);
+                if (act)
+                    clamped = update_cell<R>(v, c, bf, cs, mc, dt, ft, prev, dxc, dyc, st,
+                                             [&](const SrcFwd<R> &f, bool cl) {
+                                                 // a wet cell is active: its branch byte as recorded below
+                                                 epi(t, i, v, c, prev, bf, uint8_t(kcode | 8 | (cl ? 4 : 0)), b.gz[c],
+                                                     cs, pre, f);
+                                             });
+                const uint8_t code = RECORD ? uint8_t(kcode | (act ? 8 : 0) | (clamped ? 4 : 0)) : 0;
                 if (RECORD) mask[i] = code;
                 if (!isfinite(st[0]) || !isfinite(st[1]) || !isfinite(st[2])) raise_err(sc, DA_ERR_NAN);
                 O.h[i] = st[0];
@@ -400,7 +408,6 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 O.hv[i] = st[2];
                 vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
-                epi(t, i, v, c, prev, bf, code, b.gz[c], cs, pre);
             }
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
             const unsigned act_bits = __ballot_sync(0xffffffffu, act);
