@@ -29,6 +29,7 @@ UNITS = [
     ("adjoint_fp64.cu", ["--fmad=false"]),
     ("adjoint_fp32.cu", ["-prec-div=false", "-prec-sqrt=false"]),
     ("adjoint_host.cu", []),
+    ("adjoint_ref.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
     ("snapshot.cu", []),
     ("ensemble.cu", []),

@@ -31,6 +31,9 @@ DA_ERR_UNSUPPORTED = -10
 DA_PREC_FP64 = 0
 DA_PREC_FP32_SPLIT = 1
 
+DA_JAC_EXACT = 0
+DA_JAC_REFERENCE = 1
+
 PD = C.POINTER(C.c_double)
 PF = C.POINTER(C.c_float)
 PI32 = C.POINTER(C.c_int32)
@@ -58,6 +61,8 @@ class da_params(C.Structure):
         ("grid_blocks", C.c_int32),
         ("blocks_per_sm", C.c_int32),
         ("tile_staging", C.c_int32),
+        ("jacobian_mode", C.c_int32),
+        ("pad_mode", C.c_int32),
     ]
 
 

@@ -244,8 +244,23 @@ struct Runner {
     int youturn() {
         ++fsteps;
         pos = -1;  // past the step that is being taken back
+        if (ctx->p.jacobian_mode == DA_JAC_REFERENCE) return youturn_reference();
         // the first reverse step (the horizon's last step) also seeds lambda^N from U^N
         int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box, take_pending());
+        if (!st && dwr) st = dwr_after_reverse_step(ctx, *dwr, lam_cur);
+        seeded = true;
+        lam_cur = 1 - lam_cur;
+        return st;
+    }
+    // The reference's dual-solver step instead of the fused exact one: the pending restore, the
+    // forward step (its dt and frict_tiny), the seed on the horizon's last step, then the step's
+    // adjoint from U^n, which the forward step left in the other state buffer.
+    int youturn_reference() {
+        void *pre = take_pending();
+        int st = pre ? launch_snapshot(ctx, pre, false) : DA_OK;
+        if (!st) st = launch_forward_step(ctx, nullptr);
+        if (!st && !seeded) st = launch_ref_seed(ctx, lam_cur, box);
+        if (!st) st = launch_ref_adjoint_step(ctx, ctx->cur ^ 1, lam_cur, 1 - lam_cur);
         if (!st && dwr) st = dwr_after_reverse_step(ctx, *dwr, lam_cur);
         seeded = true;
         lam_cur = 1 - lam_cur;
@@ -416,7 +431,7 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
         if (!s) s = ctx->ninst > 0 ? launch_adjoint_reduce_inst(ctx, r.lam_cur) : launch_adjoint_reduce(ctx, r.lam_cur, n_piles);
         return s;
     };
-    bool graph = !r.dwr && !ctx->trace.on;
+    bool graph = !r.dwr && !ctx->trace.on && ctx->p.jacobian_mode == DA_JAC_EXACT;
     if (graph) {
         std::vector<unsigned char> key = sweep_key(ctx, box, nsteps, nsnapshots, n_piles, r.seeded, r.sec2, r.cos_int);
         if (!ctx->sweep_graph || key != ctx->sweep_key) {
@@ -523,9 +538,10 @@ int da_adjoint_step(da_ctx *ctx, const double *lambda_next, double *lambda_out, 
     for (int v = 0; v < 3 && !st; ++v) st = upload_real(ctx, ctx->lam[0][v], lambda_next + v * n);
     // the caller's lambda differs from buffer 1 everywhere
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->lam_clean, 0, ctx->nseg, ctx->stream), "memset");
+    const bool ref = ctx->p.jacobian_mode == DA_JAC_REFERENCE;
     if (!st) st = store(ctx, 0);
-    if (!st) st = launch_forward_step(ctx, ctx->mask);
-    if (!st) st = launch_adjoint_step(ctx, 0, 1, sec2, cos_int);
+    if (!st) st = launch_forward_step(ctx, ref ? nullptr : ctx->mask);
+    if (!st) st = ref ? launch_ref_adjoint_step(ctx, ctx->cur ^ 1, 0, 1) : launch_adjoint_step(ctx, 0, 1, sec2, cos_int);
     if (!st) st = restore(ctx, 0);
     if (!st) st = sync_check(ctx);
     if (!st) st = copy_lambda_out(ctx, 1, lambda_out);

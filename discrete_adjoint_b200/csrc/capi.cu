@@ -109,6 +109,7 @@ static bool params_ok(const da_params *p) {
     if (p->grid_blocks < 0 || p->grid_blocks > (1 << 20)) return false;
     if (p->blocks_per_sm != 0 && p->blocks_per_sm != 2 && p->blocks_per_sm != 3) return false;
     if (p->tile_staging < 0 || p->tile_staging > 3) return false;
+    if (p->jacobian_mode != DA_JAC_EXACT && p->jacobian_mode != DA_JAC_REFERENCE) return false;
     return true;
 }
 
@@ -161,6 +162,9 @@ static void free_adjoint(da_ctx *ctx) {
     ctx->mask = nullptr; ctx->adjA = ctx->adjB = ctx->gbed = ctx->gint = ctx->dk_tab = nullptr;
     ctx->red_out = ctx->red_part = ctx->inst_J = ctx->seg_J = ctx->dh0 = nullptr;
     ctx->dh0_bytes = 0;
+    fr(ctx->refadj_mem);
+    ctx->refadj_mem = nullptr;
+    ctx->refadj_n = 0;
     ctx->adj_n = 0;
     ctx->adj_ninst = -1;
 }
@@ -360,6 +364,7 @@ void da_params_default(da_params *p) {
     p->grid_blocks = 0;
     p->blocks_per_sm = 0;
     p->tile_staging = 1;
+    p->jacobian_mode = DA_JAC_EXACT;
 }
 
 da_ctx *da_create(const da_params *p, int *err) {

@@ -229,6 +229,8 @@ struct da_ctx {
     int sweep_cur = 0, sweep_lam = 0;
     long long sweep_fsteps = 0;
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
+    void *refadj_mem = nullptr;      // workspace of the reference-mode adjoint (adjoint_ref.cu)
+    int refadj_n = 0;                // the mesh size it was allocated for
     int adj_n = 0;
     int adj_ninst = -1;
     da::TraceState trace;
@@ -273,8 +275,12 @@ void update_grid(da_ctx *ctx);
 // adjoint_fp64.cu / adjoint_fp32.cu
 int launch_adjoint_step(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double cos_int);
 // replayed forward step + adjoint step in one cooperative launch (k_youturn)
-int launch_adjoint_seed(da_ctx *ctx, int lam_out, const double box[4]);
 int launch_adjoint_reduce(da_ctx *ctx, int lam0, int n_piles);
+// adjoint_ref.cu: one reverse step of the reference's own dual solver (jacobian_mode
+// DA_JAC_REFERENCE): U^n in state buffer un, dt and frict_tiny of the step in the device scalars
+int launch_ref_adjoint_step(da_ctx *ctx, int un, int lam_in, int lam_out);
+int launch_ref_seed(da_ctx *ctx, int lam_out, const double box[4]);
+int ref_adjoint_alloc(da_ctx *ctx);
 int forward_state_changed(da_ctx *ctx);
 // adjoint_host.cu: d kact / d phi_bed and d phi_int of each material's three branches
 void kact_derivatives(const da_params &p, double *dkb, double *dki);

@@ -308,6 +308,8 @@ int da_ensemble_get_state(da_ctx *ctx, int32_t member, double *h, double *hu, do
 int da_ensemble_adjoint(da_ctx *ctx, int32_t nsteps, int32_t nsnapshots, da_gradient *out, double *device_ms) {
     if (!ctx || !out || nsteps <= 0 || nsnapshots < 0) return DA_ERR_INVALID;
     if (ctx->ninst <= 0) return set_error(ctx, DA_ERR_INVALID, "da_ensemble_adjoint: not an ensemble context");
+    if (ctx->p.jacobian_mode != DA_JAC_EXACT)
+        return set_error(ctx, DA_ERR_UNSUPPORTED, "da_ensemble_adjoint: ensembles use the exact adjoint");
     cudaSetDevice(ctx->device);
     const int nm = ctx->ninst, nout = ctx->p.n_materials + 2;
     int lam0 = 0;

@@ -52,7 +52,7 @@ class TimeProps:
 def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64, device: int = 0,
                 influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
                 tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
-                tile_staging: int = 1) -> _ffi.da_params:
+                tile_staging: int = 1, jacobian_mode: int = 0) -> _ffi.da_params:
     p = _ffi.da_params()
     _ffi.load().da_params_default(C.byref(p))
     p.precision = precision
@@ -76,6 +76,7 @@ def make_params(mat: MatProps, tp: TimeProps, precision: int = _ffi.DA_PREC_FP64
     p.grid_blocks = int(grid_blocks)
     p.blocks_per_sm = int(blocks_per_sm)
     p.tile_staging = int(tile_staging)
+    p.jacobian_mode = int(jacobian_mode)
     return p
 
 
@@ -94,13 +95,16 @@ class GeoflowContext:
     def __init__(self, mat: MatProps, tp: TimeProps | None = None, precision: int = _ffi.DA_PREC_FP64,
                  device: int = 0, influx_dt: float = math.inf, fp32_sign_floor: float = 0.0,
                  tile_culling: bool = True, grid_blocks: int = 0, blocks_per_sm: int = 0,
-                 tile_staging: int = 1):
+                 tile_staging: int = 1, jacobian_mode: int = _ffi.DA_JAC_EXACT):
+        """jacobian_mode: DA_JAC_EXACT (the exact transpose of this forward step) or DA_JAC_REFERENCE
+        (the reference's own dual-solver adjoint, calc_jacobain.C:40-153 and calc_adjoint.C:35-167,
+        FP64 only)."""
         self.lib = _ffi.load()
         self.mat = mat
         self.tp = tp or TimeProps()
         self.precision = precision
         self.params = make_params(mat, self.tp, precision, device, influx_dt, fp32_sign_floor, tile_culling,
-                                  grid_blocks, blocks_per_sm, tile_staging)
+                                  grid_blocks, blocks_per_sm, tile_staging, jacobian_mode)
         err = C.c_int(0)
         self.ctx = self.lib.da_create(C.byref(self.params), C.byref(err))
         if not self.ctx:

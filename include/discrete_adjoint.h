@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define DA_ABI_VERSION 1
+#define DA_ABI_VERSION 2
 
 #define DA_MAX_MATERIALS 16
 #define DA_MAX_PILES 8
@@ -59,6 +59,12 @@ extern "C" {
 #define DA_ERR_OOM (-8)         /* device allocation failed */
 #define DA_ERR_NO_DEVICE (-9)   /* no CUDA device visible */
 #define DA_ERR_UNSUPPORTED (-10)
+
+/* adjoint modes (da_params.jacobian_mode) */
+#define DA_JAC_EXACT 0          /* the exact transpose of the forward step as computed here */
+#define DA_JAC_REFERENCE 1      /* the reference's own dual-solver adjoint, its approximations included
+                                 * (calc_jacobian / calc_adjoint, calc_jacobain.C:40-153,
+                                 * calc_adjoint.C:35-167); FP64 only */
 
 /* precision modes */
 #define DA_PREC_FP64 0          /* plain: every operation in FP64, no contraction, reference order */
@@ -103,6 +109,17 @@ typedef struct da_params {
                                   * quarter tile and a thread per cell side when the flow covers
                                   * few tiles, else a block per tile; 2 and 3 fix it to tiles and to
                                   * quarters.  Results do not depend on it.  Default 1. */
+    int32_t jacobian_mode;       /* DA_JAC_EXACT (default) or DA_JAC_REFERENCE: which adjoint
+                                  * da_adjoint_step / da_adjoint_run apply.  The reference mode
+                                  * reproduces the reference's dual solver step for step: it freezes
+                                  * dry cells, drops derivatives with respect to cells whose record
+                                  * is zero, gates the neighbours' slope terms with the friction-stop
+                                  * flags, and flushes adjoint entries below 1e-16, as
+                                  * calc_jacobian_elem / calc_adjoint_elem do.  It forms lambda and
+                                  * the pile-height gradient; the friction-angle gradients, which the
+                                  * reference does not have, are 0 in it.  FP64 contexts only;
+                                  * ensembles use the exact mode. */
+    int32_t pad_mode;
 } da_params;
 
 /* Flattened mesh, host memory, caller-owned.  n = n_cells.  See the file comment. */
@@ -159,9 +176,10 @@ int da_forward_run_timed(da_ctx *ctx, int32_t nsteps, da_step_stats *last, doubl
 /* ---- adjoint ------------------------------------------------------------------------------
  * Replaces dual_solver() (src/adjoint/dual_solver.C:80-273) with calc_jacobian()/calc_adjoint()
  * (calc_jacobain.C:40-153, calc_adjoint.C:35-167) taken over every step, backward in time.
- * The adjoint is the exact transpose of the forward step as it is computed here (k act/pass and
- * all thresholds replayed from recorded branch codes, the time-step sequence frozen), so it is
- * checked against central finite differences of the same forward step.  Forward states are kept
+ * By default (DA_JAC_EXACT) the adjoint is the exact transpose of the forward step as it is
+ * computed here (k act/pass and all thresholds replayed from recorded branch codes, the time-step
+ * sequence frozen), checked against central finite differences of the same forward step;
+ * DA_JAC_REFERENCE gives the reference's own adjoint instead (see da_params.jacobian_mode).  Forward states are kept
  * in HBM at nsnapshots checkpoints placed by an optimal binomial schedule and recomputed between
  * them (the reference stores every step to gz files instead, dualmesh.C:82-147). */
 #define DA_FUNC_H2_BOX 1          /* J = sum over cells with centre in box of h^2 dx dy, final step */

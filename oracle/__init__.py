@@ -41,6 +41,10 @@ def load() -> C.CDLL:
     lib.orc_coef_eigen.argtypes = [P, M, PD, PD, PD, PD, PD, PD, PD]
     lib.orc_edge_fluxes.restype = None
     lib.orc_edge_fluxes.argtypes = [P, M, PD, PD, PD, PD, PD]
+    lib.orc_adjoint_step_ref.restype = C.c_int
+    lib.orc_adjoint_step_ref.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD]
+    lib.orc_adjoint_step_var.restype = C.c_int
+    lib.orc_adjoint_step_var.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD, C.c_int]
     _lib = lib
     return lib
 
@@ -82,11 +86,38 @@ class Oracle:
                                      _ffi.dptr(hv), _ffi.dptr(slopes), _ffi.dptr(kact), C.byref(mn), C.byref(hm))
         return rc, kact, mn.value, hm.value
 
+    def adjoint_step_ref(self, h, hu, hv, dt: float, frict_tiny: float, lam_next, keep: int = None):
+        """The reference's dual-solver step (restated): lambda of U^{n-1} from lambda of U^n, with
+        (h, hu, hv) = U^{n-1}, the step's dt and frict_tiny.  Returns [3][n].  keep: the reference
+        approximations to keep (Q_* bits; all by default, 0 gives the exact transpose)."""
+        lam_next = np.ascontiguousarray(lam_next, dtype=np.float64).reshape(3, self.mesh.n)
+        out = np.zeros((3, self.mesh.n))
+        h, hu, hv = (np.ascontiguousarray(a, dtype=np.float64) for a in (h, hu, hv))
+        if keep is None:
+            rc = self.lib.orc_adjoint_step_ref(C.byref(self.params), C.byref(self.soa), _ffi.dptr(h),
+                                               _ffi.dptr(hu), _ffi.dptr(hv), dt, frict_tiny, _ffi.dptr(lam_next),
+                                               _ffi.dptr(out))
+        else:
+            rc = self.lib.orc_adjoint_step_var(C.byref(self.params), C.byref(self.soa), _ffi.dptr(h),
+                                               _ffi.dptr(hu), _ffi.dptr(hv), dt, frict_tiny, _ffi.dptr(lam_next),
+                                               _ffi.dptr(out), int(keep))
+        assert rc == 0
+        return out
+
     def edge_fluxes(self, h, hu, hv, kact):
         F = np.zeros((4, 3, self.mesh.n))
         self.lib.orc_edge_fluxes(C.byref(self.params), C.byref(self.soa), _ffi.dptr(h), _ffi.dptr(hu),
                                  _ffi.dptr(hv), _ffi.dptr(kact), _ffi.dptr(F))
         return F
+
+
+# the reference's approximations of the exact transpose (oracle/da_oracle_adjoint.c)
+Q_RECORD, Q_VOID, Q_STOP, Q_SLOPEFAC, Q_DRYVDIFF, Q_SRTIE, Q_FLUSH = 1, 2, 4, 8, 16, 32, 64
+Q_ALL = 127
+Q_NAMES = {Q_RECORD: "zero records of dry cells", Q_VOID: "no derivative w.r.t. void cells",
+           Q_STOP: "stop-gated neighbour slope terms", Q_SLOPEFAC: "slope sensitivity without sign factor",
+           Q_DRYVDIFF: "HLL state-difference term on dry sides", Q_SRTIE: "right-speed ties from the left",
+           Q_FLUSH: "flush below 1e-16"}
 
 
 # ---------------------------------------------------------------- reference harness
@@ -214,3 +245,51 @@ def ref_read_solution(directory: str, rank: int, step: int, keys):
     found = np.frombuffer(raw, dtype="<i4", offset=8, count=n).copy()
     state = np.frombuffer(raw, dtype="<f8", offset=8 + 4 * n).reshape(n, 3).copy()
     return found, state
+
+
+def run_reference_adjoint(mesh, mat, states, iters, dts, lam_end, workdir: str | None = None) -> dict:
+    """The reference's own dual-solver steps (oracle/_ref/ref_harness, mode 'DAJ1').
+
+    Reverse step k takes back the forward step iters[k] (U^{iters[k]-1} -> U^{iters[k]}), with
+    states[k] = (h, hu, hv) of U^{iters[k]-1} and dts[k] that step's dt; lam_end ([3][n]) is the
+    adjoint of U^{iters[0]}.  Each step runs update_dual_grid, calc_jacobian and calc_adjoint
+    (src/adjoint/dual_grid_routines.C:15-93, calc_jacobain.C:40-153, calc_adjoint.C:35-167) with
+    a zero functional sensitivity.  Returns {"lam": [K][3][n] the adjoint after each reverse step,
+    "seconds": time of the K steps}.
+    """
+    import struct
+    import subprocess
+    import tempfile
+
+    from discrete_adjoint_b200.solver import MatProps
+    n = mesh.n
+    K = len(iters)
+    assert len(states) == K and len(dts) == K
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<6i", 0x314A4144, n, mesh.max_level, len(mat.bedfrict_deg), K, 0))
+            f.write(np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma,
+                              float("inf")], dtype="<f8").tobytes())
+            f.write(bed.astype("<f8").tobytes())
+            for a in (mesh.nbr, mesh.level, mesh.ix, mesh.iy, mesh.material):
+                f.write(np.ascontiguousarray(a, dtype="<i4").tobytes())
+            for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature):
+                f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+            f.write(np.asarray(iters, dtype="<i4").tobytes())
+            f.write(np.asarray(dts, dtype="<f8").tobytes())
+            for (h, hu, hv) in states:
+                for a in (h, hu, hv):
+                    f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+            f.write(np.ascontiguousarray(lam_end, dtype="<f8").reshape(3, n).tobytes())
+        r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    magic, n2, k2 = struct.unpack_from("<3i", raw, 0)
+    assert magic == 0x314F4A44 and n2 == n and k2 == K
+    arr = np.frombuffer(raw, dtype="<f8", offset=12)
+    return {"lam": arr[:K * 3 * n].reshape(K, 3, n).copy(), "seconds": float(arr[K * 3 * n])}

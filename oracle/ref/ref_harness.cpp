@@ -31,6 +31,9 @@
 //   'DAR1' rank, step, n, uint32 key[2n]  ->  'DAR2' n, int32 found[n] (0 none, 1 zero record,
 //       2 state record), double state[3n]: the reference's SolRec reads solution_<rank>_<step>
 //       (read_sol_from_disk) and each key is looked up.
+//   'DAJ1' (mesh as 'DAH1', then reverse-step records; see adjoint_mode) -> 'DJO1': the
+//       reference's own dual solver steps -- update_dual_grid, calc_jacobian, calc_adjoint --
+//       taken backward from a given adjoint.
 #include <sys/sysinfo.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -64,6 +67,9 @@
 #undef protected
 
 int REFINE_LEVEL = 0;  // global of the reference's driver (hpfem.C)
+// the driver's max-h functional (adjoint.h:299); default-constructed, its iteration (0) never
+// matches a reverse step, so calc_adjoint's functional sensitivity is zero
+MaxH_Functional maxh_func;
 
 void step(HashTable *El_Table, HashTable *NodeTable, int myid, int nump, MatProps *matprops_ptr,
           TimeProps *timeprops_ptr, PileProps *pileprops_ptr, FluxProps *fluxprops, StatProps *statprops_ptr,
@@ -188,88 +194,90 @@ int read_mode(FILE *f, const char *out) {
 
 }  // namespace
 
-int main(int argc, char **argv) {
-    if (argc != 3) {
-        std::fprintf(stderr, "usage: ref_harness in.bin out.bin\n");
-        return 2;
-    }
-    FILE *f = std::fopen(argv[1], "rb");
-    if (!f) return 2;
-    int32_t magic;
-    rd(f, &magic, 1);
-    if (magic == 0x314B4144) return keys_mode(f, argv[2]);
-    if (magic == 0x31574144) return write_mode(f, argv[2]);
-    if (magic == 0x31524144) return read_mode(f, argv[2]);
-    int32_t hdr[6];
-    hdr[0] = magic;
-    rd(f, hdr + 1, 5);
-    if (hdr[0] != 0x31484144) return 3;
-    const int n = hdr[1], L = hdr[2], nmat = hdr[3], nsteps = hdr[4], ref_static = hdr[5];
+namespace {
+
+// ---- the flattened mesh every table-building mode reads (see the file comment)
+struct MeshIn {
+    int n = 0, L = 0, nmat = 0, nsteps = 0, flag = 0;
     double sc[5], bed[16];
-    rd(f, sc, 5);
-    rd(f, bed, 16);
-    std::vector<int32_t> nbr(8 * (size_t)n), level(n), ix(n), iy(n), mat(n);
-    rd(f, nbr.data(), nbr.size());
-    rd(f, level.data(), n);
-    rd(f, ix.data(), n);
-    rd(f, iy.data(), n);
-    rd(f, mat.data(), n);
-    std::vector<double> x(n), y(n), dx(n), dy(n), zeta(2 * (size_t)n), grav(3 * (size_t)n), dgrav(2 * (size_t)n),
-        curv(2 * (size_t)n), h(n), hu(n), hv(n);
-    rd(f, x.data(), n); rd(f, y.data(), n); rd(f, dx.data(), n); rd(f, dy.data(), n);
-    rd(f, zeta.data(), zeta.size()); rd(f, grav.data(), grav.size()); rd(f, dgrav.data(), dgrav.size());
-    rd(f, curv.data(), curv.size());
-    rd(f, h.data(), n); rd(f, hu.data(), n); rd(f, hv.data(), n);
-    // statistics inputs (StatProps, properties.h:180-200; DISCHARGE planes): test point height and
-    // position, Vslump, then the discharge planes (xa, xb, ya, yb each)
-    double stat_in[4];
-    rd(f, stat_in, 4);
-    int32_t n_planes = 0;
-    rd(f, &n_planes, 1);
-    std::vector<double> plane_in(4 * (size_t)n_planes);
-    if (n_planes > 0) rd(f, plane_in.data(), plane_in.size());
-    std::fclose(f);
+    std::vector<int32_t> nbr, level, ix, iy, mat;
+    std::vector<double> x, y, dx, dy, zeta, grav, dgrav, curv;
+};
 
-    // ---- MatProps (properties.h:527-640): material ids are 1-based in the reference
-    std::vector<double> bedin(nmat + 1, 0.0);
-    std::vector<char *> names(nmat + 1, nullptr);
+void read_mesh(FILE *f, const int32_t hdr[6], MeshIn &m) {
+    m.n = hdr[1];
+    m.L = hdr[2];
+    m.nmat = hdr[3];
+    m.nsteps = hdr[4];
+    m.flag = hdr[5];
+    const size_t n = (size_t)m.n;
+    rd(f, m.sc, 5);
+    rd(f, m.bed, 16);
+    m.nbr.resize(8 * n);
+    m.level.resize(n);
+    m.ix.resize(n);
+    m.iy.resize(n);
+    m.mat.resize(n);
+    rd(f, m.nbr.data(), m.nbr.size());
+    rd(f, m.level.data(), n);
+    rd(f, m.ix.data(), n);
+    rd(f, m.iy.data(), n);
+    rd(f, m.mat.data(), n);
+    m.x.resize(n); m.y.resize(n); m.dx.resize(n); m.dy.resize(n);
+    m.zeta.resize(2 * n); m.grav.resize(3 * n); m.dgrav.resize(2 * n); m.curv.resize(2 * n);
+    rd(f, m.x.data(), n); rd(f, m.y.data(), n); rd(f, m.dx.data(), n); rd(f, m.dy.data(), n);
+    rd(f, m.zeta.data(), m.zeta.size()); rd(f, m.grav.data(), m.grav.size()); rd(f, m.dgrav.data(), m.dgrav.size());
+    rd(f, m.curv.data(), m.curv.size());
+}
+
+// MatProps (properties.h:527-640): material ids are 1-based in the reference
+struct Props {
+    std::vector<double> bedin;
+    std::vector<char *> names;
+    MatProps *matprops = nullptr;
+};
+
+void make_props(const MeshIn &m, Props &pr) {
     static char nm[] = "m";
-    for (int m = 1; m <= nmat; ++m) {
-        bedin[m] = bed[m - 1];
-        names[m] = nm;
+    pr.bedin.assign(m.nmat + 1, 0.0);
+    pr.names.assign(m.nmat + 1, nullptr);
+    for (int k = 1; k <= m.nmat; ++k) {
+        pr.bedin[k] = m.bed[k - 1];
+        pr.names[k] = nm;
     }
-    MatProps matprops(nmat, names.data(), sc[0], bedin.data(), 0.0, 0.0, sc[1], sc[3], 0.1, 1.0, sc[1], sc[2]);
-    matprops.epsilon = sc[1];
-    matprops.GRAVITY_SCALE = sc[2];
-    matprops.LENGTH_SCALE = 1.0;
-    matprops.HEIGHT_SCALE = sc[1];
-    matprops.gamma = sc[3];
-    matprops.MAX_NEGLIGIBLE_HEIGHT = matprops.HEIGHT_SCALE / 10000.0;  // datread.C:210
-    matprops.Vslump = stat_in[3];
-    TimeProps timeprops;
-    timeprops.inittime(1 << 30, sc[4], HUGE_VAL, HUGE_VAL, 1.0);
-    PileProps pileprops;
-    FluxProps fluxprops;
-    StatProps statprops;
-    statprops.hxyminmax = matprops.MAX_NEGLIGIBLE_HEIGHT * 10.0;  // datread.C:315-316
-    statprops.heightifreach = stat_in[0];
-    statprops.xyifreach[0] = stat_in[1];
-    statprops.xyifreach[1] = stat_in[2];
-    statprops.timereached = -1.0;
-    DISCHARGE discharge;
-    std::vector<double *> plane_rows(n_planes);
-    for (int k = 0; k < n_planes; ++k) plane_rows[k] = &plane_in[4 * (size_t)k];
-    if (n_planes > 0) discharge.init(n_planes, plane_rows.data());
-    OutLine outline;
+    const double *sc = m.sc;
+    pr.matprops = new MatProps(m.nmat, pr.names.data(), sc[0], pr.bedin.data(), 0.0, 0.0, sc[1], sc[3], 0.1, 1.0,
+                               sc[1], sc[2]);
+    MatProps &mp = *pr.matprops;
+    mp.epsilon = sc[1];
+    mp.GRAVITY_SCALE = sc[2];
+    mp.LENGTH_SCALE = 1.0;
+    mp.HEIGHT_SCALE = sc[1];
+    mp.gamma = sc[3];
+    mp.MAX_NEGLIGIBLE_HEIGHT = mp.HEIGHT_SCALE / 10000.0;  // datread.C:210
+}
 
-    // ---- nodes at integer positions (units of half the finest cell)
+// The reference's Node and Element hash tables of a flattened mesh with state (h, hu, hv):
+// nodes at integer positions (units of half the finest cell), node info as constant.h:39-43
+// defines it, elements with positive_x_side = 1.
+struct Tables {
+    HashTable *NodeTable = nullptr, *El_Table = nullptr;
+    std::vector<Element *> els;
+};
+
+Tables build_tables(const MeshIn &m, const double *h, const double *hu, const double *hv, MatProps &matprops,
+                    bool ref_static) {
+    const int n = m.n, L = m.L;
+    const int32_t *nbr = m.nbr.data();
+    const auto &level = m.level;
+    const auto &x = m.x, &y = m.y, &dx = m.dx, &dy = m.dy;
     double fine_dx = 0, fine_dy = 0, x0 = 0, y0 = 0;
     {
         const int sh = L - level[0];
         fine_dx = dx[0] / double(1 << sh);
         fine_dy = dy[0] / double(1 << sh);
-        x0 = x[0] - (ix[0] + 0.5) * dx[0];
-        y0 = y[0] - (iy[0] + 0.5) * dy[0];
+        x0 = x[0] - (m.ix[0] + 0.5) * dx[0];
+        y0 = y[0] - (m.iy[0] + 0.5) * dy[0];
     }
     std::map<std::pair<int64_t, int64_t>, NodeRec> nodes;
     std::vector<std::array<std::pair<int64_t, int64_t>, 9>> cell_nodes(n);
@@ -283,7 +291,7 @@ int main(int argc, char **argv) {
     };
     for (int c = 0; c < n; ++c) {
         const int64_t s = int64_t(1) << (L - level[c] + 1);
-        const int64_t X0 = ix[c] * s, Y0 = iy[c] * s;
+        const int64_t X0 = m.ix[c] * s, Y0 = m.iy[c] * s;
         const int64_t P[9][2] = {{X0, Y0}, {X0 + s, Y0}, {X0 + s, Y0 + s}, {X0, Y0 + s},
                                  {X0 + s / 2, Y0}, {X0 + s, Y0 + s / 2}, {X0 + s / 2, Y0 + s}, {X0, Y0 + s / 2},
                                  {X0 + s / 2, Y0 + s / 2}};
@@ -307,8 +315,9 @@ int main(int argc, char **argv) {
     double dkr[2] = {double(maxX + 2), double(maxY + 2)};
     double XR[2] = {x0, x0 + (maxX + 1) * 0.5 * fine_dx}, YR[2] = {y0, y0 + (maxY + 1) * 0.5 * fine_dy};
     const int nb = std::max(1024, 2 * (int)nodes.size());
-    HashTable *NodeTable = new HashTable(dkr, nb, 2017, XR, YR, 0);
-    HashTable *El_Table = new HashTable(dkr, std::max(1024, 2 * n), 2017, XR, YR, 0);
+    Tables t;
+    t.NodeTable = new HashTable(dkr, nb, 2017, XR, YR, 0);
+    t.El_Table = new HashTable(dkr, std::max(1024, 2 * n), 2017, XR, YR, 0);
     auto keyof = [](const std::pair<int64_t, int64_t> &p, unsigned k[2]) {
         k[0] = unsigned(p.first + 1);  // +1 keeps {0,0} free: it is the boundary's "NULL" neighbour key
         k[1] = unsigned(p.second + 1);
@@ -318,9 +327,10 @@ int main(int argc, char **argv) {
         keyof(kv.first, k);
         double co[2] = {kv.second.x, kv.second.y};
         Node *nd = new Node(k, co, kv.second.info, 0.0, 0);
-        NodeTable->add(k, nd);
+        t.NodeTable->add(k, nd);
     }
-    std::vector<Element *> els(n);
+    t.els.resize(n);
+    const double eps = m.sc[1];
     for (int c = 0; c < n; ++c) {
         Element *e = new Element();
         keyof(cell_nodes[c][8], e->key);
@@ -343,7 +353,7 @@ int main(int argc, char **argv) {
             e->neigh_gen[a] = e->neigh_gen[a + 4] = e1 >= 0 ? level[e1] : 0;
         }
         e->generation = level[c];
-        e->material = mat[c] + 1;
+        e->material = m.mat[c] + 1;
         e->adapted = NOTRECADAPTED;
         e->refined = 0;
         e->myprocess = 0;
@@ -356,27 +366,185 @@ int main(int argc, char **argv) {
         e->state_vars[2] = hv[c];
         for (int v = 0; v < 3; ++v) e->prev_state_vars[v] = e->state_vars[v];
         for (int v = 0; v < 6; ++v) e->d_state_vars[v] = 0.0;
-        e->kactxy[0] = e->kactxy[1] = sc[1];
-        e->effect_kactxy[0] = e->effect_kactxy[1] = sc[1];
-        e->zeta[0] = zeta[c];
-        e->zeta[1] = zeta[(size_t)n + c];
-        e->curvature[0] = curv[c];
-        e->curvature[1] = curv[(size_t)n + c];
-        for (int k = 0; k < 3; ++k) e->gravity[k] = grav[(size_t)k * n + c];
-        for (int k = 0; k < 2; ++k) e->d_gravity[k] = dgrav[(size_t)k * n + c];
+        e->kactxy[0] = e->kactxy[1] = eps;
+        e->effect_kactxy[0] = e->effect_kactxy[1] = eps;
+        e->zeta[0] = m.zeta[c];
+        e->zeta[1] = m.zeta[(size_t)n + c];
+        e->curvature[0] = m.curv[c];
+        e->curvature[1] = m.curv[(size_t)n + c];
+        for (int k = 0; k < 3; ++k) e->gravity[k] = m.grav[(size_t)k * n + c];
+        for (int k = 0; k < 2; ++k) e->d_gravity[k] = m.dgrav[(size_t)k * n + c];
         e->elevation = 0.0;
         for (int v = 0; v < 3; ++v) e->Influx[v] = 0.0;
         e->stoppedflags = 0;
         e->Awet = 1.0;
         e->Swet = 1.0;
         e->iwetnode = 8;
-        El_Table->add(e->key, e);
-        els[c] = e;
+        t.El_Table->add(e->key, e);
+        t.els[c] = e;
     }
     if (ref_static) {
-        for (int c = 0; c < n; ++c) els[c]->calc_gravity_vector(&matprops);
-        for (int c = 0; c < n; ++c) els[c]->calc_d_gravity(El_Table);
+        for (int c = 0; c < n; ++c) t.els[c]->calc_gravity_vector(&matprops);
+        for (int c = 0; c < n; ++c) t.els[c]->calc_d_gravity(t.El_Table);
     }
+    return t;
+}
+
+// ---- 'DAJ1': the reference's own adjoint, reverse steps from a given lambda
+//
+// Input after the mesh (header: 'DAJ1', n, max_level, n_materials, K reverse steps, 0):
+//   int32 iter[K]           the adjoint iteration of each reverse step, descending (iter = the
+//                           forward step U^{iter-1} -> U^iter that is taken back)
+//   double dt[K]            TimeProps::dt.at(iter - 1) of each
+//   double state[K][3][n]   U^{iter-1}: h, hu, hv
+//   double lambda[3][n]     the adjoint of the first reverse step's U^{iter}
+// Output: 'DJO1', n, K; double lambda[K][3][n] after each reverse step; double seconds.
+//
+// The forward states go through the reference's SolRec (record_solution's rule: a zero record
+// for h <= 0), the dual elements are the reference's DualElem copies of the elements
+// (dual_solver.C:101-106), and each reverse step runs update_dual_grid (prev state and
+// prev adjoint, get_slopes_prev + hslope_sens, gmfggetcoef, calc_flux with the flux Jacobians,
+// dual_grid_routines.C:15-93), calc_jacobian (calc_jacobain.C:40-153) and calc_adjoint
+// (calc_adjoint.C:35-167) as dual_solver does at dual_solver.C:197-206, with the functional
+// sensitivity zero (the MaxH functional's iteration never matches).
+int adjoint_mode(FILE *f, const int32_t hdr[6], const char *out) {
+    MeshIn m;
+    read_mesh(f, hdr, m);
+    const int n = m.n, K = m.nsteps;
+    std::vector<int32_t> iters(K);
+    std::vector<double> dts(K), states((size_t)K * 3 * n), lam((size_t)3 * n);
+    rd(f, iters.data(), K);
+    rd(f, dts.data(), K);
+    rd(f, states.data(), states.size());
+    rd(f, lam.data(), lam.size());
+    std::fclose(f);
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    Tables t = build_tables(m, states.data(), states.data() + n, states.data() + 2 * (size_t)n, matprops, false);
+
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, HUGE_VAL, HUGE_VAL, HUGE_VAL, 1.0);
+    int maxit = 0;
+    for (int k = 0; k < K; ++k) maxit = std::max(maxit, (int)iters[k]);
+    timeprops.dt.assign(maxit + 1, 0.0);
+    for (int k = 0; k < K; ++k) timeprops.dt[iters[k] - 1] = dts[k];
+    timeprops.adjiter = 1;  // not the seeding pass of calc_adjoint_elem
+
+    // dual grid: one DualElem per element, in the element table's own bucket structure
+    HashTable *Dual_El_Tab = new HashTable(t.El_Table);
+    std::vector<DualElem *> duals(n);
+    for (int c = 0; c < n; ++c) {
+        DualElem *d = new DualElem(t.els[c]);
+        Dual_El_Tab->add(d->pass_key(), d);
+        duals[c] = d;
+        for (int v = 0; v < 3; ++v) d->get_adjoint()[v] = lam[(size_t)v * n + c];
+    }
+    // forward records of every state the sweep takes back
+    SolRec *solrec = make_solrec();
+    for (int c = 0; c < n; ++c) {
+        Jacobian *j = new Jacobian(t.els[c]->key);
+        solrec->add(j->get_key(), j);
+        for (int k = 0; k < K; ++k) {
+            const double *U = states.data() + (size_t)k * 3 * n;
+            if (U[c] > 0.) {
+                double s[3] = {U[c], U[(size_t)n + c], U[(size_t)2 * n + c]};
+                j->put_solution(new Solution(s), iters[k] - 1);
+            } else {
+                j->put_solution(&(Solution::solution_zero), iters[k] - 1);
+            }
+        }
+    }
+    MeshCTX mctx;
+    mctx.el_table = Dual_El_Tab;
+    mctx.nd_table = t.NodeTable;
+    PropCTX pctx;
+    pctx.matprops = &matprops;
+    pctx.timeprops = &timeprops;
+    pctx.mapnames = nullptr;
+    pctx.outline = nullptr;
+    pctx.numproc = 1;
+    pctx.myid = 0;
+    pctx.adapt_flag = 0;
+
+    std::vector<double> outv((size_t)K * 3 * n);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < K; ++k) {
+        timeprops.iter = iters[k];
+        update_dual_grid(solrec, &mctx, &pctx);
+        calc_jacobian(&mctx, &pctx);
+        calc_adjoint(&mctx, &pctx);
+        for (int c = 0; c < n; ++c)
+            for (int v = 0; v < 3; ++v) outv[((size_t)k * 3 + v) * n + c] = duals[c]->get_adjoint()[v];
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    FILE *o = std::fopen(out, "wb");
+    if (!o) return 2;
+    const int32_t oh[3] = {0x314F4A44, n, K};
+    wr(o, oh, 3);
+    wr(o, outv.data(), outv.size());
+    wr(o, &secs, 1);
+    std::fclose(o);
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    if (argc != 3) {
+        std::fprintf(stderr, "usage: ref_harness in.bin out.bin\n");
+        return 2;
+    }
+    FILE *f = std::fopen(argv[1], "rb");
+    if (!f) return 2;
+    int32_t magic;
+    rd(f, &magic, 1);
+    if (magic == 0x314B4144) return keys_mode(f, argv[2]);
+    if (magic == 0x31574144) return write_mode(f, argv[2]);
+    if (magic == 0x31524144) return read_mode(f, argv[2]);
+    int32_t hdr[6];
+    hdr[0] = magic;
+    rd(f, hdr + 1, 5);
+    if (hdr[0] == 0x314A4144) return adjoint_mode(f, hdr, argv[2]);
+    if (hdr[0] != 0x31484144) return 3;
+    MeshIn m;
+    read_mesh(f, hdr, m);
+    const int n = m.n, nsteps = m.nsteps, ref_static = m.flag;
+    std::vector<double> h(n), hu(n), hv(n);
+    rd(f, h.data(), n); rd(f, hu.data(), n); rd(f, hv.data(), n);
+    // statistics inputs (StatProps, properties.h:180-200; DISCHARGE planes): test point height and
+    // position, Vslump, then the discharge planes (xa, xb, ya, yb each)
+    double stat_in[4];
+    rd(f, stat_in, 4);
+    int32_t n_planes = 0;
+    rd(f, &n_planes, 1);
+    std::vector<double> plane_in(4 * (size_t)n_planes);
+    if (n_planes > 0) rd(f, plane_in.data(), plane_in.size());
+    std::fclose(f);
+
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    matprops.Vslump = stat_in[3];
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, m.sc[4], HUGE_VAL, HUGE_VAL, 1.0);
+    PileProps pileprops;
+    FluxProps fluxprops;
+    StatProps statprops;
+    statprops.hxyminmax = matprops.MAX_NEGLIGIBLE_HEIGHT * 10.0;  // datread.C:315-316
+    statprops.heightifreach = stat_in[0];
+    statprops.xyifreach[0] = stat_in[1];
+    statprops.xyifreach[1] = stat_in[2];
+    statprops.timereached = -1.0;
+    DISCHARGE discharge;
+    std::vector<double *> plane_rows(n_planes);
+    for (int k = 0; k < n_planes; ++k) plane_rows[k] = &plane_in[4 * (size_t)k];
+    if (n_planes > 0) discharge.init(n_planes, plane_rows.data());
+    OutLine outline;
+
+    Tables t = build_tables(m, h.data(), hu.data(), hv.data(), matprops, ref_static != 0);
+    HashTable *El_Table = t.El_Table, *NodeTable = t.NodeTable;
+    std::vector<Element *> &els = t.els;
 
     // ---- time loop of the driver (hpfem.C:222-357) with adaptation off
     std::vector<double> dts(nsteps);

@@ -1,4 +1,4 @@
-"""Recipe: compile the reference's own step() numerics into oracle/_ref/ref_harness.
+"""Recipe: compile the reference's own step() and adjoint numerics into oracle/_ref/ref_harness.
 
 TEST INFRASTRUCTURE ONLY (the checker, never the product).  Reads the reference sources where
 they lie under /root/reference/src and writes only into oracle/_ref/.  The reference's own
@@ -31,6 +31,9 @@ UNITS = [
     "geoflow/corrector.C", "geoflow/stats.C", "geoflow/move_data.C", "geoflow/flux_srcs.C",
     "datstr/element2.C", "datstr/node.C", "datstr/hashtab2.C", "datstr/dualmesh.C", "datstr/jacobian.C",
     "adjoint/residual.C", "useful/useful_lib.C", "main/compare_key.C", "main/hilbert.C",
+    # the reference's adjoint of one step (the harness's 'DAJ1' mode)
+    "adjoint/dual_grid_routines.C", "adjoint/calc_jacobain.C", "adjoint/compute_jacobian_elem.C",
+    "adjoint/calc_adjoint.C", "adjoint/debug_routines.C",
 ]
 PATCH = {
     "geoflow/edge_states.C": [(r"Curr_El->calc_edge_states<T>\(", "Curr_El->template calc_edge_states<T>(")],

@@ -9,6 +9,16 @@ Fixture "static_*" also holds gravity and d_gravity from Element::calc_gravity_v
 Element::calc_d_gravity.  Fixture "stats_*" holds calc_stats' StatProps after the last step and
 the discharge through two planes accumulated over all steps (DISCHARGE::update), with the test
 point, Vslump and planes it was run with.
+
+Fixtures "adj_*" hold the reference's own discrete adjoint (its dual solver's update_dual_grid,
+calc_jacobian and calc_adjoint, run through the harness's 'DAJ1' mode):
+  adj_s11_60     the reverse sweep over the 60 steps of fwd_s11_60's mesh and initial state,
+                 seeded with lambda^N = dJ/dU^N of J = sum h^2 dx dy over a box, with lambda after
+                 1, 10, 30 and 60 reverse steps (the forward states are the oracle's, which equal
+                 the reference's step() bit for bit; checked here against a harness run);
+  adj_stress_s12 one reverse step from a synthetic state (thin and dry cells, dry cells with
+                 momentum, random adjoint) at an iteration past the frict_tiny switch.
+Run only these with:   python tests/golden/make_golden.py adj
 """
 import os
 import sys
@@ -75,8 +85,92 @@ def hilbert_keys():
     print(p)
 
 
+ADJ_KEEP = (1, 10, 30, 60)
+
+
+def adjoint_sweep_case(name="adj_s11_60", seed=11, nsteps=60):
+    from discrete_adjoint_b200 import TimeProps, make_params
+    w = inputs.test_case(seed=seed, nx0=12, ny0=8, max_level=2, random_frac=0.4)
+    m = w.mesh
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+    states, dts = [(h.copy(), hu.copy(), hv.copy())], []
+    for _ in range(nsteps):
+        rc, dt, _st = o.run(h, hu, hv, 1)
+        assert rc == 0
+        dts.append(float(dt[0]))
+        states.append((h.copy(), hu.copy(), hv.copy()))
+    r = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, nsteps)
+    assert np.array_equal(r["h"], states[-1][0]) and np.array_equal(r["dt"], np.array(dts))
+    wet = states[-1][0] > 1e-4
+    cx, cy = float(m.x[wet].mean()), float(m.y[wet].mean())
+    box = np.array([cx - 150.0, cx + 150.0, cy - 150.0, cy + 150.0])
+    inb = (m.x >= box[0]) & (m.x <= box[1]) & (m.y >= box[2]) & (m.y <= box[3])
+    lam_end = np.zeros((3, m.n))
+    lam_end[0] = np.where(inb, 2.0 * states[-1][0] * m.dx * m.dy, 0.0)
+    iters = list(range(nsteps, 0, -1))
+    ra = oracle.run_reference_adjoint(m, w.mat, [states[i - 1] for i in iters], iters, [dts[i - 1] for i in iters],
+                                      lam_end)
+    arrs = {("mesh_" + k): v for k, v in m.arrays().items()}
+    arrs["nsteps"] = np.int64(nsteps)
+    arrs["dts"] = np.array(dts)
+    arrs["box"] = box
+    arrs["lam_end"] = lam_end
+    arrs["keep_steps"] = np.array(ADJ_KEEP)
+    arrs["ref_lam"] = np.stack([ra["lam"][k - 1] for k in ADJ_KEEP])
+    arrs["intfrict_deg"] = np.float64(w.mat.intfrict_deg)
+    arrs["bedfrict_deg"] = np.array(w.mat.bedfrict_deg, dtype=np.float64)
+    p = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(p, **arrs)
+    print(p, m.n, "cells", os.path.getsize(p) // 1024, "KiB")
+
+
+def stress_state(m, rng):
+    """A synthetic state with deep, thin (below GEOFLOW_TINY) and dry cells, some dry cells
+    carrying momentum."""
+    n = m.n
+    h = np.maximum(0.0, rng.normal(0.6, 1.0, n))
+    thin = rng.random(n) < 0.1
+    h[thin] = rng.uniform(0.0, 3e-4, thin.sum())
+    hu = rng.normal(0, 3.0, n) * np.minimum(h, 1.0)
+    hv = rng.normal(0, 3.0, n) * np.minimum(h, 1.0)
+    vm = (h == 0) & (rng.random(n) < 0.5)
+    hu[vm] = rng.normal(0, 1e-3, vm.sum())
+    hv[vm] = rng.normal(0, 1e-3, vm.sum())
+    return h, hu, hv
+
+
+def adjoint_stress_case(name="adj_stress_s12", seed=12, it=70):
+    from discrete_adjoint_b200 import TimeProps, make_params
+    w = inputs.test_case(seed=seed, nx0=12, ny0=8, max_level=2, random_frac=0.3)
+    m = w.mesh
+    rng = np.random.default_rng(seed)
+    h, hu, hv = stress_state(m, rng)
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    o.set_time(0.0, it - 1)
+    h2, hu2, hv2 = h.copy(), hu.copy(), hv.copy()
+    rc, dts, _st = o.run(h2, hu2, hv2, 1)
+    assert rc == 0
+    lam = rng.standard_normal((3, m.n))
+    ra = oracle.run_reference_adjoint(m, w.mat, [(h, hu, hv)], [it], [float(dts[0])], lam)
+    arrs = {("mesh_" + k): v for k, v in m.arrays().items()}
+    arrs.update({"h": h, "hu": hu, "hv": hv, "iter": np.int64(it), "dt": np.float64(dts[0]), "lam_next": lam,
+                 "ref_lam": ra["lam"][0]})
+    arrs["intfrict_deg"] = np.float64(w.mat.intfrict_deg)
+    arrs["bedfrict_deg"] = np.array(w.mat.bedfrict_deg, dtype=np.float64)
+    p = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(p, **arrs)
+    print(p, m.n, "cells", os.path.getsize(p) // 1024, "KiB")
+
+
 def main():
     ref_build.build()
+    if sys.argv[1:] == ["adj"]:
+        adjoint_sweep_case()
+        adjoint_stress_case()
+        return
+    adjoint_sweep_case()
+    adjoint_stress_case()
     hilbert_keys()
     for case in STATS_CASES:
         stats_case(*case)
