@@ -25,8 +25,13 @@ rank, "weak" scaling, no data-path collective); the ensemble's members are split
 (size-balanced greedy partition) with one gather of the per-member results; barrier and max over
 ranks stay.
 
---impl reference: the reference's own step() compiled from its sources (oracle/_ref/ref_harness,
-when built) timed on this host, else the oracle restatement; rank 0 only.
+--impl reference: the reference's own forward + adjoint compiled from its sources
+(oracle/_ref/ref_harness, mode 'DAF1': step() with the driver's solution recording, then the dual
+solver's update_dual_grid / calc_jacobian / calc_adjoint) on the same 1M-cell workload, timed on
+this host, one step at a time; rank 0 only.  Its mesh comes from oracle/meshgen.py (numpy, equal
+to the product's mesh builder bit for bit), so the process never loads libda_b200.so.  One
+"step" of that arm is one forward step and its reverse step over all 1M cells (the metric's unit
+of work); --warmup steps run forward first and are neither timed nor taken back.
 """
 from __future__ import annotations
 
@@ -45,6 +50,7 @@ if ROOT not in sys.path:
 import numpy as np  # noqa: E402
 
 METRIC = "cell-updates/s fwd+adjoint, FP32-split & batched vs plain FP64 GPU at ≤1e-5 rel err"
+HEADLINE_WORKLOAD = "inclined-plane 5km x 5km uniform 1024^2, 1 pile"
 HORIZON = 512
 SNAPSHOTS = 32
 ENS_STEPS = 300
@@ -114,15 +120,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples_under_load": len(sm)}
 
 
-def dist_init():
+def dist_init(impl: str = "ours"):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
+    if ws > 1 and impl == "ours":
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        # each rank's collectives and barriers on its own GPU
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     return ws, rank, local
 
 
@@ -171,34 +180,32 @@ def wet_counts(m, h) -> tuple[int, int]:
     return int(wet.sum()), int(act.sum())
 
 
-def algorithmic_bytes(precision: str, n: int, n_wet: float, n_act: float) -> dict:
-    """Algorithmic HBM bytes of one launch of each kernel over the whole mesh: every array a cell
-    needs is touched once; neighbour re-reads are halo traffic, not algorithmic.  Layout of
-    csrc/da_internal.h, r = bytes per real (8 FP64, 4 FP32):
-      k_coef        every cell reads h; a wet cell reads hu, hv, bflag, mat, nbr (4 x int32), dx,
-                    dy, g_z (+ x, y in FP64) and writes k_act
-      k_update      every cell reads bflag, the state, dx, dy and writes the state; an active cell
-                    also reads nbr, k_act, g (3), d_gravity (2), curvature (2), mat
-      k_*_record    as above plus one mask byte written per cell
-      k_adj_src     every cell reads h; a wet cell reads hu, hv, lambda (hu, hv), mask, bflag, mat,
-                    nbr, statics (dx, dy, g, dg, curv [+ x, y]) and writes A (3 x 8) and B (4 x 8)
-                    and updates two FP64 sensitivities
-      k_adj_gather  every cell reads its mask byte and lambda and writes lambda; an active cell also
-                    reads h, bflag, nbr, A (3 x 8) and updates two FP64 sensitivities
-    The multi-step kernel k_steps counts coef + update per time step; the fused reverse step
-    k_youturn counts the two recording phases, k_adj_src and k_adj_gather; a snapshot copy
-    reads and writes the state once (3 x r x n each way).
-    These are full-sweep figures: tile culling skips the cells of dry tiles, so a culled launch
-    touches fewer bytes than this (the ncu capture's DRAM traffic shows how many)."""
+def bytes_per_cell_update(precision: str) -> dict:
+    """Algorithmic HBM bytes of one cell through one step (each array the cell needs touched once;
+    neighbour re-reads are halo traffic, intermediates such as k act/pass are not counted), the rule
+    of the per-unit figures for this path with the arrays of the committed layout
+    (csrc/da_internal.h), r = 8 (FP64) / 4 (FP32-split) bytes per real:
+      forward:  state in 3r + state out 3r + g (3), d_gravity (2), curvature (2) 7r + material and
+                boundary flags 2 + neighbour table 4 x int32 16 + cell sizes 2r (+ centres 2 x 8 in
+                FP64, whose slopes take centre differences as the reference does)
+      adjoint:  lambda in 3r + U 3r + the same statics, flags, neighbours, sizes (and centres) +
+                branch byte 1 + lambda out 3r
+    FP64: forward 154 B, adjoint 179 B; FP32-split: 78 B and 91 B."""
     r = 8 if precision == "fp64" else 4
-    xy = 2 * r if precision == "fp64" else 0
-    coef = n * r + n_wet * (2 * r + 1 + 1 + 16 + 2 * r + r + xy + r)
-    upd = n * (1 + 3 * r + 2 * r + 3 * r) + n_act * (16 + r + 3 * r + 2 * r + 2 * r + 1)
-    src = n * r + n_wet * (2 * r + 2 * r + 1 + 1 + 1 + 16 + 2 * r + 7 * r + xy + 24 + 32 + 32)
-    gat = n * (1 + 3 * r + 3 * r) + n_act * (r + 1 + 16 + 24 + 32)
-    return {"k_coef": coef, "k_update": upd, "k_coef_record": coef + n, "k_update_record": upd + n,
-            "k_adj_src": src, "k_adj_gather": gat, "k_steps": coef + upd,
-            "k_youturn": coef + upd + 2 * n + src + gat, "snapshot_copy": 2 * 3 * r * n}
+    xy = 16 if precision == "fp64" else 0
+    statics = 7 * r + 2 + 16 + 2 * r + xy
+    return {"forward": 6 * r + statics, "adjoint": 9 * r + statics + 1}
+
+
+def algorithmic_bytes(precision: str, n_act: float) -> dict:
+    """Algorithmic bytes of one launch of each kernel per time step it covers, over the cells the
+    step actually processes (n_act: wet cells and their face neighbours; tile culling leaves the
+    others untouched): k_steps one forward step, k_youturn one reverse step (the replayed forward
+    step and the adjoint step), a checkpoint copy the state of those cells each way."""
+    b = bytes_per_cell_update(precision)
+    r = 8 if precision == "fp64" else 4
+    return {"k_steps": b["forward"] * n_act, "k_youturn": (b["forward"] + b["adjoint"]) * n_act,
+            "snapshot_copy": 2 * 3 * r * n_act}
 
 
 # DRAM bytes (read + write) per launch from the committed ncu captures (profiles/), keyed by
@@ -216,46 +223,53 @@ def traffic_per_launch(precision: str, kernel: str):
     return TRAFFIC.get((precision, kernel))
 
 
-def reference_forward_rate(w, max_seconds: float = 20.0):
-    """cell-updates/s of the reference's own step() (oracle/_ref/ref_harness) on this host, or of the
-    oracle restatement when the harness is not built; (rate, kind, sample)."""
+def reference_fwdadj(steps: int, warm: int, side: int = 1024) -> dict:
+    """The reference's own forward + adjoint on the headline workload, timed on this host: `warm`
+    forward steps untimed, then `steps` forward steps with the driver's solution recording and
+    their `steps` reverse steps of the dual solver, each timed (oracle/_ref/ref_harness, mode
+    'DAF1'); the oracle's restatement when the harness is not built.  One cell-update is one cell
+    advanced one forward step and taken back through its reverse step, as in the GPU arm.  The
+    mesh comes from oracle/meshgen.py, so libda_b200.so is never loaded."""
     import oracle
-    from discrete_adjoint_b200 import TimeProps, make_params
-    m = w.mesh
+    from discrete_adjoint_b200.inputs import WORKLOAD3_BOX
+    from discrete_adjoint_b200.mesh import Mesh
+    from discrete_adjoint_b200.solver import MatProps
+    from oracle import meshgen
+    m = Mesh(**meshgen.headline_mesh(side))
+    mat = MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0])
     if oracle.reference_available():
-        r1 = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, 2)
-        per = max(r1["step_seconds"] / 2, 1e-6)
-        steps = int(max(2, min(200, max_seconds / per)))
-        r = oracle.run_reference(m, w.mat, m.h0, m.hu0, m.hv0, steps)
-        return (m.n * steps / r["step_seconds"], "reference",
-                f"{steps} steps of the {m.n}-cell workload through the reference's own step() "
-                "(compiled from its sources by oracle/ref_build.py), 1 thread, wall time of the step loop")
-    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
-    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
-    t0 = time.perf_counter()
-    o.run(h, hu, hv, 1)
-    per = time.perf_counter() - t0
-    steps = int(max(1, min(200, max_seconds / max(per, 1e-6))))
-    t0 = time.perf_counter()
-    o.run(h, hu, hv, steps)
-    dt = time.perf_counter() - t0
-    return (m.n * steps / dt, "port",
-            f"{steps} steps of the {m.n}-cell workload through the oracle restatement, 1 thread")
+        r = oracle.run_reference_fwdadj(m, mat, warm + steps, warm, WORKLOAD3_BOX)
+        fwd, rev = r["fwd_seconds"][warm:], r["rev_seconds"]
+        kind = "reference"
+        how = ("the reference's own step() + SolRec::record_solution, then update_dual_grid + "
+               "calc_jacobian + calc_adjoint (compiled from its sources by oracle/ref_build.py)")
+    else:
+        fwd, rev = oracle.time_port_fwdadj(m, mat, warm, steps, WORKLOAD3_BOX)
+        kind = "port"
+        how = "the oracle's restatement of the reference's step() and dual-solver step"
+    secs = float(np.sum(fwd) + np.sum(rev))
+    return {"value": m.n * steps / secs, "ms_per_step": 1e3 * secs / steps, "kind": kind, "cells": m.n,
+            "fwd_s_per_step": float(np.mean(fwd)), "rev_s_per_step": float(np.mean(rev)),
+            "sample": f"{steps} forward steps and their {steps} reverse steps of the {m.n}-cell workload "
+                      f"(after {warm} untimed forward steps) through {how}; 1 thread (the reference "
+                      "is single-rank MPI code with no threading), wall time of each step"}
 
 
 def run_reference_arm(args, ws, rank):
     if rank != 0:
         return
-    from discrete_adjoint_b200 import inputs
-    w = inputs.workload3()
-    v, kind, sample = reference_forward_rate(w)
+    from discrete_adjoint_b200.inputs import WORKLOAD3_BOX
+    r = reference_fwdadj(args.steps, args.warmup)
+    v = r["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w.mesh.n * HORIZON / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "cells": w.mesh.n, "horizon": HORIZON,
-                       "note": "forward steps only: the reference's adjoint driver takes a single backward step "
-                               "(dual_solver.C:183-207), so its forward rate bounds a CPU fwd+adjoint rate from above"},
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": kind, "sample": sample},
+            "config": {"workload": HEADLINE_WORKLOAD, "cells": r["cells"], "horizon": HORIZON,
+                       "functional": "sum h^2 dx dy over box " + str(WORKLOAD3_BOX), "precision": "fp64",
+                       "step": "one forward step and its reverse (adjoint) step over every cell",
+                       "forward_s_per_step": r["fwd_s_per_step"], "reverse_s_per_step": r["rev_s_per_step"]},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": r["kind"],
+                             "sample": r["sample"]},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -372,10 +386,12 @@ def forward_config2(args, ws, local):
         r = {"value": m.n * 300 * ws / (ms * 1e-3), "us_per_step": 1e3 * ms / 300, "wet_cells": wv,
              "active_cells": av, "launch_shape": {"blocks_per_sm": tune["best"][0], "grid": tune["best"][1]}}
         if layer > 0:
-            bytes_step = algorithmic_bytes("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32", m.n, wv, av)["k_steps"]
+            pn = "fp64" if prec == _ffi.DA_PREC_FP64 else "fp32"
+            bytes_step = algorithmic_bytes(pn, av)["k_steps"]
             gbs = bytes_step / (ms * 1e-3 / 300) / 1e9
-            r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step, "achieved": gbs, "peak": hbm,
-                             "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind,
+            r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step,
+                             "bytes_per_cell_update": bytes_per_cell_update(pn)["forward"], "achieved": gbs,
+                             "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind,
                              "traffic": traffic_per_launch("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32",
                                                            "k_steps_dense_per_step")}
         res[name] = r
@@ -454,12 +470,11 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    ws, rank, local = dist_init()
+    ws, rank, local = dist_init(args.impl)
     if args.impl == "reference":
+        # rank 0 alone runs the CPU reference; the other ranks exit without work (no process
+        # group: nothing is exchanged)
         run_reference_arm(args, ws, rank)
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
         return
 
     from discrete_adjoint_b200 import inputs
@@ -485,7 +500,7 @@ def main():
     # roofline of the dominant kernel of the traced headline run
     tr = hr["trace"]
     dom = max(tr, key=lambda k: tr[k][0])
-    alg = algorithmic_bytes(head, m.n, r["n_wet"], r["n_act"])
+    alg = algorithmic_bytes(head, r["n_act"])
     hbm, peak_kind = peaks()
     avg_ms = tr[dom][0] / tr[dom][1]
     steps_per_launch = tr[dom][2] / tr[dom][1]
@@ -500,9 +515,9 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, kind, sample = reference_forward_rate(w, 15.0)
-        cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": kind,
-               "sample": sample + "; forward steps only (no CPU fwd+adjoint sweep exists)"}
+        rc = reference_fwdadj(2, 0)
+        cpu = {"value": rc["value"], "unit": "cell-updates/s", "cores": 1, "kind": rc["kind"],
+               "sample": rc["sample"]}
 
     if rank == 0:
         launches_per_run = sum(v[1] for v in tr.values())
@@ -510,7 +525,7 @@ def main():
             "metric": METRIC, "value": hr["value"], "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": hr["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32", "data": "synthetic",
-            "config": {"workload": w.name, "cells": m.n, "horizon": HORIZON, "snapshots": SNAPSHOTS,
+            "config": {"workload": HEADLINE_WORKLOAD, "cells": m.n, "horizon": HORIZON, "snapshots": SNAPSHOTS,
                        "functional": "sum h^2 dx dy over box " + str(inputs.WORKLOAD3_BOX),
                        "precision": "fp64" if head == "fp64" else "fp32-split",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
@@ -523,6 +538,8 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg.get(dom, 0.0) * steps_per_launch,
+                         "bytes_per_cell_update": bytes_per_cell_update(head),
+                         "alg_cells": "active cells (wet or next to a wet cell), the cells the kernel processes",
                          "steps_per_launch": steps_per_launch,
                          "avg_launch_ms": avg_ms, "wet_cells_avg": r["n_wet"], "active_cells_avg": r["n_act"],
                          "trace_ms_launches_steps": {k: [round(v[0], 4), v[1], v[2]] for k, v in tr.items()},

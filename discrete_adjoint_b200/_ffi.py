@@ -202,6 +202,7 @@ class da_member(C.Structure):
 # name -> (restype, argtypes) for every symbol the headers declare
 SIGNATURES = {
     "da_abi_version": (C.c_int, []),
+    "da_selftest_barrier": (C.c_int, [C.c_void_p, C.c_int32]),
     "da_strerror": (C.c_char_p, [C.c_int]),
     "da_params_default": (None, [C.POINTER(da_params)]),
     "da_create": (C.c_void_p, [C.POINTER(da_params), C.POINTER(C.c_int)]),

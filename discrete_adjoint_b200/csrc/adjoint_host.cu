@@ -299,7 +299,7 @@ int sync_check(da_ctx *ctx) {
     int st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
                         "read scalars");
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "device error during the adjoint sweep");
+    if (!st) st = device_error(ctx, "adjoint sweep");
     return st;
 }
 

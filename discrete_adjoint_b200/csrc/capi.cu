@@ -232,23 +232,25 @@ static int build_halo(da_ctx *ctx, const int32_t *nbr, int n) {
     return st;
 }
 
+int device_error(da_ctx *ctx, const char *where) {
+    const int code = ctx->hsc->err;
+    if (!code) return DA_OK;
+    if (code == DA_ERR_TIMEOUT) {
+        // a cooperative launch gave up at a grid barrier and every block has returned: the next
+        // launch starts from a barrier word with no arrivals and generation 0
+        cudaMemsetAsync(&ctx->dsc->bar, 0, sizeof(unsigned long long), ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    return set_error(ctx, code, std::string(where) + ": " + da_strerror(code));
+}
+
 static int sync_scalars(da_ctx *ctx) {
     int st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
                         "read scalars");
     if (st) return st;
     st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
     if (st) return st;
-    if (ctx->hsc->err == DA_ERR_TIMEOUT) {
-        // a multi-step launch gave up at a grid barrier: restart its arrival count
-        cudaMemsetAsync(&ctx->dsc->bar, 0, sizeof(unsigned), ctx->stream);  // the arrivals (low half)
-        cudaStreamSynchronize(ctx->stream);
-    }
-    if (ctx->hsc->err) {
-        const int code = ctx->hsc->err;
-        return set_error(ctx, code, code == DA_ERR_EIGEN ? "wave speed above 1e9 (get_coef_and_eigen)"
-                                                         : "non-finite state after update (update_states)");
-    }
-    return DA_OK;
+    return device_error(ctx, "forward step");
 }
 
 void update_grid(da_ctx *ctx) {
@@ -444,6 +446,24 @@ void da_destroy(da_ctx *ctx) {
 
 const char *da_last_error(const da_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int da_selftest_barrier(da_ctx *ctx, int32_t limit_us) {
+    if (!ctx || limit_us <= 0 || limit_us > 4000000) return DA_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    int st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (!st) st = launch_barrier_selftest(ctx, 1000ull * (unsigned long long)limit_us);
+    if (st) return st;
+    st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream),
+                    "read scalars");
+    if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    if (st) return st;
+    const int code = device_error(ctx, "barrier self-test");
+    // the context stays usable: the error the test provoked is cleared
+    ctx->hsc->err = 0;
+    const int st2 = cuda_check(ctx, cudaMemsetAsync(&ctx->dsc->err, 0, sizeof(int), ctx->stream), "memset");
+    const int st3 = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
+    return st2 ? st2 : (st3 ? st3 : code);
+}
+
 int da_set_params(da_ctx *ctx, const da_params *p) {
     if (!ctx) return DA_ERR_INVALID;
     if (!params_ok(p) || p->precision != ctx->p.precision || p->device != ctx->p.device ||
@@ -465,7 +485,9 @@ int da_set_time(da_ctx *ctx, double time, int64_t iter) {
     if (st) return st;
     ctx->hsc->time = time;
     ctx->hsc->iter = iter;
+    // a cleared error restarts the grid barrier too (no kernel of the context is running)
     ctx->hsc->err = 0;
+    ctx->hsc->bar = 0ull;
     return copy_h2d(ctx, ctx->dsc, ctx->hsc, sizeof(DevScalars), "write scalars");
 }
 

@@ -239,6 +239,12 @@ struct da_ctx {
 namespace da {
 
 int set_error(da_ctx *ctx, int code, const std::string &msg);
+// capi.cu: the device's sticky error code (already read into ctx->hsc) as a return status; after a
+// grid-barrier timeout it also restarts the barrier word
+int device_error(da_ctx *ctx, const char *where);
+// forward_fp64.cu: a cooperative launch in which block 0 never arrives at the grid barrier, so the
+// other blocks' bounded wait runs out after limit_ns (da_selftest_barrier)
+int launch_barrier_selftest(da_ctx *ctx, unsigned long long limit_ns);
 void trace_begin(da_ctx *ctx, int kind);
 void trace_end(da_ctx *ctx, int steps = 1);
 int trace_flush(da_ctx *ctx);

@@ -284,7 +284,7 @@ int da_dwr_step(da_ctx *ctx, const double *lambda_next, double *el_error, double
     const long long iter0 = ctx->hsc->iter;
     if (!st) st = launch_forward_step(ctx);
     if (!st) st = read_scalars(ctx);
-    if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "da_dwr_step: device error in the coarse step");
+    if (!st) st = device_error(ctx, "da_dwr_step: the coarse step");
     const double dt = ctx->hsc->dt;
     if (!st) st = dwr_indicator(ctx, 1 - ctx->cur, ctx->cur, 0, dt, time0, iter0);
     if (!st) st = launch_snapshot(ctx, ctx->snaps[0], false);

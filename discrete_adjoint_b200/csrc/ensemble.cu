@@ -264,7 +264,7 @@ int da_ensemble_forward(da_ctx *ctx, int32_t nsteps, double *device_ms) {
     if (!st) st = cuda_check(ctx, cudaMemcpyAsync(ctx->hsc, ctx->dsc, sizeof(DevScalars), cudaMemcpyDeviceToHost,
                                                   ctx->stream), "scalars");
     if (!st) st = cuda_check(ctx, cudaStreamSynchronize(ctx->stream), "sync");
-    if (!st && ctx->hsc->err) st = set_error(ctx, ctx->hsc->err, "device error during the ensemble run");
+    if (!st) st = device_error(ctx, "ensemble run");
     return st;
 }
 

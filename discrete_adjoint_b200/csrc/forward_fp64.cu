@@ -17,6 +17,24 @@ int launch_refine_info_fp64(da_ctx *ctx, double *e, uint8_t *f, double *parts, d
 
 int launch_volume(da_ctx *ctx) { return fwd::launch_volume_t(ctx); }
 
+namespace {
+// Every block but block 0 waits at the grid barrier; block 0 returns without arriving, so the wait
+// runs out after limit_ns and raises DA_ERR_TIMEOUT.
+__global__ void k_barrier_selftest(DevScalars *sc, unsigned long long limit_ns) {
+    if (blockIdx.x == 0) return;
+    fwd::grid_sync(sc, limit_ns);
+}
+}  // namespace
+
+int launch_barrier_selftest(da_ctx *ctx, unsigned long long limit_ns) {
+    // one block per SM: co-resident, as the cooperative launch checks
+    const int grid = ctx->sm_count > 1 ? ctx->sm_count : 2;
+    DevScalars *sc = ctx->dsc;
+    void *args[] = {&sc, &limit_ns};
+    return cuda_check(ctx, cudaLaunchCooperativeKernel((const void *)k_barrier_selftest, grid, 32, args, 0, ctx->stream),
+                      "barrier self-test launch");
+}
+
 int forward_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
     const size_t rs = ctx->p.precision == DA_PREC_FP64 ? sizeof(double) : sizeof(float);

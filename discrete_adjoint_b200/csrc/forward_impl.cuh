@@ -459,7 +459,10 @@ __device__ __forceinline__ unsigned long long bar_load(const unsigned long long 
     return v;
 }
 
-__device__ __forceinline__ bool grid_sync(DevScalars *sc) {
+// Waits for every block of the (co-resident) grid.  The wait is bounded: after limit_ns (4 s by
+// default) or 2^26 polls a block raises DA_ERR_TIMEOUT and returns false, and so does every block
+// that arrives or polls after that; the host restarts the barrier word when it reads the error.
+__device__ __forceinline__ bool grid_sync(DevScalars *sc, unsigned long long limit_ns = 4000000000ull) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -473,7 +476,7 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc) {
             const unsigned long long t0 = global_ns();
             for (unsigned it = 1; unsigned(bar_load(&sc->bar) >> 32) == gen; ++it) {
                 if ((it & 255u) == 0 &&
-                    (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > 4000000000ull)) {
+                    (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > limit_ns)) {
                     atomicCAS(&sc->err, 0, DA_ERR_TIMEOUT);
                     good = 0;
                     break;

@@ -373,6 +373,16 @@ typedef struct da_tune_result {
 } da_tune_result;
 int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out);
 
+/* ---- diagnostic of the bounded device-side waits ---------------------------------------------
+ * No counterpart in the reference (whose only failure handling is exit() on NaN or a runaway wave
+ * speed).  The cooperative step kernels synchronise their blocks with a grid barrier whose wait is
+ * bounded: after 4 s a waiting block raises DA_ERR_TIMEOUT and every block returns.  This call runs
+ * one cooperative launch on the context's stream in which one block never arrives at that barrier,
+ * with the wait limited to limit_us microseconds (1 .. 4e6), and returns the status the wait
+ * produced (DA_ERR_TIMEOUT when it runs out as designed).  The error is cleared and the barrier
+ * restarted afterwards, so the context's next launches run normally. */
+int da_selftest_barrier(da_ctx *ctx, int32_t limit_us);
+
 /* ---- one step without any device allocation ------------------------------------------------
  * No counterpart in the reference: an addition for callers that may not allocate device memory
  * themselves or through this library, such as a plugin whose host application owns all of the

@@ -293,3 +293,93 @@ def run_reference_adjoint(mesh, mat, states, iters, dts, lam_end, workdir: str |
     assert magic == 0x314F4A44 and n2 == n and k2 == K
     arr = np.frombuffer(raw, dtype="<f8", offset=12)
     return {"lam": arr[:K * 3 * n].reshape(K, 3, n).copy(), "seconds": float(arr[K * 3 * n])}
+
+
+def run_reference_fwdadj(mesh, mat, nsteps: int, warm: int, box, workdir: str | None = None) -> dict:
+    """The reference's own forward + adjoint, timed step by step (oracle/_ref/ref_harness, mode 'DAF1'):
+    nsteps forward steps from the mesh's initial state with the driver's solution recording, then
+    the dual solver's reverse steps back to step `warm` from lambda = dJ/dU of J = sum over the
+    cells whose centre lies in box of h^2 dx dy.  Returns {"fwd_seconds": [nsteps],
+    "rev_seconds": [nsteps - warm], "lam": [3][n] the adjoint of U^warm}."""
+    import struct
+    import subprocess
+    import tempfile
+
+    from discrete_adjoint_b200.solver import MatProps
+    n = mesh.n
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<6i", 0x31464144, n, mesh.max_level, len(mat.bedfrict_deg), nsteps, warm))
+            f.write(np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma,
+                              float("inf")], dtype="<f8").tobytes())
+            f.write(bed.astype("<f8").tobytes())
+            for a in (mesh.nbr, mesh.level, mesh.ix, mesh.iy, mesh.material):
+                f.write(np.ascontiguousarray(a, dtype="<i4").tobytes())
+            for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature,
+                      mesh.h0, mesh.hu0, mesh.hv0):
+                f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+            f.write(np.asarray(box, dtype="<f8").tobytes())
+        r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    magic, n2, k2, w2 = struct.unpack_from("<4i", raw, 0)
+    assert magic == 0x314F4644 and n2 == n and k2 == nsteps and w2 == warm
+    arr = np.frombuffer(raw, dtype="<f8", offset=16)
+    nr = nsteps - warm
+    return {"fwd_seconds": arr[:nsteps].copy(), "rev_seconds": arr[nsteps:nsteps + nr].copy(),
+            "lam": arr[nsteps + nr:nsteps + nr + 3 * n].reshape(3, n).copy()}
+
+
+def params_for(mat) -> "_ffi.da_params":
+    """da_params for the oracle filled here (the values da_params_default and make_params give),
+    so that a CPU-only caller does not load the product library."""
+    import math
+
+    from discrete_adjoint_b200.solver import MatProps
+    p = _ffi.da_params()
+    p.precision = _ffi.DA_PREC_FP64
+    p.epsilon = mat.epsilon
+    p.gravity_scale = mat.gravity_scale
+    p.gamma = mat.gamma
+    p.intfrict = MatProps.rad(mat.intfrict_deg)
+    p.n_materials = len(mat.bedfrict_deg)
+    for k, b in enumerate(mat.bedfrict_deg):
+        p.bedfrict[k] = MatProps.rad(b)
+    p.frict_tiny_iters = mat.frict_tiny_iters
+    p.frict_tiny_early = mat.frict_tiny_early
+    p.frict_tiny_late = mat.frict_tiny_late
+    p.max_time = p.next_output = p.next_save = p.influx_dt = math.inf
+    p.tile_culling = 1
+    p.tile_staging = 1
+    return p
+
+
+def time_port_fwdadj(mesh, mat, warm: int, steps: int, box):
+    """Per-step seconds of the restated forward step and reverse step (the oracle), as
+    run_reference_fwdadj times the reference: (forward seconds [steps], reverse seconds [steps])."""
+    import time
+    o = Oracle(params_for(mat), mesh)
+    h, hu, hv = mesh.h0.copy(), mesh.hu0.copy(), mesh.hv0.copy()
+    o.run(h, hu, hv, warm)
+    states, dts, fwd = [], [], []
+    for _ in range(steps):
+        states.append((h.copy(), hu.copy(), hv.copy()))
+        t0 = time.perf_counter()
+        rc, dt, _ = o.run(h, hu, hv, 1)
+        fwd.append(time.perf_counter() - t0)
+        dts.append(float(dt[0]))
+    inb = (mesh.x >= box[0]) & (mesh.x <= box[1]) & (mesh.y >= box[2]) & (mesh.y <= box[3])
+    lam = np.zeros((3, mesh.n))
+    lam[0] = np.where(inb, 2.0 * h * (mesh.dx * mesh.dy), 0.0)
+    rev = []
+    for k in range(steps - 1, -1, -1):
+        it = warm + k + 1
+        t0 = time.perf_counter()
+        lam = o.adjoint_step_ref(*states[k], dts[k], 0.1 if it < 51 else 1e-9, lam)
+        rev.append(time.perf_counter() - t0)
+    return np.array(fwd), np.array(rev)

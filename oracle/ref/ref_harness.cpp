@@ -34,6 +34,9 @@
 //   'DAJ1' (mesh as 'DAH1', then reverse-step records; see adjoint_mode) -> 'DJO1': the
 //       reference's own dual solver steps -- update_dual_grid, calc_jacobian, calc_adjoint --
 //       taken backward from a given adjoint.
+//   'DAF1' (mesh as 'DAH1', initial state, functional box; see fwdadj_mode) -> 'DFO1': the
+//       reference's forward steps with solution recording, then its dual-solver reverse steps,
+//       each timed (the CPU baseline of the forward + adjoint path).
 #include <sys/sysinfo.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -263,7 +266,15 @@ void make_props(const MeshIn &m, Props &pr) {
 struct Tables {
     HashTable *NodeTable = nullptr, *El_Table = nullptr;
     std::vector<Element *> els;
+    double dkr[2], XR[2], YR[2];  // key and coordinate ranges of the element keys
 };
+
+// A SolRec over the element keys of t (the hash table's bucket index spreads them as the
+// element table's does).
+SolRec *solrec_for(const Tables &t, int n) {
+    double dkr[2] = {t.dkr[0], t.dkr[1]}, XR[2] = {t.XR[0], t.XR[1]}, YR[2] = {t.YR[0], t.YR[1]};
+    return new SolRec(dkr, std::max(1024, 2 * n), 2017, XR, YR, 0);
+}
 
 Tables build_tables(const MeshIn &m, const double *h, const double *hu, const double *hv, MatProps &matprops,
                     bool ref_static) {
@@ -316,6 +327,11 @@ Tables build_tables(const MeshIn &m, const double *h, const double *hu, const do
     double XR[2] = {x0, x0 + (maxX + 1) * 0.5 * fine_dx}, YR[2] = {y0, y0 + (maxY + 1) * 0.5 * fine_dy};
     const int nb = std::max(1024, 2 * (int)nodes.size());
     Tables t;
+    for (int q = 0; q < 2; ++q) {
+        t.dkr[q] = dkr[q];
+        t.XR[q] = XR[q];
+        t.YR[q] = YR[q];
+    }
     t.NodeTable = new HashTable(dkr, nb, 2017, XR, YR, 0);
     t.El_Table = new HashTable(dkr, std::max(1024, 2 * n), 2017, XR, YR, 0);
     auto keyof = [](const std::pair<int64_t, int64_t> &p, unsigned k[2]) {
@@ -441,7 +457,7 @@ int adjoint_mode(FILE *f, const int32_t hdr[6], const char *out) {
         for (int v = 0; v < 3; ++v) d->get_adjoint()[v] = lam[(size_t)v * n + c];
     }
     // forward records of every state the sweep takes back
-    SolRec *solrec = make_solrec();
+    SolRec *solrec = solrec_for(t, n);
     for (int c = 0; c < n; ++c) {
         Jacobian *j = new Jacobian(t.els[c]->key);
         solrec->add(j->get_key(), j);
@@ -488,6 +504,103 @@ int adjoint_mode(FILE *f, const int32_t hdr[6], const char *out) {
     return 0;
 }
 
+// ---- 'DAF1': the reference's own forward + adjoint, timed step by step
+//
+// Header: 'DAF1', n, max_level, n_materials, K forward steps, W (the first W steps are not timed
+// and not taken back).  After the mesh: double h[n], hu[n], hv[n] (the initial state), box[4].
+// K forward steps as the driver takes them (hpfem.C:232-285: frict_tiny, step(), then
+// SolRec::record_solution of the step's starting state; the gz flushes every 50 steps are
+// skipped), then the dual grid (DualElem copies, dual_solver.C:101-106) seeded with
+// lambda^K = dJ/dU^K of J = sum over the cells whose centre lies in the box of h^2 dx dy, then
+// K - W reverse steps as dual_solver takes them (setup_dual_flow's update_dual_grid and
+// clear_empty_jacobians, calc_jacobian, calc_adjoint; dual_solver.C:183-207 without its one-step
+// gating and without the DWR estimate and the output writers).
+// Output: 'DFO1', n, K, W; double fwd_seconds[K], rev_seconds[K - W], lambda[3][n] (lambda^W).
+int fwdadj_mode(FILE *f, const int32_t hdr[6], const char *out) {
+    MeshIn m;
+    read_mesh(f, hdr, m);
+    const int n = m.n, K = m.nsteps, W = m.flag;
+    std::vector<double> h(n), hu(n), hv(n);
+    double box[4];
+    rd(f, h.data(), n); rd(f, hu.data(), n); rd(f, hv.data(), n);
+    rd(f, box, 4);
+    std::fclose(f);
+    if (W < 0 || W >= K) return 3;
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, HUGE_VAL, HUGE_VAL, HUGE_VAL, 1.0);
+    PileProps pileprops;
+    FluxProps fluxprops;
+    StatProps statprops;
+    statprops.hxyminmax = matprops.MAX_NEGLIGIBLE_HEIGHT * 10.0;
+    statprops.timereached = -1.0;
+    DISCHARGE discharge;
+    OutLine outline;
+    Tables t = build_tables(m, h.data(), hu.data(), hv.data(), matprops, false);
+    SolRec *solrec = solrec_for(t, n);
+    MeshCTX fctx;
+    fctx.el_table = t.El_Table;
+    fctx.nd_table = t.NodeTable;
+    PropCTX pctx;
+    pctx.matprops = &matprops;
+    pctx.timeprops = &timeprops;
+    pctx.mapnames = nullptr;
+    pctx.outline = nullptr;
+    pctx.numproc = 1;
+    pctx.myid = 0;
+    pctx.adapt_flag = 0;
+    int order_flag = 1;
+    std::vector<double> fwd_s(K), rev_s(K - W);
+    for (int it = 0; it < K; ++it) {
+        const auto t0 = std::chrono::steady_clock::now();
+        matprops.frict_tiny = timeprops.iter < 50 ? 0.1 : 0.000000001;
+        step(t.El_Table, t.NodeTable, 0, 1, &matprops, &timeprops, &pileprops, &fluxprops, &statprops, &order_flag,
+             &outline, &discharge, 0);
+        solrec->record_solution(&fctx, &pctx);
+        fwd_s[it] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    // dual grid seeded with dJ/dU^K
+    HashTable *Dual_El_Tab = new HashTable(t.El_Table);
+    std::vector<DualElem *> duals(n);
+    for (int c = 0; c < n; ++c) {
+        DualElem *d = new DualElem(t.els[c]);
+        Dual_El_Tab->add(d->pass_key(), d);
+        duals[c] = d;
+        const double *cc = t.els[c]->coord;
+        const bool in = cc[0] >= box[0] && cc[0] <= box[1] && cc[1] >= box[2] && cc[1] <= box[3];
+        d->get_adjoint()[0] = in ? 2.0 * t.els[c]->state_vars[0] * (t.els[c]->dx[0] * t.els[c]->dx[1]) : 0.0;
+        d->get_adjoint()[1] = d->get_adjoint()[2] = 0.0;
+    }
+    MeshCTX dctx;
+    dctx.el_table = Dual_El_Tab;
+    dctx.nd_table = t.NodeTable;
+    for (int k = 0; k < K - W; ++k) {
+        const int iter = K - k;
+        const auto t0 = std::chrono::steady_clock::now();
+        timeprops.iter = iter;
+        timeprops.adjiter++;
+        update_dual_grid(solrec, &dctx, &pctx);
+        clear_empty_jacobians(solrec, iter);
+        calc_jacobian(&dctx, &pctx);
+        calc_adjoint(&dctx, &pctx);
+        rev_s[k] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    FILE *o = std::fopen(out, "wb");
+    if (!o) return 2;
+    const int32_t oh[4] = {0x314F4644, n, K, W};
+    wr(o, oh, 4);
+    wr(o, fwd_s.data(), K);
+    wr(o, rev_s.data(), K - W);
+    std::vector<double> lam((size_t)3 * n);
+    for (int c = 0; c < n; ++c)
+        for (int v = 0; v < 3; ++v) lam[(size_t)v * n + c] = duals[c]->get_adjoint()[v];
+    wr(o, lam.data(), lam.size());
+    std::fclose(o);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -506,6 +619,7 @@ int main(int argc, char **argv) {
     hdr[0] = magic;
     rd(f, hdr + 1, 5);
     if (hdr[0] == 0x314A4144) return adjoint_mode(f, hdr, argv[2]);
+    if (hdr[0] == 0x31464144) return fwdadj_mode(f, hdr, argv[2]);
     if (hdr[0] != 0x31484144) return 3;
     MeshIn m;
     read_mesh(f, hdr, m);

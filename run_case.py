@@ -1,10 +1,10 @@
 """Run one of the synthetic workloads through the C ABI and print a JSON summary.
 
-    python -m discrete_adjoint_b200.run_case --workload 2 --precision fp32 --steps 20 [--full-sweep]
-    python -m discrete_adjoint_b200.run_case --workload 3 --precision fp64 --adjoint 64
-    python -m discrete_adjoint_b200.run_case --workload 2 --precision fp64 --layer 1 --steps 10
+    python run_case.py --workload 2 --precision fp32 --steps 20 [--full-sweep]
+    python run_case.py --workload 3 --precision fp64 --adjoint 64
+    python run_case.py --workload 2 --precision fp64 --layer 1 --steps 10
 
-A fixed, small command line for profilers (ncu -k <kernel> -s <skip> -c <count> python -m ...):
+A fixed, small command line for profilers (ncu -k <kernel> -s <skip> -c <count> python run_case.py ...):
 the forward steps go through da_forward_run (CUDA graphs), the adjoint through da_adjoint_run.
 Workloads: 1 = 40k-cell plane and runout, 2 = 3.75M-cell adaptive hill + noise, 3 = 1M-cell
 uniform plane (the forward + adjoint workload).  --layer adds that many metres of material on
@@ -14,9 +14,13 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
+import sys
 
-from . import _ffi, inputs
-from .solver import GeoflowContext, TimeProps, adjoint_run
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from discrete_adjoint_b200 import _ffi, inputs  # noqa: E402
+from discrete_adjoint_b200.solver import GeoflowContext, TimeProps, adjoint_run  # noqa: E402
 
 
 def main(argv=None):
