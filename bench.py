@@ -208,19 +208,26 @@ def algorithmic_bytes(precision: str, n_act: float) -> dict:
             "snapshot_copy": 2 * 3 * r * n_act}
 
 
-# DRAM bytes (read + write) per launch from the committed ncu captures (profiles/), keyed by
-# (precision, kernel); None where no capture exists.  k_youturn: one reverse step of the
-# headline workload (k_youturn_fwd_adjoint_1M_fp64.md); k_steps_dense_per_step: the dense
-# 3.75M-cell case, per time step (k_steps_dense_hill_3.75M_staged.md).
-TRAFFIC = {
-    ("fp64", "k_youturn"): 2.284288e6 + 2.048e3,
-    ("fp32", "k_steps_dense_per_step"): (4.346160e9 + 0.615296e9) / 10,
-    ("fp64", "k_steps_dense_per_step"): (8.427677e9 + 1.226889e9) / 10,
+# DRAM bytes (read + write) from the committed ncu captures (profiles/traffic_headline_1M.md,
+# profiles/k_steps_dense_hill_3.75M_staged.md).  Sparse headline kernels: bytes per active cell of a
+# launch captured in the steady flow (k_youturn: reverse steps of iterations 256 and 255 of the
+# 512-step sweep, 4372 and 4344 active cells; k_steps: one launch of 32 steps after 256, 4553
+# active cells per step on average), scaled by the active cells of the traced run; the dense case:
+# bytes per time step of a 10-step launch with every cell wet.
+TRAFFIC_PER_ACTIVE_CELL = {
+    ("fp64", "k_youturn"): 0.5 * (1983232 / 4372 + 1975296 / 4344),
+    ("fp32", "k_youturn"): 0.5 * (1357056 / 4372 + 1353472 / 4344),
+    ("fp64", "k_steps"): (1485568 + 17920) / (32 * 4552.6),
+}
+TRAFFIC_DENSE_PER_STEP = {
+    "fp32": (4.346160e9 + 0.615296e9) / 10,
+    "fp64": (8.427677e9 + 1.226889e9) / 10,
 }
 
 
-def traffic_per_launch(precision: str, kernel: str):
-    return TRAFFIC.get((precision, kernel))
+def traffic_per_launch(precision: str, kernel: str, n_act: float, steps_per_launch: float):
+    per = TRAFFIC_PER_ACTIVE_CELL.get((precision, kernel))
+    return None if per is None else per * n_act * steps_per_launch
 
 
 def reference_fwdadj(steps: int, warm: int, side: int = 1024) -> dict:
@@ -392,8 +399,7 @@ def forward_config2(args, ws, local):
             r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step,
                              "bytes_per_cell_update": bytes_per_cell_update(pn)["forward"], "achieved": gbs,
                              "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind,
-                             "traffic": traffic_per_launch("fp64" if prec == _ffi.DA_PREC_FP64 else "fp32",
-                                                           "k_steps_dense_per_step")}
+                             "traffic": TRAFFIC_DENSE_PER_STEP[pn]}
         res[name] = r
         c.close()
     return w, res
@@ -436,6 +442,11 @@ def ensemble_config4(args, ws, rank, local):
     out["fp32_rel_err_vs_fp64_max"] = {
         q: max(rel(grads["fp32"][k][i], grads["fp64"][k][i]) for k in grads["fp64"])
         for i, q in enumerate(("J", "dJ_dbedfrict", "dJ_dpile"))}
+    # the FP32-split batched rate counts only with every member's J and gradients within 1e-4 of FP64
+    fp32_ok = max(out["fp32_rel_err_vs_fp64_max"].values()) <= 1e-4
+    out["fp32"]["within_tolerance"] = fp32_ok
+    if not fp32_ok:
+        out["fp32_out_of_tolerance"] = out.pop("fp32")
     if ws == 1 and not args.no_sequential:
         seq_ms, worst = 0.0, 0.0
         for i, mb in enumerate(members):
@@ -450,7 +461,8 @@ def ensemble_config4(args, ws, rank, local):
             worst = max(worst, rel(e[0], gs.J), rel(e[1], gs.dJ_dbedfrict[0]), rel(e[2], gs.dJ_dpile[0]))
         out["sequential_fp64"] = {"ms": seq_ms, "value": total_cells * ENS_STEPS / (seq_ms * 1e-3)}
         out["batched_fp64_over_sequential"] = seq_ms / out["fp64"]["ms"]
-        out["batched_fp32_over_sequential"] = seq_ms / out["fp32"]["ms"]
+        if "fp32" in out:
+            out["batched_fp32_over_sequential"] = seq_ms / out["fp32"]["ms"]
         out["batched_vs_sequential_max_rel_diff"] = worst
     return out
 
@@ -543,7 +555,10 @@ def main():
                          "steps_per_launch": steps_per_launch,
                          "avg_launch_ms": avg_ms, "wet_cells_avg": r["n_wet"], "active_cells_avg": r["n_act"],
                          "trace_ms_launches_steps": {k: [round(v[0], 4), v[1], v[2]] for k, v in tr.items()},
-                         "traffic": traffic_per_launch(head, dom)},
+                         "traffic": traffic_per_launch(head, dom, r["n_act"], steps_per_launch),
+                         "note": "the flow covers ~40 of 4096 tiles: the step is bound by the latency of its "
+                                 "grid barriers and of one tile's dependent FP64 chain, not by HBM; the few "
+                                 "active tiles stay in L2 between steps"},
             "e2e": hr["e2e"],
             "gpu_launches": int(launches_per_run * args.steps),
             "clocks": hr["clocks"],

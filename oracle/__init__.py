@@ -43,6 +43,8 @@ def load() -> C.CDLL:
     lib.orc_edge_fluxes.argtypes = [P, M, PD, PD, PD, PD, PD]
     lib.orc_adjoint_step_ref.restype = C.c_int
     lib.orc_adjoint_step_ref.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD]
+    lib.orc_forward_step_split.restype = C.c_int
+    lib.orc_forward_step_split.argtypes = [P, M, PD, PD, PD, PD, C.POINTER(C.c_int64), PD]
     lib.orc_adjoint_step_var.restype = C.c_int
     lib.orc_adjoint_step_var.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD, C.c_int]
     _lib = lib
@@ -72,6 +74,19 @@ class Oracle:
                                       _ffi.dptr(hv), C.byref(self.time), C.byref(self.iter), nsteps,
                                       _ffi.dptr(dts), C.byref(st))
         return rc, dts[:nsteps], st
+
+    def run_split(self, h, hu, hv, nsteps: int):
+        """Advances (h, hu, hv) in place by nsteps with FP32 flux and source arithmetic and FP64
+        state and corrector accumulation (oracle/da_oracle_split.c); returns the dt history."""
+        dts = np.zeros(max(nsteps, 1))
+        d = C.c_double()
+        for k in range(nsteps):
+            rc = self.lib.orc_forward_step_split(C.byref(self.params), C.byref(self.soa), _ffi.dptr(h),
+                                                 _ffi.dptr(hu), _ffi.dptr(hv), C.byref(self.time),
+                                                 C.byref(self.iter), C.byref(d))
+            assert rc == 0
+            dts[k] = d.value
+        return dts[:nsteps]
 
     def slopes(self, h, hu, hv):
         out = np.zeros((6, self.mesh.n))

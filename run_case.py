@@ -28,6 +28,9 @@ def main(argv=None):
     ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--steps", type=int, default=20, help="forward steps (ignored with --adjoint)")
+    ap.add_argument("--pre-steps", type=int, default=0,
+                    help="forward steps taken in a launch of their own before the measured ones (a profiler "
+                         "then skips that launch to see the steady flow)")
     ap.add_argument("--full-sweep", action="store_true", help="switch tile culling off")
     ap.add_argument("--layer", type=float, default=0.0, help="metres of material added on every cell")
     ap.add_argument("--adjoint", type=int, default=0, metavar="HORIZON",
@@ -49,8 +52,11 @@ def main(argv=None):
             out.update({"horizon": a.adjoint, "J": g.J, "dJ_dbedfrict": g.dJ_dbedfrict, "dJ_dpile": g.dJ_dpile,
                         "forward_steps": g.forward_steps, "device_ms": g.device_ms})
         else:
+            if a.pre_steps:
+                c.run(a.pre_steps)
             s, ms = c.run_timed(a.steps)
-            out.update({"steps": a.steps, "device_ms": ms, "volume": s.volume, "iter": s.iter})
+            out.update({"pre_steps": a.pre_steps, "steps": a.steps, "device_ms": ms, "volume": s.volume,
+                        "iter": s.iter})
     print(json.dumps(out))
 
 
