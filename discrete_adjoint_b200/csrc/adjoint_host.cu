@@ -365,6 +365,8 @@ std::vector<unsigned char> sweep_key(const da_ctx *ctx, const double *box, int n
         const unsigned char *c = (const unsigned char *)p;
         k.insert(k.end(), c, c + b);
     };
+    // structs go in member by member: their padding bytes are not part of the key
+    auto val = [&](const auto &v) { put(&v, sizeof(v)); };
     const int ints[] = {nsteps, nsnap, n_piles, seeded ? 1 : 0, ctx->cur, ctx->grid, ctx->ntiles, ctx->nseg,
                         ctx->ninst, ctx->mesh.n, ctx->sm_count};
     put(ints, sizeof(ints));
@@ -373,11 +375,35 @@ std::vector<unsigned char> sweep_key(const da_ctx *ctx, const double *box, int n
     put(b4, sizeof(b4));
     put(sec2, sizeof(double) * DA_MAX_MATERIALS);
     put(&cos_int, sizeof(cos_int));
-    put(&ctx->p, sizeof(ctx->p));
-    put(&ctx->mc, sizeof(ctx->mc));
-    put(&ctx->tc, sizeof(ctx->tc));
-    put(&ctx->mesh, sizeof(ctx->mesh));
-    put(&ctx->ia, sizeof(ctx->ia));
+    const da_params &p = ctx->p;
+    for (const int32_t v : {p.precision, p.device, p.n_materials, p.frict_tiny_iters, p.tile_culling, p.grid_blocks,
+                            p.blocks_per_sm, p.tile_staging, p.jacobian_mode})
+        val(v);
+    for (const double v : {p.epsilon, p.gravity_scale, p.gamma, p.intfrict, p.frict_tiny_early, p.frict_tiny_late,
+                           p.max_time, p.next_output, p.next_save, p.influx_dt, p.fp32_sign_floor})
+        val(v);
+    put(p.bedfrict, sizeof(p.bedfrict));
+    const MatConsts &mc = ctx->mc;
+    put(mc.kact_sgn, sizeof(mc.kact_sgn));
+    put(mc.tan_bed, sizeof(mc.tan_bed));
+    for (const double v : {mc.kact_rest, mc.epsilon, mc.sin_int, mc.gamma, mc.sign_floor}) val(v);
+    val(mc.n_materials);
+    const TimeConsts &tc = ctx->tc;
+    for (const double v : {tc.next_output, tc.next_save, tc.max_time, tc.influx_dt, tc.gravity_scale, tc.epsilon,
+                           tc.frict_tiny_early, tc.frict_tiny_late})
+        val(v);
+    for (const long long v : {tc.frict_tiny_iters, tc.iter0, tc.n_replay}) val(v);
+    val(tc.dt_replay);
+    const DevMesh &dm = ctx->mesh;
+    for (const int32_t v : {dm.n, dm.epoch, dm.halo_max}) val(v);
+    const void *mptr[] = {dm.nbr, dm.mat, dm.bflag, dm.x, dm.y, dm.dx, dm.dy, dm.g, dm.dg, dm.curv, dm.fdx, dm.fdy,
+                          dm.fg, dm.fdg, dm.fcurv, dm.halo_off, dm.halo_idx, dm.nloc};
+    put(mptr, sizeof(mptr));
+    const InstArgs &ia = ctx->ia;
+    val(ia.ninst);
+    const void *iptr[] = {ia.tile_inst, ia.mcs, ia.time, ia.dt, ia.min_dxe, ia.hmax, ia.acc_min, ia.acc_max,
+                          ia.sec2_bed, ia.cos_int, ia.dk_tab, ia.box, ia.seg0};
+    put(iptr, sizeof(iptr));
     const void *ptrs[] = {ctx->U[0][0], ctx->U[0][1], ctx->U[0][2], ctx->U[1][0], ctx->U[1][1], ctx->U[1][2],
                           ctx->lam[0][0], ctx->lam[0][1], ctx->lam[0][2], ctx->lam[1][0], ctx->lam[1][1],
                           ctx->lam[1][2], ctx->kact, ctx->active, ctx->seg_clean, ctx->seg_wet, ctx->seg_vol,

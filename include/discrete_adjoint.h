@@ -393,8 +393,9 @@ int da_selftest_barrier(da_ctx *ctx, int32_t limit_us);
  * Meshes with more than DA_NOALLOC_MAX_CELLS cells are rejected with DA_ERR_UNSUPPORTED, as is
  * any precision but DA_PREC_FP64; a neighbour or material index out of range gives
  * DA_ERR_INVALID before the step runs.  time/iter are TimeProps::time and ::iter before the
- * step; out receives the step's scalars.  stream is a cudaStream_t (NULL: the default stream);
- * the call returns after the step has finished on it.
+ * step; out receives the step's scalars.  stream is a cudaStream_t of the device that is current
+ * when the call is made (NULL: that device's default stream), and the array used is that device's;
+ * the call synchronises with the stream and returns after the step has finished on it.
  * The first call on a device resolves the array's device address (cudaGetSymbolAddress) with
  * that device current; make that first call before any stream capture.  All calls share the one
  * array, which keeps the last call's contents: calls that overlap on a GPU (other streams, other

@@ -398,3 +398,46 @@ def time_port_fwdadj(mesh, mat, warm: int, steps: int, box):
         lam = o.adjoint_step_ref(*states[k], dts[k], 0.1 if it < 51 else 1e-9, lam)
         rev.append(time.perf_counter() - t0)
     return np.array(fwd), np.array(rev)
+
+
+ADAPTER_EXE = os.path.join(HERE, "_ref", "adapter_check")
+
+
+def adapter_available() -> bool:
+    return os.path.exists(ADAPTER_EXE)
+
+
+def run_adapter_check(mesh, mat, h, hu, hv, nsteps: int = 0, step: bool = False) -> dict:
+    """INTEGRATION.md's adapter, compiled against the reference (oracle/_ref/adapter_check): flattens
+    the reference's tables rebuilt from mesh and compares the flattening with mesh; with step=True it
+    also takes nsteps steps through the adapter (the device path) and through the reference's step()
+    and compares the results.  Returns the mismatch counts."""
+    import struct
+    import subprocess
+    import tempfile
+
+    from discrete_adjoint_b200.solver import MatProps
+    n = mesh.n
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<6i", 0x31494144, n, mesh.max_level, len(mat.bedfrict_deg), nsteps, int(step)))
+            f.write(np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma,
+                              float("inf")], dtype="<f8").tobytes())
+            f.write(bed.astype("<f8").tobytes())
+            for a in (mesh.nbr, mesh.level, mesh.ix, mesh.iy, mesh.material):
+                f.write(np.ascontiguousarray(a, dtype="<i4").tobytes())
+            for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature,
+                      h, hu, hv):
+                f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
+        r = subprocess.run([ADAPTER_EXE, fin, fout], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"adapter_check failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    v = struct.unpack_from("<7i", raw, 0)
+    assert v[0] == 0x314F4944 and v[1] == n
+    return {"nbr_mismatch": v[2], "field_mismatch": v[3], "state_mismatch": v[4], "dt_mismatch": v[5],
+            "steps": v[6], "max_diff": struct.unpack_from("<d", raw, 28)[0]}

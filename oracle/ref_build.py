@@ -20,9 +20,11 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/src"
+# the reference's sources: the checkout this container mounts, or DA_REFERENCE_SRC
+REF = os.environ.get("DA_REFERENCE_SRC", "/root/reference/src")
 OUT = os.path.join(HERE, "_ref")
 EXE = os.path.join(OUT, "ref_harness")
+ADAPTER = os.path.join(OUT, "adapter_check")
 STUBS = os.path.join(HERE, "ref")
 
 # translation units on the step() path (geoflow, datstr, the update kernel, helpers)
@@ -85,14 +87,34 @@ def build(verbose: bool = False, force: bool = False) -> str | None:
         else:
             _run(CXX + ["-c", src, "-o", obj], verbose)
     own = []
-    for f in ("mpi_stub.cpp", "hdf5_stub.cpp", "fortran_c.cpp", "link_stubs.cpp", "ref_harness.cpp"):
+    for f in ("mpi_stub.cpp", "hdf5_stub.cpp", "fortran_c.cpp", "link_stubs.cpp", "harness_tables.cpp",
+              "ref_harness.cpp"):
         src = os.path.join(STUBS, f)
         obj = os.path.join(OUT, f + ".o")
         own.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < os.path.getmtime(src):
             _run(CXX + ["-c", src, "-o", obj], verbose)
     _run(["g++", "-o", EXE] + own + objs + ["-lz", "-lm"], verbose)
+    build_adapter(own, objs, verbose, force)
     return EXE
+
+
+def build_adapter(own, objs, verbose=False, force=False):
+    """oracle/_ref/adapter_check: INTEGRATION.md's adapter compiled against the reference's headers,
+    linked with the reference's objects and the product library (when it has been built)."""
+    root = os.path.dirname(HERE)
+    lib_dir = os.path.join(root, "discrete_adjoint_b200")
+    if not os.path.exists(os.path.join(lib_dir, "libda_b200.so")):
+        return None
+    src = os.path.join(STUBS, "adapter_check.cpp")
+    obj = os.path.join(OUT, "adapter_check.cpp.o")
+    if force or not os.path.exists(obj) or os.path.getmtime(obj) < os.path.getmtime(src):
+        _run(CXX + ["-I" + os.path.join(root, "include"), "-c", src, "-o", obj], verbose)
+    harness_objs = [o for o in own if not o.endswith("ref_harness.cpp.o")]
+    _run(["g++", "-o", ADAPTER] + harness_objs + [obj] + objs +
+         ["-L" + lib_dir, "-l:libda_b200.so", "-Wl,-rpath,$ORIGIN/../../discrete_adjoint_b200", "-lz", "-lm"],
+         verbose)
+    return ADAPTER
 
 
 if __name__ == "__main__":
