@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
                 sc->acc_hmax = 0ull;
             }
         }
+        fwd::grid_exit(sc);
         return;
     }
     if (STAGED)
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
             sc->acc_hmax = 0ull;
         }
     }
+    fwd::grid_exit(sc);
 }
 
 // The k_youturn instantiation for the launch's flags.

@@ -238,7 +238,7 @@ int device_error(da_ctx *ctx, const char *where) {
     if (code == DA_ERR_TIMEOUT) {
         // a cooperative launch gave up at a grid barrier and every block has returned: the next
         // launch starts from a barrier word with no arrivals and generation 0
-        cudaMemsetAsync(&ctx->dsc->bar, 0, sizeof(unsigned long long), ctx->stream);
+        cudaMemsetAsync(&ctx->dsc->bar, 0, 2 * sizeof(unsigned long long), ctx->stream);  // bar, bar_exit
         cudaStreamSynchronize(ctx->stream);
     }
     return set_error(ctx, code, std::string(where) + ": " + da_strerror(code));
@@ -488,6 +488,7 @@ int da_set_time(da_ctx *ctx, double time, int64_t iter) {
     // a cleared error restarts the grid barrier too (no kernel of the context is running)
     ctx->hsc->err = 0;
     ctx->hsc->bar = 0ull;
+    ctx->hsc->bar_exit = 0ull;
     return copy_h2d(ctx, ctx->dsc, ctx->hsc, sizeof(DevScalars), "write scalars");
 }
 

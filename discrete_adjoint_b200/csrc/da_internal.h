@@ -49,8 +49,9 @@ struct DevScalars {
     unsigned listed;      // tiles the reverse step's recording update listed (sets the gather's work split)
     unsigned long long acc_alt_min_dxe;  // the multi-step kernel's second accumulator pair
     unsigned long long acc_alt_hmax;     // (odd steps of a launch), same start values
-    unsigned long long bar;  // grid barrier of the cooperative kernels: blocks arrived (low 32 bits),
-                             // generation (high 32 bits)
+    unsigned long long bar;       // grid barrier of the cooperative kernels: arrivals since the launch
+                                  // began (barrier k of a grid of G blocks opens at G (k + 1))
+    unsigned long long bar_exit;  // blocks that have left the launch; the last one restarts both at 0
 };
 
 // Time-clipping targets (TimeProps::ndnextoutput / ndnextsave / ndmaxtime) and the

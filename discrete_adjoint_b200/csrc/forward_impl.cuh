@@ -459,9 +459,12 @@ __device__ __forceinline__ unsigned long long bar_load(const unsigned long long 
     return v;
 }
 
-// Waits for every block of the (co-resident) grid.  The wait is bounded: after limit_ns (4 s by
-// default) or 2^26 polls a block raises DA_ERR_TIMEOUT and returns false, and so does every block
-// that arrives or polls after that; the host restarts the barrier word when it reads the error.
+// Waits for every block of the (co-resident) grid.  One atomic per block: the barrier word counts
+// the arrivals since the launch began, so barrier k of a grid of G blocks is open once it reaches
+// G (k + 1) -- the last arrival has nothing more to do, the others poll the word.  The wait is
+// bounded: after limit_ns (4 s by default) or 2^26 polls a block raises DA_ERR_TIMEOUT and returns
+// false, and so does every block that arrives or polls after that; the host restarts the barrier
+// word when it reads the error.  A launch that ends normally restarts it itself (grid_exit).
 __device__ __forceinline__ bool grid_sync(DevScalars *sc, unsigned long long limit_ns = 4000000000ull) {
     __shared__ int ok;
     __syncthreads();
@@ -469,12 +472,11 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc, unsigned long long lim
         volatile int *err = &sc->err;
         int good = *err != DA_ERR_TIMEOUT;
         const unsigned long long old = bar_add(&sc->bar, 1ull);
-        const unsigned gen = unsigned(old >> 32);
-        if (unsigned(old) == gridDim.x - 1) {
-            bar_add(&sc->bar, (1ull << 32) - gridDim.x);  // all arrived: next generation, no arrivals
-        } else {
+        const unsigned long long G = gridDim.x;
+        const unsigned long long target = (old / G + 1) * G;
+        if (old + 1 != target) {
             const unsigned long long t0 = global_ns();
-            for (unsigned it = 1; unsigned(bar_load(&sc->bar) >> 32) == gen; ++it) {
+            for (unsigned it = 1; bar_load(&sc->bar) < target; ++it) {
                 if ((it & 255u) == 0 &&
                     (*err == DA_ERR_TIMEOUT || it > (1u << 26) || global_ns() - t0 > limit_ns)) {
                     atomicCAS(&sc->err, 0, DA_ERR_TIMEOUT);
@@ -488,6 +490,18 @@ __device__ __forceinline__ bool grid_sync(DevScalars *sc, unsigned long long lim
     }
     __syncthreads();
     return ok != 0;
+}
+
+// The end of a cooperative launch that passed all its barriers: the last block to leave (every
+// other block has finished polling by then) puts the barrier word back at 0 for the next launch.
+__device__ __forceinline__ void grid_exit(DevScalars *sc) {
+    if (threadIdx.x == 0) {
+        const unsigned long long old = bar_add(&sc->bar_exit, 1ull);
+        if (old == gridDim.x - 1) {
+            sc->bar = 0ull;
+            sc->bar_exit = 0ull;
+        }
+    }
 }
 
 template <class R>
@@ -598,6 +612,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
         snap::snap_segments<R>(post);
         snap::snap_scalars<R>(post);
     }
+    grid_exit(sc);
 }
 
 template <class R>

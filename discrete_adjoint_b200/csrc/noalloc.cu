@@ -74,6 +74,7 @@ __global__ void k_init(DevScalars *sc, double time, long long iter) {
     sc->acc_alt_min_dxe = __double_as_longlong(10000000.0);
     sc->acc_alt_hmax = 0ull;
     sc->bar = 0ull;
+    sc->bar_exit = 0ull;
 }
 
 // Boundary / two-neighbour flags and byte materials from the caller's tables; an index out of

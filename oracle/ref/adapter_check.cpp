@@ -128,9 +128,8 @@ int pull_state() {
     return DA_OK;
 }
 
-// The body of step(): the MatProps / TimeProps fields the path reads, one device step, the
-// TimeProps bookkeeping incrtime does.
-int adapter_step(MatProps *mp, TimeProps *tp, StatProps *sp) {
+// The MatProps / TimeProps fields the path reads (angles already in radians).
+da_params params_of(const MatProps *mp, const TimeProps *tp) {
     da_params p;
     da_params_default(&p);
     p.epsilon = mp->epsilon;
@@ -142,6 +141,12 @@ int adapter_step(MatProps *mp, TimeProps *tp, StatProps *sp) {
     p.max_time = tp->ndmaxtime;
     p.next_output = tp->ndnextoutput;
     p.next_save = tp->ndnextsave;
+    return p;
+}
+
+// The body of step(): the parameters, one device step, the TimeProps bookkeeping incrtime does.
+int adapter_step(MatProps *mp, TimeProps *tp, StatProps *sp) {
+    const da_params p = params_of(mp, tp);
     int rc = da_set_params(g_da, &p);
     if (rc == DA_OK) rc = da_set_time(g_da, tp->time, tp->iter);
     da_step_stats s;
@@ -224,13 +229,15 @@ int main(int argc, char **argv) {
         DISCHARGE discharge;
         OutLine outline;
         int order_flag = 1;
-        // the device context and the adapter's tables
-        da_params p;
-        da_params_default(&p);
+        // the device context (created with the run's materials) and the adapter's tables
+        const da_params p = adapter::params_of(pa.matprops, &ta);
         int err = 0;
         adapter::g_da = da_create(&p, &err);
         if (!adapter::g_da) return 6;
-        if (adapter::da_flatten(A.El_Table, 0, true) != DA_OK || adapter::push_state() != DA_OK) return 7;
+        if (adapter::da_flatten(A.El_Table, 0, true) != DA_OK || adapter::push_state() != DA_OK) {
+            std::fprintf(stderr, "adapter: %s\n", da_last_error(adapter::g_da));
+            return 7;
+        }
         for (int it = 0; it < nsteps; ++it) {
             pb.matprops->frict_tiny = tb.iter < 50 ? 0.1 : 0.000000001;
             step(B.El_Table, B.NodeTable, 0, 1, pb.matprops, &tb, &pile, &flux, &sb, &order_flag, &outline,
