@@ -31,6 +31,7 @@ UNITS = [
     ("adjoint_host.cu", []),
     ("adjoint_ref.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
+    ("domain.cu", []),
     ("snapshot.cu", []),
     ("ensemble.cu", []),
     ("dwr.cu", []),

@@ -203,6 +203,13 @@ class da_member(C.Structure):
 SIGNATURES = {
     "da_abi_version": (C.c_int, []),
     "da_selftest_barrier": (C.c_int, [C.c_void_p, C.c_int32]),
+    "da_set_owned": (C.c_int, [C.c_void_p, C.c_int32]),
+    "da_get_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "da_step_bounds": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "da_step_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "da_halo_pack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "da_halo_unpack": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "da_sync": (C.c_int, [C.c_void_p]),
     "da_strerror": (C.c_char_p, [C.c_int]),
     "da_params_default": (None, [C.POINTER(da_params)]),
     "da_create": (C.c_void_p, [C.POINTER(da_params), C.POINTER(C.c_int)]),

@@ -128,6 +128,7 @@ static void free_mesh(da_ctx *ctx) {
     dfree(d.halo_off); dfree(d.halo_idx); dfree(d.nloc);
     d.halo_max = 0;
     d.n = 0;
+    d.n_owned = 0;
     d.epoch = -1;
 }
 
@@ -142,6 +143,7 @@ static void free_state(da_ctx *ctx) {
     dfree(ctx->seg_wet);
     dfree(ctx->seg_dirty);
     dfree(ctx->stage);
+    dfree(ctx->dd_bounds);
     dfree(ctx->tile_epoch);
     dfree(ctx->seg_act);
     dfree(ctx->lam_clean);
@@ -530,6 +532,7 @@ int da_upload_mesh(da_ctx *ctx, const da_mesh_soa *m, int32_t epoch) {
     free_adjoint(ctx);
     DevMesh &d = ctx->mesh;
     d.n = n;
+    d.n_owned = n;
     d.epoch = epoch;
     const bool fp64 = ctx->p.precision == DA_PREC_FP64;
     if (!st) st = upload(ctx, &d.nbr, m->nbr, (size_t)8 * n);

@@ -115,6 +115,7 @@ struct DwrState {
 // path reads the float copies.
 struct DevMesh {
     int32_t n = 0;
+    int32_t n_owned = 0;            // cells [n_owned, n) are ghosts (da_set_owned); n after an upload
     int32_t epoch = -1;
     int32_t *nbr = nullptr;         // [8][n]
     uint8_t *mat = nullptr;         // [n], zero-padded to whole tiles
@@ -175,6 +176,7 @@ struct da_ctx {
     uint8_t *seg_wet = nullptr;      // [nseg] 1 when the segment held a wet cell after the last update
     uint8_t *seg_dirty = nullptr;    // [nseg] 1 when the segment may differ from the base checkpoint
     double *stage = nullptr;         // [n] FP64 staging for host transfers of FP32 arrays
+    double *dd_bounds = nullptr;     // [2] a subdomain step's bounds passed by host pointer (domain.cu)
     double *seg_J = nullptr;         // [nseg] functional part of each segment at the final step
     // ensemble mode (ninst > 0): device tables of InstArgs, host copies of the member layout
     int ninst = 0;

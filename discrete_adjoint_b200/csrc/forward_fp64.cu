@@ -15,6 +15,10 @@ int launch_refine_info_fp64(da_ctx *ctx, double *e, uint8_t *f, double *parts, d
     return fwd::refine_info_t<double>(ctx, e, f, parts, t);
 }
 
+int launch_step_half_fp64(da_ctx *ctx, int half, double *bounds) {
+    return fwd::launch_step_half_t<double>(ctx, half, bounds);
+}
+
 int launch_volume(da_ctx *ctx) { return fwd::launch_volume_t(ctx); }
 
 namespace {
@@ -81,12 +85,21 @@ int forward_state_changed(da_ctx *ctx) {
     return st;
 }
 
+// A context with ghost cells (da_set_owned) must not form dt from its own cells alone: it steps
+// through da_step_bounds / da_step_apply, with the bounds combined over the subdomains.
+static int ghosts_refused(da_ctx *ctx) {
+    return set_error(ctx, DA_ERR_UNSUPPORTED,
+                     "context with ghost cells: step it with da_step_bounds / da_step_apply");
+}
+
 int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
+    if (ctx->mesh.n_owned != ctx->mesh.n) return ghosts_refused(ctx);
     if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps, pre_slot, post_slot);
     return launch_forward_steps_fp32(ctx, nsteps, pre_slot, post_slot);
 }
 
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {
+    if (ctx->mesh.n_owned != ctx->mesh.n) return ghosts_refused(ctx);
     if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, record_mask);
     return launch_forward_step_fp32(ctx, record_mask);
 }

@@ -162,8 +162,10 @@ __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> 
                         const R dxm = cell_dx<R>(m, i), dym = cell_dy<R>(m, i);
                         const unsigned long long rb = __double_as_longlong(double((dxm > dym ? dym : dxm) / ev));
                         const unsigned long long hb = __double_as_longlong(double(h));
-                        my_min = rb < my_min ? rb : my_min;
-                        my_max = hb > my_max ? hb : my_max;
+                        if (i < m.n_owned) {  // ghost cells are another subdomain's
+                            my_min = rb < my_min ? rb : my_min;
+                            my_max = hb > my_max ? hb : my_max;
+                        }
                     }
                 }
                 if (RECORD) mask[i] = code;
@@ -179,11 +181,14 @@ __device__ __forceinline__ void coef_phase(const MeshArgs &m, const StateRef<R> 
     }
 }
 
+// bounds (or null): the step's first half alone -- the last block writes the subdomain's CFL bound
+// and -hmax to bounds[0..1] instead of forming dt, so that one MIN all-reduce over the two doubles
+// combines the subdomains (get_coef_and_eigen.C:173) before k_apply_bounds forms dt.
 template <class R, bool RECORD = false>
 __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *__restrict__ kact,
                                                  unsigned *__restrict__ active, const uint8_t *__restrict__ seg_wet,
                                                  int ntiles, int cull, MatConsts mc, TimeConsts tc, DevScalars *sc,
-                                                 uint8_t *__restrict__ mask = nullptr) {
+                                                 uint8_t *__restrict__ mask = nullptr, double *bounds = nullptr) {
     __shared__ int list[kBlock];
     unsigned long long my_min = 0x7FF0000000000000ull;  // +inf
     unsigned long long my_max = 0ull;
@@ -191,10 +196,25 @@ __global__ void __launch_bounds__(kBlock) k_coef(MeshArgs m, StateRef<R> U, R *_
     push_minmax(my_min, my_max, &sc->acc_min_dxe, &sc->acc_hmax);
     if (last_block(&sc->blocks_done[0])) {
         if (threadIdx.x == 0) {
-            finalize_dt(sc, tc);
+            if (bounds) {
+                volatile unsigned long long *acc = &sc->acc_min_dxe, *acx = &sc->acc_hmax;
+                bounds[0] = __longlong_as_double(*acc);
+                bounds[1] = -__longlong_as_double(*acx);
+                sc->acc_min_dxe = kMinDxeStart;
+                sc->acc_hmax = 0ull;
+            } else {
+                finalize_dt(sc, tc);
+            }
             sc->blocks_done[0] = 0;
         }
     }
+}
+
+// dt of the combined subdomains: bounds = the MIN all-reduce of every subdomain's k_coef bounds.
+__global__ void k_apply_bounds(DevScalars *sc, TimeConsts tc, const double *bounds) {
+    sc->acc_min_dxe = __double_as_longlong(bounds[0]);
+    sc->acc_hmax = __double_as_longlong(-bounds[1]);
+    finalize_dt(sc, tc);
 }
 
 // The flux differences F(+side) - F(-side) of one cell in x (div[0]) and y (div[1]): the edge
@@ -355,7 +375,7 @@ __device__ __forceinline__ void update_phase(const MeshArgs &m, const StateRef<R
                 O.h[i] = st[0];
                 O.hu[i] = st[1];
                 O.hv[i] = st[2];
-                vol = double(dxc) * double(dyc) * double(st[0]);
+                if (i < m.n_owned) vol = double(dxc) * double(dyc) * double(st[0]);
                 wet_after = st[0] >= R(DA_TINY);
             }
             const unsigned wet_bits = __ballot_sync(0xffffffffu, wet_after);
@@ -648,6 +668,32 @@ int launch_step_t(da_ctx *ctx, uint8_t *record_mask = nullptr) {
     }
     ctx->cur = o;
     return cuda_check(ctx, cudaGetLastError(), "forward step launch");
+}
+
+// One step in two halves for a subdomain: half 0 is the coefficient phase writing bounds (device
+// memory), half 1 forms dt from the all-reduced bounds and runs the update phase.
+template <class R>
+int launch_step_half_t(da_ctx *ctx, int half, double *bounds) {
+    const MeshArgs m = mesh_args(ctx);
+    const int c = ctx->cur, o = 1 - c;
+    StateRef<R> U{(const R *)ctx->U[c][0], (const R *)ctx->U[c][1], (const R *)ctx->U[c][2]};
+    R *kact = (R *)ctx->kact;
+    const int tiles = ctx->ntiles, grid = ctx->grid, cull = ctx->p.tile_culling;
+    if (half == 0) {
+        trace_begin(ctx, TR_COEF);
+        k_coef<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, kact, ctx->active, ctx->seg_wet, tiles, cull, ctx->mc,
+                                                    ctx->tc, ctx->dsc, nullptr, bounds);
+        trace_end(ctx);
+    } else {
+        StateOut<R> O{(R *)ctx->U[o][0], (R *)ctx->U[o][1], (R *)ctx->U[o][2]};
+        k_apply_bounds<<<1, 1, 0, ctx->stream>>>(ctx->dsc, ctx->tc, bounds);
+        trace_begin(ctx, TR_UPDATE);
+        k_update<R><<<grid, kBlock, 0, ctx->stream>>>(m, U, O, kact, ctx->active, ctx->seg_clean, ctx->seg_wet,
+                                                      ctx->seg_vol, ctx->seg_dirty, tiles, cull, ctx->mc, ctx->dsc);
+        trace_end(ctx);
+        ctx->cur = o;
+    }
+    return cuda_check(ctx, cudaGetLastError(), "forward half-step launch");
 }
 
 // nsteps steps in one cooperative launch of k_steps; the grid is capped at the number of blocks

@@ -57,6 +57,7 @@ __device__ __forceinline__ R tiny_sgn(R num, R tiny) {
 
 struct MeshArgs {
     int n;
+    int n_owned;  // cells [n_owned, n) are ghost copies of another subdomain's cells (n_owned = n: none)
     const int32_t *__restrict__ nbr;
     const uint8_t *__restrict__ mat;
     const uint8_t *__restrict__ bflag;
@@ -77,7 +78,7 @@ struct MeshArgs {
 inline MeshArgs mesh_args(const da_ctx *ctx) {
     const DevMesh &d = ctx->mesh;
     MeshArgs a;
-    a.n = d.n; a.nbr = d.nbr; a.mat = d.mat; a.bflag = d.bflag;
+    a.n = d.n; a.n_owned = d.n_owned; a.nbr = d.nbr; a.mat = d.mat; a.bflag = d.bflag;
     a.x = d.x; a.y = d.y; a.dx = d.dx; a.dy = d.dy; a.g = d.g; a.dg = d.dg; a.curv = d.curv;
     a.fdx = d.fdx; a.fdy = d.fdy; a.fg = d.fg; a.fdg = d.fdg; a.fcurv = d.fcurv;
     return a;

@@ -156,6 +156,7 @@ extern "C" int da_forward_step_noalloc(const da_params *p, const da_mesh_soa *me
 
     fv::MeshArgs m;
     m.n = n;
+    m.n_owned = n;
     m.nbr = mesh->nbr;
     m.mat = mat8;
     m.bflag = bflag;

@@ -107,8 +107,9 @@ __device__ double plane_flux(const double nodes[9][2], double hu, double hv, con
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_stats_parts(MeshArgs m, StateRef<R> U, StatArgs a, double *parts) {
     __shared__ double sh[kBlock];
-    const int per = (m.n + kParts - 1) / kParts;
-    const int i0 = blockIdx.x * per, i1 = min(m.n, i0 + per);
+    // the owned cells (a subdomain's ghosts are another subdomain's)
+    const int per = (m.n_owned + kParts - 1) / kParts;
+    const int i0 = blockIdx.x * per, i1 = min(m.n_owned, i0 + per);
     double s[kSums] = {}, mx[kMax] = {}, mn[kMin], dis[DA_MAX_PLANES] = {};
     for (int q = 0; q < kMin; ++q) mn[q] = HUGE_VAL;
     double tdist = pow(2.0, 30.0), treach = 0.0;  // stats.C:58
@@ -263,7 +264,7 @@ int stats_t(da_ctx *ctx, const StatArgs &a, double vslump, double d_time, double
 // integer atomicMax is exact).
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_outline(MeshArgs m, StateRef<R> U, OutlineGrid g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n_owned; i += gridDim.x * blockDim.x) {
         const double height = double(U.h[i]);
         if (!(height > 0.0)) continue;  // the map starts at zero
         const double x = m.x[i], y = m.y[i], dx = m.dx ? m.dx[i] : double(m.fdx[i]), dy = m.dy ? m.dy[i] : double(m.fdy[i]);

@@ -383,6 +383,48 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out);
  * restarted afterwards, so the context's next launches run normally. */
 int da_selftest_barrier(da_ctx *ctx, int32_t limit_us);
 
+/* ---- domain decomposition: one mesh over several contexts -----------------------------------
+ * The reference's only parallel strategy: each MPI rank owns a weighted range of the elements'
+ * Hilbert keys (repartition_BSFC.C:540, weights :38-40), refreshes its ghost elements every step
+ * (move_data.C:28-300) and takes dt from MPI_Allreduce(MIN) over the ranks
+ * (get_coef_and_eigen.C:173).  Here a subdomain is a context whose mesh holds the owned cells
+ * first and ghost cells after them: two rings, the cells a step of the owned cells reads (face
+ * neighbours, including both fine neighbours of a hanging side, and their face neighbours), with
+ * the ghosts' neighbour entries that leave the subdomain set to -1.  discrete_adjoint_b200.domain
+ * builds the subdomains and the exchange lists.  One step of all subdomains:
+ *   da_step_bounds(ctx_r, b_r)          every subdomain
+ *   b = elementwise MIN over r of b_r   (ncclAllReduce(ncclMin, 2 doubles), or on the host)
+ *   da_step_apply(ctx_r, b, NULL)       every subdomain: the same dt bits everywhere
+ *   da_halo_pack(ctx_r, send cells, n, buf)  ->  transfer  ->  da_halo_unpack(ctx_s, recv cells, n, buf)
+ * after which the owned cells hold the undivided mesh's step bit for bit.  Contexts with ghosts
+ * refuse the whole-step calls (da_forward_step, da_forward_run, the adjoint: DA_ERR_UNSUPPORTED);
+ * their volume and da_compute_stats cover the owned cells only.
+ *
+ * da_set_owned: cells [n_owned, n_cells) of the uploaded mesh are ghosts (until the next upload).
+ * da_get_stream: the context's cudaStream_t, on which every call below is ordered; a collective
+ *   that consumes or produces device buffers of these calls must be ordered on it too.
+ * da_step_bounds: the first half of a step (slopes, k act/pass, wave speeds of every cell);
+ *   bounds[0] = min over the owned wet cells of min(dx, dy) / wave speed (1e7 when none),
+ *   bounds[1] = -(max depth over the owned wet cells), so that one MIN over the pair combines the
+ *   subdomains.  bounds: 2 doubles, device memory of the context's GPU (the call returns at once)
+ *   or host memory (the call waits for the pair).
+ * da_step_apply: dt from the combined pair (get_coef_and_eigen.C:168-179 and
+ *   TimeProps::incrtime), then the update of every cell; bounds as above.  stats NULL: returns at
+ *   once; otherwise waits and fills stats (volume over the owned cells).
+ * da_halo_pack: buf = the current h[cells], hu[cells], hv[cells] (3 n reals of the context's
+ *   precision, planar); cells must be owned ([0, n_owned)).
+ * da_halo_unpack: the reverse into ghost cells ([n_owned, n_cells)).  cells and buf of both are
+ *   device memory of the context's GPU; an index outside its range is skipped and reported as
+ *   DA_ERR_INVALID by the next call that waits (da_sync, da_step_apply with stats).
+ * da_sync: waits for the context's stream and returns the first error its kernels raised. */
+int da_set_owned(da_ctx *ctx, int32_t n_owned);
+int da_get_stream(da_ctx *ctx, void **stream);
+int da_step_bounds(da_ctx *ctx, double *bounds);
+int da_step_apply(da_ctx *ctx, const double *bounds, da_step_stats *stats);
+int da_halo_pack(da_ctx *ctx, const int32_t *cells, int32_t n, void *buf);
+int da_halo_unpack(da_ctx *ctx, const int32_t *cells, int32_t n, const void *buf);
+int da_sync(da_ctx *ctx);
+
 /* ---- one step without any device allocation ------------------------------------------------
  * No counterpart in the reference: an addition for callers that may not allocate device memory
  * themselves or through this library, such as a plugin whose host application owns all of the

@@ -47,6 +47,10 @@ def load() -> C.CDLL:
     lib.orc_forward_step_split.argtypes = [P, M, PD, PD, PD, PD, C.POINTER(C.c_int64), PD]
     lib.orc_adjoint_step_var.restype = C.c_int
     lib.orc_adjoint_step_var.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD, C.c_int]
+    lib.orc_step_bounds.restype = C.c_int
+    lib.orc_step_bounds.argtypes = [P, M, C.c_int, PD, PD, PD, PD, PD]
+    lib.orc_step_apply.restype = C.c_int
+    lib.orc_step_apply.argtypes = [P, M, PD, PD, PD, PD, PD, PD, C.POINTER(C.c_int64), PD]
     _lib = lib
     return lib
 
@@ -87,6 +91,25 @@ class Oracle:
             assert rc == 0
             dts[k] = d.value
         return dts[:nsteps]
+
+    def step_bounds(self, n_owned: int, h, hu, hv, work) -> np.ndarray:
+        """First half of a subdomain's step (cells [n_owned, n) are ghosts): fills work (7n) and
+        returns [min dx/eigen of the owned wet cells, -hmax]."""
+        b = np.zeros(2)
+        rc = self.lib.orc_step_bounds(C.byref(self.params), C.byref(self.soa), int(n_owned), _ffi.dptr(h),
+                                      _ffi.dptr(hu), _ffi.dptr(hv), _ffi.dptr(work), _ffi.dptr(b))
+        assert rc == 0, rc
+        return b
+
+    def step_apply(self, bounds, work, h, hu, hv) -> float:
+        """Second half: dt from the combined bounds, the update in place; returns dt."""
+        b = np.ascontiguousarray(bounds, dtype=np.float64)
+        d = C.c_double()
+        rc = self.lib.orc_step_apply(C.byref(self.params), C.byref(self.soa), _ffi.dptr(b), _ffi.dptr(work),
+                                     _ffi.dptr(h), _ffi.dptr(hu), _ffi.dptr(hv), C.byref(self.time),
+                                     C.byref(self.iter), C.byref(d))
+        assert rc == 0, rc
+        return d.value
 
     def slopes(self, h, hu, hv):
         out = np.zeros((6, self.mesh.n))

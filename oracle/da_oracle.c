@@ -134,15 +134,16 @@ double orc_kact_cell(const da_params *p, int mat, double h, double hu, double hv
 /* get_coef_and_eigen, src/geoflow/get_coef_and_eigen.C:86-166 (+ eigen.f:19-49).
  * kact: [n].  Returns via min_dxe (min over wet cells of min(dx,dy)/evalue, init 1e7),
  * hmax; returns DA_ERR_EIGEN if a wave speed exceeds 1e9. */
-int orc_coef_eigen(const da_params *p, const da_mesh_soa *m, const double *h, const double *hu,
-                   const double *hv, const double *slopes, double *kact, double *min_dxe_out,
-                   double *hmax_out) {
+static int coef_eigen_owned(const da_params *p, const da_mesh_soa *m, int n_owned, const double *h,
+                            const double *hu, const double *hv, const double *slopes, double *kact,
+                            double *min_dxe_out, double *hmax_out) {
     const int n = m->n_cells;
     double min_dx_dy_evalue = 10000000, hmax = 0;
     int status = DA_OK;
     for (int i = 0; i < n; ++i) {
         if (h[i] > TINY) {
-            if (hmax < h[i]) hmax = h[i];
+            const int own = i < n_owned;  /* ghosts of a subdomain enter no reduction */
+            if (own && hmax < h[i]) hmax = h[i];
             double dudx[3], dudy[3];
             for (int j = 0; j < 3; ++j) {
                 dudx[j] = slopes[(size_t)j * n + i];
@@ -157,7 +158,7 @@ int orc_coef_eigen(const da_params *p, const da_mesh_soa *m, const double *h, co
             const double evy = dabs(vy) + sqrt(k * gz * h[i]);
             const double evalue = evx > evy ? evx : evy;
             if (evalue > 1000000000.) status = DA_ERR_EIGEN;
-            min_dx_dy_evalue = c_dmin1_2(c_dmin1_2(m->dx[i], m->dy[i]) / evalue, min_dx_dy_evalue);
+            if (own) min_dx_dy_evalue = c_dmin1_2(c_dmin1_2(m->dx[i], m->dy[i]) / evalue, min_dx_dy_evalue);
         } else {
             kact[i] = p->epsilon;
         }
@@ -165,6 +166,12 @@ int orc_coef_eigen(const da_params *p, const da_mesh_soa *m, const double *h, co
     *min_dxe_out = min_dx_dy_evalue;
     *hmax_out = hmax;
     return status;
+}
+
+int orc_coef_eigen(const da_params *p, const da_mesh_soa *m, const double *h, const double *hu,
+                   const double *hv, const double *slopes, double *kact, double *min_dxe_out,
+                   double *hmax_out) {
+    return coef_eigen_owned(p, m, m->n_cells, h, hu, hv, slopes, kact, min_dxe_out, hmax_out);
 }
 
 /* dt of get_coef_and_eigen.C:168-179 followed by TimeProps::incrtime (properties.h:397-410).
@@ -433,4 +440,47 @@ int orc_forward_run(const da_params *p, const da_mesh_soa *m, double *h, double 
         if (st != DA_OK) return st;
     }
     return DA_OK;
+}
+
+/* The two halves of one step on a subdomain whose cells [n_owned, n) are ghost copies of other
+ * subdomains' cells (the domain-decomposed step: the ranks' CFL bounds meet in
+ * MPI_Allreduce(MIN), get_coef_and_eigen.C:173, between the halves).
+ * orc_step_bounds: slopes and k act/pass of every cell into work (7n doubles: slopes 6n, kact n);
+ *   bounds[0] = min over the owned wet cells of min(dx,dy)/eigen (1e7 if none), bounds[1] = -hmax.
+ * orc_step_apply: dt from the combined bounds (orc_dt), then the fluxes and the corrector of
+ *   orc_forward_step from the same work array; *dt_out receives dt. */
+int orc_step_bounds(const da_params *p, const da_mesh_soa *m, int n_owned, const double *h, const double *hu,
+                    const double *hv, double *work, double *bounds) {
+    const int n = m->n_cells;
+    double *slopes = work, *kact = work + 6 * (size_t)n;
+    orc_slopes(p, m, h, hu, hv, slopes);
+    double min_dxe, hmax;
+    const int st = coef_eigen_owned(p, m, n_owned, h, hu, hv, slopes, kact, &min_dxe, &hmax);
+    bounds[0] = min_dxe;
+    bounds[1] = -hmax;
+    return st;
+}
+
+int orc_step_apply(const da_params *p, const da_mesh_soa *m, const double *bounds, const double *work,
+                   double *h, double *hu, double *hv, double *time, int64_t *iter, double *dt_out) {
+    const int n = m->n_cells;
+    const double *slopes = work, *kact = work + 6 * (size_t)n;
+    double *F = (double *)calloc(12 * (size_t)n, sizeof(double));
+    double *prev = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+    if (!F || !prev) {
+        free(F); free(prev);
+        return DA_ERR_OOM;
+    }
+    const double frict_tiny = (*iter < p->frict_tiny_iters) ? p->frict_tiny_early : p->frict_tiny_late;
+    const double dt = orc_dt(p, bounds[0], -bounds[1], time);
+    *iter += 1;
+    orc_edge_fluxes(p, m, h, hu, hv, kact, F);
+    memcpy(prev, h, sizeof(double) * n);
+    memcpy(prev + n, hu, sizeof(double) * n);
+    memcpy(prev + 2 * (size_t)n, hv, sizeof(double) * n);
+    const int st = orc_correct(p, m, prev, prev + n, prev + 2 * (size_t)n, slopes, kact, F, dt, frict_tiny, h, hu,
+                               hv, NULL, NULL);
+    if (dt_out) *dt_out = dt;
+    free(F); free(prev);
+    return st;
 }
