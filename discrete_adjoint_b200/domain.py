@@ -312,7 +312,7 @@ class LocalDomain:
             for q in d.sub.recv:
                 src = self.doms[q]
                 d.stream.wait_event(events[(q, d.sub.rank)])
-                buf = src.send_buf[q]
+                buf = src.send_buf[d.sub.rank]
                 if src.device != d.device:
                     with torch.cuda.stream(d.stream):
                         d.recv_buf[q].copy_(buf, non_blocking=True)
