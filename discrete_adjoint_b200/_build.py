@@ -38,6 +38,7 @@ UNITS = [
     ("stats.cu", []),
     ("mesh_host.cpp", []),
     ("solution_io.cpp", []),
+    ("restart_io.cpp", []),
 ]
 
 

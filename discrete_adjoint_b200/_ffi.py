@@ -27,6 +27,7 @@ DA_ERR_NO_MESH = -7
 DA_ERR_OOM = -8
 DA_ERR_NO_DEVICE = -9
 DA_ERR_UNSUPPORTED = -10
+DA_ERR_IO = -11
 
 DA_PREC_FP64 = 0
 DA_PREC_FP32_SPLIT = 1
@@ -63,6 +64,29 @@ class da_params(C.Structure):
         ("tile_staging", C.c_int32),
         ("jacobian_mode", C.c_int32),
         ("pad_mode", C.c_int32),
+    ]
+
+
+class da_restart_header(C.Structure):
+    _fields_ = [
+        ("min_dx", C.c_double * 2), ("min_gen", C.c_double),
+        ("maxh_iter", C.c_int32), ("maxh_hmax", C.c_double),
+        ("iter", C.c_int32), ("adjiter", C.c_int32), ("time", C.c_double),
+        ("solrec_last_step", C.c_int32),
+        ("n_nodes", C.c_int32), ("n_elements", C.c_int32), ("n_unresolved", C.c_int32),
+        ("xrange", C.c_double * 2), ("yrange", C.c_double * 2),
+    ]
+
+
+class da_restart_cells(C.Structure):
+    _fields_ = [
+        ("keys", C.POINTER(C.c_uint32)), ("nbr", C.POINTER(C.c_int32)),
+        ("level", C.POINTER(C.c_int32)), ("material", C.POINTER(C.c_int32)),
+        ("x", C.POINTER(C.c_double)), ("y", C.POINTER(C.c_double)), ("dx", C.POINTER(C.c_double)),
+        ("dy", C.POINTER(C.c_double)), ("elevation", C.POINTER(C.c_double)),
+        ("zeta", C.POINTER(C.c_double)), ("curvature", C.POINTER(C.c_double)),
+        ("d_gravity", C.POINTER(C.c_double)), ("gravity", C.POINTER(C.c_double)),
+        ("h", C.POINTER(C.c_double)), ("hu", C.POINTER(C.c_double)), ("hv", C.POINTER(C.c_double)),
     ]
 
 
@@ -261,6 +285,11 @@ SIGNATURES = {
     "da_write_solution": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_uint32), PD, PD, PD]),
     "da_read_solution": (C.c_int, [C.c_char_p, C.c_int32, C.POINTER(C.c_uint32), PD, PD, PD,
                                    C.POINTER(C.c_int32)]),
+    "da_write_restart": (C.c_int, [C.c_char_p, C.POINTER(da_restart_header), PD, C.c_int32, C.POINTER(da_mesh_soa),
+                                   PI32, PI32, PI32, PD, PD, PD, PD, PD, PD]),
+    "da_read_restart": (C.c_int, [C.c_char_p, C.POINTER(da_restart_header), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_int32), PD, C.POINTER(da_restart_cells)]),
+    "da_write_outline": (C.c_int, [C.c_char_p, PD, PD, PD, C.c_int32, C.c_int32, PD]),
 }
 
 _lib = None

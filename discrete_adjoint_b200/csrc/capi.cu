@@ -341,6 +341,7 @@ const char *da_strerror(int code) {
         case DA_ERR_OOM: return "device out of memory";
         case DA_ERR_NO_DEVICE: return "no CUDA device";
         case DA_ERR_UNSUPPORTED: return "unsupported";
+        case DA_ERR_IO: return "file could not be opened, read or written";
         default: return "unknown error";
     }
 }

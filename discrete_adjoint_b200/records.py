@@ -69,3 +69,75 @@ def record_forward(ctx, nsteps: int, directory: str, keys: np.ndarray, rank: int
         h, hu, hv = ctx.get_state()
         write_solution(os.path.join(directory, solution_name(rank, step0 + k)), keys, h, hu, hv)
         ctx.step()
+
+
+# ---------------------------------------------------------------------------- restart files
+def write_restart(path: str, mesh, h, hu, hv, time: float = 0.0, iteration: int = 0, dt_hist=(),
+                  bedfrict=None, adjiter: int = 0, min_dx=(0.0, 0.0), min_gen: float = 0.0,
+                  maxh=(0, 0.0), solrec_last_step: int = 0):
+    """restart_<rank> of the reference (save_forward, src/main/restart.C:21-125) for a mesh built
+    by this package (its level / ix / iy give the node lattice) and a state: the reference's
+    loadrun rebuilds the tables from it and its step() continues the run."""
+    hd = _ffi.da_restart_header()
+    hd.min_dx[0], hd.min_dx[1] = min_dx
+    hd.min_gen = min_gen
+    hd.maxh_iter, hd.maxh_hmax = int(maxh[0]), float(maxh[1])
+    hd.iter, hd.adjiter, hd.time = int(iteration), int(adjiter), float(time)
+    hd.solrec_last_step = int(solrec_last_step)
+    dts = np.ascontiguousarray(dt_hist, dtype=np.float64)
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (h, hu, hv)]
+    bf = None if bedfrict is None else np.ascontiguousarray(bedfrict, dtype=np.float64)
+    st = _ffi.load().da_write_restart(os.fsencode(path), C.byref(hd), _ffi.dptr(dts) if len(dts) else None,
+                                      len(dts), C.byref(mesh.soa()), _ffi.iptr(mesh.level), _ffi.iptr(mesh.ix),
+                                      _ffi.iptr(mesh.iy), _ffi.dptr(mesh.zeta), _ffi.dptr(mesh.elevation),
+                                      _ffi.dptr(bf) if bf is not None else None, *[_ffi.dptr(v) for v in a])
+    if st:
+        raise _ffi.DAError(st, f"da_write_restart {path}")
+
+
+def read_restart(path: str) -> dict:
+    """The active elements of a reference restart file as a flattened mesh in key order: a dict
+    with 'mesh' (Mesh), 'keys', 'h', 'hu', 'hv', 'iter', 'adjiter', 'time', 'dt' (the history)
+    and the file's other header fields."""
+    from .mesh import Mesh
+    lib = _ffi.load()
+    hd = _ffi.da_restart_header()
+    n, ndt = C.c_int32(0), C.c_int32(0)
+    st = lib.da_read_restart(os.fsencode(path), C.byref(hd), C.byref(n), C.byref(ndt), None, None)
+    if st:
+        raise _ffi.DAError(st, f"da_read_restart {path}")
+    N = n.value
+    arr = {"keys": np.zeros((N, 2), np.uint32), "nbr": np.zeros((8, N), np.int32), "level": np.zeros(N, np.int32),
+           "material": np.zeros(N, np.int32), "x": np.zeros(N), "y": np.zeros(N), "dx": np.zeros(N),
+           "dy": np.zeros(N), "elevation": np.zeros(N), "zeta": np.zeros((2, N)), "curvature": np.zeros((2, N)),
+           "d_gravity": np.zeros((2, N)), "gravity": np.zeros((3, N)), "h": np.zeros(N), "hu": np.zeros(N),
+           "hv": np.zeros(N)}
+    dts = np.zeros(max(ndt.value, 1))
+    cells = _ffi.da_restart_cells(
+        arr["keys"].ctypes.data_as(C.POINTER(C.c_uint32)), _ffi.iptr(arr["nbr"]), _ffi.iptr(arr["level"]),
+        _ffi.iptr(arr["material"]), *[_ffi.dptr(arr[k]) for k in ("x", "y", "dx", "dy", "elevation", "zeta",
+                                                                   "curvature", "d_gravity", "gravity", "h", "hu",
+                                                                   "hv")])
+    st = lib.da_read_restart(os.fsencode(path), C.byref(hd), C.byref(n), C.byref(ndt), _ffi.dptr(dts),
+                             C.byref(cells))
+    if st:
+        raise _ffi.DAError(st, f"da_read_restart {path}")
+    mesh = Mesh(n=N, nbr=arr["nbr"], material=arr["material"], level=arr["level"], x=arr["x"], y=arr["y"],
+                dx=arr["dx"], dy=arr["dy"], elevation=arr["elevation"], zeta=arr["zeta"],
+                curvature=arr["curvature"], gravity=arr["gravity"], d_gravity=arr["d_gravity"],
+                h0=arr["h"], hu0=arr["hu"], hv0=arr["hv"])
+    return {"mesh": mesh, "keys": arr["keys"], "h": arr["h"], "hu": arr["hu"], "hv": arr["hv"],
+            "iter": hd.iter, "adjiter": hd.adjiter, "time": hd.time, "dt": dts[:ndt.value],
+            "min_dx": tuple(hd.min_dx), "min_gen": hd.min_gen, "maxh": (hd.maxh_iter, hd.maxh_hmax),
+            "solrec_last_step": hd.solrec_last_step, "n_nodes": hd.n_nodes, "n_elements": hd.n_elements,
+            "n_unresolved": hd.n_unresolved, "xrange": tuple(hd.xrange), "yrange": tuple(hd.yrange)}
+
+
+def write_outline(path: str, dxy, xrange, yrange, grid: np.ndarray):
+    """outline_<rank> beside a restart file (restart.C:104-121): grid is [ny][nx]."""
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (dxy, xrange, yrange)]
+    st = _ffi.load().da_write_outline(os.fsencode(path), *[_ffi.dptr(v) for v in a], g.shape[1], g.shape[0],
+                                      _ffi.dptr(g))
+    if st:
+        raise _ffi.DAError(st, f"da_write_outline {path}")

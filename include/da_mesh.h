@@ -100,6 +100,57 @@ int da_write_solution(const char *path, int32_t n, const uint32_t *keys, const d
 int da_read_solution(const char *path, int32_t n, const uint32_t *keys, double *h, double *hu, double *hv,
                      int32_t *n_missing);
 
+/* ---- the reference's restart files (host) --------------------------------------------------
+ * restart_<rank> as save_forward writes it and loadrun reads it (src/main/restart.C:21-239): the
+ * driver's min_dx / min_gen, MaxH_Functional's iteration and hmax, TimeProps (iter, adjiter, time,
+ * the dt history), the node table, the element table and the SolRec table header, one gzip stream.
+ *
+ * da_write_restart: the tables of a flattened quadtree mesh (level, ix, iy of each cell at its own
+ * level, as the mesh builder gives them) with its state, in the reference's layout -- nodes on the
+ * lattice of half the finest cell with their CORNER / SIDE / BUBBLE / S_C_CON / S_S_CON info,
+ * Hilbert keys of the coordinates, positive_x_side 1, every cell NOTRECADAPTED -- so that the
+ * reference's loadrun rebuilds them and its step() continues the run.  zeta, elevation, bedfrict
+ * (per material, radians; effect_bedfrict and its tangent) may be NULL (zeros).  Node elevations
+ * are written as 0.
+ * da_read_restart: the active elements (adapted flag > 0) in key order as a flattened mesh: call
+ * with out NULL to get *n_cells and *n_dt, then with arrays of at least those sizes (*n_cells and
+ * *n_dt in: the capacities).  A neighbour that is not in the file (another rank's) is -1 and
+ * counted in n_unresolved.
+ * da_write_outline: outline_<rank> (restart.C:104-121): dxy, x and y ranges, ny rows of nx
+ * maximum depths. */
+typedef struct da_restart_header {
+    double min_dx[2];
+    double min_gen;
+    int32_t maxh_iter;
+    double maxh_hmax;
+    int32_t iter;               /* TimeProps::iter */
+    int32_t adjiter;            /* TimeProps::adjiter */
+    double time;                /* TimeProps::time (dimensionless) */
+    int32_t solrec_last_step;   /* SolRec::last_solution_time_step */
+    /* filled by da_read_restart */
+    int32_t n_nodes, n_elements, n_unresolved;
+    double xrange[2], yrange[2];  /* the element table's */
+} da_restart_header;
+
+typedef struct da_restart_cells {  /* any pointer may be NULL (not returned) */
+    uint32_t *keys;                /* [n][2] */
+    int32_t *nbr;                  /* [8][n], the layout of da_mesh_soa.nbr */
+    int32_t *level, *material;     /* generation; material from 0 */
+    double *x, *y, *dx, *dy, *elevation;
+    double *zeta, *curvature, *d_gravity;  /* [2][n] */
+    double *gravity;               /* [3][n] */
+    double *h, *hu, *hv;
+} da_restart_cells;
+
+int da_write_restart(const char *path, const da_restart_header *hd, const double *dt_hist, int32_t n_dt,
+                     const da_mesh_soa *m, const int32_t *level, const int32_t *ix, const int32_t *iy,
+                     const double *zeta, const double *elevation, const double *bedfrict, const double *h,
+                     const double *hu, const double *hv);
+int da_read_restart(const char *path, da_restart_header *hd, int32_t *n_cells, int32_t *n_dt, double *dt_hist,
+                    const da_restart_cells *out);
+int da_write_outline(const char *path, const double dxy[2], const double xrange[2], const double yrange[2],
+                     int32_t nx, int32_t ny, const double *map);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,7 @@ extern "C" {
 #define DA_ERR_OOM (-8)         /* device allocation failed */
 #define DA_ERR_NO_DEVICE (-9)   /* no CUDA device visible */
 #define DA_ERR_UNSUPPORTED (-10)
+#define DA_ERR_IO (-11)         /* a file could not be opened, read or written */
 
 /* adjoint modes (da_params.jacobian_mode) */
 #define DA_JAC_EXACT 0          /* the exact transpose of the forward step as computed here */

@@ -464,3 +464,74 @@ def run_adapter_check(mesh, mat, h, hu, hv, nsteps: int = 0, step: bool = False)
     assert v[0] == 0x314F4944 and v[1] == n
     return {"nbr_mismatch": v[2], "field_mismatch": v[3], "state_mismatch": v[4], "dt_mismatch": v[5],
             "steps": v[6], "max_diff": struct.unpack_from("<d", raw, 28)[0]}
+
+
+def _mesh_payload(magic: int, mesh, mat, nsteps: int, flag: int, h, hu, hv) -> bytes:
+    """The flattened mesh and a state in the harness's 'DAH1' layout (header magic, n, max_level,
+    n_materials, nsteps, flag; scalars; tables; fields; h, hu, hv)."""
+    import struct
+
+    from discrete_adjoint_b200.solver import MatProps
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    parts = [struct.pack("<6i", magic, mesh.n, mesh.max_level, len(mat.bedfrict_deg), nsteps, flag),
+             np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma, float("inf")],
+                      dtype="<f8").tobytes(), bed.astype("<f8").tobytes()]
+    for a in (mesh.nbr, mesh.level, mesh.ix, mesh.iy, mesh.material):
+        parts.append(np.ascontiguousarray(a, dtype="<i4").tobytes())
+    for a in (mesh.x, mesh.y, mesh.dx, mesh.dy, mesh.zeta, mesh.gravity, mesh.d_gravity, mesh.curvature, h, hu, hv):
+        parts.append(np.ascontiguousarray(a, dtype="<f8").tobytes())
+    return b"".join(parts)
+
+
+def _elements_out(raw: bytes, magic: int) -> dict:
+    import struct
+    m, n, it, ndt = struct.unpack_from("<4i", raw, 0)
+    assert m == magic, hex(m)
+    arr = np.frombuffer(raw, dtype="<f8", offset=16)
+    time_, dts = float(arr[0]), arr[1:1 + ndt].copy()
+    rec = np.frombuffer(raw, dtype=np.uint8, offset=16 + 8 * (1 + ndt)).reshape(n, 8 + 16 + 24)
+    keys = rec[:, :8].copy().view("<u4").reshape(n, 2)
+    xy = rec[:, 8:24].copy().view("<f8").reshape(n, 2)
+    st = rec[:, 24:].copy().view("<f8").reshape(n, 3)
+    return {"iter": it, "time": time_, "dt": dts, "keys": keys, "x": xy[:, 0], "y": xy[:, 1],
+            "h": st[:, 0], "hu": st[:, 1], "hv": st[:, 2]}
+
+
+def run_reference_save(mesh, mat, h, hu, hv, nsteps: int, outline, directory: str) -> dict:
+    """The reference's step() nsteps times from (h, hu, hv) on the mesh's tables, then its
+    save_forward (restart.C:21-125): restart_0000 and outline_0000 land in `directory`.
+    outline = (dxy, xrange, yrange) of the max-depth grid.  Returns the active elements' keys,
+    centres and states and the TimeProps history (harness mode 'DAS1')."""
+    import subprocess
+    payload = _mesh_payload(0x31534144, mesh, mat, nsteps, 0, h, hu, hv)
+    payload += np.concatenate([np.asarray(v, dtype="<f8") for v in outline]).astype("<f8").tobytes()
+    fin, fout = os.path.join(directory, "save_in.bin"), os.path.join(directory, "save_out.bin")
+    open(fin, "wb").write(payload)
+    r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True, cwd=directory)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_harness save failed ({r.returncode}): {r.stderr[-2000:]}")
+    return _elements_out(open(fout, "rb").read(), 0x314F5344)
+
+
+def run_reference_load(mat, nsteps: int, outline, directory: str) -> dict:
+    """The reference's loadrun (restart.C:127-239) of restart_0000 / outline_0000 in `directory`,
+    then its step() nsteps times (harness mode 'DAL1').  Returns as run_reference_save."""
+    import struct
+    import subprocess
+
+    from discrete_adjoint_b200.solver import MatProps
+    bed = np.zeros(16)
+    for k, b in enumerate(mat.bedfrict_deg):
+        bed[k] = MatProps.rad(b)
+    payload = struct.pack("<3i", 0x314C4144, len(mat.bedfrict_deg), nsteps)
+    payload += np.array([MatProps.rad(mat.intfrict_deg), mat.epsilon, mat.gravity_scale, mat.gamma, float("inf")],
+                        dtype="<f8").tobytes() + bed.astype("<f8").tobytes()
+    payload += np.concatenate([np.asarray(v, dtype="<f8") for v in outline]).astype("<f8").tobytes()
+    fin, fout = os.path.join(directory, "load_in.bin"), os.path.join(directory, "load_out.bin")
+    open(fin, "wb").write(payload)
+    r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True, cwd=directory)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_harness load failed ({r.returncode}): {r.stderr[-2000:]}")
+    return _elements_out(open(fout, "rb").read(), 0x314F4C44)

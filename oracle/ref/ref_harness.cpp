@@ -37,6 +37,10 @@
 //   'DAF1' (mesh as 'DAH1', initial state, functional box; see fwdadj_mode) -> 'DFO1': the
 //       reference's forward steps with solution recording, then its dual-solver reverse steps,
 //       each timed (the CPU baseline of the forward + adjoint path).
+//   'DAS1' (mesh as 'DAH1', state, outline grid; see save_mode) -> 'DSO1': nsteps reference
+//       steps, then save_forward writes restart_0000 and outline_0000 in the working directory.
+//   'DAL1' (materials, nsteps, outline grid; see load_mode) -> 'DLO1': loadrun reads restart_0000
+//       and outline_0000 from the working directory, then nsteps reference steps.
 #include <sys/sysinfo.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -376,6 +380,115 @@ int fwdadj_mode(FILE *f, const int32_t hdr[6], const char *out) {
     return 0;
 }
 
+// The driver's time loop with adaptation off (hpfem.C:222-357): frict_tiny by iteration, step().
+void drive(HashTable *El_Table, HashTable *NodeTable, MatProps &matprops, TimeProps &timeprops, int nsteps) {
+    PileProps pileprops;
+    FluxProps fluxprops;
+    StatProps statprops;
+    statprops.hxyminmax = matprops.MAX_NEGLIGIBLE_HEIGHT * 10.0;
+    statprops.timereached = -1.0;
+    DISCHARGE discharge;
+    OutLine outline;
+    int order_flag = 1;
+    for (int it = 0; it < nsteps; ++it) {
+        matprops.frict_tiny = timeprops.iter < 50 ? 0.1 : 0.000000001;
+        step(El_Table, NodeTable, 0, 1, &matprops, &timeprops, &pileprops, &fluxprops, &statprops, &order_flag,
+             &outline, &discharge, 0);
+    }
+}
+
+// Every active element (adapted > 0): coordinates and state, then the TimeProps history.
+int write_elements(const char *out, int32_t magic, HashTable *El_Table, const TimeProps &tp) {
+    std::vector<Element *> act;
+    HashEntryPtr *buck = El_Table->getbucketptr();
+    for (int b = 0; b < El_Table->get_no_of_buckets(); ++b)
+        for (HashEntryPtr e = buck[b]; e; e = e->next) {
+            Element *el = (Element *)e->value;
+            if (el->adapted > 0) act.push_back(el);
+        }
+    FILE *o = std::fopen(out, "wb");
+    if (!o) return 2;
+    const int32_t oh[4] = {magic, (int32_t)act.size(), tp.iter, (int32_t)tp.dt.size()};
+    wr(o, oh, 4);
+    wr(o, &tp.time, 1);
+    if (!tp.dt.empty()) wr(o, tp.dt.data(), tp.dt.size());
+    for (Element *el : act) {
+        wr(o, el->key, 2);
+        wr(o, el->coord, 2);
+        wr(o, el->state_vars, 3);
+    }
+    std::fclose(o);
+    return 0;
+}
+
+// 'DAS1': the mesh and state as 'DAH1' (nsteps in the header), then double dxy[2], xr[2], yr[2]
+// of the outline grid.  nsteps reference steps, then save_forward (restart.C:21-125) writes
+// restart_0000 and outline_0000 into the working directory.  Output: 'DSO1' as write_elements.
+int save_mode(FILE *f, const int32_t hdr[6], const char *out) {
+    MeshIn m;
+    read_mesh(f, hdr, m);
+    const int n = m.n;
+    std::vector<double> h(n), hu(n), hv(n);
+    rd(f, h.data(), n); rd(f, hu.data(), n); rd(f, hv.data(), n);
+    double dxy[2], xr[2], yr[2];
+    rd(f, dxy, 2); rd(f, xr, 2); rd(f, yr, 2);
+    std::fclose(f);
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, HUGE_VAL, HUGE_VAL, HUGE_VAL, 1.0);
+    Tables t = build_tables(m, h.data(), hu.data(), hv.data(), matprops, false);
+    drive(t.El_Table, t.NodeTable, matprops, timeprops, m.nsteps);
+    OutLine outline;
+    outline.init2(dxy, xr, yr);
+    SolRec *solrec = solrec_for(t, n);
+    MeshCTX mctx;
+    mctx.el_table = t.El_Table;
+    mctx.nd_table = t.NodeTable;
+    PropCTX pctx;
+    pctx.matprops = &matprops;
+    pctx.timeprops = &timeprops;
+    pctx.mapnames = nullptr;
+    pctx.outline = &outline;
+    pctx.numproc = 1;
+    pctx.myid = 0;
+    pctx.adapt_flag = 0;
+    save_forward(mctx, pctx, solrec);
+    return write_elements(out, 0x314F5344, t.El_Table, timeprops);
+}
+
+// 'DAL1': int32 magic, n_materials, nsteps; double intfrict, epsilon, gravity_scale, gamma,
+// maxtime, bedfrict[16]; double dxy[2], xr[2], yr[2] of the outline grid in the file.  loadrun
+// (restart.C:127-239) rebuilds the tables from restart_0000 / outline_0000 in the working
+// directory, then nsteps reference steps.  Output: 'DLO1' as write_elements.
+int load_mode(FILE *f, const char *out) {
+    MeshIn m;
+    int32_t a[2];
+    rd(f, a, 2);
+    m.nmat = a[0];
+    m.nsteps = a[1];
+    rd(f, m.sc, 5);
+    rd(f, m.bed, 16);
+    double dxy[2], xr[2], yr[2];
+    rd(f, dxy, 2); rd(f, xr, 2); rd(f, yr, 2);
+    std::fclose(f);
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    matprops.number_of_cells_across_axis = 1;
+    matprops.smallest_axis = 1.0;
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, HUGE_VAL, HUGE_VAL, HUGE_VAL, 1.0);
+    OutLine outline;
+    outline.init2(dxy, xr, yr);   // loadrun reads the grid with the caller's dimensions
+    HashTable *NodeTable = nullptr, *El_Table = nullptr;
+    SolRec *solrec = nullptr;
+    if (!loadrun(0, 1, &NodeTable, &El_Table, &solrec, &matprops, &timeprops, &outline)) return 4;
+    drive(El_Table, NodeTable, matprops, timeprops, m.nsteps);
+    return write_elements(out, 0x314F4C44, El_Table, timeprops);
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -390,11 +503,13 @@ int main(int argc, char **argv) {
     if (magic == 0x314B4144) return keys_mode(f, argv[2]);
     if (magic == 0x31574144) return write_mode(f, argv[2]);
     if (magic == 0x31524144) return read_mode(f, argv[2]);
+    if (magic == 0x314C4144) return load_mode(f, argv[2]);
     int32_t hdr[6];
     hdr[0] = magic;
     rd(f, hdr + 1, 5);
     if (hdr[0] == 0x314A4144) return adjoint_mode(f, hdr, argv[2]);
     if (hdr[0] == 0x31464144) return fwdadj_mode(f, hdr, argv[2]);
+    if (hdr[0] == 0x31534144) return save_mode(f, hdr, argv[2]);
     if (hdr[0] != 0x31484144) return 3;
     MeshIn m;
     read_mesh(f, hdr, m);

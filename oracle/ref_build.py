@@ -36,6 +36,8 @@ UNITS = [
     # the reference's adjoint of one step (the harness's 'DAJ1' mode)
     "adjoint/dual_grid_routines.C", "adjoint/calc_jacobain.C", "adjoint/compute_jacobian_elem.C",
     "adjoint/calc_adjoint.C", "adjoint/debug_routines.C",
+    # restart files (the harness's 'DAS1' / 'DAL1' modes)
+    "main/restart.C",
 ]
 PATCH = {
     "geoflow/edge_states.C": [(r"Curr_El->calc_edge_states<T>\(", "Curr_El->template calc_edge_states<T>(")],
