@@ -548,20 +548,40 @@ __global__ void __launch_bounds__(kBlock) k_ref_seed(MeshArgs m, StateRef<double
     }
 }
 
+// The neighbour table with each side's two finer neighbours in the reference's order: an element
+// keeps them counter-clockwise around its boundary (adapt/refine2.C:590-805), the flattened table
+// lists the lower (sides +-x) or left (sides +-y) one first, so the +y and -x pairs swap.  The dual
+// solver sums its blocks in slot order; this table gives its sums their order.
+__global__ void k_ref_ccw(const int32_t *__restrict__ nbr, int32_t *__restrict__ ccw, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (int k = 0; k < 8; ++k) {
+            const int r = k & 3;
+            const int src = (r == 1 || r == 2) ? (k ^ 4) : k;
+            ccw[(size_t)k * n + i] = nbr[(size_t)src * n + i];
+        }
+}
+
 }  // namespace
 }  // namespace refadj
 
 // Workspace of the reference mode: one allocation sized for the mesh (about 1 KB per cell,
-// mostly the 108 flux-Jacobian entries), zeroed once so that entries no rule writes read as 0.
+// mostly the 108 flux-Jacobian entries), zeroed once so that entries no rule writes read as 0,
+// and the counter-clockwise neighbour table.
 int ref_adjoint_alloc(da_ctx *ctx) {
     const size_t n = (size_t)ctx->mesh.n;
     if (ctx->refadj_mem && ctx->refadj_n == (int)n) return DA_OK;
     if (ctx->refadj_mem) cudaFree(ctx->refadj_mem);
     ctx->refadj_mem = nullptr;
     ctx->refadj_n = 0;
-    const size_t bytes = n * (sizeof(double) * (6 + 10 + 1 + refadj::kFJ) + 4 + 1) + 256;
+    const size_t bytes = n * (sizeof(double) * (6 + 10 + 1 + refadj::kFJ) + sizeof(int32_t) * 8 + 4 + 1) + 256;
     int st = cuda_check(ctx, cudaMalloc(&ctx->refadj_mem, bytes), "cudaMalloc(reference-mode adjoint)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->refadj_mem, 0, bytes, ctx->stream), "memset");
+    if (!st) {
+        int32_t *ccw = (int32_t *)((char *)ctx->refadj_mem + sizeof(double) * (6 + 10 + 1 + refadj::kFJ) * n);
+        const int sms = ctx->sm_count > 0 ? ctx->sm_count : 148;
+        refadj::k_ref_ccw<<<sms * 4, 256, 0, ctx->stream>>>(ctx->mesh.nbr, ccw, (int)n);
+        st = cuda_check(ctx, cudaGetLastError(), "neighbour order launch");
+    }
     if (!st) ctx->refadj_n = (int)n;
     return st;
 }
@@ -581,9 +601,11 @@ int launch_ref_adjoint_step(da_ctx *ctx, int un, int lam_in, int lam_out) {
     b.hs = (double *)p; p += sizeof(double) * 10 * n;
     b.kact = (double *)p; p += sizeof(double) * n;
     b.fj = (double *)p; p += sizeof(double) * refadj::kFJ * n;
+    const int32_t *ccw = (const int32_t *)p; p += sizeof(int32_t) * 8 * n;
     b.sgn = (int8_t *)p; p += 4 * n;
     b.stop = (uint8_t *)p;
-    const fv::MeshArgs m = fv::mesh_args(ctx);
+    fv::MeshArgs m = fv::mesh_args(ctx);
+    m.nbr = ccw;   // the reference's pair order on every side
     const refadj::Rec P{(const double *)ctx->U[un][0], (const double *)ctx->U[un][1], (const double *)ctx->U[un][2]};
     const fv::StateRef<double> Ln{(const double *)ctx->lam[lam_in][0], (const double *)ctx->lam[lam_in][1],
                                   (const double *)ctx->lam[lam_in][2]};

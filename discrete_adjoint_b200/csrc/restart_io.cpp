@@ -16,7 +16,9 @@
 // Reading keeps the elements whose adapted flag is positive (the active cells of every loop of the
 // reference), orders them by key (the space-filling curve) and resolves their neighbour keys
 // into the flattened neighbour table: relative side r = (absolute side a - positive_x_side) mod 4,
-// a domain edge where neigh_proc[a] is INIT.
+// a domain edge where neigh_proc[a] is INIT.  An element keeps a side's two finer neighbours in
+// the counter-clockwise order of its boundary (adapt/refine2.C:590-805), the table lists the
+// lower (sides +-x) or left (sides +-y) one first: the pair is swapped on +y and -x, both ways.
 //
 // Writing builds the tables of a flattened quadtree mesh the way the reference lays them out:
 // nodes on the lattice of half the finest cell -- corners 0-3 counter-clockwise from the lower
@@ -294,10 +296,13 @@ int da_write_restart(const char *path, const da_restart_header *hd, const double
                 nbk[a] = nbk[a + 4] = zero2;
                 ngen[a] = ngen[a + 4] = 0;
             } else {
+                // two finer neighbours go counter-clockwise around the element: on +y and -x the
+                // table's second one comes first
+                const bool swap = r == 1 || r == 2;
                 nproc[a] = 0;
                 nproc[a + 4] = e2 != e1 ? 0 : kOneSideNeigh;
-                nbk[a] = nkey(e1, 8);
-                nbk[a + 4] = nkey(e2, 8);
+                nbk[a] = nkey(swap ? e2 : e1, 8);
+                nbk[a + 4] = nkey(swap ? e1 : e2, 8);
                 ngen[a] = ngen[a + 4] = level[e1];
             }
         }
@@ -477,8 +482,9 @@ int da_read_restart(const char *path, da_restart_header *hd, int32_t *n_cells, i
                         i1 = i2 = -1;
                     }
                 }
-                out->nbr[(size_t)r * n + i] = i1;
-                out->nbr[(size_t)(r + 4) * n + i] = i2;
+                const bool swap = r == 1 || r == 2;   // counter-clockwise pair -> lower / left first
+                out->nbr[(size_t)r * n + i] = swap ? i2 : i1;
+                out->nbr[(size_t)(r + 4) * n + i] = swap ? i1 : i2;
             }
         }
         if (out->level) out->level[i] = e.gen;

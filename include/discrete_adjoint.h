@@ -29,7 +29,10 @@
  *   side 0 = +x (xp), 1 = +y (yp), 2 = -x (xm), 3 = -y (ym).
  * nbr[s*n + i] (s = 0..3) is the first neighbour across side s (Element::neighbor[s]),
  * nbr[(s+4)*n + i] the second one (Element::neighbor[s+4]); the two differ only where
- * the side carries two finer neighbours (edge-midpoint node S_C_CON, constant.h:42);
+ * the side carries two finer neighbours (edge-midpoint node S_C_CON, constant.h:42), and
+ * then the lower one (sides 0 and 2) or the left one (sides 1 and 3) comes first -- the
+ * reference keeps the pair counter-clockwise around the element, the other way round on
+ * sides 1 and 2 (adapt/refine2.C:590-805);
  * -1 marks the domain boundary (neigh_proc == INIT, constant.h:48).
  */
 #ifndef DISCRETE_ADJOINT_H

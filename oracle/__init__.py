@@ -49,6 +49,8 @@ def load() -> C.CDLL:
     lib.orc_adjoint_step_var.argtypes = [P, M, PD, PD, PD, C.c_double, C.c_double, PD, PD, C.c_int]
     lib.orc_step_bounds.restype = C.c_int
     lib.orc_step_bounds.argtypes = [P, M, C.c_int, PD, PD, PD, PD, PD]
+    lib.orc_step_frozen.restype = C.c_int
+    lib.orc_step_frozen.argtypes = [P, M, C.c_double, PD, PD, PD, C.c_int64]
     lib.orc_step_apply.restype = C.c_int
     lib.orc_step_apply.argtypes = [P, M, PD, PD, PD, PD, PD, PD, C.POINTER(C.c_int64), PD]
     _lib = lib
@@ -110,6 +112,12 @@ class Oracle:
                                      C.byref(self.iter), C.byref(d))
         assert rc == 0, rc
         return d.value
+
+    def step_frozen(self, dt: float, h, hu, hv, iteration: int):
+        """One step with the given dt in place (no CFL reduction; frict_tiny by `iteration`)."""
+        rc = self.lib.orc_step_frozen(C.byref(self.params), C.byref(self.soa), float(dt), _ffi.dptr(h),
+                                      _ffi.dptr(hu), _ffi.dptr(hv), int(iteration))
+        assert rc == 0, rc
 
     def slopes(self, h, hu, hv):
         out = np.zeros((6, self.mesh.n))
@@ -535,3 +543,38 @@ def run_reference_load(mat, nsteps: int, outline, directory: str) -> dict:
     if r.returncode != 0:
         raise RuntimeError(f"ref_harness load failed ({r.returncode}): {r.stderr[-2000:]}")
     return _elements_out(open(fout, "rb").read(), 0x314F4C44)
+
+
+def run_reference_dwr(fine, parent, mat, prev, state, adjoint, dt: float, iteration: int,
+                      workdir: str | None = None) -> dict:
+    """The reference's DWR estimate of one step on the error grid (harness mode 'DAE1'):
+    bilinear_interp, update_bilinear_error_grid and error_compute (dual_solver.C:213-230) on
+    `fine` (the coarse mesh refined once, `parent` its coarse cell per fine cell), every fine cell
+    starting from its father's prev = U^{iteration-1}, state = U^{iteration} and adjoint (each
+    [3][n]); dt the step's.  Returns per fine cell bilin_state, bilin_prev, bilin_adj,
+    residual ([3][nf] each), el_error ([2][nf]) and correction ([nf])."""
+    import struct
+    import subprocess
+    import tempfile
+    n = np.asarray(prev).shape[-1]
+    payload = _mesh_payload(0x31454144, fine, mat, 0, 0, np.zeros(fine.n), np.zeros(fine.n), np.zeros(fine.n))
+    # the header's nsteps / flag words carry the iteration and the coarse cell count; the zero
+    # state the layout ends with is not part of this mode's input
+    payload = bytearray(payload[: len(payload) - 24 * fine.n])
+    struct.pack_into("<2i", payload, 16, int(iteration), int(n))
+    payload += np.ascontiguousarray(parent, dtype="<i4").tobytes()
+    for a in (prev, state, adjoint):
+        payload += np.ascontiguousarray(a, dtype="<f8").reshape(3 * n).tobytes()
+    payload += struct.pack("<d", float(dt))
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        open(fin, "wb").write(bytes(payload))
+        r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"ref_harness dwr failed ({r.returncode}): {r.stderr[-2000:]}")
+        raw = open(fout, "rb").read()
+    magic, nf = struct.unpack_from("<2i", raw, 0)
+    assert magic == 0x314F4544 and nf == fine.n
+    a = np.frombuffer(raw, dtype="<f8", offset=8).reshape(nf, 15)
+    return {"bilin_state": a[:, 0:3].T.copy(), "bilin_prev": a[:, 3:6].T.copy(), "bilin_adj": a[:, 6:9].T.copy(),
+            "residual": a[:, 9:12].T.copy(), "el_error": a[:, 12:14].T.copy(), "correction": a[:, 14].copy()}

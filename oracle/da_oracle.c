@@ -484,3 +484,30 @@ int orc_step_apply(const da_params *p, const da_mesh_soa *m, const double *bound
     free(F); free(prev);
     return st;
 }
+
+/* One step with a given dt (no CFL reduction): slopes, k act/pass, fluxes and the corrector of
+ * orc_forward_step, frict_tiny by *iter as there.  The error grid's step of the DWR estimate takes
+ * the coarse step's dt (error_grid_routines.C:13-55, error_compute.C:24-119). */
+int orc_step_frozen(const da_params *p, const da_mesh_soa *m, double dt, double *h, double *hu, double *hv,
+                    int64_t iter) {
+    const int n = m->n_cells;
+    double *work = (double *)malloc(sizeof(double) * 7 * (size_t)n);
+    if (!work) return DA_ERR_OOM;
+    double b[2];
+    int st = orc_step_bounds(p, m, n, h, hu, hv, work, b);
+    double *F = (double *)calloc(12 * (size_t)n, sizeof(double));
+    double *prev = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+    if (!F || !prev) {
+        free(work); free(F); free(prev);
+        return DA_ERR_OOM;
+    }
+    const double frict_tiny = (iter < p->frict_tiny_iters) ? p->frict_tiny_early : p->frict_tiny_late;
+    orc_edge_fluxes(p, m, h, hu, hv, work + 6 * (size_t)n, F);
+    memcpy(prev, h, sizeof(double) * n);
+    memcpy(prev + n, hu, sizeof(double) * n);
+    memcpy(prev + 2 * (size_t)n, hv, sizeof(double) * n);
+    const int st2 = orc_correct(p, m, prev, prev + n, prev + 2 * (size_t)n, work, work + 6 * (size_t)n, F, dt,
+                                frict_tiny, h, hu, hv, NULL, NULL);
+    free(work); free(F); free(prev);
+    return st ? st : st2;
+}

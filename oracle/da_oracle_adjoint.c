@@ -363,9 +363,38 @@ static void dual_slopes_dir(const da_mesh_soa *m, const double *P[3], int i, int
  * threshold (calc_jacobain.C:82-85); lam_next [3][n]: the adjoint of U^n; lam_out [3][n]: the
  * adjoint of U^{n-1} with a zero functional sensitivity.  Returns DA_OK or DA_ERR_OOM.
  */
+static int adjoint_step_ccw(const da_params *p, const da_mesh_soa *m, const double *h, const double *hu,
+                            const double *hv, double dt, double frict_tiny, const double *lam_next, double *lam_out,
+                            int keep);
+
+/* The reference keeps a side's two finer neighbours in the counter-clockwise order of the element's
+ * boundary (adapt/refine2.C:590-805): +x lower then upper, +y right then left, -x upper then lower,
+ * -y left then right; the flattened table lists the lower / left one first.  The dual solver sums
+ * its blocks in slot order, so the step below runs on the table with the +y and -x pairs in the
+ * reference's order. */
 int orc_adjoint_step_var(const da_params *p, const da_mesh_soa *m, const double *h, const double *hu,
                          const double *hv, double dt, double frict_tiny, const double *lam_next, double *lam_out,
                          int keep) {
+    const int n = m->n_cells;
+    int32_t *nb = (int32_t *)malloc(sizeof(int32_t) * 8 * (size_t)n);
+    if (!nb) return DA_ERR_OOM;
+    memcpy(nb, m->nbr, sizeof(int32_t) * 8 * (size_t)n);
+    for (int r = 1; r <= 2; ++r)
+        for (int c = 0; c < n; ++c) {
+            const int32_t t = nb[(size_t)r * n + c];
+            nb[(size_t)r * n + c] = nb[(size_t)(r + 4) * n + c];
+            nb[(size_t)(r + 4) * n + c] = t;
+        }
+    da_mesh_soa mc = *m;
+    mc.nbr = nb;
+    const int st = adjoint_step_ccw(p, &mc, h, hu, hv, dt, frict_tiny, lam_next, lam_out, keep);
+    free(nb);
+    return st;
+}
+
+static int adjoint_step_ccw(const da_params *p, const da_mesh_soa *m, const double *h, const double *hu,
+                            const double *hv, double dt, double frict_tiny, const double *lam_next, double *lam_out,
+                            int keep) {
     const int n = m->n_cells;
     double *P = (double *)malloc(sizeof(double) * 3 * (size_t)n);
     double *S = (double *)malloc(sizeof(double) * 6 * (size_t)n);

@@ -84,8 +84,11 @@ int da_flatten(HashTable *El_Table, int epoch, bool upload) {
         for (int r = 0; r < 4; ++r) {  // relative side: +x, +y, -x, -y
             const int a = (xp + r) % 4;
             if (el->get_neigh_proc()[a] == INIT) continue;  // domain edge stays -1
-            nbr[(size_t)r * n + i] = index.at(key64(el->get_neighbors() + 2 * a));
-            nbr[(size_t)(r + 4) * n + i] = index.at(key64(el->get_neighbors() + 2 * (a + 4)));
+            // the table lists a side's two finer neighbours lower / left first; the element keeps
+            // them counter-clockwise, which on +y and -x is the other way round
+            const int s1 = (r == 1 || r == 2) ? 4 : 0;
+            nbr[(size_t)r * n + i] = index.at(key64(el->get_neighbors() + 2 * (a + s1)));
+            nbr[(size_t)(r + 4) * n + i] = index.at(key64(el->get_neighbors() + 2 * (a + 4 - s1)));
         }
         x[i] = el->get_coord()[0];
         y[i] = el->get_coord()[1];

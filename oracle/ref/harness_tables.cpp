@@ -192,7 +192,12 @@ Tables build_tables(const MeshIn &m, const double *h, const double *hu, const do
         e->positive_x_side = 1;
         for (int a = 0; a < 4; ++a) {
             const int r = (a + 3) % 4;
-            const int e1 = nbr[(size_t)r * n + c], e2 = nbr[(size_t)(r + 4) * n + c];
+            // the reference stores a side's two finer neighbours in the counter-clockwise order of
+            // the element's boundary (+x: lower, upper; +y: right, left; -x: upper, lower; -y: left,
+            // right -- adapt/refine2.C:590-805); the flattened table lists them lower/left first
+            const bool ccw_swap = r == 1 || r == 2;
+            const int f1 = nbr[(size_t)r * n + c], f2 = nbr[(size_t)(r + 4) * n + c];
+            const int e1 = ccw_swap ? f2 : f1, e2 = ccw_swap ? f1 : f2;
             if (e1 < 0) {
                 e->neigh_proc[a] = -1;
                 e->neigh_proc[a + 4] = -2;

@@ -41,6 +41,9 @@
 //       steps, then save_forward writes restart_0000 and outline_0000 in the working directory.
 //   'DAL1' (materials, nsteps, outline grid; see load_mode) -> 'DLO1': loadrun reads restart_0000
 //       and outline_0000 from the working directory, then nsteps reference steps.
+//   'DAE1' (the refined error grid, its parents, a coarse step's states and adjoint; see
+//       dwr_mode) -> 'DEO1': the reference's DWR estimate of that step -- bilinear_interp,
+//       update_bilinear_error_grid, error_compute -- on the error grid.
 #include <sys/sysinfo.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -489,6 +492,101 @@ int load_mode(FILE *f, const char *out) {
     return write_elements(out, 0x314F4C44, El_Table, timeprops);
 }
 
+// 'DAE1': header (magic, nf, L, n_materials, iter, n); scalars and bed friction as 'DAH1'; the
+// error grid as a flattened mesh of nf cells ('DAH1' arrays); int32 parent[nf] (the coarse cell
+// each fine cell was split from); double prev[3][n] = U^{iter-1}, state[3][n] = U^{iter},
+// adjoint[3][n] of the coarse cells, dt of the step.  As dual_solver does after an adjoint step
+// (dual_solver.C:213-230): every fine cell takes its father's prev/state/adjoint
+// (send_from_dual_to_error, error_grid_routines.C:129-183), then bilinear_interp,
+// update_bilinear_error_grid and error_compute with TimeProps::iter = iter and dt[iter - 1] = dt.
+// Output 'DEO1' nf; per fine cell (input order) bilin_state[3] bilin_prev_state[3] bilin_adj[3]
+// residual[3] el_error[2] correction.
+int dwr_mode(FILE *f, const int32_t hdr[6], const char *out) {
+    const int32_t fh[6] = {hdr[0], hdr[1], hdr[2], hdr[3], 0, 0};
+    MeshIn m;
+    read_mesh(f, fh, m);
+    const int nf = m.n, iter = hdr[4], n = hdr[5];
+    std::vector<int32_t> parent(nf);
+    rd(f, parent.data(), nf);
+    std::vector<double> prev((size_t)3 * n), st((size_t)3 * n), adj((size_t)3 * n);
+    double dt = 0;
+    rd(f, prev.data(), prev.size());
+    rd(f, st.data(), st.size());
+    rd(f, adj.data(), adj.size());
+    rd(f, &dt, 1);
+    std::fclose(f);
+    if (iter < 1) return 3;
+    for (int c = 0; c < nf; ++c)
+        if (parent[c] < 0 || parent[c] >= n || m.level[c] < 1) return 3;
+    Props pr;
+    make_props(m, pr);
+    MatProps &matprops = *pr.matprops;
+    std::vector<double> zero(nf, 0.0);
+    Tables t = build_tables(m, zero.data(), zero.data(), zero.data(), matprops, false);
+    // lattice keys of the build (harness_tables.cpp): bubble of a cell at (level, ix, iy), +1 per word
+    auto bubble_key = [&](int lev, int64_t ix, int64_t iy, unsigned k[2]) {
+        const int64_t s = int64_t(1) << (m.L - lev + 1);
+        k[0] = unsigned(ix * s + s / 2 + 1);
+        k[1] = unsigned(iy * s + s / 2 + 1);
+    };
+    static const int off[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};   // sons counter-clockwise
+    std::vector<ErrorElem *> errs(nf);
+    for (int c = 0; c < nf; ++c) {
+        Element *e = t.els[c];
+        const int lev = m.level[c];
+        const int64_t fx = m.ix[c] >> 1, fy = m.iy[c] >> 1;
+        bubble_key(lev - 1, fx, fy, e->father);
+        for (int j = 0; j < 4; ++j) {
+            bubble_key(lev, 2 * fx + off[j][0], 2 * fy + off[j][1], e->brothers[j]);
+            if (2 * fx + off[j][0] == m.ix[c] && 2 * fy + off[j][1] == m.iy[c]) e->which_son = j;
+        }
+        ErrorElem *ee = new ErrorElem(e);
+        const int p = parent[c];
+        for (int v = 0; v < 3; ++v) {
+            ee->prev_state_vars[v] = prev[(size_t)v * n + p];
+            ee->state_vars[v] = st[(size_t)v * n + p];
+            ee->adjoint[v] = adj[(size_t)v * n + p];
+        }
+        t.El_Table->remove(e->key);
+        t.El_Table->add(ee->key, ee);
+        errs[c] = ee;
+    }
+    TimeProps timeprops;
+    timeprops.inittime(1 << 30, HUGE_VAL, HUGE_VAL, HUGE_VAL, 1.0);
+    timeprops.iter = iter;
+    timeprops.dt.assign(iter, 0.0);
+    timeprops.dt[iter - 1] = dt;
+    MeshCTX ectx;
+    ectx.el_table = t.El_Table;
+    ectx.nd_table = t.NodeTable;
+    PropCTX pctx;
+    pctx.matprops = &matprops;
+    pctx.timeprops = &timeprops;
+    pctx.mapnames = nullptr;
+    pctx.outline = nullptr;
+    pctx.numproc = 1;
+    pctx.myid = 0;
+    pctx.adapt_flag = 0;
+    bilinear_interp(t.El_Table);
+    update_bilinear_error_grid(&ectx, &pctx);
+    error_compute(&ectx, &pctx);
+    FILE *o = std::fopen(out, "wb");
+    if (!o) return 2;
+    const int32_t oh[2] = {0x314F4544, nf};
+    wr(o, oh, 2);
+    for (int c = 0; c < nf; ++c) {
+        ErrorElem *e = errs[c];
+        wr(o, e->bilin_state, 3);
+        wr(o, e->bilin_prev_state, 3);
+        wr(o, e->bilin_adj, 3);
+        wr(o, e->residual, 3);
+        wr(o, e->el_error, 2);
+        wr(o, &e->correction, 1);
+    }
+    std::fclose(o);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -510,6 +608,7 @@ int main(int argc, char **argv) {
     if (hdr[0] == 0x314A4144) return adjoint_mode(f, hdr, argv[2]);
     if (hdr[0] == 0x31464144) return fwdadj_mode(f, hdr, argv[2]);
     if (hdr[0] == 0x31534144) return save_mode(f, hdr, argv[2]);
+    if (hdr[0] == 0x31454144) return dwr_mode(f, hdr, argv[2]);
     if (hdr[0] != 0x31484144) return 3;
     MeshIn m;
     read_mesh(f, hdr, m);

@@ -6,7 +6,8 @@ build system (autotools, MPI, HDF5, Fortran) is not used: this recipe compiles t
 translation units on the step() path directly with g++, against
   - oracle/ref/include/mpi.h + mpi_stub.cpp   (single rank),
   - oracle/ref/include/hdf5.h + hdf5_stub.cpp (no-op),
-  - oracle/ref/fortran_c.cpp                  (C restatements of getcoef.f, eigen.f, predict.f).
+  - oracle/ref/fortran_c.cpp                  (C restatements of getcoef.f, eigen.f, predict.f),
+  - oracle/ref/lapack_c.cpp                   (dgesv, LAPACK's LU solve, restated).
 Two translation units miss the `template` keyword at dependent member-template calls
 (src/geoflow/edge_states.C:61, src/datstr/element2.C:4308-4324), which g++ rejects; they are
 preprocessed into oracle/_ref/ and the keyword is inserted there before compiling.  No source
@@ -38,6 +39,8 @@ UNITS = [
     "adjoint/calc_adjoint.C", "adjoint/debug_routines.C",
     # restart files (the harness's 'DAS1' / 'DAL1' modes)
     "main/restart.C",
+    # the DWR estimate on the error grid (the harness's 'DAE1' mode)
+    "adjoint/bilinear_interp.C", "adjoint/error_compute.C", "adjoint/error_grid_routines.C",
 ]
 PATCH = {
     "geoflow/edge_states.C": [(r"Curr_El->calc_edge_states<T>\(", "Curr_El->template calc_edge_states<T>(")],
@@ -89,8 +92,8 @@ def build(verbose: bool = False, force: bool = False) -> str | None:
         else:
             _run(CXX + ["-c", src, "-o", obj], verbose)
     own = []
-    for f in ("mpi_stub.cpp", "hdf5_stub.cpp", "fortran_c.cpp", "link_stubs.cpp", "harness_tables.cpp",
-              "ref_harness.cpp"):
+    for f in ("mpi_stub.cpp", "hdf5_stub.cpp", "fortran_c.cpp", "lapack_c.cpp", "link_stubs.cpp",
+              "harness_tables.cpp", "ref_harness.cpp"):
         src = os.path.join(STUBS, f)
         obj = os.path.join(OUT, f + ".o")
         own.append(obj)

@@ -19,6 +19,11 @@ calc_jacobian and calc_adjoint, run through the harness's 'DAJ1' mode):
   adj_stress_s12 one reverse step from a synthetic state (thin and dry cells, dry cells with
                  momentum, random adjoint) at an iteration past the frict_tiny switch.
 Run only these with:   python tests/golden/make_golden.py adj
+
+Fixture "dwr_s11_55" holds the reference's DWR estimate of one step (bilinear_interp,
+update_bilinear_error_grid, error_compute through the harness's 'DAE1' mode) on the error grid of
+fwd_s11_60's mesh: the reconstructions, the error grid's residual, el_error and correction per
+fine cell.  Run only it with:   python tests/golden/make_golden.py dwr
 """
 import os
 import sys
@@ -163,12 +168,49 @@ def adjoint_stress_case(name="adj_stress_s12", seed=12, it=70):
     print(p, m.n, "cells", os.path.getsize(p) // 1024, "KiB")
 
 
+def dwr_case(name="dwr_s11_55", seed=11, n0=55):
+    """The reference's DWR estimate (bilinear_interp, update_bilinear_error_grid, error_compute;
+    harness mode 'DAE1') of the step n0 -> n0 + 1 on the error grid of fwd_s11_60's mesh, with a
+    seeded adjoint lambda^{n0+1}; the forward states are the oracle's (bit for bit the reference's)."""
+    from discrete_adjoint_b200 import TimeProps, make_params
+    from discrete_adjoint_b200.dwr import error_grid
+    w = inputs.test_case(seed=seed, nx0=12, ny0=8, max_level=2, random_frac=0.4)
+    m = w.mesh
+    g = error_grid(w)
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    h, hu, hv = m.h0.copy(), m.hu0.copy(), m.hv0.copy()
+    rc, _dts, _st = o.run(h, hu, hv, n0)
+    assert rc == 0
+    un = np.stack([h, hu, hv]).copy()
+    rc, dts, _st = o.run(h, hu, hv, 1)
+    assert rc == 0
+    unext = np.stack([h, hu, hv])
+    rng = np.random.default_rng(seed)
+    wet = unext[0] > 1e-4
+    lam = np.stack([rng.standard_normal(m.n) * wet, 0.1 * rng.standard_normal(m.n) * wet,
+                    0.1 * rng.standard_normal(m.n) * wet])
+    r = oracle.run_reference_dwr(g.fine, g.parent, w.mat, un, unext, lam, float(dts[0]), n0 + 1)
+    arrs = {("mesh_" + k): v for k, v in m.arrays().items()}
+    arrs.update({"n0": np.int64(n0), "un": un, "dt": np.float64(dts[0]), "lam_next": lam, "parent": g.parent,
+                 "ref_bilin_prev": r["bilin_prev"], "ref_bilin_adj": r["bilin_adj"], "ref_residual": r["residual"],
+                 "ref_el_error": r["el_error"][1], "ref_correction": r["correction"]})
+    arrs["intfrict_deg"] = np.float64(w.mat.intfrict_deg)
+    arrs["bedfrict_deg"] = np.array(w.mat.bedfrict_deg, dtype=np.float64)
+    p = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(p, **arrs)
+    print(p, m.n, "cells", g.fine.n, "fine cells", os.path.getsize(p) // 1024, "KiB")
+
+
 def main():
     ref_build.build()
     if sys.argv[1:] == ["adj"]:
         adjoint_sweep_case()
         adjoint_stress_case()
         return
+    if sys.argv[1:] == ["dwr"]:
+        dwr_case()
+        return
+    dwr_case()
     adjoint_sweep_case()
     adjoint_stress_case()
     hilbert_keys()

@@ -127,3 +127,23 @@ def test_adjoint_run_accumulates_the_step_indicators():
     assert np.all(sums[:, 0] > 0)
     np.testing.assert_allclose(res.dwr_steps, sums, rtol=1e-12, atol=1e-14 * np.abs(sums).max())
     np.testing.assert_allclose(res.dwr_cell, cells, rtol=1e-12, atol=1e-14 * cells.max())
+
+
+def test_indicator_matches_the_reference_estimate_fixture():
+    # the reference's own estimate of the step n0 -> n0 + 1 (bilinear_interp, update_bilinear_error_grid,
+    # error_compute through the harness), committed as tests/golden/dwr_s11_55.npz
+    import os
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "dwr_s11_55.npz"))
+    w = inputs.test_case(seed=11, nx0=12, ny0=8, max_level=2, random_frac=0.4)
+    g = error_grid(w)
+    assert np.array_equal(g.parent, z["parent"])
+    with GeoflowContext(w.mat, TimeProps()) as c:
+        c.upload_mesh(w.mesh)
+        c.set_state(*z["un"])
+        c.set_time(0.0, int(z["n0"]))
+        el, cell, sums = Indicator(c, g).step(z["lam_next"])
+    ref = z["ref_el_error"]
+    assert np.abs(el - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert abs(sums[0] - ref.sum()) <= 1e-12 * ref.sum()
+    assert abs(sums[1] - z["ref_correction"].sum()) <= 1e-10 * np.abs(z["ref_correction"]).sum()
+    assert np.allclose(cell, np.bincount(g.parent, weights=el, minlength=w.mesh.n), rtol=1e-12, atol=0)
