@@ -136,6 +136,7 @@ static void free_state(da_ctx *ctx) {
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 3; ++v) dfree(ctx->U[b][v]);
     dfree(ctx->kact);
+    dfree(ctx->slopes);
     dfree(ctx->seg_vol);
     dfree(ctx->vol_parts);
     dfree(ctx->active);

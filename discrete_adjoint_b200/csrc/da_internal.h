@@ -167,6 +167,7 @@ struct da_ctx {
     void *U[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
     int cur = 0;
     void *kact = nullptr;            // [n] Real
+    void *slopes = nullptr;          // [6][n] Real: wet cells' limited slopes from the coefficient phase
     // segments: 32 consecutive cells (one warp), 8 per tile; arrays padded to whole tiles
     int nseg = 0;                    // ntiles * 8
     double *seg_vol = nullptr;       // [nseg] volume partial of each segment after its last update

@@ -56,6 +56,7 @@ int forward_alloc(da_ctx *ctx) {
             if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->U[b][v], 0, rs * n, ctx->stream), "memset");
         }
     if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->kact, rs * n), "cudaMalloc(kact)");
+    if (!st) st = cuda_check(ctx, cudaMalloc(&ctx->slopes, 6 * rs * n), "cudaMalloc(slopes)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->seg_wet, nseg), "cudaMalloc(seg_wet)");
     if (!st) st = cuda_check(ctx, cudaMalloc((void **)&ctx->tile_epoch, sizeof(int) * ctx->ntiles), "cudaMalloc(epoch)");
     if (!st) st = cuda_check(ctx, cudaMemsetAsync(ctx->tile_epoch, 0xff, sizeof(int) * ctx->ntiles, ctx->stream), "memset");

@@ -244,10 +244,12 @@ __device__ __forceinline__ void flux_div(const V &v, int i, uint8_t bf, const R 
 // Full corrector update of one active cell (fluxes + sources), reference order.  c is the cell in
 // the view; cs its source coefficients (read only for a wet cell, h > GEOFLOW_TINY); hook(f,
 // clamped) runs for a wet cell with the slopes, velocities and friction signs of its sources.
+// pre_s (or null): the cell's limited slopes as the coefficient phase computed them from the same
+// state (the same bits cell_slopes gives here).
 template <class R, class V, class Hook = NoSrcHook>
 __device__ __forceinline__ bool update_cell(const V &v, int c, uint8_t bf, const CellSrc<R> &cs, const MatConsts &mc,
                                             R dt, R ft, const R prev[3], R dxc, R dyc, R st[3],
-                                            const Hook &hook = Hook{}) {
+                                            const R *pre_s = nullptr, const Hook &hook = Hook{}) {
     const R ki = prev[0] >= R(DA_TINY) ? v.k(c) : R(0);
     const R gz = v.gz(c);
     const R g0 = cs.g[0], g1 = cs.g[1], dg0 = cs.dg[0], dg1 = cs.dg[1], cv0 = cs.cv[0], cv1 = cs.cv[1];
@@ -268,7 +270,12 @@ __device__ __forceinline__ bool update_cell(const V &v, int c, uint8_t bf, const
     if (clamped) st[0] = R(0);
     if (prev[0] > R(DA_TINY)) {
         R s[6];
-        cell_slopes<R>(v, c, bf, R(mc.gamma), prev, s);
+        if (pre_s) {
+#pragma unroll
+            for (int j = 0; j < 6; ++j) s[j] = pre_s[j];
+        } else {
+            cell_slopes<R>(v, c, bf, R(mc.gamma), prev, s);
+        }
         R vel0, vel1, h_inv;
         if constexpr (sizeof(R) == 8) {
             vel0 = prev[1] / prev[0];

@@ -54,9 +54,13 @@ struct HaloArgs {
     const int32_t *off;   // [ntiles + 1]
     const int32_t *idx;   // halo cells, tile after tile
     const int16_t *nloc;  // [n][8] tile-local neighbour slots
+    void *slopes;         // [6][n] reals: the limited slopes of each wet cell (h > GEOFLOW_TINY), written
+                          // by the coefficient phase and read by the same step's update phase
 };
 
-inline HaloArgs halo_args(const da_ctx *ctx) { return HaloArgs{ctx->mesh.halo_off, ctx->mesh.halo_idx, ctx->mesh.nloc}; }
+inline HaloArgs halo_args(const da_ctx *ctx) {
+    return HaloArgs{ctx->mesh.halo_off, ctx->mesh.halo_idx, ctx->mesh.nloc, ctx->slopes};
+}
 
 // The staged phases run when the parameters ask for them and the mesh's halo tables exist.
 inline bool staged_ok(const da_ctx *ctx) { return ctx->p.tile_staging >= 1 && ctx->mesh.nloc != nullptr; }
@@ -291,6 +295,11 @@ __device__ __forceinline__ void coef_phase_staged(const MeshArgs &m, const HaloA
                         const R ui[3] = {h, b.hu[c], b.hv[c]};
                         R s[6];
                         cell_slopes<R>(v, c, bf, R(mc.gamma), ui, s);
+                        if (ha.slopes) {  // kept for the update phase's source terms
+                            R *sl = (R *)ha.slopes;
+#pragma unroll
+                            for (int j = 0; j < 6; ++j) sl[(size_t)j * m.n + i] = s[j];
+                        }
                         const R k = cell_kact<R>(mc, mat, h, ui[1], ui[2], s, &code);
                         kact[i] = k;
                         const R gz = b.gz[c];
@@ -369,6 +378,14 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
             bool wet_after = false, act = false;
             if (i < m.n) {
                 const R prev[3] = {b.h[c], b.hu[c], b.hv[c]};
+                // the slopes this step's coefficient phase left for a wet cell, loaded ahead of the fluxes
+                const bool own_s = ha.slopes != nullptr && prev[0] > R(DA_TINY);
+                R pre_s[6];
+                if (own_s) {
+                    const R *sl = (const R *)ha.slopes;
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) pre_s[j] = sl[(size_t)j * m.n + i];
+                }
                 const auto pre = epi.pre(i, prev[0] > R(DA_TINY));
                 const uint8_t bf = b.bf[c];
                 StagedView<R> v{b};
@@ -394,7 +411,7 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
                 // the k act/pass code the coefficient phase recorded
                 const uint8_t kcode = RECORD && prev[0] >= R(DA_TINY) ? uint8_t(mask[i] & 3) : uint8_t(0);
                 if (act)
-                    clamped = update_cell<R>(v, c, bf, cs, mc, dt, ft, prev, dxc, dyc, st,
+                    clamped = update_cell<R>(v, c, bf, cs, mc, dt, ft, prev, dxc, dyc, st, own_s ? pre_s : nullptr,
                                              [&](const SrcFwd<R> &f, bool cl) {
                                                  // a wet cell is active: its branch byte as recorded below
                                                  epi(t, i, v, c, prev, bf, uint8_t(kcode | 8 | (cl ? 4 : 0)), b.gz[c],
