@@ -619,8 +619,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_reduce(MeshArgs m, StateRef<R> L
                                                        double *__restrict__ part) {
     __shared__ double red[kBlock / 32];
     const int o = blockIdx.y;  // 0..n_mat-1 bed per material, n_mat internal, then piles
-    const int per = (m.n + kReduceParts - 1) / kReduceParts;
-    const int i0 = blockIdx.x * per, i1 = min(m.n, i0 + per);
+    // the owned cells (a subdomain's ghosts are summed by their owner)
+    const int per = (m.n_owned + kReduceParts - 1) / kReduceParts;
+    const int i0 = blockIdx.x * per, i1 = min(m.n_owned, i0 + per);
     double acc = 0.0;
     for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         if (o < n_mat) {

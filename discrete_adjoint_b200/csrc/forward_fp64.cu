@@ -87,20 +87,23 @@ int forward_state_changed(da_ctx *ctx) {
 }
 
 // A context with ghost cells (da_set_owned) must not form dt from its own cells alone: it steps
-// through da_step_bounds / da_step_apply, with the bounds combined over the subdomains.
-static int ghosts_refused(da_ctx *ctx) {
-    return set_error(ctx, DA_ERR_UNSUPPORTED,
-                     "context with ghost cells: step it with da_step_bounds / da_step_apply");
+// through da_step_bounds / da_step_apply, with the bounds combined over the subdomains, or with a
+// replayed dt sequence (da_set_dt_replay: the subdomains' reverse steps).
+static bool ghosts_refused(da_ctx *ctx) {
+    if (ctx->mesh.n_owned == ctx->mesh.n || ctx->tc.dt_replay) return false;
+    set_error(ctx, DA_ERR_UNSUPPORTED,
+              "context with ghost cells: step it with da_step_bounds / da_step_apply or a replayed dt");
+    return true;
 }
 
 int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
-    if (ctx->mesh.n_owned != ctx->mesh.n) return ghosts_refused(ctx);
+    if (ghosts_refused(ctx)) return DA_ERR_UNSUPPORTED;
     if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps, pre_slot, post_slot);
     return launch_forward_steps_fp32(ctx, nsteps, pre_slot, post_slot);
 }
 
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {
-    if (ctx->mesh.n_owned != ctx->mesh.n) return ghosts_refused(ctx);
+    if (ghosts_refused(ctx)) return DA_ERR_UNSUPPORTED;
     if (ctx->p.precision == DA_PREC_FP64) return launch_forward_step_fp64(ctx, record_mask);
     return launch_forward_step_fp32(ctx, record_mask);
 }

@@ -137,10 +137,28 @@ def local_mesh(mesh: Mesh, cells: np.ndarray) -> Mesh:
     g2l[cells] = np.arange(len(cells))
     nb = mesh.nbr[:, cells]
     loc = np.where(nb >= 0, g2l[np.maximum(nb, 0)], -1)
-    for s in range(4):
-        cut = (loc[s] < 0) | (loc[s + 4] < 0)
-        loc[s, cut] = -1
-        loc[s + 4, cut] = -1
+    # a side is kept only when both its slots stay inside and every neighbour on it names the cell
+    # back across its opposite side (a coarser neighbour that lost the cell's sibling is cut too);
+    # cutting one side can break that for the neighbour, so repeat until nothing changes
+    n = len(cells)
+    idx = np.arange(n)
+    while True:
+        changed = False
+        for s in range(4):
+            o = (s + 2) % 4
+            a, b = loc[s], loc[s + 4]
+            cut = (a < 0) | (b < 0)
+            for e in (a, b):
+                ec = np.maximum(e, 0)
+                back = (loc[o][ec] == idx) | (loc[o + 4][ec] == idx)
+                cut |= (e >= 0) & ~back
+            cut &= (a >= 0) | (b >= 0)
+            if cut.any():
+                loc[s, cut] = -1
+                loc[s + 4, cut] = -1
+                changed = True
+        if not changed:
+            break
     arrays = dict(n=len(cells), max_level=mesh.max_level, nbr=loc.astype(np.int32),
                   material=mesh.material[cells], level=mesh.level[cells], ix=mesh.ix[cells], iy=mesh.iy[cells],
                   dh0_dpile=mesh.dh0_dpile[:, cells])
@@ -275,9 +293,10 @@ class LocalDomain:
     the receiving stream waiting on an event of the sending one."""
 
     def __init__(self, mesh: Mesh, nparts: int, mat, tp=None, precision: int = _ffi.DA_PREC_FP64,
-                 devices=(0,), part=None, h=None, **ctx_kw):
+                 devices=(0,), part=None, h=None, rings: int = GHOST_RINGS, **ctx_kw):
         self.mesh = mesh
-        self.subs = decompose(mesh, nparts, part=part, h=h)
+        self.mat = mat
+        self.subs = decompose(mesh, nparts, part=part, h=h, rings=rings)
         self.doms = [ContextSubdomain(s, mat, tp, precision, devices[k % len(devices)], **ctx_kw)
                      for k, s in enumerate(self.subs)]
 
@@ -342,6 +361,64 @@ class LocalDomain:
         """The global state assembled from the owned cells."""
         parts = [d.get_state() for d in self.doms]
         return tuple(gather_owned(self.subs, [p[v] for p in parts], self.mesh.n) for v in range(3))
+
+
+# ------------------------------------------------------------------------------ the adjoint over subdomains
+ADJOINT_RINGS = 4   # a reverse step of an owned cell reads the forward state four rings out
+
+
+def box_functional(m: Mesh, h, box, n_owned: int | None = None):
+    """J = sum of h^2 dx dy over the cells whose centre lies in box (the first n_owned cells), and
+    dJ/dU of every cell ([3][n]; the seed of the reverse sweep)."""
+    inb = (m.x >= box[0]) & (m.x <= box[1]) & (m.y >= box[2]) & (m.y <= box[3])
+    area = m.dx * m.dy
+    lam = np.zeros((3, m.n))
+    lam[0] = np.where(inb, 2.0 * h * area, 0.0)
+    k = m.n if n_owned is None else n_owned
+    return float(np.sum(np.where(inb[:k], h[:k] * h[:k] * area[:k], 0.0))), lam
+
+
+def adjoint_run_local(dd: "LocalDomain", box, nsteps: int, dh0_dpile=None) -> dict:
+    """Forward run and discrete adjoint of J = sum h^2 dx dy over a box at the final step, on the
+    subdomains of a LocalDomain built with ADJOINT_RINGS ghost rings (state set, time 0).  The forward
+    steps are the split step with its exchanges, each subdomain's states kept on the host; each
+    reverse step runs on every subdomain through da_adjoint_step with the step's dt replayed, then
+    the ghosts' lambda is refreshed from their owners.  The owned cells' lambda^0 equals the
+    undivided mesh's (the same reverse steps), the parameter parts are summed over the owned cells.
+    Returns J, lambda0 (the whole mesh's), dJ_dbedfrict, dJ_dintfrict, dJ_dpile, dts."""
+    from .solver import adjoint_step, set_dt_replay
+    states, times = [], [0.0]
+    dts = []
+    for _ in range(nsteps):
+        states.append([d.get_state() for d in dd.doms])
+        dts.append(dd.run(1)[0])
+        times.append(times[-1] + dts[-1])
+    lam, J = [], 0.0
+    for d in dd.doms:
+        u = d.get_state()
+        j, seed = box_functional(d.sub.mesh, u[0], box, d.sub.n_owned)
+        J += j
+        lam.append(seed)
+    nmat = len(dd.mat.bedfrict_deg)
+    gbed, gint = np.zeros(nmat), 0.0
+    glob = None
+    for n in range(nsteps - 1, -1, -1):
+        new = []
+        for j, d in enumerate(dd.doms):
+            d.ctx.set_state(*states[n][j])
+            d.ctx.set_time(times[n], n)
+            set_dt_replay(d.ctx, [dts[n]], n)
+            ln, part = adjoint_step(d.ctx, lam[j])
+            gbed += np.asarray(part.dJ_dbedfrict)
+            gint += part.dJ_dintfrict
+            new.append(ln)
+        glob = gather_owned(dd.subs, new, dd.mesh.n)
+        lam = [glob[:, s.cells] for s in dd.subs]
+    for d in dd.doms:
+        set_dt_replay(d.ctx, None)
+    dpile = [] if dh0_dpile is None else [float(np.dot(glob[0], np.asarray(p))) for p in np.atleast_2d(dh0_dpile)]
+    return {"J": J, "lambda0": glob, "dJ_dbedfrict": gbed, "dJ_dintfrict": gint, "dJ_dpile": dpile,
+            "dts": np.array(dts)}
 
 
 # ------------------------------------------------------------------------------ distributed driver

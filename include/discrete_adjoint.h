@@ -401,8 +401,12 @@ int da_selftest_barrier(da_ctx *ctx, int32_t limit_us);
  *   da_step_apply(ctx_r, b, NULL)       every subdomain: the same dt bits everywhere
  *   da_halo_pack(ctx_r, send cells, n, buf)  ->  transfer  ->  da_halo_unpack(ctx_s, recv cells, n, buf)
  * after which the owned cells hold the undivided mesh's step bit for bit.  Contexts with ghosts
- * refuse the whole-step calls (da_forward_step, da_forward_run, the adjoint: DA_ERR_UNSUPPORTED);
- * their volume and da_compute_stats cover the owned cells only.
+ * refuse the whole-step calls (da_forward_step, da_forward_run, the adjoint: DA_ERR_UNSUPPORTED)
+ * unless a dt sequence is replayed (da_set_dt_replay): then dt does not come from their own cells,
+ * and da_adjoint_step takes the reverse step of a subdomain -- with four ghost rings (a reverse
+ * step of an owned cell reads the forward state four rings out) its owned cells' lambda equals the
+ * undivided mesh's, and its parameter partials sum the owned cells only.  Their volume,
+ * da_compute_stats and the adjoint's parameter sums cover the owned cells only.
  *
  * da_set_owned: cells [n_owned, n_cells) of the uploaded mesh are ghosts (until the next upload).
  * da_get_stream: the context's cudaStream_t, on which every call below is ordered; a collective

@@ -196,3 +196,59 @@ def test_two_gloo_ranks_step_the_split_mesh_as_the_undivided_one():
         assert np.array_equal(hh, h[cells]) and np.array_equal(hhu, hu[cells]) and np.array_equal(hhv, hv[cells])
         seen[cells] = True
     assert seen.all()
+
+
+def oracle_reverse(mesh, mat, states, dts, lam_end, keep=0):
+    """The oracle's reverse sweep (exact transpose: keep=0) over stored states; returns lambda^0."""
+    o = oracle.Oracle(make_params(mat, TimeProps()), mesh)
+    lam = lam_end
+    for n in range(len(dts) - 1, -1, -1):
+        ft = mat.frict_tiny_early if n < mat.frict_tiny_iters else mat.frict_tiny_late
+        lam = o.adjoint_step_ref(*states[n], dts[n], ft, lam, keep=keep)
+    return lam
+
+
+@pytest.mark.parametrize("name,nparts", [("s11", 3), ("s2", 4)])
+def test_decomposed_oracle_adjoint_equals_the_undivided(name, nparts):
+    # the reverse sweep on subdomains with ADJOINT_RINGS ghost rings (each reverse step on every
+    # subdomain from its stored forward states, then the ghosts' lambda from their owners) against
+    # the undivided sweep, across the frict_tiny switch
+    rings = domain.ADJOINT_RINGS
+    w = cases()[name]
+    m = w.mesh
+    nsteps = 56
+    box = (float(np.percentile(m.x, 30)), float(np.percentile(m.x, 70)),
+           float(np.percentile(m.y, 30)), float(np.percentile(m.y, 70)))
+    # undivided
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    u = [m.h0.copy(), m.hu0.copy(), m.hv0.copy()]
+    states, dts = [], []
+    for _ in range(nsteps):
+        states.append(tuple(a.copy() for a in u))
+        rc, dt, _ = o.run(*u, 1)
+        dts.append(float(dt[0]))
+    _, seed = domain.box_functional(m, u[0], box)
+    lam_ref = oracle_reverse(m, w.mat, states, dts, seed)
+    assert np.abs(lam_ref).max() > 0
+    # subdomains: forward with exchanges, states kept per subdomain
+    subs = domain.decompose(m, nparts, h=m.h0, rings=rings)
+    doms = [OracleSubdomain(s, w.mat) for s in subs]
+    local_states = []
+    for _ in range(nsteps):
+        local_states.append([(d.h.copy(), d.hu.copy(), d.hv.copy()) for d in doms])
+        b = np.minimum.reduce([d.bounds().numpy() for d in doms])
+        for d in doms:
+            d.apply(torch.from_numpy(b))
+        bufs = {(d.sub.rank, q): d.pack(q) for d in doms for q in d.sub.send}
+        for d in doms:
+            for q in d.sub.recv:
+                d.unpack(q, bufs[(q, d.sub.rank)])
+    assert doms[0].dts == dts
+    lam = [domain.box_functional(d.sub.mesh, d.h, box, d.sub.n_owned)[1] for d in doms]
+    os_ = [oracle.Oracle(make_params(w.mat, TimeProps()), s.mesh) for s in subs]
+    for n in range(nsteps - 1, -1, -1):
+        ft = w.mat.frict_tiny_early if n < w.mat.frict_tiny_iters else w.mat.frict_tiny_late
+        new = [o_.adjoint_step_ref(*local_states[n][j], dts[n], ft, lam[j], keep=0) for j, o_ in enumerate(os_)]
+        glob = domain.gather_owned(subs, new, m.n)
+        lam = [glob[:, s.cells] for s in subs]
+    assert np.array_equal(glob, lam_ref)

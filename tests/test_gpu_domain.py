@@ -148,3 +148,35 @@ def test_two_processes_over_gloo_step_the_split_mesh():
     for rank, cells, hh, hhu, hhv, t, it in res:
         assert it == nsteps and t == pytest.approx(sum(dts), rel=1e-12)
         assert np.array_equal(hh, h[cells]) and np.array_equal(hhu, hu[cells]) and np.array_equal(hhv, hv[cells])
+
+
+def test_subdomain_adjoint_equals_the_undivided():
+    # the reverse sweep over subdomain contexts with four ghost rings (da_adjoint_step with the
+    # step's dt replayed, the ghosts' lambda refreshed from their owners) against the same
+    # reverse steps on the undivided mesh (one part): lambda^0 bit for bit, J and the parameter
+    # gradients to rounding (sums over the parts); and against the fused checkpointed sweep
+    from discrete_adjoint_b200 import adjoint_run
+    w = small()
+    m = w.mesh
+    nsteps = 56   # across the frict_tiny switch
+    box = (float(np.percentile(m.x, 30)), float(np.percentile(m.x, 70)),
+           float(np.percentile(m.y, 30)), float(np.percentile(m.y, 70)))
+    res = []
+    for nparts in (1, 3):
+        with domain.LocalDomain(m, nparts, w.mat, h=m.h0, rings=domain.ADJOINT_RINGS) as dd:
+            dd.set_state(m.h0, m.hu0, m.hv0)
+            res.append(domain.adjoint_run_local(dd, box, nsteps, m.dh0_dpile))
+    a, b = res
+    assert np.array_equal(a["dts"], b["dts"])
+    assert np.array_equal(a["lambda0"], b["lambda0"]) and np.abs(a["lambda0"]).max() > 0
+    rel = lambda x, y: abs(x - y) / max(abs(y), 1e-300)  # noqa: E731
+    assert rel(b["J"], a["J"]) < 1e-12 and rel(b["dJ_dintfrict"], a["dJ_dintfrict"]) < 1e-10
+    assert all(rel(x, y) < 1e-10 for x, y in zip(b["dJ_dbedfrict"], a["dJ_dbedfrict"]))
+    assert all(rel(x, y) < 1e-12 for x, y in zip(b["dJ_dpile"], a["dJ_dpile"]))
+    with GeoflowContext(w.mat, TimeProps()) as c:
+        c.upload_mesh(m)
+        c.set_state(m.h0, m.hu0, m.hv0)
+        g = adjoint_run(c, box, nsteps, 8, m.dh0_dpile, want_lambda0=True)
+    scale = np.abs(g.lambda0).max()
+    assert np.abs(g.lambda0 - b["lambda0"]).max() <= 1e-12 * scale
+    assert rel(b["J"], g.J) < 1e-12 and rel(b["dJ_dintfrict"], g.dJ_dintfrict) < 1e-9
