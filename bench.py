@@ -182,19 +182,20 @@ def wet_counts(m, h) -> tuple[int, int]:
 
 def bytes_per_cell_update(precision: str) -> dict:
     """Algorithmic HBM bytes of one cell through one step (each array the cell needs touched once;
-    neighbour re-reads are halo traffic, intermediates such as k act/pass are not counted), the rule
-    of the per-unit figures for this path with the arrays of the committed layout
-    (csrc/da_internal.h), r = 8 (FP64) / 4 (FP32-split) bytes per real:
+    neighbour re-reads are halo traffic), the rule of the per-unit figures for this path with the
+    arrays of the committed layout (csrc/da_internal.h), r = 8 (FP64) / 4 (FP32-split) bytes per real:
       forward:  state in 3r + state out 3r + g (3), d_gravity (2), curvature (2) 7r + material and
                 boundary flags 2 + neighbour table 4 x int32 16 + cell sizes 2r (+ centres 2 x 8 in
-                FP64, whose slopes take centre differences as the reference does)
+                FP64, whose slopes take centre differences as the reference does) + the six limited
+                slopes the coefficient phase writes and the update phase reads back 12r
       adjoint:  lambda in 3r + U 3r + the same statics, flags, neighbours, sizes (and centres) +
                 branch byte 1 + lambda out 3r
-    FP64: forward 154 B, adjoint 179 B; FP32-split: 78 B and 91 B."""
+    FP64: forward 250 B, adjoint 179 B; FP32-split: 126 B and 91 B.  (Without the kept slopes, the
+    one-pass figures of the path: FP64 154 B, FP32-split 78 B per forward cell-update.)"""
     r = 8 if precision == "fp64" else 4
     xy = 16 if precision == "fp64" else 0
     statics = 7 * r + 2 + 16 + 2 * r + xy
-    return {"forward": 6 * r + statics, "adjoint": 9 * r + statics + 1}
+    return {"forward": 6 * r + statics + 12 * r, "adjoint": 9 * r + statics + 1}
 
 
 def algorithmic_bytes(precision: str, n_act: float) -> dict:
@@ -208,20 +209,20 @@ def algorithmic_bytes(precision: str, n_act: float) -> dict:
             "snapshot_copy": 2 * 3 * r * n_act}
 
 
-# DRAM bytes (read + write) from the committed ncu captures (profiles/traffic_headline_1M.md,
-# profiles/k_steps_dense_hill_3.75M_staged.md).  Sparse headline kernels: bytes per active cell of a
+# DRAM bytes (read + write) from the committed ncu captures (the headline traffic and the dense
+# k_steps summaries under profiles/).  Sparse headline kernels: bytes per active cell of a
 # launch captured in the steady flow (k_youturn: reverse steps of iterations 256 and 255 of the
 # 512-step sweep, 4372 and 4344 active cells; k_steps: one launch of 32 steps after 256, 4553
 # active cells per step on average), scaled by the active cells of the traced run; the dense case:
 # bytes per time step of a 10-step launch with every cell wet.
 TRAFFIC_PER_ACTIVE_CELL = {
-    ("fp64", "k_youturn"): 0.5 * (1983232 / 4372 + 1975296 / 4344),
-    ("fp32", "k_youturn"): 0.5 * (1357056 / 4372 + 1353472 / 4344),
-    ("fp64", "k_steps"): (1485568 + 17920) / (32 * 4552.6),
+    ("fp64", "k_youturn"): 0.5 * (2206976 / 4372 + 2181632 / 4344),
+    ("fp32", "k_youturn"): 0.5 * (1372672 / 4372 + 1368832 / 4344),
+    ("fp64", "k_steps"): (1519616 + 26880) / (32 * 4552.6),
 }
 TRAFFIC_DENSE_PER_STEP = {
-    "fp32": (4.346160e9 + 0.615296e9) / 10,
-    "fp64": (8.427677e9 + 1.226889e9) / 10,
+    "fp32": (4.958934e9 + 1.516130e9) / 10,
+    "fp64": (9.646188e9 + 3.033419e9) / 10,
 }
 
 
@@ -366,7 +367,10 @@ def fwdadj(args, ws, local):
 DENSE_LAYER = 1.0  # m of material added on every cell for the dense forward case
 
 
-FWD_STEPS = 1000      # the workload as specified: 1000 steps
+# the path's one-pass forward bytes per cell-update without the kept slopes (state in and out,
+# static coefficients, material and level bytes, neighbour table)
+ONE_PASS_BYTES = {"fp64": 124, "fp32": 72}
+FWD_STEPS = 1000      # the forward-at-scale workload as specified: 1000 steps
 DENSE_STEPS = 300     # the dense case that carries the step kernel's roofline
 
 
@@ -408,10 +412,12 @@ def forward_config2(args, ws, local):
             pn = "fp64" if prec == _ffi.DA_PREC_FP64 else "fp32"
             bytes_step = algorithmic_bytes(pn, av)["k_steps"]
             gbs = bytes_step / (ms * 1e-3 / steps) / 1e9
+            one_pass = ONE_PASS_BYTES[pn] * av / (ms * 1e-3 / steps) / 1e9
             r["roofline"] = {"kernel": "k_steps", "alg_bytes_per_step": bytes_step,
                              "bytes_per_cell_update": bytes_per_cell_update(pn)["forward"], "achieved": gbs,
                              "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_kind": peak_kind,
-                             "traffic": TRAFFIC_DENSE_PER_STEP[pn]}
+                             "traffic": TRAFFIC_DENSE_PER_STEP[pn],
+                             "frac_one_pass": one_pass / hbm, "one_pass_bytes_per_cell": ONE_PASS_BYTES[pn]}
         res[name] = r
         c.close()
     rl2 = lambda x, y: float(np.linalg.norm(x - y) / max(np.linalg.norm(y), 1e-300))  # noqa: E731

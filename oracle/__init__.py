@@ -439,7 +439,8 @@ def adapter_available() -> bool:
 
 
 def run_adapter_check(mesh, mat, h, hu, hv, nsteps: int = 0, step: bool = False) -> dict:
-    """INTEGRATION.md's adapter, compiled against the reference (oracle/_ref/adapter_check): flattens
+    """The drop-in adapter (element-table flattening and step() replacement), compiled against the
+    reference (oracle/_ref/adapter_check): flattens
     the reference's tables rebuilt from mesh and compares the flattening with mesh; with step=True it
     also takes nsteps steps through the adapter (the device path) and through the reference's step()
     and compares the results.  Returns the mismatch counts."""

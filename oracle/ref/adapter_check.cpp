@@ -1,5 +1,6 @@
-// The adapter of INTEGRATION.md (sections 1 and 2) compiled against the reference's own headers and
-// linked with its objects and with libda_b200.so, then checked against the reference.
+// The drop-in adapter (the element-table flattening and the step() replacement) compiled against the
+// reference's own headers and linked with its objects and with libda_b200.so, then checked against
+// the reference.
 // TEST INFRASTRUCTURE ONLY: built by oracle/ref_build.py into oracle/_ref/adapter_check.
 //
 // The adapter is what a maintainer adds to the reference: da_flatten walks the reference's element

@@ -105,7 +105,8 @@ def build(verbose: bool = False, force: bool = False) -> str | None:
 
 
 def build_adapter(own, objs, verbose=False, force=False):
-    """oracle/_ref/adapter_check: INTEGRATION.md's adapter compiled against the reference's headers,
+    """oracle/_ref/adapter_check: the drop-in adapter (the element-table flattening and the step()
+    replacement a maintainer adds to the reference) compiled against the reference's headers,
     linked with the reference's objects and the product library (when it has been built)."""
     root = os.path.dirname(HERE)
     lib_dir = os.path.join(root, "discrete_adjoint_b200")

@@ -1,4 +1,4 @@
-"""INTEGRATION.md's adapter compiled against the reference (oracle/ref/adapter_check.cpp, linked with
+"""The drop-in adapter (element-table flattening, step() replacement) compiled against the reference (oracle/ref/adapter_check.cpp, linked with
 the reference's objects and libda_b200.so): it flattens the reference's own element tables
 (positive_x_side, neighbour keys, neigh_proc; src/datstr/element2.C:694-716) into exactly the
 integer neighbour table and fields of this repository's flattening, and, on a GPU, replaces step()
