@@ -329,19 +329,21 @@ def fwdadj(args, ws, local):
         adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile)
         res["trace"] = c.trace(with_steps=True)
         c.set_tracing(False)
-        # e2e through the C ABI with pinned host buffers: H2D of the initial state, the run, D2H of
-        # the gradients and lambda^0
+        # e2e through the C ABI with pinned host buffers: H2D of the initial state and the pile
+        # derivative, the run, D2H of the gradients and lambda^0
         h0, hu0, hv0, lam_host = pinned(m.n), pinned(m.n), pinned(m.n), pinned(3 * m.n)
         h0[:], hu0[:], hv0[:] = m.h0, m.hu0, m.hv0
+        dpile = pinned(m.dh0_dpile.size).reshape(m.dh0_dpile.shape)
+        dpile[:] = m.dh0_dpile
         barrier(ws, local)
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             c.set_state(h0, hu0, hv0)
             c.set_time(0.0, 0)
-            ge = adjoint_run(c, box, HORIZON, SNAPSHOTS, m.dh0_dpile, lambda0_out=lam_host)
+            ge = adjoint_run(c, box, HORIZON, SNAPSHOTS, dpile, lambda0_out=lam_host)
         e2e_s = allmax(time.perf_counter() - t0, ws, local)
         res["e2e"] = {"value": m.n * HORIZON * args.e2e_steps * ws / e2e_s, "unit": "cell-updates/s",
-                      "h2d_bytes_per_step": 3 * 8 * m.n, "d2h_bytes_per_step": 3 * 8 * m.n + 8 * 32,
+                      "h2d_bytes_per_step": 3 * 8 * m.n + 8 * dpile.size, "d2h_bytes_per_step": 3 * 8 * m.n + 8 * 32,
                       "J_matches_device_run": bool(ge.J == gl.J)}
         # forward state after the horizon, for the depth / momentum errors
         c.set_state(h0, hu0, hv0)

@@ -445,6 +445,10 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
         r.seeded = true;
     }
     if (st) return st;
+    // The sweep ends with a restore of the base checkpoint, which writes both ping-pong buffers:
+    // afterwards the live buffer is the caller's again, so the next sweep starts from the same one
+    // and replays the same captured graph.
+    const int cur_in = ctx->cur;
     r.sch.use(ctx, nsteps, nsnapshots);
     for (int s = nsnapshots; s >= 1; --s) r.free_slots.push_back(s);
     // the launches of the sweep, from the base checkpoint to the gradient sums
@@ -481,7 +485,6 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
             if (g) cudaGraphDestroy(g);
             if (!s) {
                 ctx->sweep_key = key;
-                ctx->sweep_cur = ctx->cur;
                 ctx->sweep_lam = r.lam_cur;
                 ctx->sweep_fsteps = r.fsteps;
             } else {
@@ -503,12 +506,12 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
     if (graph) {
         // the gradient sums are in the timed region
         st = cuda_check(ctx, cudaGraphLaunch(ctx->sweep_graph, ctx->stream), "sweep graph launch");
-        ctx->cur = ctx->sweep_cur;
         r.lam_cur = ctx->sweep_lam;
         r.fsteps = ctx->sweep_fsteps;
     } else {
         st = sweep();
     }
+    ctx->cur = cur_in;
     cudaEventRecord(e1, ctx->stream);
     if (!st) st = sync_check(ctx);
     float ms = 0.f;

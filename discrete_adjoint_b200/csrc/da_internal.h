@@ -230,7 +230,7 @@ struct da_ctx {
     // kernels were given (sweep_key) and the host-side results of building it
     cudaGraphExec_t sweep_graph = nullptr;
     std::vector<unsigned char> sweep_key;
-    int sweep_cur = 0, sweep_lam = 0;
+    int sweep_lam = 0;
     long long sweep_fsteps = 0;
     double *dt_replay = nullptr;     // device copy of a frozen time-step sequence
     void *refadj_mem = nullptr;      // workspace of the reference-mode adjoint (adjoint_ref.cu)

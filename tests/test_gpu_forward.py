@@ -112,20 +112,25 @@ def test_tile_culling_is_bit_identical(precision):
 def test_tile_staging_is_bit_identical(precision, layer):
     # the staged phases (tile and halo in shared memory, activity recomputed from the staged
     # depths) against the phases that read neighbours from global memory: the adaptive mesh with
-    # hanging nodes, with its piles alone (culled, sparse) and with a layer on every cell (dense)
+    # hanging nodes, with its piles alone (culled, sparse) and with a layer on every cell (dense);
+    # every staging setting at two launch shapes, with single steps (the two-launch path) between
+    # multi-step launches
     w = inputs.workload1()
     out = []
-    for staging in (False, True):
+    for staging, occ in ((0, 0), (1, 3), (2, 2), (3, 2), (3, 3)):
         with GeoflowContext(w.mat, TimeProps(), precision=precision, tile_staging=staging,
-                            blocks_per_sm=3 if staging else 0) as ctx:
+                            blocks_per_sm=occ) as ctx:
             ctx.upload_mesh(w.mesh)
             ctx.set_state(w.mesh.h0 + layer, w.mesh.hu0, w.mesh.hv0)
-            s = ctx.run(90)
-            out.append((ctx.get_state(), s))
-    (a, sa), (b, sb) = out
-    for u, v in zip(a, b):
-        assert np.array_equal(u, v)
-    assert sa.time == sb.time and sa.volume == sb.volume and sa.dt == sb.dt
+            s = ctx.run(45)
+            st = [ctx.step() for _ in range(3)]    # single steps between two multi-step launches
+            s = ctx.run(42)
+            out.append((ctx.get_state(), s, [x.dt for x in st]))
+    a, sa, da = out[0]
+    for b, sb, db in out[1:]:
+        for u, v in zip(a, b):
+            assert np.array_equal(u, v)
+        assert sa.time == sb.time and sa.volume == sb.volume and sa.dt == sb.dt and da == db
 
 
 @pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
