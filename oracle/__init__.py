@@ -341,12 +341,15 @@ def run_reference_adjoint(mesh, mat, states, iters, dts, lam_end, workdir: str |
     return {"lam": arr[:K * 3 * n].reshape(K, 3, n).copy(), "seconds": float(arr[K * 3 * n])}
 
 
-def run_reference_fwdadj(mesh, mat, nsteps: int, warm: int, box, workdir: str | None = None) -> dict:
+def run_reference_fwdadj(mesh, mat, nsteps: int, warm: int, box, workdir: str | None = None,
+                         replicas: int = 1) -> dict:
     """The reference's own forward + adjoint, timed step by step (oracle/_ref/ref_harness, mode 'DAF1'):
     nsteps forward steps from the mesh's initial state with the driver's solution recording, then
     the dual solver's reverse steps back to step `warm` from lambda = dJ/dU of J = sum over the
     cells whose centre lies in box of h^2 dx dy.  Returns {"fwd_seconds": [nsteps],
-    "rev_seconds": [nsteps - warm], "lam": [3][n] the adjoint of U^warm}."""
+    "rev_seconds": [nsteps - warm], "lam": [3][n] the adjoint of U^warm}.  replicas > 1: that many
+    harness processes run the same input at the same time (one per host core), and
+    "replica_seconds" lists each one's timed forward + reverse seconds."""
     import struct
     import subprocess
     import tempfile
@@ -369,16 +372,24 @@ def run_reference_fwdadj(mesh, mat, nsteps: int, warm: int, box, workdir: str | 
                       mesh.h0, mesh.hu0, mesh.hv0):
                 f.write(np.ascontiguousarray(a, dtype="<f8").tobytes())
             f.write(np.asarray(box, dtype="<f8").tobytes())
-        r = subprocess.run([REF_EXE, fin, fout], capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
-        raw = open(fout, "rb").read()
-    magic, n2, k2, w2 = struct.unpack_from("<4i", raw, 0)
-    assert magic == 0x314F4644 and n2 == n and k2 == nsteps and w2 == warm
-    arr = np.frombuffer(raw, dtype="<f8", offset=16)
+        outs = [fout] + [os.path.join(td, f"out{k}.bin") for k in range(1, max(1, replicas))]
+        procs = [subprocess.Popen([REF_EXE, fin, fo], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True)
+                 for fo in outs]
+        errs = [p.communicate()[1] for p in procs]
+        for p, e in zip(procs, errs):
+            if p.returncode != 0:
+                raise RuntimeError(f"ref_harness failed ({p.returncode}): {e[-2000:]}")
+        raws = [open(fo, "rb").read() for fo in outs]
     nr = nsteps - warm
+    arrs = []
+    for raw in raws:
+        magic, n2, k2, w2 = struct.unpack_from("<4i", raw, 0)
+        assert magic == 0x314F4644 and n2 == n and k2 == nsteps and w2 == warm
+        arrs.append(np.frombuffer(raw, dtype="<f8", offset=16))
+    arr = arrs[0]
     return {"fwd_seconds": arr[:nsteps].copy(), "rev_seconds": arr[nsteps:nsteps + nr].copy(),
-            "lam": arr[nsteps + nr:nsteps + nr + 3 * n].reshape(3, n).copy()}
+            "lam": arr[nsteps + nr:nsteps + nr + 3 * n].reshape(3, n).copy(),
+            "replica_seconds": [float(np.sum(a[warm:nsteps]) + np.sum(a[nsteps:nsteps + nr])) for a in arrs]}
 
 
 def params_for(mat) -> "_ffi.da_params":

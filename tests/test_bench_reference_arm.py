@@ -39,3 +39,27 @@ def test_reference_arm_runs_the_reference_without_the_product_library():
     res = json.loads(out.stdout.strip().splitlines()[-1])
     assert res["kind"] == "reference" and res["value"] > 0
     assert not res["loaded"]
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference harness not built")
+def test_reference_arm_runs_one_harness_per_core():
+    # side-by-side harness processes on the same input: each one's lambda is the single run's,
+    # the rate is their total work over the slowest one's timed seconds, and the replica count
+    # follows the usable cores and the memory they would take
+    import numpy as np
+
+    import bench
+    from discrete_adjoint_b200.inputs import WORKLOAD3_BOX
+    from discrete_adjoint_b200.mesh import Mesh
+    from oracle import meshgen
+    m = Mesh(**meshgen.headline_mesh(64))
+    mat = MatProps(intfrict_deg=30.0, bedfrict_deg=[20.0])
+    one = oracle.run_reference_fwdadj(m, mat, 3, 1, WORKLOAD3_BOX)
+    two = oracle.run_reference_fwdadj(m, mat, 3, 1, WORKLOAD3_BOX, replicas=2)
+    assert len(one["replica_seconds"]) == 1 and len(two["replica_seconds"]) == 2
+    assert np.array_equal(one["lam"], two["lam"])
+    r = bench.reference_fwdadj(1, 1, side=64, replicas=2)
+    assert r["cores"] == 2 and r["value"] > 0 and "2 harness processes" in r["sample"]
+    cores = len(os.sched_getaffinity(0))
+    assert 1 <= bench.reference_replicas(64 * 64) <= cores
+    assert bench.reference_replicas(10 ** 12) == 1
