@@ -130,12 +130,13 @@ __global__ void __launch_bounds__(kBlock, OCC) k_youturn(MeshArgs m, fwd::StateP
     double dt = 0.0, ft, min_dxe = 0.0, hmax = 0.0;
     if (BATCH) {
         ft = iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
-        fwd::inst_dt_pass(ia, iter, tc);
+        fwd::inst_dt_pass(ia, iter, tc, sc);
         if (!fwd::grid_sync(sc)) return;
     } else {
         min_dxe = __longlong_as_double(__ldcg(&sc->acc_min_dxe));
         hmax = __longlong_as_double(__ldcg(&sc->acc_hmax));
         fwd::step_dt(min_dxe, hmax, time, iter, tc, dt, ft);
+        if (blockIdx.x == 0 && threadIdx.x == 0 && !isfinite(dt)) raise_err(sc, DA_ERR_NAN);
     }
     const R ftr = R(ft) > R(mc.sign_floor) ? R(ft) : R(mc.sign_floor);
     if (STAGED && !SEED) {

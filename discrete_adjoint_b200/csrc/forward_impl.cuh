@@ -39,7 +39,9 @@ __device__ __forceinline__ unsigned long long seg_flags(const uint8_t *flags, in
 
 // dt from the reduced CFL bound and hmax (get_coef_and_eigen.C:168-179 with the single-rank
 // MPI_Allreduce(MIN)), then TimeProps::incrtime.  frict_tiny follows hpfem.C:232-235 with the
-// iteration count before the increment.
+// iteration count before the increment.  Its callers report a dt that is not finite as
+// DA_ERR_NAN: with no wet cell, no flux source and no output or end time it is infinite, and the
+// reference's next update is NaN in every cell, which stops its run (residual.C:272-273).
 __device__ __forceinline__ void step_dt(double min_dxe, double hmax, double time, long long iter,
                                         const TimeConsts &tc, double &dt_out, double &ft_out) {
     const double g0 = 0.5 * min_dxe;
@@ -66,6 +68,7 @@ __device__ void finalize_dt(DevScalars *sc, const TimeConsts &tc) {
     const double time = sc->time;
     double dt, ft;
     step_dt(min_dxe, hmax, time, sc->iter, tc, dt, ft);
+    if (!isfinite(dt)) raise_err(sc, DA_ERR_NAN);
     sc->frict_tiny = ft;
     sc->dt = dt;
     sc->time = time + dt;
@@ -540,13 +543,14 @@ struct StatePair {
 
 // Ensemble: the dt of every member from its reduced CFL values (threads over members), its time
 // advanced, its accumulators restarted.  Runs between two grid barriers.
-__device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter, const TimeConsts &tc) {
+__device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter, const TimeConsts &tc, DevScalars *sc) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ia.ninst; k += gridDim.x * blockDim.x) {
         const double mn = __longlong_as_double(__ldcg(ia.acc_min + k));
         const double hx = __longlong_as_double(__ldcg(ia.acc_max + k));
         const double time = ia.time[k];
         double dt, ft;
         step_dt(mn, hx, time, iter, tc, dt, ft);
+        if (!isfinite(dt)) raise_err(sc, DA_ERR_NAN);
         ia.dt[k] = dt;
         ia.time[k] = time + dt;
         ia.min_dxe[k] = mn;
@@ -596,7 +600,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
         if (!grid_sync(sc)) return;
         if (BATCH) {
             ft = iter < tc.frict_tiny_iters ? tc.frict_tiny_early : tc.frict_tiny_late;
-            inst_dt_pass(ia, iter, tc);
+            inst_dt_pass(ia, iter, tc, sc);
             iter += 1;
             if (!grid_sync(sc)) return;
         } else {
@@ -606,6 +610,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
             time += dt;
             iter += 1;
             if (blockIdx.x == 0 && threadIdx.x == 0) {
+                if (!isfinite(dt)) raise_err(sc, DA_ERR_NAN);
                 // read by every block before this step's first barrier; used again next step
                 *(p ? &sc->acc_min_dxe : &sc->acc_alt_min_dxe) = kMinDxeStart;
                 *(p ? &sc->acc_hmax : &sc->acc_alt_hmax) = 0ull;
