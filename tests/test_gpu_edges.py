@@ -98,3 +98,45 @@ def test_empty_mesh_and_missing_arguments_are_refused():
         # the context is still usable after the refusals
         s0 = c.run(3)
         assert s0.iter == 3
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+@pytest.mark.parametrize("shape", [SHAPES[1], SHAPES[2], SHAPES[5], SHAPES[6]], ids=lambda s: "x".join(map(str, s[:3])))
+def test_small_and_ragged_meshes_adjoint(shape):
+    # the reference's adjoint (jacobian_mode = reference) as a checkpointed sweep against the
+    # oracle's chained dual-solver steps, 1e-12; the exact transpose, one reverse step at a time,
+    # against the oracle's dual-solver step without the reference's approximations, 1e-9 (the
+    # tolerances of the fixture-mesh tests in test_gpu_adjoint_ref.py)
+    from discrete_adjoint_b200 import adjoint_run, adjoint_step
+    from test_oracle_adjoint import forward_states, frict_tiny
+    nx, ny, lev, rf = shape
+    w = inputs.test_case(seed=5, nx0=nx, ny0=ny, max_level=lev, random_frac=rf)
+    m = w.mesh
+    N = 30
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    states, dts = forward_states(o, m, N)
+    box = (float(m.x.min()) - 1.0, float(m.x.max()) + 1.0, float(m.y.min()) - 1.0, float(m.y.max()) + 1.0)
+    lam = np.zeros((3, m.n))
+    lam[0] = 2.0 * states[N][0] * (m.dx * m.dy)
+    for it in range(N, 0, -1):
+        lam = o.adjoint_step_ref(*states[it - 1], dts[it - 1], frict_tiny(it), lam)
+    dh0 = (m.h0 > 0).astype(np.float64).reshape(1, m.n)
+    with GeoflowContext(w.mat, TimeProps(), jacobian_mode=_ffi.DA_JAC_REFERENCE) as c:
+        c.upload_mesh(m)
+        c.set_state(m.h0, m.hu0, m.hv0)
+        g = adjoint_run(c, box, N, 4, dh0_dpile=dh0, want_lambda0=True)
+    assert rel(g.lambda0, lam) <= 1e-12
+    rng = np.random.default_rng(7)
+    with GeoflowContext(w.mat, TimeProps()) as c:
+        c.upload_mesh(m)
+        for it in (N, 17, 1):
+            lam_next = rng.standard_normal((3, m.n))
+            c.set_state(*states[it - 1])
+            c.set_time(float(np.sum(dts[:it - 1])), it - 1)
+            lam_dev, _ = adjoint_step(c, lam_next)
+            ex = o.adjoint_step_ref(*states[it - 1], dts[it - 1], frict_tiny(it), lam_next, keep=0)
+            assert rel(lam_dev, ex) <= 1e-9, it
