@@ -169,7 +169,10 @@ int da_set_state(da_ctx *ctx, const double *h, const double *hu, const double *h
 int da_get_state(da_ctx *ctx, double *h, double *hu, double *hv);
 
 /* ---- forward stepping -------------------------------------------------------------- */
-/* One step() (order_flag = 1). */
+/* One step() (order_flag = 1).  DA_ERR_NAN also reports a step whose dt is not finite: with no
+ * wet cell, no flux source (da_params.influx_dt infinite) and no output or end time, the CFL rule
+ * gives an infinite dt, and the reference's update is then NaN in every cell (its state check at
+ * residual.C:272-273 stops the run). */
 int da_forward_step(da_ctx *ctx, da_step_stats *out);
 /* nsteps step() calls back to back, device-resident, captured in a CUDA graph. */
 int da_forward_run(da_ctx *ctx, int32_t nsteps, da_step_stats *last);
