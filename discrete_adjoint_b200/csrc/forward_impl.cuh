@@ -19,6 +19,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "fv_device.cuh"
 #include "snapshot_impl.cuh"
 

@@ -62,8 +62,11 @@ inline HaloArgs halo_args(const da_ctx *ctx) {
     return HaloArgs{ctx->mesh.halo_off, ctx->mesh.halo_idx, ctx->mesh.nloc, ctx->slopes};
 }
 
-// The staged phases run when the parameters ask for them and the mesh's halo tables exist.
-inline bool staged_ok(const da_ctx *ctx) { return ctx->p.tile_staging >= 1 && ctx->mesh.nloc != nullptr; }
+// The staged phases run when the parameters ask for them, the mesh's halo tables exist and the
+// slopes are kept (the staged update of the forward step reads them instead of staging the centres).
+inline bool staged_ok(const da_ctx *ctx) {
+    return ctx->p.tile_staging >= 1 && ctx->mesh.nloc != nullptr && ctx->slopes != nullptr;
+}
 
 // cp.async of BYTES (4 or 8) from global to shared memory; completes at the group's wait.
 template <int BYTES>
@@ -100,8 +103,10 @@ __device__ __forceinline__ void load_slots(const int16_t *nloc, int i, int nl[8]
 }
 
 // Copies of one slot's values.  UPD: also k act/pass and g_z (the update phase reads them at
-// neighbours; the coefficient phase reads g_z at the cell itself only).
-template <class R, bool UPD>
+// neighbours; the coefficient phase reads g_z at the cell itself only).  XY (FP64): the centres,
+// which only the limited slopes read (the coefficient phase, and the reverse step's source
+// adjoint inside its update phase).
+template <class R, bool UPD, bool XY = true>
 __device__ __forceinline__ void stage_slot(StageBuf<R> &b, int s, int e, bool own, const MeshArgs &m,
                                            const StateRef<R> &U, const R *kact) {
     constexpr int B = sizeof(R);
@@ -111,8 +116,10 @@ __device__ __forceinline__ void stage_slot(StageBuf<R> &b, int s, int e, bool ow
     if (UPD) cp_async<B>(&b.k[s], kact + e);
     if constexpr (sizeof(R) == 8) {
         if (UPD || own) cp_async<B>(&b.gz[s], m.g + (size_t)2 * m.n + e);
-        cp_async<B>(&b.c0[s], m.x + e);
-        cp_async<B>(&b.c1[s], m.y + e);
+        if (XY) {
+            cp_async<B>(&b.c0[s], m.x + e);
+            cp_async<B>(&b.c1[s], m.y + e);
+        }
     } else {
         if (UPD || own) cp_async<B>(&b.gz[s], m.fg + (size_t)2 * m.n + e);
         cp_async<B>(&b.c0[s], m.fdx + e);
@@ -178,13 +185,14 @@ __device__ __forceinline__ void staged_slots(const StageBuf<R> &b, int c, int nl
 }
 
 // Tile t's own cells and its halo (halo list already in shared memory) into buffer b.
-template <class R, bool UPD>
+template <class R, bool UPD, bool XY = true>
 __device__ __forceinline__ void stage_tile(StageBuf<R> &b, int t, const int *hidx, int hcnt, const MeshArgs &m,
                                            const StateRef<R> &U, const R *kact, const int16_t *nloc) {
     const int i = t * kTileCells + (int)threadIdx.x;
-    if (i < m.n) stage_slot<R, UPD>(b, threadIdx.x, i, true, m, U, kact);
+    if (i < m.n) stage_slot<R, UPD, XY>(b, threadIdx.x, i, true, m, U, kact);
     stage_own<R, UPD>(b, t, m, nloc);
-    for (int k = threadIdx.x; k < hcnt; k += kTileCells) stage_slot<R, UPD>(b, kTileCells + k, hidx[k], false, m, U, kact);
+    for (int k = threadIdx.x; k < hcnt; k += kTileCells)
+        stage_slot<R, UPD, XY>(b, kTileCells + k, hidx[k], false, m, U, kact);
 }
 
 __device__ __forceinline__ void stage_halo_list(int *dst, const int32_t *src, int cnt) {
@@ -206,19 +214,19 @@ __device__ __forceinline__ void halo_range(const HaloArgs &ha, int tq, int ntile
 // memory.  Needs blockDim.x == kTileCells; every thread of the block calls it with the same cnt;
 // S.hoff / S.hcnt hold the listed tiles' halo ranges (compact_tiles).  The first tile's halo
 // cells are read by the threads that copy them; later tiles' lists arrive two tiles ahead.
-template <class R, bool UPD, class F>
+template <class R, bool UPD, bool XY = true, class F>
 __device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &ha, const StateRef<R> &U,
                                              const R *kact, int cnt, const int *list, StageSmem<R> &S, F &&fn) {
     {
         const int t0 = list[0], hc = S.hcnt[0];
         const int32_t *src = ha.idx + S.hoff[0];
         const int i = t0 * kTileCells + (int)threadIdx.x;
-        if (i < m.n) stage_slot<R, UPD>(S.buf[0], threadIdx.x, i, true, m, U, kact);
+        if (i < m.n) stage_slot<R, UPD, XY>(S.buf[0], threadIdx.x, i, true, m, U, kact);
         stage_own<R, UPD>(S.buf[0], t0, m, ha.nloc);
         for (int k = threadIdx.x; k < hc; k += kTileCells) {
             const int e = src[k];
             S.hidx[0][k] = e;
-            stage_slot<R, UPD>(S.buf[0], kTileCells + k, e, false, m, U, kact);
+            stage_slot<R, UPD, XY>(S.buf[0], kTileCells + k, e, false, m, U, kact);
         }
     }
     if (cnt > 1) stage_halo_list(S.hidx[1], ha.idx + S.hoff[1], S.hcnt[1]);
@@ -228,8 +236,8 @@ __device__ __forceinline__ void staged_tiles(const MeshArgs &m, const HaloArgs &
         cp_async_wait_all();
         __syncthreads();
         if (q + 1 < cnt) {
-            stage_tile<R, UPD>(S.buf[(q + 1) & 1], list[q + 1], S.hidx[(q + 1) % 3], S.hcnt[q + 1], m, U, kact,
-                               ha.nloc);
+            stage_tile<R, UPD, XY>(S.buf[(q + 1) & 1], list[q + 1], S.hidx[(q + 1) % 3], S.hcnt[q + 1], m, U,
+                                   kact, ha.nloc);
             if (q + 2 < cnt) stage_halo_list(S.hidx[(q + 2) % 3], ha.idx + S.hoff[q + 2], S.hcnt[q + 2]);
         }
         cp_async_commit();
@@ -366,7 +374,10 @@ __device__ __forceinline__ void update_phase_staged(const MeshArgs &m, const Hal
         const int cnt = compact_tiles(need, tq, list, ho, hc, S.hoff, S.hcnt);
         if (cnt == 0) continue;
         if (RECORD && threadIdx.x == 0) atomicAdd(&sc->listed, (unsigned)cnt);
-        staged_tiles<R, true>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *) {
+        // the centres only for an epilogue (the source adjoint's slope derivatives read them); the
+        // update itself takes the kept slopes
+        constexpr bool XY = !std::is_same<Epi, NoEpilogue>::value;
+        staged_tiles<R, true, XY>(m, ha, U, kact, cnt, list, S, [&](int t, const StageBuf<R> &b, const int *) {
             const int inst = BATCH ? ia.tile_inst[t] : 0;
             const MatConsts &mc = BATCH ? ia.mcs[inst] : mc0;
             const R dt = BATCH ? R(ia.dt[inst]) : dt0;
