@@ -218,11 +218,11 @@ def algorithmic_bytes(precision: str, n_act: float) -> dict:
 TRAFFIC_PER_ACTIVE_CELL = {
     ("fp64", "k_youturn"): 0.5 * (2206976 / 4372 + 2181632 / 4344),
     ("fp32", "k_youturn"): 0.5 * (1372672 / 4372 + 1368832 / 4344),
-    ("fp64", "k_steps"): (1519616 + 26880) / (32 * 4552.6),
+    ("fp64", "k_steps"): (1511680 + 15104) / (32 * 4552.6),
 }
 TRAFFIC_DENSE_PER_STEP = {
     "fp32": (4.958934e9 + 1.516130e9) / 10,
-    "fp64": (9.646188e9 + 3.033419e9) / 10,
+    "fp64": (9.034467e9 + 3.031311e9) / 10,
 }
 
 
