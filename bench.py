@@ -236,6 +236,9 @@ def traffic_per_launch(precision: str, kernel: str, n_act: float, steps_per_laun
 REF_RSS_BYTES_PER_CELL = 5200
 
 
+REF_MAX_STEPS, REF_MAX_WARMUP = 8, 3
+
+
 def reference_replicas(cells: int) -> int:
     """Harness processes to run side by side: one per usable host core, as long as their resident
     memory stays under half of what the host has available."""
@@ -297,7 +300,10 @@ def run_reference_arm(args, ws, rank):
     if rank != 0:
         return
     from discrete_adjoint_b200.inputs import WORKLOAD3_BOX
-    r = reference_fwdadj(args.steps, args.warmup, replicas=reference_replicas(1024 * 1024))
+    # a bounded sample: each forward + reverse step of the reference takes seconds per process,
+    # so at most REF_MAX_STEPS timed steps after at most REF_MAX_WARMUP untimed ones
+    r = reference_fwdadj(max(1, min(args.steps, REF_MAX_STEPS)), min(args.warmup, REF_MAX_WARMUP),
+                         replicas=reference_replicas(1024 * 1024))
     v = r["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
