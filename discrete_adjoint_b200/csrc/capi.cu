@@ -334,7 +334,7 @@ const char *da_strerror(int code) {
         case DA_OK: return "ok";
         case DA_ERR_INVALID: return "invalid argument or call order";
         case DA_ERR_CUDA: return "CUDA runtime error";
-        case DA_ERR_NAN: return "non-finite state";
+        case DA_ERR_NAN: return "non-finite state or time step";
         case DA_ERR_NEG_DEPTH: return "negative depth";
         case DA_ERR_EIGEN: return "wave speed above 1e9";
         case DA_ERR_TIMEOUT: return "device wait timed out";

@@ -54,7 +54,7 @@ extern "C" {
 #define DA_OK 0
 #define DA_ERR_INVALID (-1)     /* bad argument, size or call order */
 #define DA_ERR_CUDA (-2)        /* a CUDA runtime call failed */
-#define DA_ERR_NAN (-3)         /* NaN/Inf in the state (residual.C:137-147, :272-273) */
+#define DA_ERR_NAN (-3)         /* NaN/Inf in the state or the time step (residual.C:137-147, :272-273) */
 #define DA_ERR_NEG_DEPTH (-4)   /* reserved: negative depth that the clamp could not absorb */
 #define DA_ERR_EIGEN (-5)       /* wave speed above 1e9 (get_coef_and_eigen.C:144-156) */
 #define DA_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */

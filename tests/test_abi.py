@@ -35,7 +35,7 @@ def test_library_loads_and_exports_all_declared_symbols():
 def test_abi_version_and_strerror():
     lib = _ffi.load()
     assert lib.da_abi_version() == 2
-    assert lib.da_strerror(_ffi.DA_ERR_NAN) == b"non-finite state"
+    assert lib.da_strerror(_ffi.DA_ERR_NAN) == b"non-finite state or time step"
     assert lib.da_strerror(12345) == b"unknown error"
 
 
