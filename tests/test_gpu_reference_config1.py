@@ -42,3 +42,35 @@ def test_device_equals_the_reference_step_on_config1(reference_run, how):
     else:
         assert dts[0] == ref["dt"][0]
     assert st.time == ref["time"] and st.iter == NSTEPS
+
+
+def test_reference_adjoint_steps_on_config1(reference_run):
+    # the reference's own dual-solver steps (harness mode 'DAJ1', run live) against the device's
+    # reverse steps in reference mode, on the same mesh: chained from lambda^N of J = sum h^2 dx dy
+    # over the wet cells' box, back across the frict_tiny switch at step 50; 1e-12 relative, the
+    # tolerance of the fixture-mesh tests in test_gpu_adjoint_ref.py
+    from discrete_adjoint_b200 import _ffi, adjoint_step, make_params
+    from test_oracle_adjoint import forward_states
+    w, _ = reference_run
+    m = w.mesh
+    N, K = 56, 10
+    o = oracle.Oracle(make_params(w.mat, TimeProps()), m)
+    states, dts = forward_states(o, m, N)
+    wet = states[N][0] > 0
+    box = (m.x[wet].min(), m.x[wet].max(), m.y[wet].min(), m.y[wet].max())
+    inb = (m.x >= box[0]) & (m.x <= box[1]) & (m.y >= box[2]) & (m.y <= box[3])
+    lam_end = np.zeros((3, m.n))
+    lam_end[0] = np.where(inb, 2.0 * states[N][0] * (m.dx * m.dy), 0.0)
+    iters = [N - k for k in range(K)]
+    ref = oracle.run_reference_adjoint(m, w.mat, [states[it - 1] for it in iters], iters,
+                                       [dts[it - 1] for it in iters], lam_end)
+    times = np.concatenate([[0.0], np.cumsum(dts)])
+    with GeoflowContext(w.mat, TimeProps(), jacobian_mode=_ffi.DA_JAC_REFERENCE) as c:
+        c.upload_mesh(m)
+        lam = lam_end.copy()
+        for k, it in enumerate(iters):
+            c.set_state(*states[it - 1])
+            c.set_time(float(times[it - 1]), it - 1)
+            lam, _ = adjoint_step(c, lam)
+            r = np.linalg.norm(lam - ref["lam"][k]) / np.linalg.norm(ref["lam"][k])
+            assert r <= 1e-12, (k, it, r)
