@@ -242,7 +242,13 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     }
     const int cap = cap_ref;
     if (cap <= 0) return set_error(ctx, DA_ERR_UNSUPPORTED, "reverse-step kernel cannot be resident");
-    const int grid = ctx->grid < cap ? ctx->grid : cap;
+    // FP64: every co-resident block, at most four per tile, whatever the forward steps' tuned grid:
+    // the gather spreads a sparse flow's quarter tiles over them, which outweighs the dearer
+    // barriers (the forward phases split no tile and keep the tuned grid; in FP32 the shorter
+    // gather gains less than the barriers cost).  Results do not depend on it.
+    int want = ctx->grid;
+    if (sizeof(R) == 8 && want < 4 * ctx->ntiles) want = 4 * ctx->ntiles;
+    const int grid = want < cap ? want : cap;
     ++ctx->rec_id;
     MeshArgs m = mesh_args(ctx);
     fwd::StatePair<R> S;
