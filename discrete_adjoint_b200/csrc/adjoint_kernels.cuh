@@ -245,8 +245,12 @@ int youturn_t(da_ctx *ctx, int lam_in, int lam_out, const double *sec2, double c
     // FP64: every co-resident block, at most four per tile, whatever the forward steps' tuned grid:
     // the gather spreads a sparse flow's quarter tiles over them, which outweighs the dearer
     // barriers (the forward phases split no tile and keep the tuned grid; in FP32 the shorter
-    // gather gains less than the barriers cost).  Results do not depend on it.
+    // gather gains less than the barriers cost).  FP32: the tuned grid, but never below one block
+    // per SM (a forward grid of half the SMs leaves the reverse step short of memory parallelism).
+    // Results do not depend on it.
     int want = ctx->grid;
+    const int per_sm1 = ctx->sm_count > 0 ? ctx->sm_count : 148;
+    if (want < per_sm1) want = per_sm1 < ctx->ntiles ? per_sm1 : ctx->ntiles;
     if (sizeof(R) == 8 && want < 4 * ctx->ntiles) want = 4 * ctx->ntiles;
     const int grid = want < cap ? want : cap;
     ++ctx->rec_id;

@@ -719,9 +719,9 @@ int da_trace_steps(da_ctx *ctx, int32_t k, int64_t *steps) {
 
 // ---------------------------------------------------------------------------- autotuner
 // Times nsteps forward steps from the current state for each candidate launch shape (register
-// budget of 2 or 3 resident blocks per SM x grids of 1..budget blocks per SM) and keeps the
-// fastest.  The state, time and
-// iteration are put back after every trial, so the tuning leaves the run where it was.
+// budget of 2 or 3 resident blocks per SM x grids of half the SMs and of 1..budget blocks per SM)
+// and keeps the fastest.  The state, time and iteration are put back after every trial, so the
+// tuning leaves the run where it was.
 int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
     using namespace da;
     if (!ctx || nsteps < 1) return DA_ERR_INVALID;
@@ -762,11 +762,12 @@ int da_autotune(da_ctx *ctx, int32_t nsteps, da_tune_result *out) {
         return s;
     };
     const int sm = ctx->sm_count > 0 ? ctx->sm_count : 148;
-    // (blocks per SM of the register budget, grid): grids of 1, 2, 3 blocks per SM up to the budget
+    // (blocks per SM of the register budget, grid): grids of half the SMs, then 1, 2, 3 blocks per
+    // SM up to the budget (a sparse flow's few wet tiles can prefer fewer, cheaper barriers)
     int cand_occ[DA_TUNE_MAX], cand[DA_TUNE_MAX], nc = 0;
     for (int occ = 2; occ <= 3; ++occ)
-        for (int mult = 1; mult <= occ; ++mult) {
-            int g = mult * sm;
+        for (int halves = 1; halves <= 2 * occ; halves = halves == 1 ? 2 : halves + 2) {
+            int g = halves * sm / 2;
             if (g > ctx->ntiles) g = ctx->ntiles;
             bool dup = false;
             for (int j = 0; j < nc; ++j) dup |= cand[j] == g && cand_occ[j] == occ;

@@ -365,8 +365,9 @@ int da_adjoint_run_dwr(da_ctx *ctx, const da_functional *f, int32_t nsteps, int3
 
 /* ---- autotuner (no counterpart in the reference, which has no device launches) ------------
  * Times nsteps forward steps from the current state for each candidate launch shape of the
- * step kernels (register budget of 2 or 3 resident blocks per SM; 1, 2 or 3 blocks of 256
- * threads per SM, capped at the resident count and the tile count), three times each from the
+ * step kernels (register budget of 2 or 3 resident blocks per SM; a block of 256 threads on
+ * half the SMs, or 1, 2 or 3 per SM, capped at the resident count and the tile count; the
+ * reverse-step kernel keeps at least one block per SM), three times each from the
  * same state, keeps the one with the least time as da_params.blocks_per_sm / grid_blocks and
  * puts the state, time and iteration back after every trial.  Results of later steps do not
  * depend on the choice.  out (optional) receives the candidates and their least mean ms per
