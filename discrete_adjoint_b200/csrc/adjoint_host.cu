@@ -223,9 +223,24 @@ struct Runner {
     // restore becomes the first phase of the next step launch (no launch of its own).
     int restore_at(int slot, int step) {
         if (pos == step) return DA_OK;
+        const int st = flush();
         pos = step;
         pending = slot;
-        return DA_OK;
+        return st;
+    }
+    // Consecutive forward advances (a chain of checkpoint stores between a restore and the next
+    // reverse step) go out as one multi-step launch that stores the checkpoints on its way: the
+    // advances wait here until a restore, a reverse step or the end of the sweep needs the state.
+    int def_k = 0;
+    void *def_pre = nullptr;
+    MidStoreList def_mid;
+    int flush() {
+        if (def_k == 0) return DA_OK;
+        const int st = launch_forward_steps(ctx, def_k, def_pre, nullptr, &def_mid);
+        def_k = 0;
+        def_pre = nullptr;
+        def_mid.n = 0;
+        return st;
     }
     void *take_pending() {
         void *p = pending >= 0 ? ctx->snaps[pending] : nullptr;
@@ -235,15 +250,25 @@ struct Runner {
     // k forward steps; store_slot >= 0: the state after them is stored, in the same launch
     int advance(int k, int store_slot = -1) {
         if (k == 0) return DA_OK;  // a pending restore waits for the next launch
-        const int st = launch_forward_steps(ctx, k, take_pending(), store_slot >= 0 ? ctx->snaps[store_slot] : nullptr);
         fsteps += k;
         pos += k;
+        void *slot = store_slot >= 0 ? ctx->snaps[store_slot] : nullptr;
+        if (ctx->ninst > 0) return launch_forward_steps(ctx, k, take_pending(), slot);  // one launch each
+        int st = DA_OK;
+        if (slot && def_mid.n == kMidStores) st = flush();
+        if (def_k == 0) def_pre = take_pending();
+        def_k += k;
+        if (slot) {
+            def_mid.after[def_mid.n] = def_k - 1;
+            def_mid.slot[def_mid.n++] = slot;
+        }
         return st;
     }
     // every reverse(a, b) ends with a youturn, which takes any restore still pending
     int youturn() {
         ++fsteps;
         pos = -1;  // past the step that is being taken back
+        if (const int st = flush()) return st;
         if (ctx->p.jacobian_mode == DA_JAC_REFERENCE) return youturn_reference();
         // the first reverse step (the horizon's last step) also seeds lambda^N from U^N
         int st = launch_youturn(ctx, lam_cur, 1 - lam_cur, sec2, cos_int, !seeded, box, take_pending());
@@ -456,6 +481,7 @@ int adjoint_sweep(da_ctx *ctx, const double *box, int32_t nsteps, int32_t nsnaps
         int s = store(ctx, 0);
         r.pos = 0;
         if (!s) s = r.reverse(0, nsteps, 0);
+        if (!s) s = r.flush();
         if (!s) s = restore(ctx, 0);
         if (!s) s = launch_functional(ctx, ctx->inst_J);
         if (!s) s = ctx->ninst > 0 ? launch_adjoint_reduce_inst(ctx, r.lam_cur) : launch_adjoint_reduce(ctx, r.lam_cur, n_piles);

@@ -272,9 +272,18 @@ int launch_volume(da_ctx *ctx);
 // nsteps whole steps in one cooperative launch (k_steps); same results as nsteps single steps
 // nsteps steps in one cooperative launch; pre_slot / post_slot (checkpoint slots, or null): a
 // restore before the first step and a store after the last one inside the same launch.
-int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot = nullptr, void *post_slot = nullptr);
-int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot);
-int launch_forward_steps_fp32(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot);
+// Checkpoint stores inside one multi-step launch (single instance): slot[k] receives the state
+// after step after[k] of the launch (0-based, increasing), as a store after a launch would.
+constexpr int kMidStores = 32;
+struct MidStoreList {
+    int n = 0;
+    int after[kMidStores];
+    void *slot[kMidStores];
+};
+int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot = nullptr, void *post_slot = nullptr,
+                         const MidStoreList *mid = nullptr);
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot, const MidStoreList *mid);
+int launch_forward_steps_fp32(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot, const MidStoreList *mid);
 int forward_alloc(da_ctx *ctx);
 // capi.cu: one FP64 host array to / from a device array of the context's precision (stream-ordered;
 // an FP32 download must finish before the next one reuses the staging buffer)

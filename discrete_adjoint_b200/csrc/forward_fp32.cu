@@ -7,8 +7,8 @@ namespace da {
 int launch_forward_step_fp32(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<float>(ctx, record_mask);
 }
-int launch_forward_steps_fp32(da_ctx *ctx, int nsteps, void *pre, void *post) {
-    return fwd::launch_steps_t<float>(ctx, nsteps, pre, post);
+int launch_forward_steps_fp32(da_ctx *ctx, int nsteps, void *pre, void *post, const MidStoreList *mid) {
+    return fwd::launch_steps_t<float>(ctx, nsteps, pre, post, mid);
 }
 int launch_step_half_fp32(da_ctx *ctx, int half, double *bounds) {
     return fwd::launch_step_half_t<float>(ctx, half, bounds);

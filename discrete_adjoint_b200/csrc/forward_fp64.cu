@@ -8,8 +8,8 @@ namespace da {
 int launch_forward_step_fp64(da_ctx *ctx, uint8_t *record_mask) {
     return fwd::launch_step_t<double>(ctx, record_mask);
 }
-int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre, void *post) {
-    return fwd::launch_steps_t<double>(ctx, nsteps, pre, post);
+int launch_forward_steps_fp64(da_ctx *ctx, int nsteps, void *pre, void *post, const MidStoreList *mid) {
+    return fwd::launch_steps_t<double>(ctx, nsteps, pre, post, mid);
 }
 int launch_refine_info_fp64(da_ctx *ctx, double *e, uint8_t *f, double *parts, double *t) {
     return fwd::refine_info_t<double>(ctx, e, f, parts, t);
@@ -96,10 +96,10 @@ static bool ghosts_refused(da_ctx *ctx) {
     return true;
 }
 
-int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
+int launch_forward_steps(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot, const MidStoreList *mid) {
     if (ghosts_refused(ctx)) return DA_ERR_UNSUPPORTED;
-    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps, pre_slot, post_slot);
-    return launch_forward_steps_fp32(ctx, nsteps, pre_slot, post_slot);
+    if (ctx->p.precision == DA_PREC_FP64) return launch_forward_steps_fp64(ctx, nsteps, pre_slot, post_slot, mid);
+    return launch_forward_steps_fp32(ctx, nsteps, pre_slot, post_slot, mid);
 }
 
 int launch_forward_step(da_ctx *ctx, uint8_t *record_mask) {

@@ -543,6 +543,17 @@ struct StatePair {
     R *hv[2];
 };
 
+// The checkpoint stores inside a multi-step launch (MidStoreList on the device): the arrays of
+// each slot and the number of segments.
+template <class R>
+struct MidStores {
+    int n, nseg;
+    int after[kMidStores];
+    R *snap[kMidStores][3];
+    uint8_t *dirty[kMidStores];
+    DevScalars *ssc[kMidStores];
+};
+
 // Ensemble: the dt of every member from its reduced CFL values (threads over members), its time
 // advanced, its accumulators restarted.  Runs between two grid barriers.
 __device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter, const TimeConsts &tc, DevScalars *sc) {
@@ -571,7 +582,8 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
                                                   MatConsts mc, TimeConsts tc, DevScalars *sc, InstArgs ia,
-                                                  snap::SnapArgs<R> pre, snap::SnapArgs<R> post, HaloArgs ha) {
+                                                  snap::SnapArgs<R> pre, snap::SnapArgs<R> post, HaloArgs ha,
+                                                  MidStores<R> mid) {
     __shared__ int list[kBlock];
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     StageSmem<R> &stg = *reinterpret_cast<StageSmem<R> *>(dyn_smem);
@@ -585,6 +597,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
     long long iter = __ldcg(&sc->iter);
     double dt = __ldcg(&sc->dt), ft = __ldcg(&sc->frict_tiny), min_dxe = __ldcg(&sc->min_dxe),
            hmax = __ldcg(&sc->hmax);
+    int ms = 0;  // the next of the launch's checkpoint stores
     for (int s = 0; s < nsteps; ++s) {
         const int c = (cur + s) & 1, p = s & 1;
         unsigned long long *acc_min = p ? &sc->acc_alt_min_dxe : &sc->acc_min_dxe;
@@ -627,6 +640,27 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
             update_phase<R, false, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull,
                                           mc, sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list, ia);
         if (!grid_sync(sc)) return;
+        if (!BATCH && ms < mid.n && mid.after[ms] == s) {
+            // a checkpoint of the state after this step, with no barrier of its own: the next
+            // two steps do not write this buffer, and the next update changes the dirty flags
+            // only after the next barrier, which every block reaches after its part of the copy
+            snap::store_segments<R>(O.h, O.hu, O.hv, mid.snap[ms][0], mid.snap[ms][1], mid.snap[ms][2], seg_dirty,
+                                    mid.dirty[ms], mid.nseg, m.n);
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                // the step scalars as a launch ending after this step leaves them
+                DevScalars *d = mid.ssc[ms];
+                snap::copy_step_scalars(d, sc);
+                d->time = time;
+                d->dt = dt;
+                d->hmax = hmax;
+                d->min_dxe = min_dxe;
+                d->frict_tiny = ft;
+                d->iter = iter;
+                d->acc_min_dxe = d->acc_alt_min_dxe = kMinDxeStart;
+                d->acc_hmax = d->acc_alt_hmax = 0ull;
+            }
+            ++ms;
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->iter = iter;
@@ -715,7 +749,7 @@ int launch_step_half_t(da_ctx *ctx, int half, double *bounds) {
 // pre_slot / post_slot (or null): a checkpoint slot restored before the first step / stored after
 // the last one, in the same launch.
 template <class R>
-int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
+int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot, const MidStoreList *ml = nullptr) {
     if (nsteps <= 0) return DA_OK;
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
@@ -765,8 +799,25 @@ int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot) {
     snap::SnapArgs<R> post =
         post_slot ? snap::snap_args<R>(ctx, post_slot, true, (cur + nsteps) & 1) : snap::no_snap<R>();
     HaloArgs ha = halo_args(ctx);
+    MidStores<R> mid{};
+    if (ml && ml->n > 0) {
+        if (batch || ml->n > kMidStores || post_slot)
+            return set_error(ctx, DA_ERR_INVALID, "multi-step launch: checkpoint stores inside an ensemble launch");
+        for (int k = 0; k < ml->n; ++k) {
+            if (ml->after[k] < 0 || ml->after[k] >= nsteps || (k > 0 && ml->after[k] <= ml->after[k - 1]) ||
+                ml->slot[k] == ctx->snaps[0])
+                return set_error(ctx, DA_ERR_INVALID, "multi-step launch: bad checkpoint store list");
+            const snap::SnapArgs<R> a = snap::snap_args<R>(ctx, ml->slot[k], true, 0);
+            mid.after[k] = ml->after[k];
+            for (int v = 0; v < 3; ++v) mid.snap[k][v] = a.snap[v];
+            mid.dirty[k] = a.snap_dirty;
+            mid.ssc[k] = a.snap_sc;
+        }
+        mid.n = ml->n;
+        mid.nseg = ctx->nseg;
+    }
     void *args[] = {&m,         &S,      &cur,  &n,  &kact, &active, &seg_clean, &seg_wet, &seg_vol,
-                    &seg_dirty, &ntiles, &cull, &mc, &tc,   &sc,     &ia,        &pre,     &post, &ha};
+                    &seg_dirty, &ntiles, &cull, &mc, &tc,   &sc,     &ia,        &pre,     &post, &ha, &mid};
     trace_begin(ctx, TR_STEPS);
     const cudaError_t e = cudaLaunchCooperativeKernel(kern, grid, kBlock, args, smem, ctx->stream);
     trace_end(ctx, nsteps);

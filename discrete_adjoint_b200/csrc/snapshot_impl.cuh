@@ -128,6 +128,37 @@ __device__ __forceinline__ void snap_segments(const SnapArgs<R> &a) {
     }
 }
 
+// A STORE (not the base slot) from explicit arrays, for the checkpoints a multi-step launch takes
+// on its way: the live dirty flags into the slot's, and the dirty segments of the live buffer
+// (h, hu, hv) into the slot's arrays (s_h, s_hu, s_hv), with snap_segments' division of the work.
+template <class R>
+__device__ __forceinline__ void store_segments(const R *h, const R *hu, const R *hv, R *s_h, R *s_hu, R *s_hv,
+                                               const uint8_t *seg_dirty, uint8_t *snap_dirty, int nseg, int n) {
+    const int lane = threadIdx.x & 31;
+    const int W = (gridDim.x * blockDim.x) >> 5;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    for (int s0 = 0; s0 < nseg; s0 += 32 * W) {
+        const int s = s0 + lane * W + w;
+        bool work = false;
+        if (s < nseg) {
+            const uint8_t d = seg_dirty[s];
+            snap_dirty[s] = d;
+            work = d != 0;
+        }
+        unsigned bits = __ballot_sync(0xffffffffu, work);
+        while (bits) {
+            const int k = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int i = (s0 + k * W + w) * 32 + lane;
+            if (i < n) {
+                s_h[i] = h[i];
+                s_hu[i] = hu[i];
+                s_hv[i] = hv[i];
+            }
+        }
+    }
+}
+
 // The state of the time stepping (time, dt, iteration, CFL values, volume and accumulators); the
 // error flag stays sticky and the barrier counters are not touched (a restore runs while the other
 // blocks of a cooperative launch may already wait at the barrier).

@@ -153,6 +153,28 @@ def test_checkpoint_schedule_does_not_change_the_result():
 
 
 @pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
+def test_long_checkpoint_chains_do_not_change_the_result(precision):
+    # consecutive forward advances of the sweep go out as one launch that stores their
+    # checkpoints on the way (at most 32 a launch): with 40 and 71 snapshots over 72 steps the
+    # first chain stores after nearly every step and is split into several launches; lambda^0 and
+    # the gradients equal the sweep without checkpoints bit for bit
+    w = inputs.test_case(seed=2)
+    m = w.mesh
+    out = []
+    for snaps in (0, 3, 40, 71):
+        with GeoflowContext(w.mat, TimeProps(), precision=precision) as c:
+            c.upload_mesh(m)
+            c.set_state(m.h0, m.hu0, m.hv0)
+            out.append(adjoint_run(c, box_of(w), 72, snaps, m.dh0_dpile, want_lambda0=True))
+    a = out[0]
+    for b in out[1:]:
+        assert np.array_equal(a.lambda0, b.lambda0)
+        assert a.J == b.J and a.dJ_dintfrict == b.dJ_dintfrict
+        assert np.array_equal(a.dJ_dbedfrict, b.dJ_dbedfrict) and np.array_equal(a.dJ_dpile, b.dJ_dpile)
+    assert out[0].forward_steps > out[1].forward_steps > out[2].forward_steps >= out[3].forward_steps
+
+
+@pytest.mark.parametrize("precision", [_ffi.DA_PREC_FP64, _ffi.DA_PREC_FP32_SPLIT])
 def test_tile_staging_does_not_change_the_adjoint(precision):
     # the replayed forward steps of the reverse sweep (and its recomputation) with tiles and halos
     # staged in shared memory, against neighbour reads from global memory, and the staged gather
