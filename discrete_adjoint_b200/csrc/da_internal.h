@@ -198,8 +198,9 @@ struct da_ctx {
     int ntiles = 0;                  // tiles of 256 consecutive cells
     int nblocks = 0;                 // grid of the seed kernel (fixed at allocation)
     int grid = 0;                    // grid of the tiled step kernels (da_params.grid_blocks)
-    // resident blocks of k_steps [FP32, FP64] x [single, ensemble] x [2, 3 per SM] x [staged]
-    int coop_cap[16] = {};
+    // resident blocks of k_steps [FP32, FP64] x [single, ensemble] x [2, 3 per SM] x [staged] x
+    // [checkpoint stores inside the launch]
+    int coop_cap[32] = {};
     // of k_youturn [FP32, FP64] x [single, ensemble] x [seed] x [2, 3 per SM] x [staged]
     int coop_cap_yt[32] = {};
     int sm_count = 0;

@@ -577,7 +577,7 @@ __device__ __forceinline__ void inst_dt_pass(const InstArgs &ia, long long iter,
 // members' dt pass); the shared iteration count lives in the scalars.  OCC: resident blocks per
 // SM the register budget is set for (da_params.blocks_per_sm).  STAGED: the phases stage each
 // tile and its halo in dynamic shared memory (staged_impl.cuh).
-template <class R, bool BATCH = false, int OCC = 2, bool STAGED = false>
+template <class R, bool BATCH = false, int OCC = 2, bool STAGED = false, bool MID = false>
 __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> S, int cur, int nsteps, R *kact,
                                                   unsigned *active, uint8_t *seg_clean, uint8_t *seg_wet,
                                                   double *seg_vol, uint8_t *seg_dirty, int ntiles, int cull,
@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(kBlock, OCC) k_steps(MeshArgs m, StatePair<R> 
             update_phase<R, false, BATCH>(m, U, O, kact, active, seg_clean, seg_wet, seg_vol, seg_dirty, ntiles, cull,
                                           mc, sc, R(dt), ftr, nullptr, nullptr, nullptr, 0, list, ia);
         if (!grid_sync(sc)) return;
-        if (!BATCH && ms < mid.n && mid.after[ms] == s) {
+        if (MID && ms < mid.n && mid.after[ms] == s) {
             // a checkpoint of the state after this step, with no barrier of its own: the next
             // two steps do not write this buffer, and the next update changes the dirty flags
             // only after the next barrier, which every block reaches after its part of the copy
@@ -754,15 +754,23 @@ int launch_steps_t(da_ctx *ctx, int nsteps, void *pre_slot, void *post_slot, con
     const bool batch = ctx->ninst > 0;
     const int occ3 = ctx->p.blocks_per_sm == 3;
     const bool staged = staged_ok(ctx);
+    // the checkpoint stores inside a launch are compiled only into their own single-instance
+    // kernels: the plain ones keep their register allocation
+    const bool mids = ml && ml->n > 0 && !batch;
     const void *kern;
-    if (staged)
+    if (mids)
+        kern = staged ? (occ3 ? (const void *)k_steps<R, false, 3, true, true>
+                              : (const void *)k_steps<R, false, 2, true, true>)
+                      : (occ3 ? (const void *)k_steps<R, false, 3, false, true>
+                              : (const void *)k_steps<R, false, 2, false, true>);
+    else if (staged)
         kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3, true> : (const void *)k_steps<R, true, 2, true>)
                      : (occ3 ? (const void *)k_steps<R, false, 3, true> : (const void *)k_steps<R, false, 2, true>);
     else
         kern = batch ? (occ3 ? (const void *)k_steps<R, true, 3> : (const void *)k_steps<R, true, 2>)
                      : (occ3 ? (const void *)k_steps<R, false, 3> : (const void *)k_steps<R, false, 2>);
     const size_t smem = staged ? stage_smem_bytes<R>() : 0;
-    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch + 4 * occ3 + 8 * staged];
+    int &cap_ref = ctx->coop_cap[(sizeof(R) == 8) + 2 * batch + 4 * occ3 + 8 * staged + 16 * mids];
     if (cap_ref <= 0) {
         int st = DA_OK;
         if (staged)
